@@ -1,0 +1,424 @@
+#!/usr/bin/env python
+"""Throughput of Ash3d's transport step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config C2]
+
+One "step" is one reference time step of the transport path through the
+C-ABI (src/Ash3d.F90:376-595): step prologue, device met-step interpolation,
+Adjust_DT, source insertion, Set_BC(1), AdvectHorz, AdvectVert, Set_BC(2),
+DiffuseHorz, DiffuseVert, TimeStepTotals.  The workload is the lon/lat
+720x360x60 grid with 10 grain bins, Crank-Nicolson diffusion and hourly FP32
+met steps (a 0.25-degree jet plus a meridional wave with seeded 5% noise), on
+synthetic data.  The concentration starts from a seeded field that fills the
+whole domain, so every cell exercises the limiter.
+
+value  = cell-grain-steps/s with the met steps already on the device.
+e2e    = the same through the same public calls with the met pair uploaded from
+         pinned host memory at the start of the timed window (and whenever the
+         clock crosses an hour), the source column uploaded and dt + totals read
+         back every step.
+N > 1: grains are sharded across GPUs (weak scaling: 10 grains per GPU of a
+10*N-grain run); the only exchange is an all-reduce MAX of three CFL maxima
+and an all-reduce SUM of the totals per step (NCCL).
+
+--impl reference times the CPU restatement of the reference (the oracle,
+OpenMP in the advection rows as the reference) on the host cores, on a
+bounded y-slab of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import math
+import os
+import pathlib
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+
+
+def _load_pkg():
+    if "volcano_ash3d_b200" in sys.modules:
+        return sys.modules["volcano_ash3d_b200"]
+    d = ROOT / "volcano-ash3d_b200"
+    spec = importlib.util.spec_from_file_location("volcano_ash3d_b200", d / "__init__.py",
+                                                  submodule_search_locations=[str(d)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["volcano_ash3d_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+_load_pkg()
+from volcano_ash3d_b200 import driver, synthetic as syn  # noqa: E402
+
+METRIC = "cell-grain-steps/s FP64"
+UNIT = "cell-grain-steps/s"
+WORKLOAD = {
+    "C2": "lon/lat 720x360x60 (0.25 deg, dz 0.5 km), 10 grains (v_s 1e-3..3 m/s), superbee, "
+          "Crank-Nicolson diffusion 500 m^2/s, hourly FP32 met steps (jet + wave + 5% noise)",
+    "C1": "projected 100x100x40 (5 km, dz 0.5 km), 4 grains, superbee, explicit diffusion",
+    "C4": "projected 200x200x50, 6 grains, superbee, explicit diffusion",
+    "C5": "projected 1500x1000x80 (3 km, dz 0.4 km), 20 grains, superbee, Crank-Nicolson",
+}
+
+
+def _load_oracle():
+    p = str(ROOT / "oracle")
+    if p not in sys.path:
+        sys.path.insert(0, p)
+    import ash3d_oracle
+    ash3d_oracle.build()
+    return ash3d_oracle
+
+
+def filled_state(cfg, seed=17):
+    """A seeded concentration filling the whole domain (kg/km^3), (nx,ny,nz,ns)."""
+    rng = np.random.default_rng(seed)
+    nx, ny, nz, ns = cfg.nx, cfg.ny, cfg.nz, cfg.ns
+    x = np.sin(np.linspace(0, 6 * math.pi, nx))[:, None, None]
+    y = np.cos(np.linspace(0, 4 * math.pi, ny))[None, :, None]
+    z = np.exp(-((np.linspace(0, 1, nz) - 0.4) ** 2) * 4)[None, None, :]
+    base = (2.0 + x + y) * z * 100.0
+    q = np.empty((nx, ny, nz, ns), order="F")
+    for g in range(ns):
+        noise = rng.random((nx, ny, nz), dtype=np.float32)
+        q[:, :, :, g] = base * (0.2 + 0.1 * g) * (0.9 + 0.2 * noise)
+    return q
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu_index = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu_index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# algorithmic bytes per launch, per kernel class (see DESIGN.md roofline)
+# ---------------------------------------------------------------------------
+def algorithmic_bytes(cfg, kclass: str) -> float:
+    cells = cfg.nx * cfg.ny * cfg.nz
+    cg = cells * cfg.ns
+    table = {
+        "advect_x": 16 * cg + 8 * cells, "advect_y": 16 * cg + 8 * cells,
+        "advect_z": 16 * cg + 8 * cells, "diff_x": 16 * cg, "diff_y": 16 * cg, "diff_z": 16 * cg,
+        "cn_solve_x": 16 * cg, "cn_solve_y": 16 * cg, "cn_solve_z": 16 * cg,
+        "cfl": 24 * cells, "totals": 8 * cg, "winds": 48 * cells,
+    }
+    return float(table.get(kclass, 0.0))
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback 6.65 TB/s"
+
+
+def ncu_traffic(config: str, kclass: str):
+    """dram read+write bytes per launch from the committed ncu summary."""
+    p = ROOT / "profiles" / "ncu_traffic.json"
+    if not p.exists():
+        return None
+    d = json.loads(p.read_text())
+    v = d.get(config, {}).get(kclass)
+    return float(v) if v is not None else None
+
+
+# ---------------------------------------------------------------------------
+# CPU arm: the oracle on a bounded slab of the workload
+# ---------------------------------------------------------------------------
+def cpu_sample(config: str, steps: int, warmup: int, ny_sample: int | None = None):
+    orc = _load_oracle()
+    cfg = syn.make_config(config)
+    full_cells = cfg.cells
+    if ny_sample is None:
+        # about 1-3 s of CPU work per step: keep ~0.8M cells per sample step
+        ny_sample = max(4, min(cfg.ny, int(8.0e5 // (cfg.nx * cfg.nz))))
+    cfg.ny = ny_sample
+    cfg.jvent = max(1, ny_sample // 2)
+    m = orc.OracleModel(cfg)
+    m.set_interior(filled_state(cfg))
+    st = driver.new_state(cfg)
+    for _ in range(warmup):
+        driver.step(m, st)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        driver.step(m, st)
+    el = time.perf_counter() - t0
+    value = cfg.cell_grains * steps / el
+    threads = orc.load().orc_get_threads()
+    sample = (f"oracle port of the reference step on a y-slab {cfg.nx}x{ny_sample}x{cfg.nz}x{cfg.ns} "
+              f"({cfg.cells / full_cells:.3f} of the grid), {steps} steps after {warmup} warm-up")
+    return value, el, threads, sample
+
+
+def run_reference(args, rank: int, world: int):
+    if rank != 0:
+        return
+    steps, warmup = args.steps, args.warmup
+    value, el, threads, sample = cpu_sample(args.config, steps, warmup)
+    cfg = syn.make_config(args.config)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": steps, "warmup": warmup, "ms_per_step": 1e3 * el / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.config}: {WORKLOAD[args.config]}", "grid": [cfg.nx, cfg.ny, cfg.nz],
+                   "grains": cfg.ns, "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+class NoMetUpload:
+    """Model proxy that keeps the resident met pair (the `value` loop)."""
+
+    def __init__(self, model):
+        self._m = model
+
+    def set_met_steps(self, last, nxt):
+        return None
+
+    def __getattr__(self, name):
+        return getattr(self._m, name)
+
+
+class PinnedMet:
+    """Met steps generated before timing, held in pinned host memory."""
+
+    def __init__(self, met: syn.MetSource, hours, torch):
+        self.cache = {}
+        for h in hours:
+            arrs = []
+            for a in met.step(h):
+                t = torch.empty(a.shape[::-1], dtype=torch.float32, pin_memory=True)
+                v = t.numpy().reshape(-1)
+                v[:] = np.asarray(a, dtype=np.float32).reshape(-1, order="F")
+                arrs.append(v)
+            self.cache[h] = tuple(arrs)
+
+    def step(self, h):
+        return self.cache[h]
+
+
+def run_ours(args, rank: int, world: int, local_rank: int):
+    import torch
+    import torch.distributed as dist
+    from volcano_ash3d_b200.model import Ash3dGPU
+
+    torch.cuda.set_device(local_rank)
+    comm = None
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+        comm = driver.Comm(device=torch.device("cuda", local_rank))
+    cfg_g = syn.make_config(args.config)
+    cfg = driver.shard_config(cfg_g, rank, world)
+    geo = syn.geometry(cfg)
+    gpu = Ash3dGPU(cfg, device=local_rank, geo=geo)
+    gpu.set_interior(filled_state(cfg, seed=17 + rank))
+    stream = torch.cuda.ExternalStream(gpu.stream_handle(), device=torch.device("cuda", local_rank))
+    n_total = cfg.ns * world
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    st = driver.new_state(cfg, geo)
+    kw = dict(comm=comm, n_gs_aloft_total=n_total)
+    for _ in range(args.warmup):
+        driver.step(gpu, st, **kw)
+
+    # ---- value: met steps resident --------------------------------------
+    resident = NoMetUpload(gpu)
+    sampler = ClockSampler(local_rank)
+    n0 = gpu.kernel_launches()
+    barrier()
+    torch.cuda.synchronize()
+    gpu.sync()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler.start()
+    time.sleep(0.3)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        driver.step(resident, st, **kw)
+    ev1.record(stream)
+    gpu.sync()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    barrier()
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    launches = gpu.kernel_launches() - n0
+    value = cfg.cell_grains * world * args.steps / (ms / 1e3)
+
+    # ---- per-kernel CUDA-event times (same workload, short pass) ---------
+    gpu.kernel_timing(True)
+    nk = min(args.steps, 5)
+    for _ in range(nk):
+        driver.step(resident, st, **kw)
+    ktimes = gpu.kernel_times()
+    gpu.kernel_timing(False)
+
+    # ---- e2e: met uploads from pinned memory + per-step H2D/D2H ----------
+    h0 = int(math.floor(st.time))
+    pinned = PinnedMet(st.met, range(h0, h0 + 3 + int(args.steps * 0.2)), torch)
+    st.met = pinned
+    st.hour = -1  # the timed window starts with a met-pair upload
+    met_bytes = 6 * cfg.cells * 4
+    hours_before = st.hour
+    barrier()
+    torch.cuda.synchronize()
+    gpu.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    uploads = 0
+    e0.record(stream)
+    for _ in range(args.steps):
+        before = st.hour
+        driver.step(gpu, st, **kw)
+        if st.hour != before:
+            uploads += 1
+    e1.record(stream)
+    gpu.sync()
+    torch.cuda.synchronize()
+    barrier()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1))
+    e2e_value = cfg.cell_grains * world * args.steps / (ms_e2e / 1e3)
+    h2d = (uploads * met_bytes) / args.steps + 8 * (cfg.nz + 1) * cfg.ns
+    d2h = 8 * 3 + 8 * (4 + cfg.ns)  # dt word + device scalars; totals
+
+    if rank == 0:
+        # dominant kernel and its roofline
+        cand = {k: v for k, v in ktimes.items() if k not in ("other",) and v[1] > 0}
+        dom = max(cand, key=lambda k: cand[k][0])
+        tot_ms, cnt = cand[dom]
+        avg_s = tot_ms / cnt / 1e3
+        alg = algorithmic_bytes(cfg, dom)
+        achieved = alg / avg_s / 1e9
+        peak, peak_src = measured_peak()
+        roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": ncu_traffic(args.config, dom),
+                "alg_bytes_per_launch": alg, "avg_launch_ms": avg_s * 1e3, "peak_source": peak_src,
+                "step_frac": None}
+        step_bytes = (48 + 24 / cfg.ns) * cfg.cell_grains if cfg.use_cn else (16 + 24 / cfg.ns) * cfg.cell_grains
+        roof["step_frac"] = (step_bytes * args.steps / (ms / 1e3) / 1e9) / peak
+        kt = {k: {"ms": round(v[0] / max(v[1], 1), 4), "launches_per_step": v[1] / nk}
+              for k, v in ktimes.items() if v[1] > 0}
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cv, cel, thr, sample = cpu_sample(args.config, steps=2, warmup=1)
+            cpu = {"value": cv, "unit": UNIT, "cores": thr, "kind": "port", "sample": sample}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded filled concentration, analytic winds with seeded noise)",
+            "config": {"workload": f"{args.config}: {WORKLOAD[args.config]}",
+                       "grid": [cfg.nx, cfg.ny, cfg.nz], "grains_per_gpu": cfg.ns,
+                       "grains_total": n_total, "parallelism": f"grain-sharded x{world}",
+                       "l2": "inputs larger than L2 (one concentration level is "
+                             f"{cfg.cell_grains * 8 / 1e9:.2f} GB)"},
+            "roofline": roof,
+            "kernel_ms": kt,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e / args.steps,
+                    "met_uploads": uploads},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    gpu.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="C2", choices=sorted(WORKLOAD))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

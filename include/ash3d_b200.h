@@ -1,0 +1,231 @@
+/*
+ * ash3d_b200.h -- C-ABI of the B200 (sm_100a) transport path for Ash3d.
+ *
+ * The Fortran host (Ash3d.F90's main loop) reaches the GPU through these
+ * functions, bound with ISO_C_BINDING (see INTEGRATION.md for the shim).
+ * Every function returns an int status (A3G_OK = 0); a nonzero status is
+ * what the reference turns into "write(errlog) ... ; stop 1".
+ *
+ * Arrays cross this boundary in the reference's own Fortran layouts
+ * (column-major, ghost cells included) so that the shim can pass c_loc() of
+ * the module arrays directly (USEPOINTERS=T build, src/makefile:80):
+ *   concen level   (-1:nx+2,-1:ny+2,-1:nz+2,1:ns)  one of ts0/ts1
+ *   vx/vy/vz, kappa, sigma_n{x,y,z}  (-1:nx+2,-1:ny+2,-1:nz+2)
+ *   vf             (-1:nx+2,-1:ny+2,-1:nz+2,1:ns)
+ *   dz_vec         (-1:nz+2)
+ *   kx/ky/kz       (0:nx+1,0:ny+1,0:nz+1)
+ *   outflow_yz1/2  (-1:ny+2,-1:nz+2,1:ns); _xz1/2 (-1:nx+2,-1:nz+2,1:ns);
+ *   outflow_xy1/2  (-1:nx+2,-1:ny+2,1:ns); DepositGranularity (nx,ny,ns)
+ * All floating point is FP64 except the FP32 met steps.  The concentration
+ * stays resident on the device between calls; only the calls that return a
+ * host value (Adjust_DT, TimeStepTotals, the subgrid box, downloads)
+ * synchronise the context's stream.
+ */
+#ifndef ASH3D_B200_H
+#define ASH3D_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define A3G_ABI_VERSION 1
+
+/* status codes */
+#define A3G_OK              0
+#define A3G_ERR_ARG         1   /* bad argument (sizes, pointers, codes) */
+#define A3G_ERR_CUDA        2   /* a CUDA call failed */
+#define A3G_ERR_NOMEM       3   /* device allocation failed */
+#define A3G_ERR_BC_CODE     4   /* Set_BC code not 1 or 2 (src/Set_BC.f90:119-123) */
+#define A3G_ERR_SUBGRID     5   /* kmax<kmin in get_minmax_index (src/Calc_Mesh.f90:522-527) */
+#define A3G_ERR_PIVOT       6   /* a Crank-Nicolson line needed a row interchange or hit a zero pivot */
+#define A3G_ERR_STATE       7   /* call out of order (e.g. no geometry bound yet) */
+#define A3G_ERR_UNSUPPORTED 8   /* option outside the implemented variants */
+#define A3G_ERR_NONFINITE   9   /* NaN/Inf detected in a device reduction */
+
+/* limiters: the LIM_* preprocessor choices of src/makefile:126 */
+#define A3G_LIM_NONE     0
+#define A3G_LIM_LAXWEN   1
+#define A3G_LIM_BW       2
+#define A3G_LIM_FROMM    3
+#define A3G_LIM_MINMOD   4
+#define A3G_LIM_SUPERBEE 5
+#define A3G_LIM_MC       6
+
+typedef struct a3g_ctx a3g_ctx;
+
+/* Grid extents and flags: module mesh (src/Ash3d_VariableModules.f90:600-760). */
+typedef struct a3g_grid_desc {
+  int32_t nx, ny, nz, ns;   /* nxmax, nymax, nzmax, nsmax (ash grain bins) */
+  int32_t periodic;         /* IsPeriodic */
+  int32_t latlon;           /* IsLatLon */
+  double dx, dy;            /* projected cell sizes (km); Adjust_DT uses them when !latlon */
+} a3g_grid_desc;
+
+/* Run-time forms of the reference's compile-time and control-file options
+ * (src/makefile:91-206, src/ResetParams.f90:18-37). */
+typedef struct a3g_params {
+  int32_t limiter;          /* A3G_LIM_*; reference default build: SUPERBEE */
+  int32_t use_cn;           /* 1: CRANKNIC (diffCN_*), 0: EXPLDIFF (diff_*) */
+  int32_t use_diffusion;    /* useDiffusion */
+  int32_t fast_subgrid;     /* FAST_SUBGRID */
+  int32_t nocycle;          /* NOCYCLE */
+  int32_t zscaling_id;      /* ZScaling_ID; only 0 and 1 are implemented */
+  double cfl;               /* CFL (0.8) */
+  double dt_min, dt_max;    /* DT_MIN, DT_MAX (hours) */
+  double imp_fac;           /* Imp_fac (0.5) */
+  double imp_dt_fac;        /* Imp_DT_fac (4.0) */
+  double eps_thresh;        /* EPS_THRESH (1e-10) */
+  double eps_small;         /* EPS_SMALL (1e-6) */
+  double cloudcon_grid_thresh; /* CLOUDCON_GRID_THRESH (1e-7) */
+  double magma_density;     /* MagmaDensity (2500) */
+} a3g_params;
+
+/* Fills *p with the reference defaults (superbee, CN, no subgrid). */
+void a3g_default_params(a3g_params *p);
+int  a3g_abi_version(void);
+/* Message for the last failing call on this thread ("" if none). */
+const char *a3g_last_error(void);
+
+/* ---- lifetime: replaces the device-side half of alloc_arrays,
+ *      src/Alloc_Arrays.f90:14-55 ---- */
+int a3g_create(const a3g_grid_desc *grid, const a3g_params *params, int device, a3g_ctx **out);
+int a3g_destroy(a3g_ctx *ctx);
+/* Blocks until all work queued on the context is done. */
+int a3g_sync(a3g_ctx *ctx);
+/* Device bytes held by the context. */
+int a3g_device_bytes(a3g_ctx *ctx, size_t *bytes);
+
+/* ---- static inputs ---- */
+/* Geometry from calc_mesh_params (src/Calc_Mesh.f90:23-220).  Arrays that do
+ * not vary along i (or j) are stored once per (j,k) (or k) on the device. */
+int a3g_set_geometry(a3g_ctx *ctx, const double *kappa_pd, const double *sigma_nx_pd,
+                     const double *sigma_ny_pd, const double *sigma_nz_pd,
+                     const double *dz_vec_pd);
+/* kx/ky/kz from Allocate_Diff (src/Diffusion.F90:83-104), km^2/h. */
+int a3g_set_diffusivity(a3g_ctx *ctx, const double *kx, const double *ky, const double *kz);
+/* Fall velocities vf_pd (km/h, negative downward; src/Input_Data.f90:3669).
+ * Stored once per (k,grain) when they do not vary in x and y. */
+int a3g_set_fall_velocity(a3g_ctx *ctx, const double *vf_pd);
+/* IsAloft(1:ns) (Prune_GS, src/Tephra.f90:782-812); n_gs_aloft is recounted. */
+int a3g_set_aloft(a3g_ctx *ctx, const int32_t *is_aloft);
+
+/* ---- winds (MesoInterpolater, src/MesoInterpolater.f90:201-263) ---- */
+/* FP64 winds already interpolated on the host (vx_pd,vy_pd,vz_pd, km/h). */
+int a3g_set_winds(a3g_ctx *ctx, const double *vx_pd, const double *vy_pd, const double *vz_pd);
+/* FP32 met steps on the computational grid (nx,ny,nz; m/s), the pair that
+ * brackets the current time.  Uploaded once per met step. */
+int a3g_set_met_steps(a3g_ctx *ctx, const float *vx_last, const float *vy_last,
+                      const float *vz_last, const float *vx_next, const float *vy_next,
+                      const float *vz_next);
+/* Device form of src/MesoInterpolater.f90:207-223:
+ * v = (dble(last) + dble(next-last)*frac)*3.6 */
+int a3g_interp_winds(a3g_ctx *ctx, double interval_frac);
+
+/* ---- concentration state ---- */
+/* Uploads/downloads the interior of one level (ghosts of the download are
+ * written as zero: the state of ts0 after the step prologue). */
+int a3g_upload_concen(a3g_ctx *ctx, const double *concen_level);
+int a3g_download_concen(a3g_ctx *ctx, double *concen_level);
+/* Outflow accumulators and DepositGranularity (any pointer may be NULL). */
+int a3g_upload_outflow(a3g_ctx *ctx, const double *yz1, const double *yz2, const double *xz1,
+                       const double *xz2, const double *xy1, const double *xy2);
+int a3g_download_outflow(a3g_ctx *ctx, double *yz1, double *yz2, double *xz1, double *xz2,
+                         double *xy1, double *xy2, double *deposit);
+
+/* ---- the per-step path (callers: src/Ash3d.F90:372-642) ---- */
+/* Step prologue, src/Ash3d.F90:376-378 (ts0 <- ts1; ts1 <- 0). */
+int a3g_step_prologue(a3g_ctx *ctx);
+/* Sets dt (hours) for the next operators, as Adjust_DT/FAST_DT leave it in
+ * time_data::dt (src/Ash3d_VariableModules.f90:1071-1072). */
+int a3g_set_dt(a3g_ctx *ctx, double dt);
+/* Source insertion, src/Ash3d.F90:428-431: concen(ivent,jvent,1:nz+1,:,ts0)
+ * += dt*SourceNodeFlux; flux is (nz+1) x ns, k fastest (kg/km^3/h). */
+int a3g_add_source_column(a3g_ctx *ctx, int32_t ivent, int32_t jvent, const double *flux,
+                          double dt);
+/* Set_BC(bc_code), src/Set_BC.f90:15-126.  Ghost cells are generated inside
+ * the sweep kernels, so this validates the code and records it. */
+int a3g_set_bc(a3g_ctx *ctx, int32_t bc_code);
+/* AdvectHorz(itoggle), src/AdvectionHorz.f90:47-85 (with get_minmax_index,
+ * src/Calc_Mesh.f90:432-542, when fast_subgrid; ivent/jvent/kvent used then). */
+int a3g_advect_horz(a3g_ctx *ctx, int32_t itoggle, int32_t ivent, int32_t jvent, int32_t kvent);
+/* advect_x / advect_y, src/AdvectionHorz_DCU.f90:68-305 / 322-556. */
+int a3g_advect_x(a3g_ctx *ctx);
+int a3g_advect_y(a3g_ctx *ctx);
+/* AdvectVert -> advect_z, src/AdvectionVert_DCU.f90:64-323. */
+int a3g_advect_vert(a3g_ctx *ctx);
+/* DiffuseHorz(i), src/Diffusion.F90:151-216 (diff_x/y or diffCN_x/y). */
+int a3g_diffuse_horz(a3g_ctx *ctx, int32_t itime);
+/* DiffuseVert, src/Diffusion.F90:232-247 (diff_z or diffCN_z). */
+int a3g_diffuse_vert(a3g_ctx *ctx);
+/* Adjust_DT(mesostep=.false.), src/Adjust_dt.f90:19-339.  Computes dt on the
+ * device from the current winds, then clips it to the next write time and
+ * the simulation end exactly as :321-332; *dt_out receives it. */
+int a3g_adjust_dt(a3g_ctx *ctx, double time, double next_write_time, double simtime,
+                  double *dt_out);
+/* The two halves of Adjust_DT for grain-sharded runs (grains split across
+ * GPUs, each rank one context): a3g_cfl_maxima returns this context's three
+ * CFL maxima {vx term, vy term, (|vz|+max|vf|)/dz term} (src/Adjust_dt.f90:
+ * 136-173); after a MAX all-reduce of those over the ranks,
+ * a3g_adjust_dt_from_maxima applies :176-332 to them, so every rank gets the
+ * dt the reference computes over all grains. */
+int a3g_cfl_maxima(a3g_ctx *ctx, double *vmax3);
+int a3g_adjust_dt_from_maxima(a3g_ctx *ctx, const double *vmax3, int32_t n_gs_aloft_total,
+                              double time, double next_write_time, double simtime,
+                              double *dt_out);
+/* TimeStepTotals sums, src/TimeStepTotals.f90:57-66 with Calc_AshVol_Aloft/
+ * Deposit/Outflow (src/Output_Vars.f90:1255-1459).  out4 = {aloft_vol,
+ * dep_vol, outflow_vol, tot_vol} (km^3 DRE); mass_aloft (ns, kg) may be NULL. */
+int a3g_timestep_totals(a3g_ctx *ctx, double *out4, double *mass_aloft);
+/* get_minmax_index, src/Calc_Mesh.f90:432-542: box = {imin,imax,jmin,jmax,kmin,kmax}. */
+int a3g_get_minmax_index(a3g_ctx *ctx, int32_t ivent, int32_t jvent, int32_t kvent,
+                         int32_t *box);
+/* Sets the current box (solution::imin..kmax) explicitly. */
+int a3g_set_subgrid(a3g_ctx *ctx, const int32_t *box);
+int a3g_get_subgrid(a3g_ctx *ctx, int32_t *box);
+
+/* One whole transport step in the order of src/Ash3d.F90:376-510 with the
+ * dt already set: prologue, source column (flux may be NULL), Set_BC(1),
+ * AdvectHorz(itime), AdvectVert, [Set_BC(2), DiffuseHorz(itime),
+ * DiffuseVert].  Nothing is allocated inside. */
+int a3g_step(a3g_ctx *ctx, int32_t itime, int32_t ivent, int32_t jvent, int32_t kvent,
+             const double *flux);
+
+/* Count of kernels this context has launched (diagnostics). */
+int a3g_kernel_launches(a3g_ctx *ctx, uint64_t *count);
+
+/* ---- measurement (no counterpart in the reference, which only reports
+ *      cpu_time/system_clock totals, src/Ash3d.F90:727-759) ---- */
+/* The cudaStream_t all of this context's work is queued on. */
+int a3g_get_stream(a3g_ctx *ctx, void **stream);
+/* Kernel classes reported by a3g_kernel_times. */
+#define A3G_K_ADVECT_X   0
+#define A3G_K_ADVECT_Y   1
+#define A3G_K_ADVECT_Z   2
+#define A3G_K_DIFF_X     3
+#define A3G_K_DIFF_Y     4
+#define A3G_K_DIFF_Z     5
+#define A3G_K_CN_TABLE   6
+#define A3G_K_CN_SOLVE_X 7
+#define A3G_K_CN_SOLVE_Y 8
+#define A3G_K_CN_SOLVE_Z 9
+#define A3G_K_CFL        10
+#define A3G_K_TOTALS     11
+#define A3G_K_WINDS      12
+#define A3G_K_OTHER      13
+#define A3G_K_COUNT      14
+/* Starts (enable=1) or stops per-kernel CUDA-event timing; starting clears
+ * the accumulators.  Timing brackets every launch with two events on the
+ * context's stream. */
+int a3g_kernel_timing(a3g_ctx *ctx, int32_t enable);
+/* Sums per kernel class since timing was enabled (synchronises the stream):
+ * ms[A3G_K_COUNT] total milliseconds, count[A3G_K_COUNT] launches. */
+int a3g_kernel_times(a3g_ctx *ctx, double *ms, uint64_t *count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,955 @@
+/*
+ * ash3d_oracle.c -- CPU restatement of Ash3d's per-time-step transport path.
+ *
+ * TEST INFRASTRUCTURE ONLY (the checker and the timed CPU baseline); see
+ * ash3d_oracle.h.  Every routine cites the reference file:line it restates.
+ * Compiled with -O3 -fno-fast-math -ffp-contract=off so that each Fortran
+ * expression rounds exactly as written (left-to-right, one rounding per
+ * operation, no fused multiply-add).
+ */
+#include "ash3d_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* ---- index helpers for the Fortran layouts (1-based, ghosts at -1,0) ---- */
+#define NXG(s) ((s)->nx + 4)
+#define NYG(s) ((s)->ny + 4)
+#define NZG(s) ((s)->nz + 4)
+
+static inline size_t i3(const orc_state *s, int i, int j, int k) {
+  return (size_t)(i + 1) + (size_t)NXG(s) * ((size_t)(j + 1) + (size_t)NYG(s) * (size_t)(k + 1));
+}
+static inline size_t c5(const orc_state *s, int i, int j, int k, int n, int t) {
+  return i3(s, i, j, k) + (size_t)NXG(s) * NYG(s) * NZG(s) * ((size_t)(n - 1) + (size_t)s->ns * t);
+}
+static inline size_t v4(const orc_state *s, int i, int j, int k, int n) {
+  return i3(s, i, j, k) + (size_t)NXG(s) * NYG(s) * NZG(s) * (size_t)(n - 1);
+}
+static inline size_t k3(const orc_state *s, int i, int j, int k) { /* (0:nx+1,0:ny+1,0:nz+1) */
+  return (size_t)i + (size_t)(s->nx + 2) * ((size_t)j + (size_t)(s->ny + 2) * (size_t)k);
+}
+static inline size_t oyz(const orc_state *s, int j, int k, int n) {
+  return (size_t)(j + 1) + (size_t)NYG(s) * ((size_t)(k + 1) + (size_t)NZG(s) * (size_t)(n - 1));
+}
+static inline size_t oxz(const orc_state *s, int i, int k, int n) {
+  return (size_t)(i + 1) + (size_t)NXG(s) * ((size_t)(k + 1) + (size_t)NZG(s) * (size_t)(n - 1));
+}
+static inline size_t oxy(const orc_state *s, int i, int j, int n) {
+  return (size_t)(i + 1) + (size_t)NXG(s) * ((size_t)(j + 1) + (size_t)NYG(s) * (size_t)(n - 1));
+}
+static inline size_t dep(const orc_state *s, int i, int j, int n) {
+  return (size_t)(i - 1) + (size_t)s->nx * ((size_t)(j - 1) + (size_t)s->ny * (size_t)(n - 1));
+}
+
+/* Fortran MAX/MIN of two reals (no NaNs reach these). */
+static inline double fmx(double a, double b) { return a > b ? a : b; }
+static inline double fmn(double a, double b) { return a < b ? a : b; }
+
+static int g_threads = 0;
+void orc_set_threads(int n) { g_threads = n; }
+int orc_get_threads(void) {
+#ifdef _OPENMP
+  return g_threads > 0 ? g_threads : omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+/* ======================================================================== */
+/* Set_BC(bc_code), src/Set_BC.f90:15-126                                   */
+/* ======================================================================== */
+int orc_set_bc(orc_state *s, int code) {
+  const int nx = s->nx, ny = s->ny, nz = s->nz, ns = s->ns;
+  double *c = s->concen;
+  if (code == 1) {
+    /* velocities: zero-order extrapolation (periodic wrap in x), :44-70 */
+    for (int k = -1; k <= nz + 2; k++)
+      for (int j = -1; j <= ny + 2; j++) {
+        if (s->periodic) {
+          s->vx[i3(s, -1, j, k)] = s->vx[i3(s, nx - 1, j, k)];
+          s->vx[i3(s, 0, j, k)] = s->vx[i3(s, nx, j, k)];
+          s->vx[i3(s, nx + 1, j, k)] = s->vx[i3(s, 1, j, k)];
+          s->vx[i3(s, nx + 2, j, k)] = s->vx[i3(s, 2, j, k)];
+        } else {
+          s->vx[i3(s, -1, j, k)] = s->vx[i3(s, 1, j, k)];
+          s->vx[i3(s, 0, j, k)] = s->vx[i3(s, 1, j, k)];
+          s->vx[i3(s, nx + 1, j, k)] = s->vx[i3(s, nx, j, k)];
+          s->vx[i3(s, nx + 2, j, k)] = s->vx[i3(s, nx, j, k)];
+        }
+      }
+    for (int k = -1; k <= nz + 2; k++)
+      for (int i = -1; i <= nx + 2; i++) {
+        s->vy[i3(s, i, -1, k)] = s->vy[i3(s, i, 1, k)];
+        s->vy[i3(s, i, 0, k)] = s->vy[i3(s, i, 1, k)];
+        s->vy[i3(s, i, ny + 1, k)] = s->vy[i3(s, i, ny, k)];
+        s->vy[i3(s, i, ny + 2, k)] = s->vy[i3(s, i, ny, k)];
+      }
+    for (int j = -1; j <= ny + 2; j++)
+      for (int i = -1; i <= nx + 2; i++) {
+        s->vz[i3(s, i, j, -1)] = s->vz[i3(s, i, j, 1)];
+        s->vz[i3(s, i, j, 0)] = s->vz[i3(s, i, j, 1)];
+        s->vz[i3(s, i, j, nz + 1)] = s->vz[i3(s, i, j, nz)];
+        s->vz[i3(s, i, j, nz + 2)] = s->vz[i3(s, i, j, nz)];
+      }
+    for (int n = 1; n <= ns; n++)
+      for (int j = -1; j <= ny + 2; j++)
+        for (int i = -1; i <= nx + 2; i++) {
+          s->vf[v4(s, i, j, -1, n)] = s->vf[v4(s, i, j, 1, n)];
+          s->vf[v4(s, i, j, 0, n)] = s->vf[v4(s, i, j, 1, n)];
+          s->vf[v4(s, i, j, nz + 1, n)] = s->vf[v4(s, i, j, nz, n)];
+          s->vf[v4(s, i, j, nz + 2, n)] = s->vf[v4(s, i, j, nz, n)];
+        }
+    /* concentrations: zero all ghost shells of ts0, then periodic x, :77-91 */
+    for (int n = 1; n <= ns; n++) {
+      for (int k = -1; k <= nz + 2; k++)
+        for (int j = -1; j <= ny + 2; j++) {
+          c[c5(s, -1, j, k, n, 0)] = 0.0; c[c5(s, 0, j, k, n, 0)] = 0.0;
+          c[c5(s, nx + 1, j, k, n, 0)] = 0.0; c[c5(s, nx + 2, j, k, n, 0)] = 0.0;
+        }
+      for (int k = -1; k <= nz + 2; k++)
+        for (int i = -1; i <= nx + 2; i++) {
+          c[c5(s, i, -1, k, n, 0)] = 0.0; c[c5(s, i, 0, k, n, 0)] = 0.0;
+          c[c5(s, i, ny + 1, k, n, 0)] = 0.0; c[c5(s, i, ny + 2, k, n, 0)] = 0.0;
+        }
+      for (int j = -1; j <= ny + 2; j++)
+        for (int i = -1; i <= nx + 2; i++) {
+          c[c5(s, i, j, -1, n, 0)] = 0.0; c[c5(s, i, j, 0, n, 0)] = 0.0;
+          c[c5(s, i, j, nz + 1, n, 0)] = 0.0; c[c5(s, i, j, nz + 2, n, 0)] = 0.0;
+        }
+      if (s->periodic)
+        for (int k = -1; k <= nz + 2; k++)
+          for (int j = -1; j <= ny + 2; j++) {
+            c[c5(s, -1, j, k, n, 0)] = c[c5(s, nx - 1, j, k, n, 0)];
+            c[c5(s, 0, j, k, n, 0)] = c[c5(s, nx, j, k, n, 0)];
+            c[c5(s, nx + 1, j, k, n, 0)] = c[c5(s, 1, j, k, n, 0)];
+            c[c5(s, nx + 2, j, k, n, 0)] = c[c5(s, 2, j, k, n, 0)];
+          }
+    }
+    return 0;
+  } else if (code == 2) {
+    /* Neumann mirror of the concentration ghosts, :98-118 */
+    for (int n = 1; n <= ns; n++) {
+      for (int k = -1; k <= nz + 2; k++)
+        for (int j = -1; j <= ny + 2; j++) {
+          c[c5(s, -1, j, k, n, 0)] = c[c5(s, 1, j, k, n, 0)];
+          c[c5(s, 0, j, k, n, 0)] = c[c5(s, 1, j, k, n, 0)];
+          c[c5(s, nx + 1, j, k, n, 0)] = c[c5(s, nx, j, k, n, 0)];
+          c[c5(s, nx + 2, j, k, n, 0)] = c[c5(s, nx, j, k, n, 0)];
+          if (s->periodic) {
+            c[c5(s, -1, j, k, n, 0)] = c[c5(s, nx - 1, j, k, n, 0)];
+            c[c5(s, 0, j, k, n, 0)] = c[c5(s, nx, j, k, n, 0)];
+            c[c5(s, nx + 1, j, k, n, 0)] = c[c5(s, 1, j, k, n, 0)];
+            c[c5(s, nx + 2, j, k, n, 0)] = c[c5(s, 2, j, k, n, 0)];
+          }
+        }
+      for (int k = -1; k <= nz + 2; k++)
+        for (int i = -1; i <= nx + 2; i++) {
+          c[c5(s, i, -1, k, n, 0)] = c[c5(s, i, 1, k, n, 0)];
+          c[c5(s, i, 0, k, n, 0)] = c[c5(s, i, 1, k, n, 0)];
+          c[c5(s, i, ny + 1, k, n, 0)] = c[c5(s, i, ny, k, n, 0)];
+          c[c5(s, i, ny + 2, k, n, 0)] = c[c5(s, i, ny, k, n, 0)];
+        }
+      for (int j = -1; j <= ny + 2; j++)
+        for (int i = -1; i <= nx + 2; i++) {
+          c[c5(s, i, j, -1, n, 0)] = c[c5(s, i, j, 1, n, 0)];
+          c[c5(s, i, j, 0, n, 0)] = c[c5(s, i, j, 1, n, 0)];
+          c[c5(s, i, j, nz + 1, n, 0)] = c[c5(s, i, j, nz, n, 0)];
+          c[c5(s, i, j, nz + 2, n, 0)] = c[c5(s, i, j, nz, n, 0)];
+        }
+    }
+    return 0;
+  }
+  return 1; /* "ERROR BC code not recognized", :119-123 */
+}
+
+/* ======================================================================== */
+/* One DCU row: the body shared by advect_x/y/z                              */
+/* src/AdvectionHorz_DCU.f90:153-281 (identical in :485-533 and              */
+/* src/AdvectionVert_DCU.f90:183-298).  All arrays are indexed -1..len+2     */
+/* through pointers offset by one element; the topography term (:251-257)    */
+/* is identically zero for ZScaling_ID 0/1 and is not restated.              */
+/* ======================================================================== */
+typedef struct {
+  double *q, *vel, *sig, *kap, *dtv, *usig, *dq, *fss, *fsl, *fsr, *upd;
+  double *mem;
+} row_scratch;
+
+static void row_alloc(row_scratch *r, int len) {
+  size_t m = (size_t)len + 4;
+  r->mem = (double *)calloc(11 * m, sizeof(double));
+  double *p = r->mem;
+  r->q = p + 1; p += m;  r->vel = p + 1; p += m; r->sig = p + 1; p += m;
+  r->kap = p + 1; p += m; r->dtv = p + 1; p += m; r->usig = p + 1; p += m;
+  r->dq = p + 1; p += m;  r->fss = p + 1; p += m; r->fsl = p + 1; p += m;
+  r->fsr = p + 1; p += m; r->upd = p + 1;
+}
+
+static void dcu_row(const orc_state *s, row_scratch *r, int len, int rmin, int rmax) {
+  const double dt = s->dt, eps = s->eps_thresh;
+  double *q = r->q, *vel = r->vel, *sig = r->sig, *kap = r->kap;
+  double *dtv = r->dtv, *usig = r->usig, *dq = r->dq, *fss = r->fss;
+  double *fsl = r->fsl, *fsr = r->fsr, *upd = r->upd;
+  for (int i = rmin - 2; i <= rmax + 2; i++) dtv[i] = dt / kap[i];           /* :155 */
+  for (int i = -1; i <= len + 2; i++) usig[i] = 0.0;                        /* :159 */
+  for (int I = rmin - 1; I <= rmax + 1; I++)                                 /* :160 */
+    usig[I] = 0.5 * (vel[I - 1] + vel[I]) * sig[I];
+  for (int I = rmin - 1; I <= rmax + 2; I++) dq[I] = q[I] - q[I - 1];       /* :168 */
+  for (int I = rmin - 1; I <= rmax + 2; I++) { fsl[I] = 0.0; fsr[I] = 0.0; fss[I] = 0.0; }
+  if (s->limiter != ORC_LIM_NONE) {
+    for (int I = rmin; I <= rmax + 1; I++) {                                  /* :179-231 */
+      if (!s->nocycle && fabs(dq[I]) <= eps) continue;
+      double ldq;
+      if (s->limiter == ORC_LIM_LAXWEN) {
+        ldq = dq[I];
+      } else {
+        double dqu = (usig[I] > 0.0) ? dq[I - 1] : dq[I + 1];
+        double theta;
+        if (fabs(dqu) > 3.0 * fabs(dq[I]) || fabs(dq[I]) < eps)
+          theta = copysign(3.0, dqu * dq[I]);
+        else
+          theta = dqu / dq[I];
+        switch (s->limiter) {
+          case ORC_LIM_BW: ldq = dqu; break;
+          case ORC_LIM_FROMM: ldq = dq[I] * (0.5 * (1.0 + theta)); break;
+          case ORC_LIM_MINMOD: ldq = dq[I] * fmx(0.0, fmn(1.0, theta)); break;
+          case ORC_LIM_MC:
+            ldq = dq[I] * fmx(0.0, fmn(fmn((1.0 + theta) / 2.0, 2.0), 2.0 * theta));
+            break;
+          case ORC_LIM_SUPERBEE:
+          default:
+            ldq = dq[I] * fmx(fmx(0.0, fmn(1.0, 2.0 * theta)), fmn(2.0, theta));
+            break;
+        }
+      }
+      double aus = fabs(usig[I]);
+      fss[I] = 0.5 * aus * (1.0 - dtv[I] * aus) * ldq;                       /* :230 */
+    }
+  }
+  for (int I = rmin - 1; I <= rmax + 1; I++) {                                /* :238-259 */
+    fsr[I] = fmx(0.0, usig[I]) * dq[I];
+    fsl[I] = fmn(0.0, usig[I]) * dq[I];
+    double divu_p = fmx(0.0, usig[I]) - fmx(0.0, usig[I - 1]);
+    double divu_m = fmn(0.0, usig[I + 1]) - fmn(0.0, usig[I]);
+    fsr[I] = fsr[I] + q[I] * divu_m;
+    fsl[I] = fsl[I] + q[I - 1] * divu_p;
+  }
+  for (int i = rmin - 1; i <= rmax + 1; i++)                                  /* :264-281 */
+    upd[i] = -(dtv[i] * (fsl[i + 1] + fsr[i] + fss[i + 1] - fss[i]));
+}
+
+static void zero_level(orc_state *s, int t) {
+  size_t lev = (size_t)NXG(s) * NYG(s) * NZG(s) * s->ns;
+  memset(s->concen + lev * t, 0, lev * sizeof(double));
+}
+
+static void copy_back(orc_state *s) { /* ts0(1:nx,1:ny,1:nz,:) = ts1(...) */
+  for (int n = 1; n <= s->ns; n++)
+    for (int k = 1; k <= s->nz; k++)
+      for (int j = 1; j <= s->ny; j++)
+        memcpy(&s->concen[c5(s, 1, j, k, n, 0)], &s->concen[c5(s, 1, j, k, n, 1)],
+               (size_t)s->nx * sizeof(double));
+}
+
+static int max3(int a, int b, int c) { int m = a > b ? a : b; return m > c ? m : c; }
+
+/* advect_x, src/AdvectionHorz_DCU.f90:68-305 */
+void orc_advect_x(orc_state *s) {
+  orc_set_bc(s, 1);                                                           /* :115 */
+  const int rmin = s->imin, rmax = s->imax, nx = s->nx;
+  zero_level(s, 1);                                                           /* :122 */
+  const int nth = orc_get_threads();
+  for (int n = 1; n <= s->ns; n++) {
+    if (!s->is_aloft[n - 1]) continue;
+#pragma omp parallel num_threads(nth)
+    {
+      row_scratch r; row_alloc(&r, nx);
+#pragma omp for collapse(2) schedule(static)
+      for (int k = s->kmin; k <= s->kmax; k++)
+        for (int j = s->jmin; j <= s->jmax; j++) {
+          for (int i = rmin - 2; i <= rmax + 2; i++) {                        /* :143-146 */
+            r.q[i] = s->concen[c5(s, i, j, k, n, 0)];
+            r.vel[i] = s->vx[i3(s, i, j, k)];
+            r.sig[i] = s->sig_nx[i3(s, i, j, k)];
+            r.kap[i] = s->kappa[i3(s, i, j, k)];
+          }
+          dcu_row(s, &r, nx, rmin, rmax);
+          for (int i = rmin; i <= rmax; i++)                                  /* :285-287 */
+            s->concen[c5(s, i, j, k, n, 1)] = s->concen[c5(s, i, j, k, n, 0)] + r.upd[i];
+          if (rmin == 1 && !s->periodic) s->outflow_yz1[oyz(s, j, k, n)] += r.upd[0];
+          if (rmax == nx && !s->periodic) s->outflow_yz2[oyz(s, j, k, n)] += r.upd[nx + 1];
+        }
+      free(r.mem);
+    }
+  }
+  copy_back(s);                                                               /* :302-303 */
+}
+
+/* advect_y, src/AdvectionHorz_DCU.f90:322-556 */
+void orc_advect_y(orc_state *s) {
+  orc_set_bc(s, 1);
+  const int rmin = s->jmin, rmax = s->jmax, ny = s->ny;
+  zero_level(s, 1);
+  const int nth = orc_get_threads();
+  for (int n = 1; n <= s->ns; n++) {
+    if (!s->is_aloft[n - 1]) continue;
+#pragma omp parallel num_threads(nth)
+    {
+      row_scratch r; row_alloc(&r, ny);
+#pragma omp for collapse(2) schedule(static)
+      for (int k = s->kmin; k <= s->kmax; k++)
+        for (int i = s->imin; i <= s->imax; i++) {
+          for (int j = rmin - 2; j <= rmax + 2; j++) {
+            r.q[j] = s->concen[c5(s, i, j, k, n, 0)];
+            r.vel[j] = s->vy[i3(s, i, j, k)];
+            r.sig[j] = s->sig_ny[i3(s, i, j, k)];
+            r.kap[j] = s->kappa[i3(s, i, j, k)];
+          }
+          dcu_row(s, &r, ny, rmin, rmax);
+          for (int j = rmin; j <= rmax; j++)
+            s->concen[c5(s, i, j, k, n, 1)] = s->concen[c5(s, i, j, k, n, 0)] + r.upd[j];
+          if (rmin == 1) s->outflow_xz1[oxz(s, i, k, n)] += r.upd[0];          /* :540-545 */
+          if (rmax == ny) s->outflow_xz2[oxz(s, i, k, n)] += r.upd[ny + 1];
+        }
+      free(r.mem);
+    }
+  }
+  copy_back(s);
+}
+
+/* advect_z, src/AdvectionVert_DCU.f90:100-323 */
+void orc_advect_z(orc_state *s) {
+  orc_set_bc(s, 1);
+  const int rmin = s->kmin, rmax = s->kmax, nz = s->nz;
+  const int ncells = rmax - rmin + 1;
+  zero_level(s, 1);
+  const int nth = orc_get_threads();
+  for (int n = 1; n <= s->ns; n++) {
+    if (!s->is_aloft[n - 1]) continue;
+#pragma omp parallel num_threads(nth)
+    {
+      row_scratch r; row_alloc(&r, max3(nz, ncells + 1, 1));
+#pragma omp for collapse(2) schedule(static)
+      for (int j = s->jmin; j <= s->jmax; j++)
+        for (int i = s->imin; i <= s->imax; i++) {
+          for (int k = rmin - 2; k <= rmax + 2; k++) {                        /* :171-176 */
+            r.q[k] = s->concen[c5(s, i, j, k, n, 0)];
+            r.vel[k] = s->vz[i3(s, i, j, k)] + s->vh[i3(s, i, j, k)] + s->vf[v4(s, i, j, k, n)];
+            r.sig[k] = s->sig_nz[i3(s, i, j, k)];
+            r.kap[k] = s->kappa[i3(s, i, j, k)];
+          }
+          dcu_row(s, &r, nz, rmin, rmax);
+          for (int k = rmin; k <= rmax; k++)
+            s->concen[c5(s, i, j, k, n, 1)] = s->concen[c5(s, i, j, k, n, 0)] + r.upd[k];
+          if (rmin == 1) s->outflow_xy1[oxy(s, i, j, n)] += r.upd[0];          /* :306-308 */
+          /* :309-311 uses update_cc(ncells+1), which equals rmax+1 only when
+           * kmin == 1 (the top-outflow index quirk is kept). */
+          if (rmax == nz) s->outflow_xy2[oxy(s, i, j, n)] += r.upd[ncells + 1];
+        }
+      free(r.mem);
+    }
+  }
+  copy_back(s);
+  for (int n = 1; n <= s->ns; n++)                                            /* :321 */
+    for (int j = 1; j <= s->ny; j++)
+      for (int i = 1; i <= s->nx; i++)
+        s->deposit[dep(s, i, j, n)] = s->outflow_xy1[oxy(s, i, j, n)];
+}
+
+/* get_minmax_index, src/Calc_Mesh.f90:432-542.  The per-plane maxval()s are
+ * gathered in one pass (a max does not depend on the visiting order). */
+int orc_get_minmax_index(orc_state *s, int ivent, int jvent, int kvent) {
+  const double th = s->cloudcon_grid_thresh;
+  const int nx = s->nx, ny = s->ny, nz = s->nz;
+  double *pi = (double *)malloc(sizeof(double) * (size_t)(nx + ny + nz + 3));
+  double *pj = pi + nx + 1, *pk = pj + ny + 1;
+  for (int i = 0; i <= nx; i++) pi[i] = -HUGE_VAL;
+  for (int j = 0; j <= ny; j++) pj[j] = -HUGE_VAL;
+  for (int k = 0; k <= nz; k++) pk[k] = -HUGE_VAL;
+  for (int n = 1; n <= s->ns; n++)
+    for (int k = 1; k <= nz; k++)
+      for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++) {
+          double v = s->concen[c5(s, i, j, k, n, 0)];
+          if (v > pi[i]) pi[i] = v;
+          if (v > pj[j]) pj[j] = v;
+          if (v > pk[k]) pk[k] = v;
+        }
+  s->imin = 1; s->imax = nx;
+  for (int i = 2; i <= ivent - 1; i++) { if (pi[i] < th) s->imin = i; else break; }
+  for (int i = nx; i >= s->imin + 2; i--) { if (pi[i] < th) s->imax = i; else break; }
+  if (s->periodic && (s->imin == 1 || s->imax == nx)) { s->imin = 1; s->imax = nx; }
+  s->jmin = 1; s->jmax = ny;
+  for (int j = 2; j <= jvent - 1; j++) { if (pj[j] < th) s->jmin = j; else break; }
+  for (int j = ny; j >= s->jmin + 2; j--) { if (pj[j] < th) s->jmax = j; else break; }
+  s->kmin = 1; s->kmax = nz;
+  for (int k = 2; k <= kvent - 1; k++) { if (pk[k] < th) s->kmin = k; else break; }
+  for (int k = nz; k >= s->kmin + 2; k--) { if (pk[k] < th) s->kmax = k; else break; }
+  free(pi);
+  if (s->kmax < s->kmin) return 1;
+  if (s->imax - s->imin < 2) { s->imax = (s->imax + 1 < nx) ? s->imax + 1 : nx; s->imin = s->imax - 2; }
+  if (s->jmax - s->jmin < 2) { s->jmax = (s->jmax + 1 < ny) ? s->jmax + 1 : ny; s->jmin = s->jmax - 2; }
+  if (s->kmax - s->kmin < 2) { s->kmax = (s->kmax + 1 < nz) ? s->kmax + 1 : nz; s->kmin = s->kmax - 2; }
+  return 0;
+}
+
+/* AdvectHorz(itoggle), src/AdvectionHorz.f90:47-85 */
+int orc_advect_horz(orc_state *s, int itoggle, int ivent, int jvent, int kvent) {
+  if (s->fast_subgrid) {
+    if (orc_get_minmax_index(s, ivent, jvent, kvent)) return 1;
+  } else {
+    s->imin = 1; s->imax = s->nx; s->jmin = 1; s->jmax = s->ny; s->kmin = 1; s->kmax = s->nz;
+  }
+  if (itoggle % 2 == 0) { orc_advect_y(s); orc_advect_x(s); }
+  else { orc_advect_x(s); orc_advect_y(s); }
+  return 0;
+}
+
+/* AdvectVert, src/AdvectionVert_DCU.f90:64-82 */
+void orc_advect_vert(orc_state *s) { orc_advect_z(s); }
+
+/* ======================================================================== */
+/* Explicit diffusion, src/Diffusion.F90:266-650                             */
+/* ======================================================================== */
+/* One explicit row: q,kap indexed rmin-1..rmax+1, sig 1..; kk the
+ * diffusivity along the row (indexed like q).  :335-377 */
+static void diff_row(double dt, int rmin, int rmax, const double *q, const double *kap,
+                     const double *sig, const double *kk, double *upd) {
+  /* ds_I/k_ds_I at interfaces rmin..rmax+1 */
+  for (int l = rmin; l <= rmax; l++) {
+    double dsR = 2.0 * sig[l + 1] / (kap[l] + kap[l + 1]);
+    double kdsR = 0.5 * (kk[l] + kk[l + 1]) * dsR;
+    double dsL = 2.0 * sig[l] / (kap[l - 1] + kap[l]);
+    double kdsL = 0.5 * (kk[l - 1] + kk[l]) * dsL;
+    double dqR = q[l + 1] - q[l];
+    double dqL = q[l] - q[l - 1];
+    double LF = dt * kdsR * dqR * (sig[l + 1] / kap[l]);
+    double RF = -(dt * kdsL * dqL * (sig[l] / kap[l]));
+    upd[l] = LF + RF;
+  }
+}
+
+static void neumann_x(orc_state *s) { /* :317-327 */
+  const int nx = s->nx;
+  double *c = s->concen;
+  for (int n = 1; n <= s->ns; n++)
+    for (int k = -1; k <= s->nz + 2; k++)
+      for (int j = -1; j <= s->ny + 2; j++) {
+        c[c5(s, -1, j, k, n, 0)] = c[c5(s, 1, j, k, n, 0)];
+        c[c5(s, 0, j, k, n, 0)] = c[c5(s, 1, j, k, n, 0)];
+        c[c5(s, nx + 1, j, k, n, 0)] = c[c5(s, nx, j, k, n, 0)];
+        c[c5(s, nx + 2, j, k, n, 0)] = c[c5(s, nx, j, k, n, 0)];
+        if (s->periodic) {
+          c[c5(s, -1, j, k, n, 0)] = c[c5(s, nx - 1, j, k, n, 0)];
+          c[c5(s, 0, j, k, n, 0)] = c[c5(s, nx, j, k, n, 0)];
+          c[c5(s, nx + 1, j, k, n, 0)] = c[c5(s, 1, j, k, n, 0)];
+          c[c5(s, nx + 2, j, k, n, 0)] = c[c5(s, 2, j, k, n, 0)];
+        }
+      }
+}
+static void neumann_y(orc_state *s) { /* :457-460 */
+  const int ny = s->ny;
+  double *c = s->concen;
+  for (int n = 1; n <= s->ns; n++)
+    for (int k = -1; k <= s->nz + 2; k++)
+      for (int i = -1; i <= s->nx + 2; i++) {
+        c[c5(s, i, -1, k, n, 0)] = c[c5(s, i, 1, k, n, 0)];
+        c[c5(s, i, 0, k, n, 0)] = c[c5(s, i, 1, k, n, 0)];
+        c[c5(s, i, ny + 1, k, n, 0)] = c[c5(s, i, ny, k, n, 0)];
+        c[c5(s, i, ny + 2, k, n, 0)] = c[c5(s, i, ny, k, n, 0)];
+      }
+}
+static void neumann_z(orc_state *s) { /* :587-590 */
+  const int nz = s->nz;
+  double *c = s->concen;
+  for (int n = 1; n <= s->ns; n++)
+    for (int j = -1; j <= s->ny + 2; j++)
+      for (int i = -1; i <= s->nx + 2; i++) {
+        c[c5(s, i, j, -1, n, 0)] = c[c5(s, i, j, 1, n, 0)];
+        c[c5(s, i, j, 0, n, 0)] = c[c5(s, i, j, 1, n, 0)];
+        c[c5(s, i, j, nz + 1, n, 0)] = c[c5(s, i, j, nz, n, 0)];
+        c[c5(s, i, j, nz + 2, n, 0)] = c[c5(s, i, j, nz, n, 0)];
+      }
+}
+
+typedef struct { double *q, *kap, *sig, *kk, *upd, *mem; } drow;
+static void drow_alloc(drow *r, int len) {
+  size_t m = (size_t)len + 4;
+  r->mem = (double *)calloc(5 * m, sizeof(double));
+  r->q = r->mem + 1; r->kap = r->q + m; r->sig = r->kap + m; r->kk = r->sig + m; r->upd = r->kk + m;
+}
+
+void orc_diff_x(orc_state *s) { /* :266-388 */
+  const int rmin = s->imin, rmax = s->imax;
+  zero_level(s, 1);
+  neumann_x(s);
+  drow r; drow_alloc(&r, s->nx);
+  for (int n = 1; n <= s->ns; n++) {
+    if (!s->is_aloft[n - 1]) continue;
+    for (int k = s->kmin; k <= s->kmax; k++)
+      for (int j = s->jmin; j <= s->jmax; j++) {
+        for (int i = rmin - 1; i <= rmax + 1; i++) {
+          r.q[i] = s->concen[c5(s, i, j, k, n, 0)];
+          r.kap[i] = s->kappa[i3(s, i, j, k)];
+          r.kk[i] = s->kx[k3(s, i, j, k)];
+          r.sig[i] = s->sig_nx[i3(s, i, j, k)];
+        }
+        diff_row(s->dt, rmin, rmax, r.q, r.kap, r.sig, r.kk, r.upd);
+        for (int i = rmin; i <= rmax; i++)
+          s->concen[c5(s, i, j, k, n, 1)] = s->concen[c5(s, i, j, k, n, 0)] + r.upd[i];
+      }
+  }
+  free(r.mem);
+  copy_back(s);
+}
+
+void orc_diff_y(orc_state *s) { /* :406-518 */
+  const int rmin = s->jmin, rmax = s->jmax;
+  zero_level(s, 1);
+  neumann_y(s);
+  drow r; drow_alloc(&r, s->ny);
+  for (int n = 1; n <= s->ns; n++) {
+    if (!s->is_aloft[n - 1]) continue;
+    for (int k = s->kmin; k <= s->kmax; k++)
+      for (int i = s->imin; i <= s->imax; i++) {
+        for (int j = rmin - 1; j <= rmax + 1; j++) {
+          r.q[j] = s->concen[c5(s, i, j, k, n, 0)];
+          r.kap[j] = s->kappa[i3(s, i, j, k)];
+          r.kk[j] = s->ky[k3(s, i, j, k)];
+          r.sig[j] = s->sig_ny[i3(s, i, j, k)];
+        }
+        diff_row(s->dt, rmin, rmax, r.q, r.kap, r.sig, r.kk, r.upd);
+        for (int j = rmin; j <= rmax; j++)
+          s->concen[c5(s, i, j, k, n, 1)] = s->concen[c5(s, i, j, k, n, 0)] + r.upd[j];
+      }
+  }
+  free(r.mem);
+  copy_back(s);
+}
+
+void orc_diff_z(orc_state *s) { /* :536-650 */
+  const int rmin = s->kmin, rmax = s->kmax;
+  zero_level(s, 1);
+  neumann_z(s);
+  drow r; drow_alloc(&r, s->nz);
+  for (int n = 1; n <= s->ns; n++) {
+    if (!s->is_aloft[n - 1]) continue;
+    for (int j = s->jmin; j <= s->jmax; j++)
+      for (int i = s->imin; i <= s->imax; i++) {
+        for (int k = rmin - 1; k <= rmax + 1; k++) {
+          r.q[k] = s->concen[c5(s, i, j, k, n, 0)];
+          r.kap[k] = s->kappa[i3(s, i, j, k)];
+          r.kk[k] = s->kz[k3(s, i, j, k)];
+          r.sig[k] = s->sig_nz[i3(s, i, j, k)];
+        }
+        diff_row(s->dt, rmin, rmax, r.q, r.kap, r.sig, r.kk, r.upd);
+        for (int k = rmin; k <= rmax; k++)
+          s->concen[c5(s, i, j, k, n, 1)] = s->concen[c5(s, i, j, k, n, 0)] + r.upd[k];
+      }
+  }
+  free(r.mem);
+  copy_back(s);
+}
+
+/* ======================================================================== */
+/* LAPACK dgtsv restatement (NRHS = 1).                                      */
+/* Published algorithm of reference LAPACK's DGTSV: for i = 1..n-1 eliminate */
+/* the subdiagonal with partial pivoting between rows i and i+1 (the         */
+/* interchange stores the second superdiagonal in DL), then back-substitute. */
+/* Arrays are 0-based here: dl[0..n-2], d[0..n-1], du[0..n-2], b[0..n-1].     */
+/* ======================================================================== */
+int orc_dgtsv(int n, double *dl, double *d, double *du, double *b) {
+  if (n < 0) return -1;
+  if (n == 0) return 0;
+  for (int i = 0; i < n - 2; i++) {
+    if (fabs(d[i]) >= fabs(dl[i])) {
+      if (d[i] != 0.0) {
+        double fact = dl[i] / d[i];
+        d[i + 1] = d[i + 1] - fact * du[i];
+        b[i + 1] = b[i + 1] - fact * b[i];
+      } else {
+        return i + 1;
+      }
+      dl[i] = 0.0;
+    } else {
+      double fact = d[i] / dl[i];
+      d[i] = dl[i];
+      double temp = d[i + 1];
+      d[i + 1] = du[i] - fact * temp;
+      dl[i] = du[i + 1];
+      du[i + 1] = -fact * dl[i];
+      du[i] = temp;
+      temp = b[i];
+      b[i] = b[i + 1];
+      b[i + 1] = temp - fact * b[i + 1];
+    }
+  }
+  if (n > 1) {
+    int i = n - 2;
+    if (fabs(d[i]) >= fabs(dl[i])) {
+      if (d[i] != 0.0) {
+        double fact = dl[i] / d[i];
+        d[i + 1] = d[i + 1] - fact * du[i];
+        b[i + 1] = b[i + 1] - fact * b[i];
+      } else {
+        return i + 1;
+      }
+    } else {
+      double fact = d[i] / dl[i];
+      d[i] = dl[i];
+      double temp = d[i + 1];
+      d[i + 1] = du[i] - fact * temp;
+      du[i] = temp;
+      temp = b[i];
+      b[i] = b[i + 1];
+      b[i + 1] = temp - fact * b[i + 1];
+    }
+  }
+  if (d[n - 1] == 0.0) return n;
+  b[n - 1] = b[n - 1] / d[n - 1];
+  if (n > 1) b[n - 2] = (b[n - 2] - du[n - 2] * b[n - 1]) / d[n - 2];
+  for (int i = n - 3; i >= 0; i--)
+    b[i] = (b[i] - du[i] * b[i + 1] - dl[i] * b[i + 2]) / d[i];
+  return 0;
+}
+
+/* ======================================================================== */
+/* Crank-Nicolson diffusion, src/Diffusion.F90:671-1428                      */
+/* ======================================================================== */
+typedef struct { double *q, *kap, *sig, *kk, *DL, *D, *DU, *B, *mem; } cnrow;
+static void cnrow_alloc(cnrow *r, int len) {
+  size_t m = (size_t)len + 4;
+  r->mem = (double *)calloc(8 * m, sizeof(double));
+  r->q = r->mem + 1; r->kap = r->q + m; r->sig = r->kap + m; r->kk = r->sig + m;
+  r->DL = r->kk + m; r->D = r->DL + m; r->DU = r->D + m; r->B = r->DU + m;
+}
+
+/* Builds and solves one line (q,kap,kk indexed rmin-1..rmax+1; sig rmin..rmax+1);
+ * the solution is left in r->B[0..ncells-1].  :791-890 */
+static void cn_line(double dt, double imp, int rmin, int rmax, cnrow *r) {
+  const int ncells = rmax - rmin + 1;
+  const double *q = r->q, *kap = r->kap, *sig = r->sig, *kk = r->kk;
+  double *DL = r->DL, *D = r->D, *DU = r->DU, *B = r->B;
+  for (int l = 1; l <= ncells; l++) {
+    const int c = rmin - 1 + l;   /* cell index */
+    const int IL = c, IR = c + 1; /* interface indices */
+    double vavgL = 0.5 * (kap[IL - 1] + kap[IL]);
+    double kavgL = 0.5 * (kk[IL - 1] + kk[IL]);
+    double dsL = sig[IL] / vavgL;
+    double kdsL = kavgL * dsL;
+    double vavgR = 0.5 * (kap[IR - 1] + kap[IR]);
+    double kavgR = 0.5 * (kk[IR - 1] + kk[IR]);
+    double dsR = sig[IR] / vavgR;
+    double kdsR = kavgR * dsR;
+    double LeftFac = dt * kdsL * sig[IL] / kap[c];
+    double RightFac = dt * kdsR * sig[IR] / kap[c];
+    double CenterFac = LeftFac + RightFac;
+    if (l == 1) {
+      D[0] = 1.0 + imp * CenterFac - imp * LeftFac;
+      DU[0] = -(imp * RightFac);
+      double bcl = q[rmin];
+      B[0] = (1.0 - imp) * LeftFac * bcl + (1.0 - (1.0 - imp) * CenterFac) * q[c] +
+             (1.0 - imp) * RightFac * q[c + 1];
+    } else if (l < ncells) {
+      DL[l - 2] = -(imp * LeftFac);
+      D[l - 1] = 1.0 + imp * CenterFac;
+      DU[l - 1] = -(imp * RightFac);
+      B[l - 1] = (1.0 - imp) * LeftFac * q[c - 1] + (1.0 - (1.0 - imp) * CenterFac) * q[c] +
+                 (1.0 - imp) * RightFac * q[c + 1];
+    } else {
+      DL[l - 2] = -(imp * LeftFac);
+      D[l - 1] = 1.0 + imp * CenterFac - imp * RightFac;
+      double bcr = q[rmin - 1 + ncells];
+      B[l - 1] = (1.0 - imp) * LeftFac * q[c - 1] + (1.0 - (1.0 - imp) * CenterFac) * q[c] +
+                 (1.0 - imp) * RightFac * bcr;
+    }
+  }
+  (void)orc_dgtsv(ncells, DL, D, DU, B); /* INFO is ignored, :881-890 */
+}
+
+void orc_diffcn_x(orc_state *s) { /* :671-911 */
+  const int rmin = s->imin, rmax = s->imax, ncells = rmax - rmin + 1;
+  zero_level(s, 1);
+  neumann_x(s);
+  if (ncells <= 1) return;
+  cnrow r; cnrow_alloc(&r, s->nx);
+  for (int n = 1; n <= s->ns; n++) {
+    if (!s->is_aloft[n - 1]) continue;
+    for (int k = s->kmin; k <= s->kmax; k++)
+      for (int j = s->jmin; j <= s->jmax; j++) {
+        for (int i = rmin - 1; i <= rmax + 1; i++) {
+          r.q[i] = s->concen[c5(s, i, j, k, n, 0)];
+          r.kap[i] = s->kappa[i3(s, i, j, k)];
+          r.kk[i] = s->kx[k3(s, i, j, k)];
+          r.sig[i] = s->sig_nx[i3(s, i, j, k)];
+        }
+        cn_line(s->dt, s->imp_fac, rmin, rmax, &r);
+        for (int l = 0; l < ncells; l++) s->concen[c5(s, rmin + l, j, k, n, 1)] = r.B[l];
+      }
+  }
+  free(r.mem);
+  copy_back(s);
+}
+
+void orc_diffcn_y(orc_state *s) { /* :932-1167 */
+  const int rmin = s->jmin, rmax = s->jmax, ncells = rmax - rmin + 1;
+  zero_level(s, 1);
+  neumann_y(s);
+  if (ncells <= 1) return;
+  cnrow r; cnrow_alloc(&r, s->ny);
+  for (int n = 1; n <= s->ns; n++) {
+    if (!s->is_aloft[n - 1]) continue;
+    for (int k = s->kmin; k <= s->kmax; k++)
+      for (int i = s->imin; i <= s->imax; i++) {
+        for (int j = rmin - 1; j <= rmax + 1; j++) {
+          r.q[j] = s->concen[c5(s, i, j, k, n, 0)];
+          r.kap[j] = s->kappa[i3(s, i, j, k)];
+          r.kk[j] = s->ky[k3(s, i, j, k)];
+          r.sig[j] = s->sig_ny[i3(s, i, j, k)];
+        }
+        cn_line(s->dt, s->imp_fac, rmin, rmax, &r);
+        for (int l = 0; l < ncells; l++) s->concen[c5(s, i, rmin + l, k, n, 1)] = r.B[l];
+      }
+  }
+  free(r.mem);
+  copy_back(s);
+}
+
+void orc_diffcn_z(orc_state *s) { /* :1188-1428 */
+  const int rmin = s->kmin, rmax = s->kmax, ncells = rmax - rmin + 1;
+  zero_level(s, 1);
+  neumann_z(s);
+  if (ncells <= 1) return;
+  cnrow r; cnrow_alloc(&r, s->nz);
+  for (int n = 1; n <= s->ns; n++) {
+    if (!s->is_aloft[n - 1]) continue;
+    for (int j = s->jmin; j <= s->jmax; j++)
+      for (int i = s->imin; i <= s->imax; i++) {
+        for (int k = rmin - 1; k <= rmax + 1; k++) {
+          r.q[k] = s->concen[c5(s, i, j, k, n, 0)];
+          r.kap[k] = s->kappa[i3(s, i, j, k)];
+          r.kk[k] = s->kz[k3(s, i, j, k)];
+          r.sig[k] = s->sig_nz[i3(s, i, j, k)];
+        }
+        cn_line(s->dt, s->imp_fac, rmin, rmax, &r);
+        for (int l = 0; l < ncells; l++) s->concen[c5(s, i, j, rmin + l, n, 1)] = r.B[l];
+      }
+  }
+  free(r.mem);
+  copy_back(s);
+}
+
+/* DiffuseHorz(i), src/Diffusion.F90:151-216 */
+void orc_diffuse_horz(orc_state *s, int itime) {
+  if (s->fast_subgrid) {
+    s->imin = s->imin - 1 > 1 ? s->imin - 1 : 1;
+    s->imax = s->imax + 1 < s->nx ? s->imax + 1 : s->nx;
+    s->jmin = s->jmin - 1 > 1 ? s->jmin - 1 : 1;
+    s->jmax = s->jmax + 1 < s->ny ? s->jmax + 1 : s->ny;
+    s->kmin = s->kmin - 1 > 1 ? s->kmin - 1 : 1;
+    s->kmax = s->kmax + 1 < s->nz ? s->kmax + 1 : s->nz;
+  } else {
+    s->imin = 1; s->imax = s->nx; s->jmin = 1; s->jmax = s->ny; s->kmin = 1; s->kmax = s->nz;
+  }
+  if (s->use_cn) {
+    if (itime % 2 == 0) { orc_diffcn_x(s); orc_diffcn_y(s); }
+    else { orc_diffcn_y(s); orc_diffcn_x(s); }
+  } else {
+    if (itime % 2 == 0) { orc_diff_x(s); orc_diff_y(s); }
+    else { orc_diff_y(s); orc_diff_x(s); }
+  }
+}
+
+/* DiffuseVert, src/Diffusion.F90:232-247 */
+void orc_diffuse_vert(orc_state *s) {
+  if (s->use_cn) orc_diffcn_z(s); else orc_diff_z(s);
+}
+
+/* ======================================================================== */
+/* Adjust_DT(.false.), src/Adjust_dt.f90:19-339                              */
+/* ======================================================================== */
+void orc_adjust_dt(orc_state *s, double time, double next_write_time, double simtime,
+                   double *dt_out) {
+  double v[3];
+  orc_cfl_maxima(s, v);
+  orc_dt_from_maxima(s, v, s->n_gs_aloft, time, next_write_time, simtime, dt_out);
+}
+
+/* src/Adjust_dt.f90:136-173: the three maxima (projected grids: max|vx|, max|vy|
+ * before the division by dx, dy). */
+void orc_cfl_maxima(orc_state *s, double out3[3]) {
+  const int nx = s->nx, ny = s->ny, nz = s->nz, ns = s->ns;
+  double vxmax_dx = 0.0, vymax_dy = 0.0, vzmax_dz = 0.0;
+  if (!s->latlon) {                                                           /* :137-146 */
+    double vxmax = 0.0, vymax = 0.0;
+    for (int k = 1; k <= nz; k++)
+      for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++) {
+          double a = fabs(s->vx[i3(s, i, j, k)]);
+          double b = fabs(s->vy[i3(s, i, j, k)]);
+          if (a > vxmax) vxmax = a;
+          if (b > vymax) vymax = b;
+        }
+    vxmax_dx = vxmax;   /* divided by dx, dy in orc_dt_from_maxima */
+    vymax_dy = vymax;
+  }
+  for (int i = 1; i <= nx; i++)                                               /* :147-173 */
+    for (int j = 1; j <= ny; j++)
+      for (int k = 1; k <= nz; k++) {
+        if (s->latlon) {
+          double minsig = fmn(s->sig_nx[i3(s, i, j, k)], s->sig_nx[i3(s, i + 1, j, k)]);
+          double tmp1 = fabs(s->vx[i3(s, i, j, k)]) * minsig / s->kappa[i3(s, i, j, k)];
+          if (tmp1 > vxmax_dx) vxmax_dx = tmp1;
+          minsig = fmn(s->sig_ny[i3(s, i, j, k)], s->sig_ny[i3(s, i, j + 1, k)]);
+          double tmp2 = fabs(s->vy[i3(s, i, j, k)]) * minsig / s->kappa[i3(s, i, j, k)];
+          if (tmp2 > vymax_dy) vymax_dy = tmp2;
+        }
+        double vfmax = 0.0;
+        for (int n = 1; n <= ns; n++) {
+          double a = fabs(s->vf[v4(s, i, j, k, n)]);
+          if (n == 1 || a > vfmax) vfmax = a;
+        }
+        double tmp3 = (fabs(s->vz[i3(s, i, j, k)]) + vfmax) / s->dz_vec[k + 1];
+        if (tmp3 > vzmax_dz) vzmax_dz = tmp3;
+      }
+  out3[0] = vxmax_dx; out3[1] = vymax_dy; out3[2] = vzmax_dz;
+}
+
+/* src/Adjust_dt.f90:137-146 (division by dx, dy) and :176-332. */
+void orc_dt_from_maxima(orc_state *s, const double v3[3], int n_gs_aloft, double time,
+                        double next_write_time, double simtime, double *dt_out) {
+  const int nx = s->nx, ny = s->ny, nz = s->nz;
+  double vxmax_dx = v3[0], vymax_dy = v3[1], vzmax_dz = v3[2];
+  if (!s->latlon) {
+    vxmax_dx = vxmax_dx / s->dx;
+    vymax_dy = vymax_dy / s->dy;
+  }
+  if (n_gs_aloft == 0) vzmax_dz = 0.0;                                        /* :176 */
+  double time_advect = 1.0 / fmx(fmx(vxmax_dx, vymax_dy), vzmax_dz);          /* :179 */
+  if (s->use_diffusion) {                                                      /* :184-287 */
+    if (!s->have_dt_diffus) {
+      double td = s->dt_max;
+      for (int i = 1; i <= nx; i++)
+        for (int j = 1; j <= ny; j++)
+          for (int k = 1; k <= nz; k++) {
+            double kap = s->kappa[i3(s, i, j, k)];
+            double minsig = fmn(s->sig_nx[i3(s, i, j, k)], s->sig_nx[i3(s, i + 1, j, k)]);
+            double r1 = kap / minsig;
+            double tmp1 = (r1 * r1) / s->kx[k3(s, i, j, k)];
+            minsig = fmn(s->sig_ny[i3(s, i, j, k)], s->sig_ny[i3(s, i, j + 1, k)]);
+            double r2 = kap / minsig;
+            double tmp2 = (r2 * r2) / s->ky[k3(s, i, j, k)];
+            minsig = fmn(s->sig_nz[i3(s, i, j, k)], s->sig_nz[i3(s, i, j, k + 1)]);
+            double r3 = kap / minsig;
+            double tmp3b = (r3 * r3) / s->kz[k3(s, i, j, k)];
+            double tmp4 = tmp1 + tmp2 + tmp3b;
+            if (td > tmp4) td = tmp4;
+          }
+      td = s->use_cn ? td * s->imp_dt_fac : td * 0.5;
+      s->time_diffuse = td;
+      s->have_dt_diffus = 1;
+    }
+  } else {
+    s->time_diffuse = s->dt_max;
+  }
+  double dt_tmp = fmn(time_advect, s->time_diffuse);                          /* :290-319 */
+  double dt;
+  if (dt_tmp < s->dt_min) dt = s->dt_min;
+  else if (dt_tmp > s->dt_max) dt = s->dt_max;
+  else dt = fmn(1.0, s->cfl) * dt_tmp;
+  long long fac = (long long)(dt / s->dt_min);                                /* :321-323 */
+  dt = s->dt_min * (double)fac;
+  if ((next_write_time - time) > s->eps_small && (next_write_time - time) < dt)
+    dt = next_write_time - time;                                              /* :325-327 */
+  if (time + dt > simtime) dt = simtime - time;                               /* :329-332 */
+  s->dt = dt;
+  if (dt_out) *dt_out = dt;
+}
+
+/* ======================================================================== */
+/* TimeStepTotals sums, src/TimeStepTotals.f90:57-66;                        */
+/* Calc_AshVol_Aloft/Deposit/Outflow, src/Output_Vars.f90:1255-1459.          */
+/* gfortran's SUM over an array section accumulates in array-element order.  */
+/* ======================================================================== */
+void orc_timestep_totals(orc_state *s, double out[4]) {
+  const int nx = s->nx, ny = s->ny, nz = s->nz, ns = s->ns;
+  const double rho = s->magma_density, km3 = 1.0e9;
+  double aloft = 0.0, depv = 0.0, outv = 0.0;
+  for (int n = 1; n <= ns; n++) {
+    double m = 0.0;
+    for (int k = 1; k <= nz; k++)
+      for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++)
+          m = m + s->concen[c5(s, i, j, k, n, 0)] * s->kappa[i3(s, i, j, k)];
+    s->mass_aloft[n - 1] = m;
+  }
+  for (int n = 1; n <= ns; n++) aloft = aloft + s->mass_aloft[n - 1] / rho / km3;
+  for (int n = 1; n <= ns; n++) {
+    double m = 0.0;
+    for (int j = 1; j <= ny; j++)
+      for (int i = 1; i <= nx; i++)
+        m = m + s->deposit[dep(s, i, j, n)] * s->kappa[i3(s, i, j, 0)];
+    depv = depv + m / rho / km3;
+  }
+  for (int n = 1; n <= ns; n++) {
+    double s1 = 0.0, s2 = 0.0, s3 = 0.0, s4 = 0.0, s5 = 0.0;
+    for (int k = 1; k <= nz; k++)
+      for (int j = 1; j <= ny; j++) s1 = s1 + s->outflow_yz1[oyz(s, j, k, n)] * s->kappa[i3(s, 0, j, k)];
+    for (int k = 1; k <= nz; k++)
+      for (int j = 1; j <= ny; j++) s2 = s2 + s->outflow_yz2[oyz(s, j, k, n)] * s->kappa[i3(s, nx + 1, j, k)];
+    for (int k = 1; k <= nz; k++)
+      for (int i = 1; i <= nx; i++) s3 = s3 + s->outflow_xz1[oxz(s, i, k, n)] * s->kappa[i3(s, i, 0, k)];
+    for (int k = 1; k <= nz; k++)
+      for (int i = 1; i <= nx; i++) s4 = s4 + s->outflow_xz2[oxz(s, i, k, n)] * s->kappa[i3(s, i, ny + 1, k)];
+    for (int j = 1; j <= ny; j++)
+      for (int i = 1; i <= nx; i++) s5 = s5 + s->outflow_xy2[oxy(s, i, j, n)] * s->kappa[i3(s, i, j, nz + 1)];
+    outv = outv + (s1 + s2 + s3 + s4 + s5) / rho / km3;
+  }
+  out[0] = aloft; out[1] = depv; out[2] = outv; out[3] = aloft + depv + outv;
+}
+
+/* ======================================================================== */
+/* Step pieces from the main loop, src/Ash3d.F90:376-431                     */
+/* ======================================================================== */
+void orc_step_prologue(orc_state *s) {
+  size_t lev = (size_t)NXG(s) * NYG(s) * NZG(s) * s->ns;
+  memcpy(s->concen, s->concen + lev, lev * sizeof(double));
+  memset(s->concen + lev, 0, lev * sizeof(double));
+}
+
+void orc_add_source(orc_state *s, int ivent, int jvent, const double *flux, double dt) {
+  for (int n = 1; n <= s->ns; n++)
+    for (int k = 1; k <= s->nz + 1; k++)
+      s->concen[c5(s, ivent, jvent, k, n, 0)] =
+          s->concen[c5(s, ivent, jvent, k, n, 0)] + dt * flux[(size_t)(k - 1) + (size_t)(s->nz + 1) * (n - 1)];
+}
+
+void orc_interp_winds(orc_state *s, const float *vx_last, const float *vx_next,
+                      const float *vy_last, const float *vy_next,
+                      const float *vz_last, const float *vz_next, double frac) {
+  const int nx = s->nx, ny = s->ny, nz = s->nz;
+  for (int k = 1; k <= nz; k++)
+    for (int j = 1; j <= ny; j++)
+      for (int i = 1; i <= nx; i++) {
+        size_t m = (size_t)(i - 1) + (size_t)nx * ((size_t)(j - 1) + (size_t)ny * (k - 1));
+        float dx_ = vx_next[m] - vx_last[m];
+        float dy_ = vy_next[m] - vy_last[m];
+        float dz_ = vz_next[m] - vz_last[m];
+        s->vx[i3(s, i, j, k)] = ((double)vx_last[m] + (double)dx_ * frac) * 3.6;
+        s->vy[i3(s, i, j, k)] = ((double)vy_last[m] + (double)dy_ * frac) * 3.6;
+        s->vz[i3(s, i, j, k)] = ((double)vz_last[m] + (double)dz_ * frac) * 3.6;
+      }
+}
+
+void orc_prune_gs(orc_state *s, double airborne_thresh) {
+  int naloft = 0;
+  for (int n = 0; n < s->ns; n++) {
+    if (s->is_aloft[n] && s->mass_aloft[n] < airborne_thresh) s->is_aloft[n] = 0;
+    else naloft++;
+  }
+  s->n_gs_aloft = naloft;
+}

@@ -1,0 +1,139 @@
+/*
+ * ash3d_oracle.h -- CPU restatement of Ash3d's per-time-step transport path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This oracle is the checker for the CUDA library
+ * (volcano-ash3d_b200/csrc) and the timed CPU baseline; it is never linked
+ * into, called by, or used as a fallback for the product path.  Only tests/,
+ * __graft_entry__.smoke() and the CPU-baseline legs of bench.py load it.
+ *
+ * It keeps the reference's data layout exactly: Fortran column-major arrays
+ * with two ghost cells on each side (concen_pd(-1:nx+2,-1:ny+2,-1:nz+2,1:ns,
+ * ts0:ts1), src/Ash3d_VariableModules.f90:923-946), the ts0/ts1 working and
+ * scratch levels, the zero-then-copy-back of every sweep and the operator
+ * order of src/Ash3d.F90:372-510.  OpenMP appears exactly where the reference
+ * has it: the row loops of the three advection sweeps.
+ *
+ * Parity pinning: the Fortran reference cannot be compiled in this image (no
+ * Fortran compiler, no MetReader/HoursSince/projection libraries), so the
+ * advection/diffusion restatement is "parity unpinned" against the
+ * reference's own binary.  The tridiagonal solver (a restatement of LAPACK
+ * dgtsv, the third-party routine on this path) is pinned against SciPy's
+ * LAPACK dgtsv in tests/test_oracle_dgtsv.py.
+ */
+#ifndef ASH3D_ORACLE_H
+#define ASH3D_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Limiter ids: the LIM_* preprocessor choices of src/makefile:126. */
+enum { ORC_LIM_NONE = 0, ORC_LIM_LAXWEN = 1, ORC_LIM_BW = 2, ORC_LIM_FROMM = 3,
+       ORC_LIM_MINMOD = 4, ORC_LIM_SUPERBEE = 5, ORC_LIM_MC = 6 };
+
+/*
+ * All arrays are owned by the caller and laid out exactly as the Fortran
+ * module arrays (column-major, ghost extents included):
+ *   concen   (-1:nx+2,-1:ny+2,-1:nz+2,1:ns,0:1)
+ *   vx,vy,vz,vh,kappa,sig_nx,sig_ny,sig_nz (-1:nx+2,-1:ny+2,-1:nz+2)
+ *   vf       (-1:nx+2,-1:ny+2,-1:nz+2,1:ns)
+ *   dz_vec   (-1:nz+2)
+ *   kx,ky,kz (0:nx+1,0:ny+1,0:nz+1)
+ *   outflow_yz1/2 (-1:ny+2,-1:nz+2,1:ns)
+ *   outflow_xz1/2 (-1:nx+2,-1:nz+2,1:ns)
+ *   outflow_xy1/2 (-1:nx+2,-1:ny+2,1:ns)
+ *   deposit  DepositGranularity(1:nx,1:ny,1:ns)
+ *   is_aloft IsAloft(1:ns) (0/1)
+ *   mass_aloft (1:ns)
+ */
+typedef struct orc_state {
+  int32_t nx, ny, nz, ns;
+  int32_t periodic, latlon;
+  int32_t limiter, use_cn, use_diffusion, fast_subgrid, nocycle;
+  int32_t imin, imax, jmin, jmax, kmin, kmax;
+  int32_t have_dt_diffus, n_gs_aloft;
+  int32_t nthreads, pad0;
+  double dx, dy;
+  double cfl, dt_min, dt_max, imp_fac, imp_dt_fac, eps_thresh;
+  double eps_small, cloudcon_grid_thresh, magma_density;
+  double dt;            /* time_data::dt (hours) */
+  double time_diffuse;  /* Adjust_DT's saved diffusion limit */
+  double *concen;
+  double *vx, *vy, *vz, *vh, *vf;
+  double *kappa, *sig_nx, *sig_ny, *sig_nz, *dz_vec;
+  double *kx, *ky, *kz;
+  double *outflow_yz1, *outflow_yz2, *outflow_xz1, *outflow_xz2;
+  double *outflow_xy1, *outflow_xy2;
+  double *deposit;
+  int32_t *is_aloft;
+  double *mass_aloft;
+} orc_state;
+
+/* Set_BC(bc_code), src/Set_BC.f90:15-126.  Returns 1 for an unknown code. */
+int  orc_set_bc(orc_state *s, int code);
+/* advect_x / advect_y, src/AdvectionHorz_DCU.f90:68-305 / 322-556. */
+void orc_advect_x(orc_state *s);
+void orc_advect_y(orc_state *s);
+/* advect_z, src/AdvectionVert_DCU.f90:100-323. */
+void orc_advect_z(orc_state *s);
+/* AdvectHorz(itoggle), src/AdvectionHorz.f90:47-85 (get_minmax_index when
+ * fast_subgrid, else the full box).  Returns nonzero on kmax<kmin. */
+int  orc_advect_horz(orc_state *s, int itoggle, int ivent, int jvent, int kvent);
+/* AdvectVert, src/AdvectionVert_DCU.f90:64-82 (ZScaling_ID 0/1 path). */
+void orc_advect_vert(orc_state *s);
+/* diff_x/diff_y/diff_z, src/Diffusion.F90:266-650. */
+void orc_diff_x(orc_state *s);
+void orc_diff_y(orc_state *s);
+void orc_diff_z(orc_state *s);
+/* diffCN_x/diffCN_y/diffCN_z, src/Diffusion.F90:671-1428. */
+void orc_diffcn_x(orc_state *s);
+void orc_diffcn_y(orc_state *s);
+void orc_diffcn_z(orc_state *s);
+/* DiffuseHorz(i) / DiffuseVert, src/Diffusion.F90:151-247. */
+void orc_diffuse_horz(orc_state *s, int itime);
+void orc_diffuse_vert(orc_state *s);
+/* Adjust_DT(.false.), src/Adjust_dt.f90:19-339 (per-step path).  Writes dt
+ * (hours) to s->dt and *dt_out. */
+void orc_adjust_dt(orc_state *s, double time, double next_write_time,
+                   double simtime, double *dt_out);
+/* The two halves of orc_adjust_dt (grain-sharded runs reduce the maxima
+ * across ranks in between): maxima {vx, vy, vz+vf terms}; projected grids
+ * return max|vx|, max|vy| undivided. */
+void orc_cfl_maxima(orc_state *s, double out3[3]);
+void orc_dt_from_maxima(orc_state *s, const double v3[3], int n_gs_aloft, double time,
+                        double next_write_time, double simtime, double *dt_out);
+/* Calc_AshVol_{Aloft,Deposit,Outflow} + TimeStepTotals sums,
+ * src/TimeStepTotals.f90:57-66, src/Output_Vars.f90:1255-1459.
+ * out = {aloft_vol, dep_vol, outflow_vol, tot_vol}; fills s->mass_aloft. */
+void orc_timestep_totals(orc_state *s, double out[4]);
+/* get_minmax_index, src/Calc_Mesh.f90:432-542.  Returns 1 on kmax<kmin. */
+int  orc_get_minmax_index(orc_state *s, int ivent, int jvent, int kvent);
+/* Step prologue, src/Ash3d.F90:376-378: ts0 <- ts1, ts1 <- 0. */
+void orc_step_prologue(orc_state *s);
+/* Source insertion, src/Ash3d.F90:428-431: concen(ivent,jvent,1:nz+1,g,ts0)
+ * += dt*flux(k,g); flux is (nz+1) x ns with k fastest. */
+void orc_add_source(orc_state *s, int ivent, int jvent, const double *flux,
+                    double dt);
+/* MesoInterpolater wind interpolation, src/MesoInterpolater.f90:207-223:
+ * v = (dble(last) + dble(next-last)*frac)*3.6 on the interior; inputs are
+ * nx*ny*nz FP32 met steps (i fastest). */
+void orc_interp_winds(orc_state *s, const float *vx_last, const float *vx_next,
+                      const float *vy_last, const float *vy_next,
+                      const float *vz_last, const float *vz_next, double frac);
+/* Prune_GS, src/Tephra.f90:782-812. */
+void orc_prune_gs(orc_state *s, double airborne_thresh);
+/* Restatement of LAPACK dgtsv for one right-hand side (reference LAPACK's
+ * published algorithm: Gaussian elimination with partial pivoting of a
+ * tridiagonal matrix, then back substitution).  Returns LAPACK's INFO. */
+int  orc_dgtsv(int n, double *dl, double *d, double *du, double *b);
+/* OpenMP thread count for the advection rows (<=0: runtime default). */
+void orc_set_threads(int n);
+int  orc_get_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,282 @@
+"""ctypes wrapper of the C oracle (ash3d_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: the checker and the timed CPU baseline.  The
+product path (volcano-ash3d_b200) never imports this module.
+
+``OracleModel`` owns every reference module array in its Fortran layout
+(numpy, order='F', ghost extents included) and exposes the same routine names
+as the GPU model, so a parity test drives both through one host loop.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import pathlib
+import subprocess
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+SRC = HERE / "ash3d_oracle.c"
+
+CFLAGS = ["-O3", "-fno-fast-math", "-ffp-contract=off", "-fopenmp", "-fPIC", "-shared", "-Wall"]
+
+
+def build(force: bool = False) -> pathlib.Path:
+    """Compiles the oracle (gcc; IEEE double, no contraction)."""
+    if force or not LIB.exists() or LIB.stat().st_mtime < max(SRC.stat().st_mtime,
+                                                              (HERE / "ash3d_oracle.h").stat().st_mtime):
+        subprocess.check_call(["gcc", *CFLAGS, "-o", str(LIB), str(SRC), "-lm"])
+    return LIB
+
+
+class OrcState(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("ns", C.c_int32),
+        ("periodic", C.c_int32), ("latlon", C.c_int32),
+        ("limiter", C.c_int32), ("use_cn", C.c_int32), ("use_diffusion", C.c_int32),
+        ("fast_subgrid", C.c_int32), ("nocycle", C.c_int32),
+        ("imin", C.c_int32), ("imax", C.c_int32), ("jmin", C.c_int32), ("jmax", C.c_int32),
+        ("kmin", C.c_int32), ("kmax", C.c_int32),
+        ("have_dt_diffus", C.c_int32), ("n_gs_aloft", C.c_int32),
+        ("nthreads", C.c_int32), ("pad0", C.c_int32),
+        ("dx", C.c_double), ("dy", C.c_double),
+        ("cfl", C.c_double), ("dt_min", C.c_double), ("dt_max", C.c_double),
+        ("imp_fac", C.c_double), ("imp_dt_fac", C.c_double), ("eps_thresh", C.c_double),
+        ("eps_small", C.c_double), ("cloudcon_grid_thresh", C.c_double),
+        ("magma_density", C.c_double), ("dt", C.c_double), ("time_diffuse", C.c_double),
+    ] + [(n, C.POINTER(C.c_double)) for n in (
+        "concen", "vx", "vy", "vz", "vh", "vf", "kappa", "sig_nx", "sig_ny", "sig_nz", "dz_vec",
+        "kx", "ky", "kz", "outflow_yz1", "outflow_yz2", "outflow_xz1", "outflow_xz2",
+        "outflow_xy1", "outflow_xy2", "deposit")] + [
+        ("is_aloft", C.POINTER(C.c_int32)), ("mass_aloft", C.POINTER(C.c_double))]
+
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        build()
+        lib = C.CDLL(str(LIB))
+        S = C.POINTER(OrcState)
+        D = C.POINTER(C.c_double)
+        F = C.POINTER(C.c_float)
+        for name, res, args in [
+            ("orc_set_bc", C.c_int, [S, C.c_int]),
+            ("orc_advect_x", None, [S]), ("orc_advect_y", None, [S]), ("orc_advect_z", None, [S]),
+            ("orc_advect_horz", C.c_int, [S, C.c_int, C.c_int, C.c_int, C.c_int]),
+            ("orc_advect_vert", None, [S]),
+            ("orc_diff_x", None, [S]), ("orc_diff_y", None, [S]), ("orc_diff_z", None, [S]),
+            ("orc_diffcn_x", None, [S]), ("orc_diffcn_y", None, [S]), ("orc_diffcn_z", None, [S]),
+            ("orc_diffuse_horz", None, [S, C.c_int]), ("orc_diffuse_vert", None, [S]),
+            ("orc_adjust_dt", None, [S, C.c_double, C.c_double, C.c_double, D]),
+            ("orc_cfl_maxima", None, [S, D]),
+            ("orc_dt_from_maxima", None, [S, D, C.c_int, C.c_double, C.c_double, C.c_double, D]),
+            ("orc_timestep_totals", None, [S, D]),
+            ("orc_get_minmax_index", C.c_int, [S, C.c_int, C.c_int, C.c_int]),
+            ("orc_step_prologue", None, [S]),
+            ("orc_add_source", None, [S, C.c_int, C.c_int, D, C.c_double]),
+            ("orc_interp_winds", None, [S, F, F, F, F, F, F, C.c_double]),
+            ("orc_prune_gs", None, [S, C.c_double]),
+            ("orc_dgtsv", C.c_int, [C.c_int, D, D, D, D]),
+            ("orc_set_threads", None, [C.c_int]), ("orc_get_threads", C.c_int, []),
+        ]:
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def _d(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _f(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def dgtsv(dl, d, du, b):
+    """The oracle's dgtsv restatement on copies of the inputs; returns (x, info)."""
+    lib = load()
+    dl = np.array(dl, dtype=np.float64)
+    d = np.array(d, dtype=np.float64)
+    du = np.array(du, dtype=np.float64)
+    b = np.array(b, dtype=np.float64)
+    info = lib.orc_dgtsv(len(d), _d(dl), _d(d), _d(du), _d(b))
+    return b, info
+
+
+class OracleModel:
+    """Reference module state + the restated per-step routines."""
+
+    def __init__(self, cfg, geo=None, limiter: str = None, threads: int = 0):
+        import importlib
+        syn = importlib.import_module("volcano_ash3d_b200.synthetic")
+        self.syn = syn
+        self.cfg = cfg
+        lib = load()
+        self.lib = lib
+        if threads:
+            lib.orc_set_threads(threads)
+        nx, ny, nz, ns = cfg.nx, cfg.ny, cfg.nz, cfg.ns
+        NX, NY, NZ = nx + 4, ny + 4, nz + 4
+        geo = geo if geo is not None else syn.geometry(cfg)
+        self.geo = geo
+        z = lambda *s: np.zeros(s, order="F")
+        self.concen = z(NX, NY, NZ, ns, 2)
+        self.vx, self.vy, self.vz, self.vh = z(NX, NY, NZ), z(NX, NY, NZ), z(NX, NY, NZ), z(NX, NY, NZ)
+        self.vf = np.asfortranarray(syn.fall_velocity(cfg))
+        self.kappa = np.asfortranarray(geo["kappa"])
+        self.sig_nx = np.asfortranarray(geo["sig_nx"])
+        self.sig_ny = np.asfortranarray(geo["sig_ny"])
+        self.sig_nz = np.asfortranarray(geo["sig_nz"])
+        self.dz_vec = np.ascontiguousarray(geo["dz_vec"])
+        self.kx, self.ky, self.kz = [np.asfortranarray(a) for a in syn.diffusivity(cfg)]
+        self.out_yz1, self.out_yz2 = z(NY, NZ, ns), z(NY, NZ, ns)
+        self.out_xz1, self.out_xz2 = z(NX, NZ, ns), z(NX, NZ, ns)
+        self.out_xy1, self.out_xy2 = z(NX, NY, ns), z(NX, NY, ns)
+        self.deposit = z(nx, ny, ns)
+        self.is_aloft = np.ones(ns, dtype=np.int32)
+        self.mass_aloft = np.zeros(ns)
+        dx, dy = syn.projected_dxdy(cfg)
+        lim = limiter or cfg.limiter
+        from volcano_ash3d_b200._lib import LIMITERS
+        s = OrcState()
+        s.nx, s.ny, s.nz, s.ns = nx, ny, nz, ns
+        s.periodic, s.latlon = int(cfg.periodic), int(cfg.latlon)
+        s.limiter = LIMITERS[lim]
+        s.use_cn, s.use_diffusion = int(cfg.use_cn), int(cfg.use_diffusion)
+        s.fast_subgrid, s.nocycle = int(cfg.fast_subgrid), 0
+        s.imin, s.imax, s.jmin, s.jmax, s.kmin, s.kmax = 1, nx, 1, ny, 1, nz
+        s.have_dt_diffus, s.n_gs_aloft = 0, ns
+        s.dx, s.dy = dx, dy
+        s.cfl, s.dt_min, s.dt_max = cfg.cfl, 1.0e-5, 1.0
+        s.imp_fac, s.imp_dt_fac, s.eps_thresh = 0.5, 4.0, 1.0e-10
+        s.eps_small, s.cloudcon_grid_thresh, s.magma_density = 1.0e-6, 1.0e-7, cfg.magma_density
+        for name, arr in [("concen", self.concen), ("vx", self.vx), ("vy", self.vy), ("vz", self.vz),
+                          ("vh", self.vh), ("vf", self.vf), ("kappa", self.kappa),
+                          ("sig_nx", self.sig_nx), ("sig_ny", self.sig_ny), ("sig_nz", self.sig_nz),
+                          ("dz_vec", self.dz_vec), ("kx", self.kx), ("ky", self.ky), ("kz", self.kz),
+                          ("outflow_yz1", self.out_yz1), ("outflow_yz2", self.out_yz2),
+                          ("outflow_xz1", self.out_xz1), ("outflow_xz2", self.out_xz2),
+                          ("outflow_xy1", self.out_xy1), ("outflow_xy2", self.out_xy2),
+                          ("deposit", self.deposit), ("mass_aloft", self.mass_aloft)]:
+            setattr(s, name, _d(arr))
+        s.is_aloft = self.is_aloft.ctypes.data_as(C.POINTER(C.c_int32))
+        self.s = s
+        self.ps = C.byref(s)
+
+    # --- routines with the reference names ---------------------------------
+    def Set_BC(self, code):
+        if self.lib.orc_set_bc(self.ps, code):
+            raise ValueError("ERROR BC code not recognized")
+
+    def AdvectHorz(self, itoggle):
+        cfg = self.cfg
+        if self.lib.orc_advect_horz(self.ps, itoggle, cfg.ivent, cfg.jvent, 1):
+            raise RuntimeError("ERROR: kmax<kmin in get_minmax_index")
+
+    def advect_x(self):
+        self.lib.orc_advect_x(self.ps)
+
+    def advect_y(self):
+        self.lib.orc_advect_y(self.ps)
+
+    def AdvectVert(self):
+        self.lib.orc_advect_vert(self.ps)
+
+    def DiffuseHorz(self, itime):
+        self.lib.orc_diffuse_horz(self.ps, itime)
+
+    def DiffuseVert(self):
+        self.lib.orc_diffuse_vert(self.ps)
+
+    def Adjust_DT(self, time, next_write_time, simtime):
+        out = C.c_double()
+        self.lib.orc_adjust_dt(self.ps, time, next_write_time, simtime, C.byref(out))
+        return out.value
+
+    def cfl_maxima(self):
+        v = np.zeros(3)
+        self.lib.orc_cfl_maxima(self.ps, _d(v))
+        return v
+
+    def adjust_dt_from_maxima(self, vmax3, n_gs_aloft_total, time, next_write_time, simtime):
+        v = np.ascontiguousarray(vmax3, dtype=np.float64)
+        out = C.c_double()
+        self.lib.orc_dt_from_maxima(self.ps, _d(v), n_gs_aloft_total, time, next_write_time, simtime,
+                                    C.byref(out))
+        return out.value
+
+    def set_dt(self, dt):
+        self.s.dt = dt
+
+    def TimeStepTotals(self):
+        out = np.zeros(4)
+        self.lib.orc_timestep_totals(self.ps, _d(out))
+        return out, self.mass_aloft.copy()
+
+    def get_minmax_index(self):
+        cfg = self.cfg
+        if self.lib.orc_get_minmax_index(self.ps, cfg.ivent, cfg.jvent, 1):
+            raise RuntimeError("ERROR: kmax<kmin in get_minmax_index")
+        s = self.s
+        return (s.imin, s.imax, s.jmin, s.jmax, s.kmin, s.kmax)
+
+    def set_subgrid(self, box):
+        s = self.s
+        s.imin, s.imax, s.jmin, s.jmax, s.kmin, s.kmax = box
+
+    def step_prologue(self):
+        self.lib.orc_step_prologue(self.ps)
+
+    def add_source(self, flux, dt):
+        f = np.asfortranarray(flux, dtype=np.float64)
+        self.lib.orc_add_source(self.ps, self.cfg.ivent, self.cfg.jvent, _d(f), dt)
+
+    def set_met_steps(self, last, nxt):
+        self._met = [np.asfortranarray(a, dtype=np.float32) for a in (*last, *nxt)]
+
+    def interp_winds(self, frac):
+        m = self._met
+        self.lib.orc_interp_winds(self.ps, _f(m[0]), _f(m[3]), _f(m[1]), _f(m[4]), _f(m[2]), _f(m[5]), frac)
+
+    def set_winds(self, vx, vy, vz):
+        self.vx[...] = vx
+        self.vy[...] = vy
+        self.vz[...] = vz
+
+    def set_aloft(self, flags):
+        self.is_aloft[:] = np.asarray(flags, dtype=np.int32)
+        self.s.n_gs_aloft = int(self.is_aloft.sum())
+
+    def prune_gs(self, thresh=1.0e-3):
+        self.lib.orc_prune_gs(self.ps, thresh)
+
+    # --- state access --------------------------------------------------------
+    def interior(self):
+        """Interior of ts0 as (nx, ny, nz, ns), Fortran order."""
+        c = self.cfg
+        return self.concen[2:c.nx + 2, 2:c.ny + 2, 2:c.nz + 2, :, 0].copy(order="F")
+
+    def set_interior(self, q):
+        c = self.cfg
+        self.concen[...] = 0.0
+        self.concen[2:c.nx + 2, 2:c.ny + 2, 2:c.nz + 2, :, 0] = q
+        self.concen[2:c.nx + 2, 2:c.ny + 2, 2:c.nz + 2, :, 1] = q
+
+    def outflows(self):
+        c = self.cfg
+        return dict(
+            yz1=self.out_yz1[2:c.ny + 2, 2:c.nz + 2, :].copy(), yz2=self.out_yz2[2:c.ny + 2, 2:c.nz + 2, :].copy(),
+            xz1=self.out_xz1[2:c.nx + 2, 2:c.nz + 2, :].copy(), xz2=self.out_xz2[2:c.nx + 2, 2:c.nz + 2, :].copy(),
+            xy1=self.out_xy1[2:c.nx + 2, 2:c.ny + 2, :].copy(), xy2=self.out_xy2[2:c.nx + 2, 2:c.ny + 2, :].copy(),
+            deposit=self.deposit.copy())
+
+    @property
+    def dt(self):
+        return self.s.dt

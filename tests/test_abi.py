@@ -1,0 +1,69 @@
+"""The C-ABI library loads, exports every symbol include/ash3d_b200.h
+declares, and reports errors instead of falling back to a CPU path (these
+tests make no compute calls, so they run without a GPU)."""
+import ctypes as C
+import pathlib
+import re
+
+import pytest
+
+ROOT = pathlib.Path(__file__).resolve().parents[1]
+
+
+def _declared():
+    txt = (ROOT / "include" / "ash3d_b200.h").read_text()
+    return sorted(set(re.findall(r"\b(a3g_[a-z_0-9]+)\s*\(", txt)))
+
+
+def test_header_and_binding_agree(pkg):
+    from volcano_ash3d_b200 import _lib
+    assert sorted(_lib.EXPORTED) == _declared()
+
+
+def test_library_exports_every_symbol(pkg):
+    from volcano_ash3d_b200 import _lib
+    lib = _lib.load()
+    for name in _declared():
+        assert hasattr(lib, name), name
+    assert lib.a3g_abi_version() == 1
+
+
+def test_default_params_are_reference_defaults(pkg):
+    from volcano_ash3d_b200 import _lib
+    lib = _lib.load()
+    p = _lib.Params()
+    lib.a3g_default_params(C.byref(p))
+    assert p.limiter == _lib.LIMITERS["superbee"]
+    assert (p.cfl, p.dt_min, p.dt_max) == (0.8, 1.0e-5, 1.0)       # Ash3d_VariableModules.f90:367-371
+    assert (p.imp_fac, p.imp_dt_fac) == (0.5, 4.0)                # Diffusion.F90:53-54
+    assert p.eps_thresh == 1.0e-10 and p.cloudcon_grid_thresh == 1.0e-7
+    assert p.magma_density == 2500.0
+
+
+def test_create_rejects_bad_arguments(pkg):
+    from volcano_ash3d_b200 import _lib
+    lib = _lib.load()
+    g = _lib.GridDesc(nx=0, ny=4, nz=4, ns=1)
+    p = _lib.Params()
+    lib.a3g_default_params(C.byref(p))
+    ctx = C.c_void_p()
+    rc = lib.a3g_create(C.byref(g), C.byref(p), 0, C.byref(ctx))
+    assert rc == 1 and not ctx
+    g = _lib.GridDesc(nx=4, ny=4, nz=4, ns=1)
+    p.zscaling_id = 2
+    rc = lib.a3g_create(C.byref(g), C.byref(p), 0, C.byref(ctx))
+    assert rc == 8 and b"ZScaling_ID 2" in lib.a3g_last_error()
+
+
+def test_no_cpu_fallback_without_gpu(pkg):
+    from conftest import gpu_available
+    if gpu_available():
+        pytest.skip("a GPU is present")
+    from volcano_ash3d_b200 import _lib
+    lib = _lib.load()
+    g = _lib.GridDesc(nx=4, ny=4, nz=4, ns=1)
+    p = _lib.Params()
+    lib.a3g_default_params(C.byref(p))
+    ctx = C.c_void_p()
+    rc = lib.a3g_create(C.byref(g), C.byref(p), 0, C.byref(ctx))
+    assert rc != 0 and not ctx

@@ -1,0 +1,152 @@
+"""ctypes binding of the C-ABI in include/ash3d_b200.h.
+
+The shared library is built in-tree (``libash3d_b200.so`` next to this file)
+by ``build.py``.  There is no CPU path: loading fails loudly when the library
+is missing, and every call that fails raises ``A3GError`` with the library's
+own message.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import pathlib
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = HERE / "libash3d_b200.so"
+
+A3G_OK = 0
+ERR_NAMES = {
+    1: "A3G_ERR_ARG", 2: "A3G_ERR_CUDA", 3: "A3G_ERR_NOMEM", 4: "A3G_ERR_BC_CODE",
+    5: "A3G_ERR_SUBGRID", 6: "A3G_ERR_PIVOT", 7: "A3G_ERR_STATE",
+    8: "A3G_ERR_UNSUPPORTED", 9: "A3G_ERR_NONFINITE",
+}
+LIMITERS = {"none": 0, "laxwen": 1, "bw": 2, "fromm": 3, "minmod": 4, "superbee": 5, "mc": 6}
+
+# every symbol include/ash3d_b200.h declares (checked by the CPU test suite)
+EXPORTED = [
+    "a3g_default_params", "a3g_abi_version", "a3g_last_error", "a3g_create", "a3g_destroy",
+    "a3g_sync", "a3g_device_bytes", "a3g_set_geometry", "a3g_set_diffusivity",
+    "a3g_set_fall_velocity", "a3g_set_aloft", "a3g_set_winds", "a3g_set_met_steps",
+    "a3g_interp_winds", "a3g_upload_concen", "a3g_download_concen", "a3g_upload_outflow",
+    "a3g_download_outflow", "a3g_step_prologue", "a3g_set_dt", "a3g_add_source_column",
+    "a3g_set_bc", "a3g_advect_horz", "a3g_advect_x", "a3g_advect_y", "a3g_advect_vert",
+    "a3g_diffuse_horz", "a3g_diffuse_vert", "a3g_adjust_dt", "a3g_timestep_totals",
+    "a3g_get_minmax_index", "a3g_set_subgrid", "a3g_get_subgrid", "a3g_step",
+    "a3g_kernel_launches", "a3g_get_stream", "a3g_kernel_timing", "a3g_kernel_times",
+    "a3g_cfl_maxima", "a3g_adjust_dt_from_maxima",
+]
+KERNEL_CLASSES = ["advect_x", "advect_y", "advect_z", "diff_x", "diff_y", "diff_z", "cn_table",
+                  "cn_solve_x", "cn_solve_y", "cn_solve_z", "cfl", "totals", "winds", "other"]
+
+
+class A3GError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class GridDesc(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("ns", C.c_int32),
+                ("periodic", C.c_int32), ("latlon", C.c_int32), ("dx", C.c_double), ("dy", C.c_double)]
+
+
+class Params(C.Structure):
+    _fields_ = [("limiter", C.c_int32), ("use_cn", C.c_int32), ("use_diffusion", C.c_int32),
+                ("fast_subgrid", C.c_int32), ("nocycle", C.c_int32), ("zscaling_id", C.c_int32),
+                ("cfl", C.c_double), ("dt_min", C.c_double), ("dt_max", C.c_double),
+                ("imp_fac", C.c_double), ("imp_dt_fac", C.c_double), ("eps_thresh", C.c_double),
+                ("eps_small", C.c_double), ("cloudcon_grid_thresh", C.c_double),
+                ("magma_density", C.c_double)]
+
+
+_lib = None
+
+
+def load(path: os.PathLike | str | None = None) -> C.CDLL:
+    """Loads the in-tree library (once).  Raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = pathlib.Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise FileNotFoundError(
+            f"{p} is missing: build it with `python __graft_entry__.py build` "
+            "(the transport path has no CPU fallback)")
+    lib = C.CDLL(str(p))
+    P = C.c_void_p
+    D = C.POINTER(C.c_double)
+    F = C.POINTER(C.c_float)
+    I = C.POINTER(C.c_int32)
+    sig = {
+        "a3g_default_params": (None, [C.POINTER(Params)]),
+        "a3g_abi_version": (C.c_int, []),
+        "a3g_last_error": (C.c_char_p, []),
+        "a3g_create": (C.c_int, [C.POINTER(GridDesc), C.POINTER(Params), C.c_int, C.POINTER(P)]),
+        "a3g_destroy": (C.c_int, [P]),
+        "a3g_sync": (C.c_int, [P]),
+        "a3g_device_bytes": (C.c_int, [P, C.POINTER(C.c_size_t)]),
+        "a3g_set_geometry": (C.c_int, [P, D, D, D, D, D]),
+        "a3g_set_diffusivity": (C.c_int, [P, D, D, D]),
+        "a3g_set_fall_velocity": (C.c_int, [P, D]),
+        "a3g_set_aloft": (C.c_int, [P, I]),
+        "a3g_set_winds": (C.c_int, [P, D, D, D]),
+        "a3g_set_met_steps": (C.c_int, [P, F, F, F, F, F, F]),
+        "a3g_interp_winds": (C.c_int, [P, C.c_double]),
+        "a3g_upload_concen": (C.c_int, [P, D]),
+        "a3g_download_concen": (C.c_int, [P, D]),
+        "a3g_upload_outflow": (C.c_int, [P, D, D, D, D, D, D]),
+        "a3g_download_outflow": (C.c_int, [P, D, D, D, D, D, D, D]),
+        "a3g_step_prologue": (C.c_int, [P]),
+        "a3g_set_dt": (C.c_int, [P, C.c_double]),
+        "a3g_add_source_column": (C.c_int, [P, C.c_int32, C.c_int32, D, C.c_double]),
+        "a3g_set_bc": (C.c_int, [P, C.c_int32]),
+        "a3g_advect_horz": (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+        "a3g_advect_x": (C.c_int, [P]),
+        "a3g_advect_y": (C.c_int, [P]),
+        "a3g_advect_vert": (C.c_int, [P]),
+        "a3g_diffuse_horz": (C.c_int, [P, C.c_int32]),
+        "a3g_diffuse_vert": (C.c_int, [P]),
+        "a3g_adjust_dt": (C.c_int, [P, C.c_double, C.c_double, C.c_double, D]),
+        "a3g_timestep_totals": (C.c_int, [P, D, D]),
+        "a3g_cfl_maxima": (C.c_int, [P, D]),
+        "a3g_adjust_dt_from_maxima": (C.c_int, [P, D, C.c_int32, C.c_double, C.c_double, C.c_double, D]),
+        "a3g_get_minmax_index": (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, I]),
+        "a3g_set_subgrid": (C.c_int, [P, I]),
+        "a3g_get_subgrid": (C.c_int, [P, I]),
+        "a3g_step": (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, D]),
+        "a3g_kernel_launches": (C.c_int, [P, C.POINTER(C.c_uint64)]),
+        "a3g_get_stream": (C.c_int, [P, C.POINTER(C.c_void_p)]),
+        "a3g_kernel_timing": (C.c_int, [P, C.c_int32]),
+        "a3g_kernel_times": (C.c_int, [P, D, C.POINTER(C.c_uint64)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc: int) -> None:
+    if rc != A3G_OK:
+        msg = _lib.a3g_last_error().decode() if _lib is not None else ""
+        raise A3GError(rc, msg)
+
+
+def dptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and (a.flags.f_contiguous or a.flags.c_contiguous), "need a contiguous float64 array"
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def fptr(a: np.ndarray):
+    assert a.dtype == np.float32 and (a.flags.f_contiguous or a.flags.c_contiguous)
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def iptr(a: np.ndarray):
+    assert a.dtype == np.int32
+    return a.ctypes.data_as(C.POINTER(C.c_int32))

@@ -1,0 +1,771 @@
+// a3g_api.cu -- the C-ABI (include/ash3d_b200.h): context lifetime, data
+// movement between the Fortran-layout host arrays and the device layout,
+// and the per-step entry points that mirror the reference subroutines.
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "a3g_internal.cuh"
+
+namespace a3g {
+
+static thread_local std::string g_err;
+void set_error(const std::string &msg) { g_err = msg; }
+int cuda_fail(cudaError_t e, const char *what) {
+  g_err = std::string(what) + ": " + cudaGetErrorString(e);
+  return A3G_ERR_CUDA;
+}
+size_t cn_table_doubles(const a3g_ctx *ctx, int dir);
+
+static int fail(int code, const std::string &msg) {
+  set_error(msg);
+  return code;
+}
+
+static bool same_bits(double a, double b) { return std::memcmp(&a, &b, sizeof(double)) == 0; }
+
+// Compresses a column-major array with extents n0 x n1 x n2 (x ng blocks) to
+// the indices it actually varies along.  Returns the strides of the
+// compressed copy (0 where the array is constant along that index).
+static void compress(const double *src, long n0, long n1, long n2, long ng, std::vector<double> &out,
+                     long &si, long &sj, long &sk, long &sg) {
+  bool vi = false, vj = false, vk = false;
+  for (long g = 0; g < ng; g++)
+    for (long c = 0; c < n2; c++)
+      for (long b = 0; b < n1; b++) {
+        const double *row = src + n0 * (b + n1 * (c + n2 * g));
+        const double *row0 = src + n0 * (0 + n1 * (c + n2 * g));
+        const double *row00 = src + n0 * (b + n1 * (0 + n2 * g));
+        for (long a = 0; a < n0; a++) {
+          if (!vi && !same_bits(row[a], row[0])) vi = true;
+          if (!vj && !same_bits(row[a], row0[a])) vj = true;
+          if (!vk && !same_bits(row[a], row00[a])) vk = true;
+        }
+      }
+  const long m0 = vi ? n0 : 1, m1 = vj ? n1 : 1, m2 = vk ? n2 : 1;
+  out.assign((size_t)(m0 * m1 * m2 * ng), 0.0);
+  for (long g = 0; g < ng; g++)
+    for (long c = 0; c < m2; c++)
+      for (long b = 0; b < m1; b++)
+        for (long a = 0; a < m0; a++)
+          out[(size_t)(a + m0 * (b + m1 * (c + m2 * g)))] = src[a + n0 * (b + n1 * (c + n2 * g))];
+  si = vi ? 1 : 0;
+  sj = vj ? m0 : 0;
+  sk = vk ? m0 * m1 : 0;
+  sg = m0 * m1 * m2;
+}
+
+static int upload_vec(a3g_ctx *ctx, const std::vector<double> &v, double **dptr) {
+  if (*dptr) { cudaFree(*dptr); ctx->bytes -= 0; *dptr = nullptr; }
+  A3G_CUDA(cudaMalloc(dptr, v.size() * sizeof(double)));
+  ctx->bytes += v.size() * sizeof(double);
+  A3G_CUDA(cudaMemcpy(*dptr, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
+  return A3G_OK;
+}
+
+// host ghosted level <-> device interior level (one 3-D copy per grain)
+static int copy_level(a3g_ctx *ctx, double *host, double *dev, bool to_device, long nxg, long nyg,
+                      long nzg, long ghost, int nx, int ny, int nz, int ng, long dpitch, long dslab,
+                      long dgrain) {
+  for (int g = 0; g < ng; g++) {
+    cudaMemcpy3DParms p;
+    std::memset(&p, 0, sizeof(p));
+    cudaPitchedPtr hp = make_cudaPitchedPtr(host + (size_t)g * nxg * nyg * nzg, nxg * sizeof(double),
+                                            nxg * sizeof(double), nyg);
+    cudaPitchedPtr dp = make_cudaPitchedPtr(dev + (size_t)g * dgrain, dpitch * sizeof(double),
+                                            nx * sizeof(double), dslab / dpitch);
+    cudaPos hpos = make_cudaPos(ghost * sizeof(double), ghost, ghost);
+    cudaPos dpos = make_cudaPos(0, 0, 0);
+    if (to_device) { p.srcPtr = hp; p.srcPos = hpos; p.dstPtr = dp; p.dstPos = dpos; p.kind = cudaMemcpyHostToDevice; }
+    else { p.srcPtr = dp; p.srcPos = dpos; p.dstPtr = hp; p.dstPos = hpos; p.kind = cudaMemcpyDeviceToHost; }
+    p.extent = make_cudaExtent(nx * sizeof(double), ny, nz);
+    A3G_CUDA(cudaMemcpy3DAsync(&p, ctx->stream));
+  }
+  return A3G_OK;
+}
+
+int check_device_error(a3g_ctx *ctx) {
+  if (ctx->h_sc->err != 0) {
+    char buf[160];
+    std::snprintf(buf, sizeof(buf), "device error %d (info %d)", ctx->h_sc->err, ctx->h_sc->err_info);
+    set_error(buf);
+    return ctx->h_sc->err;
+  }
+  return A3G_OK;
+}
+
+static int sync_scalars(a3g_ctx *ctx) {
+  A3G_CUDA(cudaMemcpyAsync(ctx->h_sc, ctx->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, ctx->stream));
+  A3G_CUDA(cudaStreamSynchronize(ctx->stream));
+  return check_device_error(ctx);
+}
+
+void tbegin(a3g_ctx *ctx, int kind) {
+  if (!ctx->timing) return;
+  while (ctx->ev_pool.size() < ctx->ev_used + 2) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) { ctx->timing = false; return; }
+    ctx->ev_pool.push_back(e);
+  }
+  cudaEventRecord(ctx->ev_pool[ctx->ev_used], ctx->stream);
+  ctx->ev_kind.push_back(kind);
+}
+
+void tend(a3g_ctx *ctx) {
+  if (!ctx->timing || ctx->ev_kind.size() * 2 != ctx->ev_used + 2) return;
+  cudaEventRecord(ctx->ev_pool[ctx->ev_used + 1], ctx->stream);
+  ctx->ev_used += 2;
+}
+
+static void full_box(a3g_ctx *ctx) {
+  ctx->box = Box{1, ctx->grid.nx, 1, ctx->grid.ny, 1, ctx->grid.nz};
+}
+
+}  // namespace a3g
+
+using namespace a3g;
+
+#define CTX_CHECK(ctx)                                                   \
+  do {                                                                   \
+    if (!(ctx)) return fail(A3G_ERR_ARG, "null context");                \
+    cudaError_t e__ = cudaSetDevice((ctx)->device);                      \
+    if (e__ != cudaSuccess) return cuda_fail(e__, "cudaSetDevice");      \
+  } while (0)
+
+extern "C" {
+
+void a3g_default_params(a3g_params *p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->limiter = A3G_LIM_SUPERBEE;
+  p->use_cn = 1;
+  p->use_diffusion = 1;
+  p->fast_subgrid = 0;
+  p->nocycle = 0;
+  p->zscaling_id = 0;
+  p->cfl = 0.8;
+  p->dt_min = 1.0e-5;
+  p->dt_max = 1.0;
+  p->imp_fac = 0.5;
+  p->imp_dt_fac = 4.0;
+  p->eps_thresh = 1.0e-10;
+  p->eps_small = 1.0e-6;
+  p->cloudcon_grid_thresh = 1.0e-7;
+  p->magma_density = 2500.0;
+}
+
+int a3g_abi_version(void) { return A3G_ABI_VERSION; }
+const char *a3g_last_error(void) { return g_err.c_str(); }
+
+int a3g_create(const a3g_grid_desc *grid, const a3g_params *params, int device, a3g_ctx **out) {
+  if (!grid || !params || !out) return fail(A3G_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (grid->nx < 1 || grid->ny < 1 || grid->nz < 1 || grid->ns < 1)
+    return fail(A3G_ERR_ARG, "grid extents must be >= 1");
+  if (grid->periodic && grid->nx < 2) return fail(A3G_ERR_ARG, "periodic grid needs nx >= 2");
+  if (params->zscaling_id != 0 && params->zscaling_id != 1)
+    return fail(A3G_ERR_UNSUPPORTED, "ZScaling_ID 2 (advect_sigma) is not implemented");
+  if (params->limiter < A3G_LIM_NONE || params->limiter > A3G_LIM_MC)
+    return fail(A3G_ERR_ARG, "unknown limiter");
+  if (!(params->dt_min > 0.0) || !(params->dt_max >= params->dt_min))
+    return fail(A3G_ERR_ARG, "need 0 < DT_MIN <= DT_MAX");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
+    return fail(A3G_ERR_CUDA, "no CUDA device (the library has no CPU path)");
+  if (device < 0 || device >= ndev) return fail(A3G_ERR_ARG, "bad device ordinal");
+  A3G_CUDA(cudaSetDevice(device));
+  a3g_ctx *ctx = new (std::nothrow) a3g_ctx();
+  if (!ctx) return fail(A3G_ERR_NOMEM, "host allocation failed");
+  ctx->grid = *grid;
+  ctx->prm = *params;
+  ctx->device = device;
+  Layout &L = ctx->L;
+  L.nx = grid->nx; L.ny = grid->ny; L.nz = grid->nz; L.ns = grid->ns;
+  L.P = ((long)grid->nx + 3) / 4 * 4;
+  L.PY = L.P * grid->ny;
+  L.PG = L.PY * grid->nz;
+  full_box(ctx);
+  ctx->h_aloft.assign(grid->ns, 1);
+  ctx->n_gs_aloft = grid->ns;
+  ctx->last_bc = 0;
+  auto dmalloc = [&](void **p, size_t n) -> cudaError_t {
+    cudaError_t e = cudaMalloc(p, n);
+    if (e == cudaSuccess) { ctx->bytes += n; cudaMemsetAsync(*p, 0, n, ctx->stream); }
+    return e;
+  };
+  cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  const size_t lev = (size_t)L.PG * L.ns * sizeof(double);
+  const size_t w3 = (size_t)L.PG * sizeof(double);
+  const int ns = L.ns;
+  if (e == cudaSuccess) e = dmalloc((void **)&ctx->c0, lev);
+  if (e == cudaSuccess) e = dmalloc((void **)&ctx->c1, lev);
+  if (e == cudaSuccess) e = dmalloc((void **)&ctx->vx, w3);
+  if (e == cudaSuccess) e = dmalloc((void **)&ctx->vy, w3);
+  if (e == cudaSuccess) e = dmalloc((void **)&ctx->vz, w3);
+  if (e == cudaSuccess) e = dmalloc((void **)&ctx->out_yz1, sizeof(double) * ns * L.ny * L.nz);
+  if (e == cudaSuccess) e = dmalloc((void **)&ctx->out_yz2, sizeof(double) * ns * L.ny * L.nz);
+  if (e == cudaSuccess) e = dmalloc((void **)&ctx->out_xz1, sizeof(double) * ns * L.nx * L.nz);
+  if (e == cudaSuccess) e = dmalloc((void **)&ctx->out_xz2, sizeof(double) * ns * L.nx * L.nz);
+  if (e == cudaSuccess) e = dmalloc((void **)&ctx->out_xy1, sizeof(double) * ns * L.nx * L.ny);
+  if (e == cudaSuccess) e = dmalloc((void **)&ctx->out_xy2, sizeof(double) * ns * L.nx * L.ny);
+  if (e == cudaSuccess) e = dmalloc((void **)&ctx->aloft, sizeof(int32_t) * ns);
+  if (e == cudaSuccess) e = dmalloc((void **)&ctx->sc, sizeof(DevScalars));
+  ctx->red_len = (size_t)2 * 296 * 7 * ns + 7 * ns;
+  if (e == cudaSuccess) e = dmalloc((void **)&ctx->red_buf, sizeof(double) * ctx->red_len);
+  if (e == cudaSuccess) e = dmalloc((void **)&ctx->plane_flags, sizeof(int32_t) * (L.nx + L.ny + L.nz + 3));
+  if (e == cudaSuccess) e = dmalloc((void **)&ctx->src_buf, sizeof(double) * (L.nz + 1) * ns);
+  if (e == cudaSuccess) e = cudaMallocHost((void **)&ctx->h_sc, sizeof(DevScalars));
+  if (e == cudaSuccess) e = cudaMallocHost((void **)&ctx->h_plane_flags, sizeof(int32_t) * (L.nx + L.ny + L.nz + 3));
+  if (e == cudaSuccess) e = cudaMallocHost((void **)&ctx->h_src, sizeof(double) * (L.nz + 1) * ns);
+  if (e == cudaSuccess) e = cudaMallocHost((void **)&ctx->h_tot, sizeof(double) * 7 * ns);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->src_event, cudaEventDisableTiming);
+  if (e == cudaSuccess) {
+    std::memset(ctx->h_sc, 0, sizeof(DevScalars));
+    std::vector<int32_t> ones(ns, 1);
+    e = cudaMemcpyAsync(ctx->aloft, ones.data(), sizeof(int32_t) * ns, cudaMemcpyHostToDevice, ctx->stream);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) {
+    int rc = (e == cudaErrorMemoryAllocation) ? fail(A3G_ERR_NOMEM, "device allocation failed")
+                                              : cuda_fail(e, "a3g_create");
+    a3g_destroy(ctx);
+    return rc;
+  }
+  ctx->ts1_zeroed = false;
+  *out = ctx;
+  return A3G_OK;
+}
+
+int a3g_destroy(a3g_ctx *ctx) {
+  if (!ctx) return A3G_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  double *dptrs[] = {ctx->c0, ctx->c1, ctx->vx, ctx->vy, ctx->vz, ctx->out_yz1, ctx->out_yz2,
+                     ctx->out_xz1, ctx->out_xz2, ctx->out_xy1, ctx->out_xy2, ctx->red_buf,
+                     ctx->src_buf, ctx->cn_buf, ctx->dz_vec};
+  for (double *p : dptrs) if (p) cudaFree(p);
+  for (double *p : ctx->geo_ptrs) if (p) cudaFree(p);
+  if (ctx->met) cudaFree(ctx->met);
+  if (ctx->aloft) cudaFree(ctx->aloft);
+  if (ctx->sc) cudaFree(ctx->sc);
+  if (ctx->plane_flags) cudaFree(ctx->plane_flags);
+  if (ctx->h_sc) cudaFreeHost(ctx->h_sc);
+  if (ctx->h_plane_flags) cudaFreeHost(ctx->h_plane_flags);
+  if (ctx->h_src) cudaFreeHost(ctx->h_src);
+  if (ctx->h_tot) cudaFreeHost(ctx->h_tot);
+  if (ctx->src_event) cudaEventDestroy(ctx->src_event);
+  for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return A3G_OK;
+}
+
+int a3g_sync(a3g_ctx *ctx) {
+  CTX_CHECK(ctx);
+  return sync_scalars(ctx);
+}
+
+int a3g_device_bytes(a3g_ctx *ctx, size_t *bytes) {
+  if (!ctx || !bytes) return fail(A3G_ERR_ARG, "null argument");
+  *bytes = ctx->bytes;
+  return A3G_OK;
+}
+
+static int set_geo3(a3g_ctx *ctx, const double *src, long n0, long n1, long n2, int lower, Geo3 *g,
+                    int slot) {
+  std::vector<double> v;
+  long si, sj, sk, sg;
+  compress(src, n0, n1, n2, 1, v, si, sj, sk, sg);
+  double *d = ctx->geo_ptrs[slot];
+  ctx->geo_ptrs[slot] = nullptr;
+  if (d) cudaFree(d);
+  int rc = upload_vec(ctx, v, &ctx->geo_ptrs[slot]);
+  if (rc) return rc;
+  g->p = ctx->geo_ptrs[slot];
+  g->si = si; g->sj = sj; g->sk = sk; g->o = lower;
+  return A3G_OK;
+}
+
+static int ensure_cn_buf(a3g_ctx *ctx) {
+  if (!ctx->have_geometry || !ctx->have_diffusivity) return A3G_OK;
+  size_t need = 0;
+  for (int d = 0; d < 3; d++) {
+    size_t n = cn_table_doubles(ctx, d);
+    if (n > need) need = n;
+  }
+  if (need <= ctx->cn_len) return A3G_OK;
+  if (ctx->cn_buf) { cudaFree(ctx->cn_buf); ctx->bytes -= ctx->cn_len * sizeof(double); ctx->cn_buf = nullptr; }
+  cudaError_t e = cudaMalloc((void **)&ctx->cn_buf, need * sizeof(double));
+  if (e != cudaSuccess) { ctx->cn_len = 0; return fail(A3G_ERR_NOMEM, "CN table allocation failed"); }
+  ctx->cn_len = need;
+  ctx->bytes += need * sizeof(double);
+  return A3G_OK;
+}
+
+int a3g_set_geometry(a3g_ctx *ctx, const double *kappa_pd, const double *sigma_nx_pd,
+                     const double *sigma_ny_pd, const double *sigma_nz_pd, const double *dz_vec_pd) {
+  CTX_CHECK(ctx);
+  if (!kappa_pd || !sigma_nx_pd || !sigma_ny_pd || !sigma_nz_pd || !dz_vec_pd)
+    return fail(A3G_ERR_ARG, "null geometry array");
+  const long n0 = ctx->grid.nx + 4, n1 = ctx->grid.ny + 4, n2 = ctx->grid.nz + 4;
+  int rc;
+  if ((rc = set_geo3(ctx, kappa_pd, n0, n1, n2, -1, &ctx->kappa, 0))) return rc;
+  if ((rc = set_geo3(ctx, sigma_nx_pd, n0, n1, n2, -1, &ctx->snx, 1))) return rc;
+  if ((rc = set_geo3(ctx, sigma_ny_pd, n0, n1, n2, -1, &ctx->sny, 2))) return rc;
+  if ((rc = set_geo3(ctx, sigma_nz_pd, n0, n1, n2, -1, &ctx->snz, 3))) return rc;
+  ctx->h_dz.assign(dz_vec_pd, dz_vec_pd + n2);
+  if (ctx->dz_vec) { cudaFree(ctx->dz_vec); ctx->dz_vec = nullptr; }
+  if ((rc = upload_vec(ctx, ctx->h_dz, &ctx->dz_vec))) return rc;
+  ctx->have_geometry = true;
+  return ensure_cn_buf(ctx);
+}
+
+int a3g_set_diffusivity(a3g_ctx *ctx, const double *kx, const double *ky, const double *kz) {
+  CTX_CHECK(ctx);
+  if (!kx || !ky || !kz) return fail(A3G_ERR_ARG, "null diffusivity array");
+  const long n0 = ctx->grid.nx + 2, n1 = ctx->grid.ny + 2, n2 = ctx->grid.nz + 2;
+  int rc;
+  if ((rc = set_geo3(ctx, kx, n0, n1, n2, 0, &ctx->kx, 4))) return rc;
+  if ((rc = set_geo3(ctx, ky, n0, n1, n2, 0, &ctx->ky, 5))) return rc;
+  if ((rc = set_geo3(ctx, kz, n0, n1, n2, 0, &ctx->kz, 6))) return rc;
+  ctx->have_diffusivity = true;
+  ctx->h_sc->have_diffuse = 0;  // Adjust_DT recomputes its diffusion limit
+  A3G_CUDA(cudaMemsetAsync(&ctx->sc->have_diffuse, 0, sizeof(int32_t), ctx->stream));
+  return ensure_cn_buf(ctx);
+}
+
+int a3g_set_fall_velocity(a3g_ctx *ctx, const double *vf_pd) {
+  CTX_CHECK(ctx);
+  if (!vf_pd) return fail(A3G_ERR_ARG, "null vf_pd");
+  const long n0 = ctx->grid.nx + 4, n1 = ctx->grid.ny + 4, n2 = ctx->grid.nz + 4;
+  std::vector<double> v;
+  long si, sj, sk, sg;
+  compress(vf_pd, n0, n1, n2, ctx->grid.ns, v, si, sj, sk, sg);
+  double *d = ctx->geo_ptrs[7];
+  ctx->geo_ptrs[7] = nullptr;
+  if (d) cudaFree(d);
+  int rc = upload_vec(ctx, v, &ctx->geo_ptrs[7]);
+  if (rc) return rc;
+  ctx->vf = Geo4{ctx->geo_ptrs[7], si, sj, sk, sg};
+  ctx->have_vf = true;
+  return A3G_OK;
+}
+
+int a3g_set_aloft(a3g_ctx *ctx, const int32_t *is_aloft) {
+  CTX_CHECK(ctx);
+  if (!is_aloft) return fail(A3G_ERR_ARG, "null IsAloft");
+  int n = 0;
+  for (int g = 0; g < ctx->grid.ns; g++) {
+    ctx->h_aloft[g] = is_aloft[g] ? 1 : 0;
+    n += ctx->h_aloft[g];
+  }
+  ctx->n_gs_aloft = n;
+  A3G_CUDA(cudaMemcpyAsync(ctx->aloft, ctx->h_aloft.data(), sizeof(int32_t) * ctx->grid.ns,
+                           cudaMemcpyHostToDevice, ctx->stream));
+  A3G_CUDA(cudaStreamSynchronize(ctx->stream));
+  return A3G_OK;
+}
+
+int a3g_set_winds(a3g_ctx *ctx, const double *vx_pd, const double *vy_pd, const double *vz_pd) {
+  CTX_CHECK(ctx);
+  if (!vx_pd || !vy_pd || !vz_pd) return fail(A3G_ERR_ARG, "null wind array");
+  const Layout &L = ctx->L;
+  const double *src[3] = {vx_pd, vy_pd, vz_pd};
+  double *dst[3] = {ctx->vx, ctx->vy, ctx->vz};
+  for (int c = 0; c < 3; c++) {
+    int rc = copy_level(ctx, const_cast<double *>(src[c]), dst[c], true, L.nx + 4, L.ny + 4, L.nz + 4, 2,
+                        L.nx, L.ny, L.nz, 1, L.P, L.PY, L.PG);
+    if (rc) return rc;
+  }
+  A3G_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->have_winds = true;
+  return A3G_OK;
+}
+
+int a3g_set_met_steps(a3g_ctx *ctx, const float *vx_last, const float *vy_last, const float *vz_last,
+                      const float *vx_next, const float *vy_next, const float *vz_next) {
+  CTX_CHECK(ctx);
+  const float *src[6] = {vx_last, vy_last, vz_last, vx_next, vy_next, vz_next};
+  for (int c = 0; c < 6; c++)
+    if (!src[c]) return fail(A3G_ERR_ARG, "null met-step array");
+  const long n = (long)ctx->grid.nx * ctx->grid.ny * ctx->grid.nz;
+  if (!ctx->met) {
+    A3G_CUDA(cudaMalloc((void **)&ctx->met, sizeof(float) * 6 * n));
+    ctx->bytes += sizeof(float) * 6 * n;
+    ctx->met_n = n;
+  }
+  for (int c = 0; c < 6; c++)
+    A3G_CUDA(cudaMemcpyAsync(ctx->met + c * n, src[c], sizeof(float) * n, cudaMemcpyHostToDevice,
+                             ctx->stream));
+  return A3G_OK;
+}
+
+int a3g_interp_winds(a3g_ctx *ctx, double interval_frac) {
+  CTX_CHECK(ctx);
+  if (!ctx->met) return fail(A3G_ERR_STATE, "a3g_set_met_steps has not been called");
+  int rc = launch_interp_winds(ctx, interval_frac);
+  if (!rc) ctx->have_winds = true;
+  return rc;
+}
+
+int a3g_upload_concen(a3g_ctx *ctx, const double *concen_level) {
+  CTX_CHECK(ctx);
+  if (!concen_level) return fail(A3G_ERR_ARG, "null concen");
+  const Layout &L = ctx->L;
+  int rc = copy_level(ctx, const_cast<double *>(concen_level), ctx->c0, true, L.nx + 4, L.ny + 4,
+                      L.nz + 4, 2, L.nx, L.ny, L.nz, L.ns, L.P, L.PY, L.PG);
+  if (rc) return rc;
+  A3G_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->ts1_zeroed = false;
+  return A3G_OK;
+}
+
+int a3g_download_concen(a3g_ctx *ctx, double *concen_level) {
+  CTX_CHECK(ctx);
+  if (!concen_level) return fail(A3G_ERR_ARG, "null concen");
+  const Layout &L = ctx->L;
+  A3G_CUDA(cudaStreamSynchronize(ctx->stream));
+  std::memset(concen_level, 0, sizeof(double) * (size_t)(L.nx + 4) * (L.ny + 4) * (L.nz + 4) * L.ns);
+  int rc = copy_level(ctx, concen_level, ctx->c0, false, L.nx + 4, L.ny + 4, L.nz + 4, 2, L.nx, L.ny,
+                      L.nz, L.ns, L.P, L.PY, L.PG);
+  if (rc) return rc;
+  return sync_scalars(ctx);
+}
+
+// outflow arrays: host (-1:a+2,-1:b+2,1:ns) <-> device [g][b][a] interior
+static int copy_outflow(a3g_ctx *ctx, double *host, double *dev, int na, int nb, bool to_device) {
+  if (!host) return A3G_OK;
+  cudaMemcpy3DParms p;
+  std::memset(&p, 0, sizeof(p));
+  cudaPitchedPtr hp = make_cudaPitchedPtr(host, (na + 4) * sizeof(double), (na + 4) * sizeof(double), nb + 4);
+  cudaPitchedPtr dp = make_cudaPitchedPtr(dev, na * sizeof(double), na * sizeof(double), nb);
+  cudaPos hpos = make_cudaPos(2 * sizeof(double), 2, 0);
+  if (to_device) { p.srcPtr = hp; p.srcPos = hpos; p.dstPtr = dp; p.kind = cudaMemcpyHostToDevice; }
+  else { p.srcPtr = dp; p.dstPtr = hp; p.dstPos = hpos; p.kind = cudaMemcpyDeviceToHost; }
+  p.extent = make_cudaExtent(na * sizeof(double), nb, ctx->grid.ns);
+  A3G_CUDA(cudaMemcpy3DAsync(&p, ctx->stream));
+  return A3G_OK;
+}
+
+int a3g_upload_outflow(a3g_ctx *ctx, const double *yz1, const double *yz2, const double *xz1,
+                       const double *xz2, const double *xy1, const double *xy2) {
+  CTX_CHECK(ctx);
+  const int nx = ctx->grid.nx, ny = ctx->grid.ny, nz = ctx->grid.nz;
+  int rc = 0;
+  if (!rc) rc = copy_outflow(ctx, const_cast<double *>(yz1), ctx->out_yz1, ny, nz, true);
+  if (!rc) rc = copy_outflow(ctx, const_cast<double *>(yz2), ctx->out_yz2, ny, nz, true);
+  if (!rc) rc = copy_outflow(ctx, const_cast<double *>(xz1), ctx->out_xz1, nx, nz, true);
+  if (!rc) rc = copy_outflow(ctx, const_cast<double *>(xz2), ctx->out_xz2, nx, nz, true);
+  if (!rc) rc = copy_outflow(ctx, const_cast<double *>(xy1), ctx->out_xy1, nx, ny, true);
+  if (!rc) rc = copy_outflow(ctx, const_cast<double *>(xy2), ctx->out_xy2, nx, ny, true);
+  if (rc) return rc;
+  A3G_CUDA(cudaStreamSynchronize(ctx->stream));
+  return A3G_OK;
+}
+
+int a3g_download_outflow(a3g_ctx *ctx, double *yz1, double *yz2, double *xz1, double *xz2,
+                         double *xy1, double *xy2, double *deposit) {
+  CTX_CHECK(ctx);
+  const int nx = ctx->grid.nx, ny = ctx->grid.ny, nz = ctx->grid.nz;
+  int rc = 0;
+  if (!rc) rc = copy_outflow(ctx, yz1, ctx->out_yz1, ny, nz, false);
+  if (!rc) rc = copy_outflow(ctx, yz2, ctx->out_yz2, ny, nz, false);
+  if (!rc) rc = copy_outflow(ctx, xz1, ctx->out_xz1, nx, nz, false);
+  if (!rc) rc = copy_outflow(ctx, xz2, ctx->out_xz2, nx, nz, false);
+  if (!rc) rc = copy_outflow(ctx, xy1, ctx->out_xy1, nx, ny, false);
+  if (!rc) rc = copy_outflow(ctx, xy2, ctx->out_xy2, nx, ny, false);
+  if (rc) return rc;
+  if (deposit)  // DepositGranularity = outflow_xy1(1:nx,1:ny,:), src/AdvectionVert_DCU.f90:321
+    A3G_CUDA(cudaMemcpyAsync(deposit, ctx->out_xy1, sizeof(double) * nx * ny * ctx->grid.ns,
+                             cudaMemcpyDeviceToHost, ctx->stream));
+  return sync_scalars(ctx);
+}
+
+int a3g_step_prologue(a3g_ctx *ctx) {
+  CTX_CHECK(ctx);
+  // ts0 <- ts1: the state is unchanged unless the last sweep left ts1 zero.
+  if (ctx->ts1_zeroed)
+    A3G_CUDA(cudaMemsetAsync(ctx->c0, 0, sizeof(double) * ctx->L.PG * ctx->L.ns, ctx->stream));
+  ctx->ts1_zeroed = true;  // ts1 <- 0; the next sweep that copies back clears this
+  return A3G_OK;
+}
+
+int a3g_set_dt(a3g_ctx *ctx, double dt) {
+  CTX_CHECK(ctx);
+  ctx->host_dt = dt;
+  A3G_CUDA(cudaMemcpyAsync(&ctx->sc->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  return A3G_OK;
+}
+
+int a3g_add_source_column(a3g_ctx *ctx, int32_t ivent, int32_t jvent, const double *flux, double dt) {
+  CTX_CHECK(ctx);
+  if (!flux) return fail(A3G_ERR_ARG, "null flux");
+  if (ivent < 1 || ivent > ctx->grid.nx || jvent < 1 || jvent > ctx->grid.ny)
+    return fail(A3G_ERR_ARG, "vent outside the grid");
+  A3G_CUDA(cudaEventSynchronize(ctx->src_event));  // previous staging copy done
+  const size_t n = (size_t)(ctx->grid.nz + 1) * ctx->grid.ns;
+  std::memcpy(ctx->h_src, flux, n * sizeof(double));
+  A3G_CUDA(cudaMemcpyAsync(ctx->src_buf, ctx->h_src, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  A3G_CUDA(cudaEventRecord(ctx->src_event, ctx->stream));
+  return launch_source(ctx, ivent, jvent, dt);
+}
+
+int a3g_set_bc(a3g_ctx *ctx, int32_t bc_code) {
+  CTX_CHECK(ctx);
+  if (bc_code != 1 && bc_code != 2) return fail(A3G_ERR_BC_CODE, "ERROR BC code not recognized");
+  ctx->last_bc = bc_code;
+  return A3G_OK;
+}
+
+static int ready(a3g_ctx *ctx) {
+  if (!ctx->have_geometry) return fail(A3G_ERR_STATE, "geometry not set");
+  if (!ctx->have_vf) return fail(A3G_ERR_STATE, "fall velocities not set");
+  if (!ctx->have_winds) return fail(A3G_ERR_STATE, "winds not set");
+  return A3G_OK;
+}
+
+int a3g_advect_x(a3g_ctx *ctx) {
+  CTX_CHECK(ctx);
+  int rc = ready(ctx);
+  if (rc) return rc;
+  rc = launch_advect_x(ctx);
+  if (!rc) ctx->ts1_zeroed = false;
+  return rc;
+}
+
+int a3g_advect_y(a3g_ctx *ctx) {
+  CTX_CHECK(ctx);
+  int rc = ready(ctx);
+  if (rc) return rc;
+  rc = launch_advect_y(ctx);
+  if (!rc) ctx->ts1_zeroed = false;
+  return rc;
+}
+
+int a3g_get_minmax_index(a3g_ctx *ctx, int32_t ivent, int32_t jvent, int32_t kvent, int32_t *box) {
+  CTX_CHECK(ctx);
+  int rc = launch_plane_flags(ctx);
+  if (rc) return rc;
+  const int nx = ctx->grid.nx, ny = ctx->grid.ny, nz = ctx->grid.nz;
+  const int32_t *fi = ctx->h_plane_flags, *fj = fi + nx + 1, *fk = fj + ny + 1;
+  Box b;
+  // "maxval(plane) < CLOUDCON_GRID_THRESH" <=> no cell of the plane reaches it
+  b.imin = 1; b.imax = nx;
+  for (int i = 2; i <= ivent - 1; i++) { if (!fi[i]) b.imin = i; else break; }
+  for (int i = nx; i >= b.imin + 2; i--) { if (!fi[i]) b.imax = i; else break; }
+  if (ctx->grid.periodic && (b.imin == 1 || b.imax == nx)) { b.imin = 1; b.imax = nx; }
+  b.jmin = 1; b.jmax = ny;
+  for (int j = 2; j <= jvent - 1; j++) { if (!fj[j]) b.jmin = j; else break; }
+  for (int j = ny; j >= b.jmin + 2; j--) { if (!fj[j]) b.jmax = j; else break; }
+  b.kmin = 1; b.kmax = nz;
+  for (int k = 2; k <= kvent - 1; k++) { if (!fk[k]) b.kmin = k; else break; }
+  for (int k = nz; k >= b.kmin + 2; k--) { if (!fk[k]) b.kmax = k; else break; }
+  if (b.kmax < b.kmin) return fail(A3G_ERR_SUBGRID, "ERROR: kmax<kmin in get_minmax_index");
+  if (b.imax - b.imin < 2) { b.imax = (b.imax + 1 < nx) ? b.imax + 1 : nx; b.imin = b.imax - 2; }
+  if (b.jmax - b.jmin < 2) { b.jmax = (b.jmax + 1 < ny) ? b.jmax + 1 : ny; b.jmin = b.jmax - 2; }
+  if (b.kmax - b.kmin < 2) { b.kmax = (b.kmax + 1 < nz) ? b.kmax + 1 : nz; b.kmin = b.kmax - 2; }
+  ctx->box = b;
+  if (box) { box[0] = b.imin; box[1] = b.imax; box[2] = b.jmin; box[3] = b.jmax; box[4] = b.kmin; box[5] = b.kmax; }
+  return A3G_OK;
+}
+
+int a3g_set_subgrid(a3g_ctx *ctx, const int32_t *box) {
+  CTX_CHECK(ctx);
+  if (!box) return fail(A3G_ERR_ARG, "null box");
+  Box b{box[0], box[1], box[2], box[3], box[4], box[5]};
+  if (b.imin < 1 || b.imax > ctx->grid.nx || b.jmin < 1 || b.jmax > ctx->grid.ny || b.kmin < 1 ||
+      b.kmax > ctx->grid.nz || b.imin > b.imax || b.jmin > b.jmax || b.kmin > b.kmax)
+    return fail(A3G_ERR_ARG, "box outside the grid or empty");
+  ctx->box = b;
+  return A3G_OK;
+}
+
+int a3g_get_subgrid(a3g_ctx *ctx, int32_t *box) {
+  if (!ctx || !box) return fail(A3G_ERR_ARG, "null argument");
+  const Box &b = ctx->box;
+  box[0] = b.imin; box[1] = b.imax; box[2] = b.jmin; box[3] = b.jmax; box[4] = b.kmin; box[5] = b.kmax;
+  return A3G_OK;
+}
+
+int a3g_advect_horz(a3g_ctx *ctx, int32_t itoggle, int32_t ivent, int32_t jvent, int32_t kvent) {
+  CTX_CHECK(ctx);
+  int rc = ready(ctx);
+  if (rc) return rc;
+  if (ctx->prm.fast_subgrid) {
+    if ((rc = a3g_get_minmax_index(ctx, ivent, jvent, kvent, nullptr))) return rc;
+  } else {
+    full_box(ctx);
+  }
+  if (itoggle % 2 == 0) {
+    if ((rc = launch_advect_y(ctx))) return rc;
+    if ((rc = launch_advect_x(ctx))) return rc;
+  } else {
+    if ((rc = launch_advect_x(ctx))) return rc;
+    if ((rc = launch_advect_y(ctx))) return rc;
+  }
+  ctx->ts1_zeroed = false;
+  return A3G_OK;
+}
+
+int a3g_advect_vert(a3g_ctx *ctx) {
+  CTX_CHECK(ctx);
+  int rc = ready(ctx);
+  if (rc) return rc;
+  rc = launch_advect_z(ctx);
+  if (!rc) ctx->ts1_zeroed = false;
+  return rc;
+}
+
+int a3g_diffuse_horz(a3g_ctx *ctx, int32_t itime) {
+  CTX_CHECK(ctx);
+  if (!ctx->have_geometry || !ctx->have_diffusivity) return fail(A3G_ERR_STATE, "geometry/diffusivity not set");
+  Box &b = ctx->box;
+  if (ctx->prm.fast_subgrid) {  // src/Diffusion.F90:168-176
+    b.imin = b.imin - 1 > 1 ? b.imin - 1 : 1;
+    b.imax = b.imax + 1 < ctx->grid.nx ? b.imax + 1 : ctx->grid.nx;
+    b.jmin = b.jmin - 1 > 1 ? b.jmin - 1 : 1;
+    b.jmax = b.jmax + 1 < ctx->grid.ny ? b.jmax + 1 : ctx->grid.ny;
+    b.kmin = b.kmin - 1 > 1 ? b.kmin - 1 : 1;
+    b.kmax = b.kmax + 1 < ctx->grid.nz ? b.kmax + 1 : ctx->grid.nz;
+  } else {
+    full_box(ctx);
+  }
+  int rc;
+  if (ctx->prm.use_cn) {
+    if (itime % 2 == 0) {
+      if ((rc = launch_diffcn_x(ctx))) return rc;
+      if ((rc = launch_diffcn_y(ctx))) return rc;
+    } else {
+      if ((rc = launch_diffcn_y(ctx))) return rc;
+      if ((rc = launch_diffcn_x(ctx))) return rc;
+    }
+  } else {
+    if (itime % 2 == 0) {
+      if ((rc = launch_diff_x(ctx))) return rc;
+      if ((rc = launch_diff_y(ctx))) return rc;
+    } else {
+      if ((rc = launch_diff_y(ctx))) return rc;
+      if ((rc = launch_diff_x(ctx))) return rc;
+    }
+    ctx->ts1_zeroed = false;
+  }
+  return A3G_OK;
+}
+
+int a3g_diffuse_vert(a3g_ctx *ctx) {
+  CTX_CHECK(ctx);
+  if (!ctx->have_geometry || !ctx->have_diffusivity) return fail(A3G_ERR_STATE, "geometry/diffusivity not set");
+  int rc;
+  if (ctx->prm.use_cn) {
+    rc = launch_diffcn_z(ctx);
+  } else {
+    rc = launch_diff_z(ctx);
+    if (!rc) ctx->ts1_zeroed = false;
+  }
+  return rc;
+}
+
+int a3g_adjust_dt(a3g_ctx *ctx, double time, double next_write_time, double simtime, double *dt_out) {
+  CTX_CHECK(ctx);
+  if (!ctx->have_geometry || !ctx->have_vf || !ctx->have_winds)
+    return fail(A3G_ERR_STATE, "geometry, fall velocities and winds must be set");
+  if (ctx->prm.use_diffusion && !ctx->have_diffusivity) return fail(A3G_ERR_STATE, "diffusivity not set");
+  int rc = launch_cfl(ctx, time, next_write_time, simtime);
+  if (rc) return rc;
+  if ((rc = sync_scalars(ctx))) return rc;
+  ctx->host_dt = ctx->h_sc->dt;
+  if (dt_out) *dt_out = ctx->h_sc->dt;
+  return A3G_OK;
+}
+
+int a3g_cfl_maxima(a3g_ctx *ctx, double *vmax3) {
+  CTX_CHECK(ctx);
+  if (!vmax3) return fail(A3G_ERR_ARG, "null vmax3");
+  if (!ctx->have_geometry || !ctx->have_vf || !ctx->have_winds)
+    return fail(A3G_ERR_STATE, "geometry, fall velocities and winds must be set");
+  int rc = launch_cfl_maxima(ctx);
+  if (rc) return rc;
+  if ((rc = sync_scalars(ctx))) return rc;
+  for (int q = 0; q < 3; q++) vmax3[q] = ctx->h_sc->vmax[q];
+  return A3G_OK;
+}
+
+int a3g_adjust_dt_from_maxima(a3g_ctx *ctx, const double *vmax3, int32_t n_gs_aloft_total,
+                              double time, double next_write_time, double simtime, double *dt_out) {
+  CTX_CHECK(ctx);
+  if (!vmax3) return fail(A3G_ERR_ARG, "null vmax3");
+  if (ctx->prm.use_diffusion && !ctx->have_diffusivity) return fail(A3G_ERR_STATE, "diffusivity not set");
+  double v[4] = {vmax3[0], vmax3[1], vmax3[2], 0.0};
+  A3G_CUDA(cudaMemcpyAsync(ctx->sc->vmax, v, sizeof(v), cudaMemcpyHostToDevice, ctx->stream));
+  int rc = launch_dt_from_maxima(ctx, n_gs_aloft_total, time, next_write_time, simtime);
+  if (rc) return rc;
+  if ((rc = sync_scalars(ctx))) return rc;
+  ctx->host_dt = ctx->h_sc->dt;
+  if (dt_out) *dt_out = ctx->h_sc->dt;
+  return A3G_OK;
+}
+
+int a3g_timestep_totals(a3g_ctx *ctx, double *out4, double *mass_aloft) {
+  CTX_CHECK(ctx);
+  if (!out4) return fail(A3G_ERR_ARG, "null out4");
+  if (!ctx->have_geometry) return fail(A3G_ERR_STATE, "geometry not set");
+  int rc = launch_totals(ctx, out4, mass_aloft);
+  if (rc) return rc;
+  return sync_scalars(ctx);
+}
+
+int a3g_step(a3g_ctx *ctx, int32_t itime, int32_t ivent, int32_t jvent, int32_t kvent, const double *flux) {
+  CTX_CHECK(ctx);
+  int rc;
+  if ((rc = a3g_step_prologue(ctx))) return rc;
+  if (flux && (rc = a3g_add_source_column(ctx, ivent, jvent, flux, ctx->host_dt))) return rc;
+  if ((rc = a3g_set_bc(ctx, 1))) return rc;
+  if ((rc = a3g_advect_horz(ctx, itime, ivent, jvent, kvent))) return rc;
+  if ((rc = a3g_advect_vert(ctx))) return rc;
+  if (ctx->prm.use_diffusion) {
+    if ((rc = a3g_set_bc(ctx, 2))) return rc;
+    if ((rc = a3g_diffuse_horz(ctx, itime))) return rc;
+    if ((rc = a3g_diffuse_vert(ctx))) return rc;
+  }
+  return A3G_OK;
+}
+
+int a3g_get_stream(a3g_ctx *ctx, void **stream) {
+  if (!ctx || !stream) return fail(A3G_ERR_ARG, "null argument");
+  *stream = (void *)ctx->stream;
+  return A3G_OK;
+}
+
+int a3g_kernel_timing(a3g_ctx *ctx, int32_t enable) {
+  CTX_CHECK(ctx);
+  ctx->timing = enable != 0;
+  ctx->ev_kind.clear();
+  ctx->ev_used = 0;
+  return A3G_OK;
+}
+
+int a3g_kernel_times(a3g_ctx *ctx, double *ms, uint64_t *count) {
+  CTX_CHECK(ctx);
+  if (!ms || !count) return fail(A3G_ERR_ARG, "null argument");
+  A3G_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (int k = 0; k < A3G_K_COUNT; k++) { ms[k] = 0.0; count[k] = 0; }
+  const size_t pairs = ctx->ev_used / 2;
+  for (size_t p = 0; p < pairs && p < ctx->ev_kind.size(); p++) {
+    float t = 0.0f;
+    A3G_CUDA(cudaEventElapsedTime(&t, ctx->ev_pool[2 * p], ctx->ev_pool[2 * p + 1]));
+    const int k = ctx->ev_kind[p];
+    ms[k] += t;
+    count[k] += 1;
+  }
+  return A3G_OK;
+}
+
+int a3g_kernel_launches(a3g_ctx *ctx, uint64_t *count) {
+  if (!ctx || !count) return fail(A3G_ERR_ARG, "null argument");
+  *count = ctx->launches;
+  return A3G_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,189 @@
+// a3g_internal.cuh -- device data layout, context and shared helpers of the
+// B200 transport library.
+//
+// Device layout (chosen for the sweeps, not copied from the host):
+//   * concentration: interior cells only, [grain][k][j][i] with the x-row
+//     padded to a pitch P (a multiple of 4 doubles, 32-byte aligned rows).
+//     Ghost cells are never stored: every sweep generates the ghost values
+//     Set_BC would have written (zero / edge copy / periodic wrap) when it
+//     loads a row, which is exact because no ghost value survives from one
+//     operator to the next in the reference (each operator re-runs Set_BC or
+//     its own Neumann fill first).
+//   * two levels c0/c1 ping-pong; a sweep reads c0 and writes every interior
+//     cell of c1 (zeros outside the active box and for grains not aloft,
+//     which is the zero-then-copy-back of the reference), then they swap.
+//   * winds vx/vy/vz: interior only, same pitch.
+//   * geometry and diffusivity: stored with ghosts but compressed by
+//     broadcast strides (a stride of 0 means "does not vary along that
+//     index"), so a projected grid keeps one value per k and a lon/lat grid
+//     one per (j,k).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/ash3d_b200.h"
+
+namespace a3g {
+
+// Geometry/diffusivity array with broadcast strides.  Element at Fortran
+// indices (i,j,k) is p[(i-o)*si + (j-o)*sj + (k-o)*sk], o = lower bound
+// (-1 for the ghosted mesh arrays, 0 for kx/ky/kz).
+struct Geo3 {
+  const double *p;
+  long si, sj, sk;
+  int o;
+  __host__ __device__ __forceinline__ double at(int i, int j, int k) const {
+    return p[(long)(i - o) * si + (long)(j - o) * sj + (long)(k - o) * sk];
+  }
+};
+
+// vf_pd with broadcast strides; grain index 0-based.
+struct Geo4 {
+  const double *p;
+  long si, sj, sk, sg;
+  __host__ __device__ __forceinline__ double at(int i, int j, int k, int g) const {
+    return p[(long)(i + 1) * si + (long)(j + 1) * sj + (long)(k + 1) * sk + (long)g * sg];
+  }
+};
+
+// Interior layout of the concentration / wind arrays on the device.
+struct Layout {
+  int nx, ny, nz, ns;
+  long P, PY, PG;  // row pitch, plane stride, grain stride (elements)
+  __host__ __device__ __forceinline__ long cell(int i, int j, int k) const {  // 1-based
+    return (long)(k - 1) * PY + (long)(j - 1) * P + (long)(i - 1);
+  }
+  __host__ __device__ __forceinline__ long at(int i, int j, int k, int g) const {
+    return (long)g * PG + cell(i, j, k);
+  }
+};
+
+struct Box {
+  int imin, imax, jmin, jmax, kmin, kmax;
+};
+
+// Per-step device scalars (read by kernels so that a step can be replayed).
+struct DevScalars {
+  double dt;              // time_data::dt
+  double vmax[4];         // CFL maxima as bit patterns (atomicMax on uint64)
+  double time_diffuse;    // cached diffusion limit
+  int32_t have_diffuse;   // time_diffuse valid
+  int32_t err;            // device error word (A3G_ERR_*), first error wins
+  int32_t err_info;       // where it happened
+  int32_t flags_pad;
+};
+
+}  // namespace a3g
+
+struct a3g_ctx {
+  a3g_grid_desc grid;
+  a3g_params prm;
+  int device;
+  cudaStream_t stream;
+  a3g::Layout L;
+
+  double *c0, *c1;          // concentration levels (state = c0)
+  double *vx, *vy, *vz;     // winds (km/h)
+  float *met;               // 6 FP32 met arrays: vx_last,vy_last,vz_last,vx_next,vy_next,vz_next
+  long met_n;               // nx*ny*nz
+  double *geo_ptrs[8];      // compressed kappa,snx,sny,snz,kx,ky,kz,vf
+  a3g::Geo3 kappa, snx, sny, snz, kx, ky, kz;
+  a3g::Geo4 vf;
+  double *dz_vec;           // (-1:nz+2) on device
+  std::vector<double> h_dz; // host copy
+  // outflow accumulators, interior only: yz (ns,nz,ny), xz (ns,nz,nx), xy (ns,ny,nx)
+  double *out_yz1, *out_yz2, *out_xz1, *out_xz2, *out_xy1, *out_xy2;
+  int32_t *aloft;           // IsAloft on device
+  std::vector<int32_t> h_aloft;
+  int n_gs_aloft;
+  a3g::DevScalars *sc;      // device scalars
+  a3g::DevScalars *h_sc;    // pinned host mirror
+  double *red_buf;          // reduction partials
+  size_t red_len;
+  int32_t *plane_flags;     // subgrid plane occupancy (nx+ny+nz+3)
+  int32_t *h_plane_flags;   // pinned
+  double *src_buf;          // device source column (nz+1)*ns
+  double *h_src;            // pinned staging
+  cudaEvent_t src_event;    // guards reuse of h_src
+  double *h_tot;            // pinned totals staging
+  // CN line coefficient scratch
+  double *cn_buf;
+  size_t cn_len;
+
+  a3g::Box box;
+  int last_bc;
+  bool have_geometry, have_diffusivity, have_vf, have_winds;
+  bool ts1_zeroed;          // the last sweep left ts1 zero without copy-back
+  double host_dt;
+  uint64_t launches;
+  size_t bytes;
+  // optional per-kernel timing (a3g_kernel_timing)
+  bool timing;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<int> ev_kind;   // kind of each recorded (start, stop) pair
+  size_t ev_used;             // events consumed from the pool
+};
+
+namespace a3g {
+
+// error plumbing (thread-local message)
+void set_error(const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+
+#define A3G_CUDA(call)                                 \
+  do {                                                 \
+    cudaError_t e__ = (call);                          \
+    if (e__ != cudaSuccess) return a3g::cuda_fail(e__, #call); \
+  } while (0)
+
+#define A3G_LAUNCH_CHECK(ctx)                                        \
+  do {                                                               \
+    (ctx)->launches++;                                               \
+    cudaError_t e__ = cudaGetLastError();                            \
+    if (e__ != cudaSuccess) return a3g::cuda_fail(e__, "kernel launch"); \
+  } while (0)
+
+// launchers (kernels live in k_*.cu)
+int launch_advect_x(a3g_ctx *ctx);
+int launch_advect_y(a3g_ctx *ctx);
+int launch_advect_z(a3g_ctx *ctx);
+int launch_diff_x(a3g_ctx *ctx);
+int launch_diff_y(a3g_ctx *ctx);
+int launch_diff_z(a3g_ctx *ctx);
+int launch_diffcn_x(a3g_ctx *ctx);
+int launch_diffcn_y(a3g_ctx *ctx);
+int launch_diffcn_z(a3g_ctx *ctx);
+int launch_cfl(a3g_ctx *ctx, double time, double next_write_time, double simtime);
+int launch_cfl_maxima(a3g_ctx *ctx);
+int launch_dt_from_maxima(a3g_ctx *ctx, int n_gs_aloft, double time, double next_write_time,
+                          double simtime);
+int launch_totals(a3g_ctx *ctx, double *out4, double *mass_aloft);
+int launch_plane_flags(a3g_ctx *ctx);
+int launch_interp_winds(a3g_ctx *ctx, double frac);
+int launch_source(a3g_ctx *ctx, int ivent, int jvent, double dt);
+int launch_zero_state(a3g_ctx *ctx);
+int check_device_error(a3g_ctx *ctx);
+// per-kernel timing brackets (no-ops unless a3g_kernel_timing(ctx,1))
+void tbegin(a3g_ctx *ctx, int kind);
+void tend(a3g_ctx *ctx);
+
+inline void swap_levels(a3g_ctx *ctx) {
+  double *t = ctx->c0;
+  ctx->c0 = ctx->c1;
+  ctx->c1 = t;
+}
+
+// Fortran MAX/MIN for reals (no NaNs reach these in the transport path).
+__device__ __forceinline__ double fmx(double a, double b) { return a > b ? a : b; }
+__device__ __forceinline__ double fmn(double a, double b) { return a < b ? a : b; }
+
+__device__ __forceinline__ void raise_error(DevScalars *sc, int code, int info) {
+  if (atomicCAS(&sc->err, 0, code) == 0) sc->err_info = info;
+}
+
+}  // namespace a3g

@@ -1,0 +1,454 @@
+// k_reduce.cu -- reductions and small per-step kernels.
+//
+//  * CFL maxima and the dt arithmetic of Adjust_DT (src/Adjust_dt.f90:136-332):
+//    maxima are exact and order independent, so the result is bit-identical
+//    to the CPU loop; they are combined with atomicMax on the IEEE bit
+//    patterns (valid for non-negative doubles; NaNs are skipped as the
+//    reference's `if (tmp.gt.max)` skips them).
+//  * mass totals (src/Output_Vars.f90:1255-1459): per-grain sums of c*kappa
+//    accumulated in double-double (TwoSum) and combined in a fixed order, so
+//    the result is deterministic and within a few ulp of the exact sum.
+//  * subgrid plane occupancy for get_minmax_index (src/Calc_Mesh.f90:432-542).
+//  * met-step interpolation (src/MesoInterpolater.f90:207-223) and the vent
+//    column source insertion (src/Ash3d.F90:428-431).
+#include "a3g_internal.cuh"
+
+namespace a3g {
+
+__device__ __forceinline__ void atomic_max_pos(double *addr, double v) {
+  if (!(v == v)) return;  // NaN: ignored like the reference's comparisons
+  atomicMax(reinterpret_cast<unsigned long long *>(addr),
+            (unsigned long long)__double_as_longlong(v));
+}
+__device__ __forceinline__ void atomic_min_pos(double *addr, double v) {
+  if (!(v == v)) return;
+  atomicMin(reinterpret_cast<unsigned long long *>(addr),
+            (unsigned long long)__double_as_longlong(v));
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmx(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_min(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmn(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// One thread per interior cell (grid-stride).  vmax[0]: |vx| (projected) or
+// max |vx|*minsig/kappa (lon/lat); vmax[1] the same for y; vmax[2] the
+// vertical (|vz| + max_g |vf|)/dz_k.  src/Adjust_dt.f90:136-173.
+__global__ void __launch_bounds__(256) k_cfl(Layout L, int latlon, const double *__restrict__ vx,
+                                             const double *__restrict__ vy,
+                                             const double *__restrict__ vz, Geo4 vf, Geo3 snx,
+                                             Geo3 sny, Geo3 kap, const double *__restrict__ dz_vec,
+                                             DevScalars *sc) {
+  const long ncell = (long)L.nx * L.ny * L.nz;
+  double m0 = 0.0, m1 = 0.0, m2 = 0.0;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < ncell; t += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % L.nx) + 1;
+    const long r = t / L.nx;
+    const int j = (int)(r % L.ny) + 1;
+    const int k = (int)(r / L.ny) + 1;
+    const long c = L.cell(i, j, k);
+    const double ax = fabs(vx[c]), ay = fabs(vy[c]);
+    double t1, t2;
+    if (latlon) {
+      const double kp = kap.at(i, j, k);
+      t1 = ax * fmn(snx.at(i, j, k), snx.at(i + 1, j, k)) / kp;
+      t2 = ay * fmn(sny.at(i, j, k), sny.at(i, j + 1, k)) / kp;
+    } else {
+      t1 = ax;
+      t2 = ay;
+    }
+    double vfm = 0.0;
+    for (int g = 0; g < L.ns; g++) {
+      const double a = fabs(vf.at(i, j, k, g));
+      if (g == 0 || a > vfm) vfm = a;
+    }
+    const double t3 = (fabs(vz[c]) + vfm) / dz_vec[k + 1];
+    if (t1 > m0) m0 = t1;
+    if (t2 > m1) m1 = t2;
+    if (t3 > m2) m2 = t3;
+  }
+  m0 = warp_max(m0);
+  m1 = warp_max(m1);
+  m2 = warp_max(m2);
+  if ((threadIdx.x & 31) == 0) {
+    atomic_max_pos(&sc->vmax[0], m0);
+    atomic_max_pos(&sc->vmax[1], m1);
+    atomic_max_pos(&sc->vmax[2], m2);
+  }
+}
+
+// Diffusion time limit, src/Adjust_dt.f90:191-235 (min over cells of
+// sum_d (kappa/minsig_d)^2 / k_d, starting from DT_MAX).
+__global__ void __launch_bounds__(256) k_diff_limit(Layout L, Geo3 snx, Geo3 sny, Geo3 snz,
+                                                    Geo3 kap, Geo3 kx, Geo3 ky, Geo3 kz,
+                                                    DevScalars *sc) {
+  const long ncell = (long)L.nx * L.ny * L.nz;
+  double m = 1.0e300;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < ncell; t += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % L.nx) + 1;
+    const long r = t / L.nx;
+    const int j = (int)(r % L.ny) + 1;
+    const int k = (int)(r / L.ny) + 1;
+    const double kp = kap.at(i, j, k);
+    const double r1 = kp / fmn(snx.at(i, j, k), snx.at(i + 1, j, k));
+    const double t1 = (r1 * r1) / kx.at(i, j, k);
+    const double r2 = kp / fmn(sny.at(i, j, k), sny.at(i, j + 1, k));
+    const double t2 = (r2 * r2) / ky.at(i, j, k);
+    const double r3 = kp / fmn(snz.at(i, j, k), snz.at(i, j, k + 1));
+    const double t3 = (r3 * r3) / kz.at(i, j, k);
+    const double t4 = t1 + t2 + t3;
+    if (t4 < m) m = t4;
+  }
+  m = warp_min(m);
+  if ((threadIdx.x & 31) == 0) atomic_min_pos(&sc->time_diffuse, m);
+}
+
+// dt arithmetic, src/Adjust_dt.f90:176-179 and :288-332.
+__global__ void k_dt_finalize(int latlon, int use_diffusion, int use_cn, int n_gs_aloft, double dx,
+                              double dy, double cfl, double dt_min, double dt_max, double imp_dt_fac,
+                              double eps_small, double time, double next_write_time,
+                              double simtime, int diff_fresh, DevScalars *sc) {
+  double vx_dx = sc->vmax[0], vy_dy = sc->vmax[1], vz_dz = sc->vmax[2];
+  if (!latlon) {
+    vx_dx = vx_dx / dx;
+    vy_dy = vy_dy / dy;
+  }
+  if (n_gs_aloft == 0) vz_dz = 0.0;
+  const double time_advect = 1.0 / fmx(fmx(vx_dx, vy_dy), vz_dz);
+  double td;
+  if (use_diffusion) {
+    if (diff_fresh) {
+      td = sc->time_diffuse;  // min(DT_MAX, min_cells tmp4)
+      td = use_cn ? td * imp_dt_fac : td * 0.5;
+      sc->time_diffuse = td;
+      sc->have_diffuse = 1;
+    } else {
+      td = sc->time_diffuse;
+    }
+  } else {
+    td = dt_max;
+  }
+  const double dt_tmp = fmn(time_advect, td);
+  double dt;
+  if (dt_tmp < dt_min) dt = dt_min;
+  else if (dt_tmp > dt_max) dt = dt_max;
+  else dt = fmn(1.0, cfl) * dt_tmp;
+  const long long fac = (long long)(dt / dt_min);
+  dt = dt_min * (double)fac;
+  if ((next_write_time - time) > eps_small && (next_write_time - time) < dt) dt = next_write_time - time;
+  if (time + dt > simtime) dt = simtime - time;
+  sc->dt = dt;
+}
+
+int launch_cfl_maxima(a3g_ctx *ctx) {
+  const Layout &L = ctx->L;
+  A3G_CUDA(cudaMemsetAsync(ctx->sc->vmax, 0, sizeof(ctx->sc->vmax), ctx->stream));
+  const long ncell = (long)L.nx * L.ny * L.nz;
+  int blocks = (int)((ncell + 255) / 256);
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  tbegin(ctx, A3G_K_CFL);
+  k_cfl<<<blocks, 256, 0, ctx->stream>>>(L, ctx->grid.latlon, ctx->vx, ctx->vy, ctx->vz, ctx->vf,
+                                         ctx->snx, ctx->sny, ctx->kappa, ctx->dz_vec, ctx->sc);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  return A3G_OK;
+}
+
+// dt from maxima already in sc->vmax (local, or set from an all-reduce).
+int launch_dt_from_maxima(a3g_ctx *ctx, int n_gs_aloft, double time, double next_write_time,
+                          double simtime) {
+  const Layout &L = ctx->L;
+  const long ncell = (long)L.nx * L.ny * L.nz;
+  int blocks = (int)((ncell + 255) / 256);
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  int fresh = 0;
+  if (ctx->prm.use_diffusion && !ctx->h_sc->have_diffuse) {
+    const double init = ctx->prm.dt_max;
+    A3G_CUDA(cudaMemcpyAsync(&ctx->sc->time_diffuse, &init, sizeof(double), cudaMemcpyHostToDevice,
+                             ctx->stream));
+    tbegin(ctx, A3G_K_CFL);
+    k_diff_limit<<<blocks, 256, 0, ctx->stream>>>(L, ctx->snx, ctx->sny, ctx->snz, ctx->kappa,
+                                                  ctx->kx, ctx->ky, ctx->kz, ctx->sc);
+    tend(ctx);
+    A3G_LAUNCH_CHECK(ctx);
+    fresh = 1;
+    ctx->h_sc->have_diffuse = 1;
+  }
+  tbegin(ctx, A3G_K_OTHER);
+  k_dt_finalize<<<1, 1, 0, ctx->stream>>>(
+      ctx->grid.latlon, ctx->prm.use_diffusion, ctx->prm.use_cn, n_gs_aloft, ctx->grid.dx,
+      ctx->grid.dy, ctx->prm.cfl, ctx->prm.dt_min, ctx->prm.dt_max, ctx->prm.imp_dt_fac,
+      ctx->prm.eps_small, time, next_write_time, simtime, fresh, ctx->sc);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  return A3G_OK;
+}
+
+int launch_cfl(a3g_ctx *ctx, double time, double next_write_time, double simtime) {
+  const Layout &L = ctx->L;
+  A3G_CUDA(cudaMemsetAsync(ctx->sc->vmax, 0, sizeof(ctx->sc->vmax), ctx->stream));
+  const long ncell = (long)L.nx * L.ny * L.nz;
+  int blocks = (int)((ncell + 255) / 256);
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  tbegin(ctx, A3G_K_CFL);
+  k_cfl<<<blocks, 256, 0, ctx->stream>>>(L, ctx->grid.latlon, ctx->vx, ctx->vy, ctx->vz, ctx->vf,
+                                         ctx->snx, ctx->sny, ctx->kappa, ctx->dz_vec, ctx->sc);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  int fresh = 0;
+  if (ctx->prm.use_diffusion && !ctx->h_sc->have_diffuse) {
+    const double init = ctx->prm.dt_max;
+    A3G_CUDA(cudaMemcpyAsync(&ctx->sc->time_diffuse, &init, sizeof(double), cudaMemcpyHostToDevice,
+                             ctx->stream));
+    tbegin(ctx, A3G_K_CFL);
+    k_diff_limit<<<blocks, 256, 0, ctx->stream>>>(L, ctx->snx, ctx->sny, ctx->snz, ctx->kappa,
+                                                  ctx->kx, ctx->ky, ctx->kz, ctx->sc);
+    tend(ctx);
+    A3G_LAUNCH_CHECK(ctx);
+    fresh = 1;
+    ctx->h_sc->have_diffuse = 1;  // host mirror; the device flag is set by finalize
+  }
+  tbegin(ctx, A3G_K_OTHER);
+  k_dt_finalize<<<1, 1, 0, ctx->stream>>>(
+      ctx->grid.latlon, ctx->prm.use_diffusion, ctx->prm.use_cn, ctx->n_gs_aloft, ctx->grid.dx,
+      ctx->grid.dy, ctx->prm.cfl, ctx->prm.dt_min, ctx->prm.dt_max, ctx->prm.imp_dt_fac,
+      ctx->prm.eps_small, time, next_write_time, simtime, fresh, ctx->sc);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  return A3G_OK;
+}
+
+// ---------------------------------------------------------------------------
+// mass totals
+// ---------------------------------------------------------------------------
+struct DD {
+  double hi, lo;
+};
+__device__ __forceinline__ DD dd_add(DD a, double b) {  // TwoSum accumulate
+  const double s = a.hi + b;
+  const double bb = s - a.hi;
+  const double err = (a.hi - (s - bb)) + (b - bb);
+  DD r;
+  r.hi = s;
+  r.lo = a.lo + err;
+  return r;
+}
+__device__ __forceinline__ DD dd_add(DD a, DD b) {
+  DD r = dd_add(a, b.hi);
+  r.lo = r.lo + b.lo;
+  return r;
+}
+__device__ __forceinline__ DD dd_shfl(DD v, int o) {
+  DD r;
+  r.hi = __shfl_xor_sync(0xffffffffu, v.hi, o);
+  r.lo = __shfl_xor_sync(0xffffffffu, v.lo, o);
+  return r;
+}
+
+// Jobs: 0 aloft (c*kappa over the interior), 1 deposit (xy1*kappa(:,:,0)),
+// 2 yz1*kappa(0,:,:), 3 yz2*kappa(nx+1,:,:), 4 xz1*kappa(:,0,:),
+// 5 xz2*kappa(:,ny+1,:), 6 xy2*kappa(:,:,nz+1).
+constexpr int NJOBS = 7;
+constexpr int TOT_BLOCKS = 296;
+
+__global__ void __launch_bounds__(256) k_totals(Layout L, const double *__restrict__ c,
+                                                Geo3 kap, const double *__restrict__ yz1,
+                                                const double *__restrict__ yz2,
+                                                const double *__restrict__ xz1,
+                                                const double *__restrict__ xz2,
+                                                const double *__restrict__ xy1,
+                                                const double *__restrict__ xy2,
+                                                double *__restrict__ part) {
+  const int job = blockIdx.y, g = blockIdx.z;
+  __shared__ double sh[2][8];
+  DD acc = {0.0, 0.0};
+  long n;
+  switch (job) {
+    case 0: n = (long)L.nx * L.ny * L.nz; break;
+    case 1: case 6: n = (long)L.nx * L.ny; break;
+    case 2: case 3: n = (long)L.ny * L.nz; break;
+    default: n = (long)L.nx * L.nz; break;
+  }
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    double v;
+    if (job == 0) {
+      const int i = (int)(t % L.nx) + 1;
+      const long r = t / L.nx;
+      const int j = (int)(r % L.ny) + 1;
+      const int k = (int)(r / L.ny) + 1;
+      v = c[(long)g * L.PG + L.cell(i, j, k)] * kap.at(i, j, k);
+    } else if (job == 1 || job == 6) {
+      const int i = (int)(t % L.nx) + 1, j = (int)(t / L.nx) + 1;
+      const double *a = (job == 1) ? xy1 : xy2;
+      v = a[(long)g * L.nx * L.ny + t] * kap.at(i, j, job == 1 ? 0 : L.nz + 1);
+    } else if (job == 2 || job == 3) {
+      const int j = (int)(t % L.ny) + 1, k = (int)(t / L.ny) + 1;
+      const double *a = (job == 2) ? yz1 : yz2;
+      v = a[(long)g * L.ny * L.nz + t] * kap.at(job == 2 ? 0 : L.nx + 1, j, k);
+    } else {
+      const int i = (int)(t % L.nx) + 1, k = (int)(t / L.nx) + 1;
+      const double *a = (job == 4) ? xz1 : xz2;
+      v = a[(long)g * L.nx * L.nz + t] * kap.at(i, job == 4 ? 0 : L.ny + 1, k);
+    }
+    acc = dd_add(acc, v);
+  }
+  for (int o = 16; o > 0; o >>= 1) acc = dd_add(acc, dd_shfl(acc, o));
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) { sh[0][w] = acc.hi; sh[1][w] = acc.lo; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    DD s = {0.0, 0.0};
+    for (int q = 0; q < (int)(blockDim.x >> 5); q++) s = dd_add(s, DD{sh[0][q], sh[1][q]});
+    const long o = (((long)g * NJOBS + job) * gridDim.x + blockIdx.x) * 2;
+    part[o] = s.hi;
+    part[o + 1] = s.lo;
+  }
+}
+
+__global__ void k_totals_final(int ns, int nblk, const double *__restrict__ part,
+                               double *__restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;  // (g, job)
+  if (t >= ns * NJOBS) return;
+  DD s = {0.0, 0.0};
+  for (int b = 0; b < nblk; b++) {
+    const long o = ((long)t * nblk + b) * 2;
+    s = dd_add(s, DD{part[o], part[o + 1]});
+  }
+  out[t] = s.hi + s.lo;  // out[g*NJOBS + job]
+}
+
+int launch_totals(a3g_ctx *ctx, double *out4, double *mass_aloft) {
+  const Layout &L = ctx->L;
+  const int ns = L.ns;
+  dim3 grid(TOT_BLOCKS, NJOBS, ns);
+  tbegin(ctx, A3G_K_TOTALS);
+  k_totals<<<grid, 256, 0, ctx->stream>>>(L, ctx->c0, ctx->kappa, ctx->out_yz1, ctx->out_yz2,
+                                          ctx->out_xz1, ctx->out_xz2, ctx->out_xy1, ctx->out_xy2,
+                                          ctx->red_buf);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  double *fin = ctx->red_buf + (size_t)2 * TOT_BLOCKS * NJOBS * ns;
+  tbegin(ctx, A3G_K_TOTALS);
+  k_totals_final<<<(ns * NJOBS + 127) / 128, 128, 0, ctx->stream>>>(ns, TOT_BLOCKS, ctx->red_buf, fin);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  A3G_CUDA(cudaMemcpyAsync(ctx->h_tot, fin, sizeof(double) * ns * NJOBS, cudaMemcpyDeviceToHost,
+                           ctx->stream));
+  A3G_CUDA(cudaStreamSynchronize(ctx->stream));
+  // volumes in the reference's order, src/Output_Vars.f90:1285-1290,1395-1401,1440-1456
+  const double rho = ctx->prm.magma_density, km3 = 1.0e9;
+  double aloft = 0.0, depv = 0.0, outv = 0.0;
+  for (int g = 0; g < ns; g++) {
+    const double *r = ctx->h_tot + (size_t)g * NJOBS;
+    if (mass_aloft) mass_aloft[g] = r[0];
+    aloft = aloft + r[0] / rho / km3;
+  }
+  for (int g = 0; g < ns; g++) depv = depv + ctx->h_tot[(size_t)g * NJOBS + 1] / rho / km3;
+  for (int g = 0; g < ns; g++) {
+    const double *r = ctx->h_tot + (size_t)g * NJOBS;
+    outv = outv + (r[2] + r[3] + r[4] + r[5] + r[6]) / rho / km3;
+  }
+  out4[0] = aloft;
+  out4[1] = depv;
+  out4[2] = outv;
+  out4[3] = aloft + depv + outv;
+  return A3G_OK;
+}
+
+// ---------------------------------------------------------------------------
+// subgrid plane occupancy: flags[i] (i=1..nx), flags[nx+1+j], flags[nx+ny+2+k]
+// set when some grain has c >= thresh in that plane.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_plane_flags(Layout L, const double *__restrict__ c,
+                                                     double thresh, int32_t *__restrict__ flags) {
+  const long ncell = (long)L.nx * L.ny * L.nz;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < ncell; t += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % L.nx) + 1;
+    const long r = t / L.nx;
+    const int j = (int)(r % L.ny) + 1;
+    const int k = (int)(r / L.ny) + 1;
+    const long cell = L.cell(i, j, k);
+    bool hit = false;
+    for (int g = 0; g < L.ns && !hit; g++) hit = c[(long)g * L.PG + cell] >= thresh;
+    if (hit) {
+      if (!flags[i]) flags[i] = 1;
+      if (!flags[L.nx + 1 + j]) flags[L.nx + 1 + j] = 1;
+      if (!flags[L.nx + L.ny + 2 + k]) flags[L.nx + L.ny + 2 + k] = 1;
+    }
+  }
+}
+
+int launch_plane_flags(a3g_ctx *ctx) {
+  const Layout &L = ctx->L;
+  const size_t nf = (size_t)L.nx + L.ny + L.nz + 3;
+  A3G_CUDA(cudaMemsetAsync(ctx->plane_flags, 0, nf * sizeof(int32_t), ctx->stream));
+  const long ncell = (long)L.nx * L.ny * L.nz;
+  int blocks = (int)((ncell + 255) / 256);
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  tbegin(ctx, A3G_K_OTHER);
+  k_plane_flags<<<blocks, 256, 0, ctx->stream>>>(L, ctx->c0, ctx->prm.cloudcon_grid_thresh,
+                                                 ctx->plane_flags);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  A3G_CUDA(cudaMemcpyAsync(ctx->h_plane_flags, ctx->plane_flags, nf * sizeof(int32_t),
+                           cudaMemcpyDeviceToHost, ctx->stream));
+  A3G_CUDA(cudaStreamSynchronize(ctx->stream));
+  return A3G_OK;
+}
+
+// ---------------------------------------------------------------------------
+// winds and source
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_interp_winds(Layout L, const float *__restrict__ met,
+                                                      long n, double frac, double *__restrict__ vx,
+                                                      double *__restrict__ vy,
+                                                      double *__restrict__ vz) {
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % L.nx) + 1;
+    const long r = t / L.nx;
+    const int j = (int)(r % L.ny) + 1;
+    const int k = (int)(r / L.ny) + 1;
+    const long c = L.cell(i, j, k);
+    const float dx = met[3 * n + t] - met[t];
+    const float dy = met[4 * n + t] - met[n + t];
+    const float dz = met[5 * n + t] - met[2 * n + t];
+    vx[c] = ((double)met[t] + (double)dx * frac) * 3.6;
+    vy[c] = ((double)met[n + t] + (double)dy * frac) * 3.6;
+    vz[c] = ((double)met[2 * n + t] + (double)dz * frac) * 3.6;
+  }
+}
+
+int launch_interp_winds(a3g_ctx *ctx, double frac) {
+  const long n = ctx->met_n;
+  int blocks = (int)((n + 255) / 256);
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  tbegin(ctx, A3G_K_WINDS);
+  k_interp_winds<<<blocks, 256, 0, ctx->stream>>>(ctx->L, ctx->met, n, frac, ctx->vx, ctx->vy, ctx->vz);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  return A3G_OK;
+}
+
+__global__ void k_source(Layout L, int ivent, int jvent, const double *__restrict__ flux, double dt,
+                         double *__restrict__ c) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;  // (k-1) + nz*g
+  if (t >= L.nz * L.ns) return;
+  const int k = t % L.nz + 1, g = t / L.nz;
+  const long a = (long)g * L.PG + L.cell(ivent, jvent, k);
+  c[a] = c[a] + dt * flux[(long)(k - 1) + (long)(L.nz + 1) * g];
+}
+
+int launch_source(a3g_ctx *ctx, int ivent, int jvent, double dt) {
+  const int n = ctx->L.nz * ctx->L.ns;
+  tbegin(ctx, A3G_K_OTHER);
+  k_source<<<(n + 127) / 128, 128, 0, ctx->stream>>>(ctx->L, ivent, jvent, ctx->src_buf, dt, ctx->c0);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  return A3G_OK;
+}
+
+}  // namespace a3g

@@ -1,0 +1,142 @@
+"""The time loop of src/Ash3d.F90:372-642, restricted to the transport path.
+
+``run`` drives any model object that exposes the reference routine names
+(``Ash3dGPU`` here; the oracle in the test suite offers the same names), in
+the reference's order:
+
+  prologue (ts0 <- ts1, :376-378) -> MesoInterpolater (FP32 met steps,
+  device interpolation, :396) -> Adjust_DT -> CheckEruptivePulses + source
+  insertion (:407-434) -> Set_BC(1) -> AdvectHorz(itime) -> AdvectVert ->
+  [Set_BC(2) -> DiffuseHorz(itime) -> DiffuseVert] -> time += dt ->
+  TimeStepTotals (every log step, :568-595) -> stop tests (:597-641).
+
+Met steps are hourly; the next pair is uploaded when the simulation clock
+crosses an hour, as Read_NextMesoStep does (src/MesoInterpolater.f90:169-197).
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+from . import synthetic as syn
+
+
+@dataclasses.dataclass
+class StepRecord:
+    itime: int
+    time: float
+    dt: float
+    aloft: float
+    dep: float
+    outflow: float
+    tot: float
+    source_cum: float
+
+
+@dataclasses.dataclass
+class RunState:
+    cfg: syn.Config
+    time: float = 0.0
+    itime: int = 0
+    hour: int = -1
+    source_cum: float = 0.0
+    norm_col: np.ndarray = None
+    kappa: np.ndarray = None
+    met: syn.MetSource = None
+    history: list = dataclasses.field(default_factory=list)
+
+
+def new_state(cfg: syn.Config, geo: dict | None = None) -> RunState:
+    geo = geo if geo is not None else syn.geometry(cfg)
+    return RunState(cfg=cfg, norm_col=syn.suzuki_column(cfg), kappa=geo["kappa"],
+                    met=syn.MetSource(cfg))
+
+
+class Comm:
+    """The two reductions a grain-sharded run needs (torch.distributed
+    all-reduces of a few doubles): MAX of the CFL maxima, SUM of the totals."""
+
+    def __init__(self, group=None, device=None):
+        import torch
+        import torch.distributed as dist
+        self.torch, self.dist, self.group, self.device = torch, dist, group, device
+
+    def _reduce(self, a: np.ndarray, op) -> np.ndarray:
+        t = self.torch.tensor(np.asarray(a, dtype=np.float64), device=self.device)
+        self.dist.all_reduce(t, op=op, group=self.group)
+        return t.cpu().numpy()
+
+    def max(self, a):
+        return self._reduce(a, self.dist.ReduceOp.MAX)
+
+    def sum(self, a):
+        return self._reduce(a, self.dist.ReduceOp.SUM)
+
+
+def shard_config(cfg: syn.Config, rank: int, world: int) -> syn.Config:
+    """Grain sharding: the global run has ns*world grain bins (fall speeds
+    log-spaced over the global range, equal mass fractions); rank r keeps bins
+    [r*ns, (r+1)*ns).  Every operator acts on grains independently, so only
+    dt (a MAX over all grains' settling speeds) and the totals couple ranks."""
+    if world == 1:
+        return cfg
+    ns = cfg.ns
+    lo, hi = min(cfg.fall_mps), max(cfg.fall_mps)
+    fall = np.logspace(math.log10(lo), math.log10(hi), ns * world)
+    c = dataclasses.replace(cfg)
+    c.fall_mps = tuple(float(v) for v in fall[rank * ns:(rank + 1) * ns])
+    c.bin_mass = tuple(1.0 / (ns * world) for _ in range(ns))
+    return c
+
+
+def step(model, st: RunState, simtime: float | None = None, totals: bool = True,
+         comm: Comm | None = None, n_gs_aloft_total: int | None = None) -> StepRecord:
+    """Advances the model by one reference time step."""
+    cfg = st.cfg
+    simtime = cfg.sim_hours if simtime is None else simtime
+    st.itime += 1
+    model.step_prologue()
+    h = int(math.floor(st.time))
+    if h != st.hour:
+        model.set_met_steps(st.met.step(h), st.met.step(h + 1))
+        st.hour = h
+    model.interp_winds(st.time - h)
+    if comm is None:
+        dt = model.Adjust_DT(st.time, simtime, simtime)
+    else:
+        vmax = comm.max(model.cfl_maxima())
+        dt = model.adjust_dt_from_maxima(vmax, n_gs_aloft_total, st.time, simtime, simtime)
+    frac = syn.pulse_fraction(cfg, st.time, dt)
+    if frac > 0.0:
+        flux = syn.source_flux(cfg, st.norm_col, st.kappa, frac)
+        model.add_source(flux, dt)
+        st.source_cum = st.source_cum + syn.source_vol_inc(cfg, flux, st.kappa, dt)
+    model.Set_BC(1)
+    model.AdvectHorz(st.itime)
+    model.AdvectVert()
+    if cfg.use_diffusion:
+        model.Set_BC(2)
+        model.DiffuseHorz(st.itime)
+        model.DiffuseVert()
+    st.time = st.time + dt
+    rec = StepRecord(st.itime, st.time, dt, 0.0, 0.0, 0.0, 0.0, st.source_cum)
+    if totals:
+        vols, _ = model.TimeStepTotals()
+        if comm is not None:
+            vols = comm.sum(vols)
+            rec.source_cum = float(comm.sum(np.array([st.source_cum]))[0])
+        rec.aloft, rec.dep, rec.outflow, rec.tot = (float(v) for v in vols)
+    st.history.append(rec)
+    return rec
+
+
+def run(model, cfg: syn.Config, max_steps: int | None = None, sim_hours: float | None = None,
+        geo: dict | None = None, totals: bool = True) -> RunState:
+    """Runs until sim_hours (or max_steps) like the reference's stop test 2."""
+    st = new_state(cfg, geo)
+    simtime = cfg.sim_hours if sim_hours is None else sim_hours
+    while st.time < simtime and (max_steps is None or st.itime < max_steps):
+        step(model, st, simtime, totals)
+    return st

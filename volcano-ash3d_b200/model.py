@@ -1,0 +1,210 @@
+"""Host-side mirror of the reference's per-step routines over the C-ABI.
+
+``Ash3dGPU`` keeps the names, argument meaning and error behaviour of the
+Fortran subroutines that Ash3d.F90's main loop calls (src/Ash3d.F90:372-642):
+``Set_BC(bc_code)``, ``AdvectHorz(itoggle)``, ``AdvectVert()``,
+``DiffuseHorz(i)``, ``DiffuseVert()``, ``Adjust_DT(...)`` and
+``TimeStepTotals()``.  All work runs on the GPU through
+``libash3d_b200.so``; a failing call raises ``A3GError`` (the reference's
+``stop 1``).  Arrays crossing the boundary use the reference's Fortran
+layouts (numpy order='F' with ghost cells).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from . import synthetic as syn
+from ._lib import check, dptr, fptr, iptr
+
+
+class Ash3dGPU:
+    def __init__(self, cfg: syn.Config, device: int = 0, geo: dict | None = None,
+                 limiter: str | None = None, use_winds_fp64: bool = False):
+        self.lib = lib = _lib.load()
+        self.cfg = cfg
+        g = _lib.GridDesc()
+        g.nx, g.ny, g.nz, g.ns = cfg.nx, cfg.ny, cfg.nz, cfg.ns
+        g.periodic, g.latlon = int(cfg.periodic), int(cfg.latlon)
+        g.dx, g.dy = syn.projected_dxdy(cfg)
+        p = _lib.Params()
+        lib.a3g_default_params(C.byref(p))
+        p.limiter = _lib.LIMITERS[limiter or cfg.limiter]
+        p.use_cn = int(cfg.use_cn)
+        p.use_diffusion = int(cfg.use_diffusion)
+        p.fast_subgrid = int(cfg.fast_subgrid)
+        p.cfl = cfg.cfl
+        p.magma_density = cfg.magma_density
+        self.ctx = C.c_void_p()
+        check(lib.a3g_create(C.byref(g), C.byref(p), device, C.byref(self.ctx)))
+        geo = geo if geo is not None else syn.geometry(cfg)
+        self.geo = geo
+        check(lib.a3g_set_geometry(self.ctx, dptr(geo["kappa"]), dptr(geo["sig_nx"]),
+                                   dptr(geo["sig_ny"]), dptr(geo["sig_nz"]), dptr(geo["dz_vec"])))
+        kx, ky, kz = syn.diffusivity(cfg)
+        check(lib.a3g_set_diffusivity(self.ctx, dptr(kx), dptr(ky), dptr(kz)))
+        self._vf = syn.fall_velocity(cfg)
+        check(lib.a3g_set_fall_velocity(self.ctx, dptr(self._vf)))
+        self._dt = 0.0
+
+    # --- lifetime ----------------------------------------------------------
+    def close(self):
+        if self.ctx:
+            self.lib.a3g_destroy(self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync(self):
+        check(self.lib.a3g_sync(self.ctx))
+
+    def stream_handle(self) -> int:
+        """cudaStream_t of this context (for torch.cuda.ExternalStream)."""
+        s = C.c_void_p()
+        check(self.lib.a3g_get_stream(self.ctx, C.byref(s)))
+        return s.value or 0
+
+    def kernel_timing(self, enable: bool):
+        check(self.lib.a3g_kernel_timing(self.ctx, 1 if enable else 0))
+
+    def kernel_times(self) -> dict:
+        """{class: (total_ms, launches)} since kernel_timing(True)."""
+        n = len(_lib.KERNEL_CLASSES)
+        ms = np.zeros(n)
+        cnt = (C.c_uint64 * n)()
+        check(self.lib.a3g_kernel_times(self.ctx, dptr(ms), cnt))
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(_lib.KERNEL_CLASSES)}
+
+    def kernel_launches(self) -> int:
+        n = C.c_uint64()
+        check(self.lib.a3g_kernel_launches(self.ctx, C.byref(n)))
+        return n.value
+
+    # --- routines with the reference names -----------------------------------
+    def Set_BC(self, bc_code: int):
+        check(self.lib.a3g_set_bc(self.ctx, bc_code))
+
+    def AdvectHorz(self, itoggle: int):
+        c = self.cfg
+        check(self.lib.a3g_advect_horz(self.ctx, itoggle, c.ivent, c.jvent, 1))
+
+    def advect_x(self):
+        check(self.lib.a3g_advect_x(self.ctx))
+
+    def advect_y(self):
+        check(self.lib.a3g_advect_y(self.ctx))
+
+    def AdvectVert(self):
+        check(self.lib.a3g_advect_vert(self.ctx))
+
+    def DiffuseHorz(self, i: int):
+        check(self.lib.a3g_diffuse_horz(self.ctx, i))
+
+    def DiffuseVert(self):
+        check(self.lib.a3g_diffuse_vert(self.ctx))
+
+    def Adjust_DT(self, time: float, next_write_time: float, simtime: float) -> float:
+        out = C.c_double()
+        check(self.lib.a3g_adjust_dt(self.ctx, time, next_write_time, simtime, C.byref(out)))
+        self._dt = out.value
+        return out.value
+
+    def cfl_maxima(self) -> np.ndarray:
+        v = np.zeros(3)
+        check(self.lib.a3g_cfl_maxima(self.ctx, dptr(v)))
+        return v
+
+    def adjust_dt_from_maxima(self, vmax3, n_gs_aloft_total: int, time: float,
+                              next_write_time: float, simtime: float) -> float:
+        v = np.ascontiguousarray(vmax3, dtype=np.float64)
+        out = C.c_double()
+        check(self.lib.a3g_adjust_dt_from_maxima(self.ctx, dptr(v), n_gs_aloft_total, time,
+                                                 next_write_time, simtime, C.byref(out)))
+        self._dt = out.value
+        return out.value
+
+    def set_dt(self, dt: float):
+        self._dt = dt
+        check(self.lib.a3g_set_dt(self.ctx, dt))
+
+    def TimeStepTotals(self):
+        out = np.zeros(4)
+        mass = np.zeros(self.cfg.ns)
+        check(self.lib.a3g_timestep_totals(self.ctx, dptr(out), dptr(mass)))
+        return out, mass
+
+    def get_minmax_index(self):
+        c = self.cfg
+        box = np.zeros(6, dtype=np.int32)
+        check(self.lib.a3g_get_minmax_index(self.ctx, c.ivent, c.jvent, 1, iptr(box)))
+        return tuple(int(v) for v in box)
+
+    def set_subgrid(self, box):
+        b = np.asarray(box, dtype=np.int32)
+        check(self.lib.a3g_set_subgrid(self.ctx, iptr(b)))
+
+    def step_prologue(self):
+        check(self.lib.a3g_step_prologue(self.ctx))
+
+    def add_source(self, flux: np.ndarray, dt: float):
+        f = np.asfortranarray(flux, dtype=np.float64)
+        check(self.lib.a3g_add_source_column(self.ctx, self.cfg.ivent, self.cfg.jvent, dptr(f), dt))
+
+    def set_met_steps(self, last, nxt):
+        arrs = [np.asfortranarray(a, dtype=np.float32) for a in (*last, *nxt)]
+        check(self.lib.a3g_set_met_steps(self.ctx, *[fptr(a) for a in arrs]))
+        self._met_keep = arrs  # the copies are asynchronous
+
+    def interp_winds(self, frac: float):
+        check(self.lib.a3g_interp_winds(self.ctx, frac))
+
+    def set_winds(self, vx, vy, vz):
+        a = [np.asfortranarray(v, dtype=np.float64) for v in (vx, vy, vz)]
+        check(self.lib.a3g_set_winds(self.ctx, *[dptr(v) for v in a]))
+
+    def set_aloft(self, flags):
+        f = np.asarray(flags, dtype=np.int32)
+        check(self.lib.a3g_set_aloft(self.ctx, iptr(f)))
+
+    # --- state access --------------------------------------------------------
+    def upload_level(self, level: np.ndarray):
+        lv = np.asfortranarray(level, dtype=np.float64)
+        check(self.lib.a3g_upload_concen(self.ctx, dptr(lv)))
+
+    def download_level(self) -> np.ndarray:
+        c = self.cfg
+        lv = np.zeros((c.nx + 4, c.ny + 4, c.nz + 4, c.ns), order="F")
+        check(self.lib.a3g_download_concen(self.ctx, dptr(lv)))
+        return lv
+
+    def interior(self) -> np.ndarray:
+        c = self.cfg
+        return self.download_level()[2:c.nx + 2, 2:c.ny + 2, 2:c.nz + 2, :].copy(order="F")
+
+    def set_interior(self, q: np.ndarray):
+        c = self.cfg
+        lv = np.zeros((c.nx + 4, c.ny + 4, c.nz + 4, c.ns), order="F")
+        lv[2:c.nx + 2, 2:c.ny + 2, 2:c.nz + 2, :] = q
+        self.upload_level(lv)
+
+    def outflows(self) -> dict:
+        c = self.cfg
+        NX, NY, NZ, ns = c.nx + 4, c.ny + 4, c.nz + 4, c.ns
+        z = lambda *s: np.zeros(s, order="F")
+        yz1, yz2, xz1, xz2, xy1, xy2 = z(NY, NZ, ns), z(NY, NZ, ns), z(NX, NZ, ns), z(NX, NZ, ns), z(NX, NY, ns), z(NX, NY, ns)
+        dep = z(c.nx, c.ny, ns)
+        check(self.lib.a3g_download_outflow(self.ctx, dptr(yz1), dptr(yz2), dptr(xz1), dptr(xz2),
+                                            dptr(xy1), dptr(xy2), dptr(dep)))
+        return dict(yz1=yz1[2:c.ny + 2, 2:c.nz + 2, :], yz2=yz2[2:c.ny + 2, 2:c.nz + 2, :],
+                    xz1=xz1[2:c.nx + 2, 2:c.nz + 2, :], xz2=xz2[2:c.nx + 2, 2:c.nz + 2, :],
+                    xy1=xy1[2:c.nx + 2, 2:c.ny + 2, :], xy2=xy2[2:c.nx + 2, 2:c.ny + 2, :], deposit=dep)
+
+    @property
+    def dt(self):
+        return self._dt

@@ -1,0 +1,361 @@
+"""Host-side set-up for the transport path: grids, geometry, winds and source.
+
+These are the pieces the reference computes on the host before and around
+the per-step path (they are inputs of the path, not part of it):
+
+* ``geometry``: cell volumes and face areas of ``calc_mesh_params``
+  (src/Calc_Mesh.f90:23-220) for projected and spherical lon/lat grids, in the
+  Fortran layouts with two ghost cells.
+* ``suzuki_column`` / ``source_flux``: the normalised Suzuki column
+  (src/Source.f90:287-490), the pulse fraction of CheckEruptivePulses
+  (:613-685) and SourceNodeFlux of TephraSourceNodes (:708-783).
+* synthetic FP32 met steps for the named workloads (no met data is read:
+  MetReader is not part of this path).  Every random draw is seeded.
+
+Workloads (interior cells x grains):
+  C1  projected 100x100x40, 4 grains, explicit diffusion, steady winds
+  C2  lon/lat 720x360x60 at 0.25 deg, 10 grains, Crank-Nicolson, hourly winds
+  C4  projected 200x200x50, 6 grains, explicit diffusion
+  C5  projected 1500x1000x80, 20 grains, Crank-Nicolson
+  plus small cases (``tiny_*``) used by the parity tests.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+DEG2RAD = 1.7453292519943295e-2
+PI = 3.141592653589793
+RAD_EARTH = 6371.229
+MPS_2_KMPHR = 3.6
+M2PS_2_KM2PHR = 3.6e-3
+KM3_2_M3 = 1.0e9
+
+
+@dataclasses.dataclass
+class Config:
+    name: str
+    nx: int
+    ny: int
+    nz: int
+    ns: int
+    latlon: bool = False
+    periodic: bool = False
+    dx: float = 5.0          # km (projected)
+    dy: float = 5.0
+    de: float = 0.25         # deg (lon/lat)
+    dn: float = 0.25
+    lonLL: float = 0.0
+    latLL: float = 0.0
+    xLL: float = 0.0
+    yLL: float = 0.0
+    dz: float = 0.5          # km
+    ivent: int = 1
+    jvent: int = 1
+    z_volcano: float = 0.0   # vent elevation (km)
+    fall_mps: tuple = (0.1,)
+    bin_mass: tuple = (1.0,)
+    plume_km: float = 15.0
+    volume_km3: float = 1.0e-2
+    duration_h: float = 3.0
+    suzuki_a: float = 4.0
+    diffusivity_m2s: float = 500.0
+    use_cn: bool = False
+    use_diffusion: bool = True
+    limiter: str = "superbee"
+    cfl: float = 0.8
+    sim_hours: float = 6.0
+    winds: str = "c1"        # 'c1' steady shear, 'c2' jet + wave + noise, 'random'
+    seed: int = 1
+    fast_subgrid: bool = False
+    magma_density: float = 2500.0
+
+    @property
+    def cells(self) -> int:
+        return self.nx * self.ny * self.nz
+
+    @property
+    def cell_grains(self) -> int:
+        return self.nx * self.ny * self.nz * self.ns
+
+
+def _logspace(a, b, n):
+    return tuple(float(x) for x in np.logspace(math.log10(a), math.log10(b), n))
+
+
+def make_config(name: str) -> Config:
+    """The workloads named in the benchmark definition, plus small test cases."""
+    if name == "C1":
+        return Config("C1", 100, 100, 40, 4, dx=5.0, dy=5.0, dz=0.5, ivent=50, jvent=50,
+                      fall_mps=(0.01, 0.1, 0.5, 2.0), bin_mass=(0.25,) * 4, plume_km=15.0,
+                      volume_km3=1.0e-2, duration_h=3.0, diffusivity_m2s=500.0, use_cn=False,
+                      sim_hours=6.0, winds="c1", seed=1)
+    if name == "C2":
+        return Config("C2", 720, 360, 60, 10, latlon=True, de=0.25, dn=0.25, lonLL=0.0, latLL=0.0,
+                      dz=0.5, ivent=360, jvent=180, fall_mps=_logspace(1e-3, 3.0, 10),
+                      bin_mass=(0.1,) * 10, plume_km=15.0, volume_km3=1.0e-2, duration_h=3.0,
+                      diffusivity_m2s=500.0, use_cn=True, sim_hours=24.0, winds="c2", seed=2)
+    if name == "C4":
+        return Config("C4", 200, 200, 50, 6, dx=5.0, dy=5.0, dz=0.5, ivent=100, jvent=100,
+                      fall_mps=_logspace(1e-2, 2.0, 6), bin_mass=(1.0 / 6,) * 6, plume_km=15.0,
+                      volume_km3=1.0e-2, duration_h=3.0, diffusivity_m2s=500.0, use_cn=False,
+                      sim_hours=24.0, winds="c1", seed=4)
+    if name == "C5":
+        return Config("C5", 1500, 1000, 80, 20, dx=3.0, dy=3.0, dz=0.4, ivent=750, jvent=500,
+                      fall_mps=_logspace(1e-3, 3.0, 20), bin_mass=(0.05,) * 20, plume_km=25.0,
+                      volume_km3=1.0e-1, duration_h=12.0, diffusivity_m2s=500.0, use_cn=True,
+                      sim_hours=48.0, winds="c2p", seed=5)
+    if name == "tiny_proj":
+        return Config("tiny_proj", 24, 20, 12, 3, dx=5.0, dy=5.0, dz=0.5, ivent=12, jvent=10,
+                      fall_mps=(0.05, 0.5, 2.0), bin_mass=(0.3, 0.3, 0.4), plume_km=5.0,
+                      volume_km3=1.0e-3, duration_h=1.0, use_cn=False, sim_hours=2.0,
+                      winds="random", seed=11)
+    if name == "tiny_cn":
+        return Config("tiny_cn", 22, 18, 14, 2, dx=4.0, dy=6.0, dz=0.5, ivent=10, jvent=9,
+                      fall_mps=(0.2, 1.0), bin_mass=(0.5, 0.5), plume_km=6.0, volume_km3=1.0e-3,
+                      duration_h=1.0, use_cn=True, sim_hours=2.0, winds="random", seed=12)
+    if name == "tiny_latlon":
+        return Config("tiny_latlon", 30, 16, 10, 2, latlon=True, de=1.0, dn=1.0, lonLL=10.0,
+                      latLL=30.0, dz=0.5, ivent=15, jvent=8, fall_mps=(0.3, 1.5),
+                      bin_mass=(0.5, 0.5), plume_km=4.0, volume_km3=1.0e-3, duration_h=1.0,
+                      use_cn=True, sim_hours=2.0, winds="random", seed=13)
+    if name == "tiny_periodic":
+        return Config("tiny_periodic", 36, 12, 8, 2, latlon=True, periodic=True, de=10.0, dn=5.0,
+                      lonLL=0.0, latLL=20.0, dz=0.5, ivent=3, jvent=6, fall_mps=(0.3, 1.5),
+                      bin_mass=(0.5, 0.5), plume_km=3.0, volume_km3=1.0e-3, duration_h=1.0,
+                      use_cn=False, sim_hours=2.0, winds="random", seed=14)
+    if name == "tiny_subgrid":
+        return Config("tiny_subgrid", 40, 36, 16, 2, dx=5.0, dy=5.0, dz=0.5, ivent=20, jvent=18,
+                      fall_mps=(0.1, 1.0), bin_mass=(0.5, 0.5), plume_km=5.0, volume_km3=1.0e-3,
+                      duration_h=1.0, use_cn=True, sim_hours=2.0, winds="random", seed=15,
+                      fast_subgrid=True)
+    raise KeyError(name)
+
+
+# ---------------------------------------------------------------------------
+# vertical grid and geometry, src/Calc_Mesh.f90:66-168
+# ---------------------------------------------------------------------------
+def zgrid(cfg: Config):
+    nz = cfg.nz
+    z_vec_init = np.array([cfg.dz * k for k in range(nz + 1)], dtype=np.float64)  # Input_Data.f90:1579
+    dz = np.zeros(nz + 4)          # index k+1 for k=-1..nz+2
+    zcc = np.zeros(nz + 4)
+    zlb = np.zeros(nz + 4)
+    for k in range(1, nz + 1):
+        dz[k + 1] = z_vec_init[k] - z_vec_init[k - 1]
+        zcc[k + 1] = z_vec_init[k] - 0.5 * dz[k + 1]
+        zlb[k + 1] = zcc[k + 1] - 0.5 * dz[k + 1]
+    zcc[1] = zcc[2] - dz[2]
+    zlb[1] = zcc[1] - dz[2]
+    zcc[0] = zcc[1] - dz[2]
+    zlb[0] = zcc[0] - dz[2]
+    zcc[nz + 2] = zcc[nz + 1] + dz[nz + 1]
+    zcc[nz + 3] = zcc[nz + 1] + dz[nz + 1] * 2.0
+    zlb[nz + 2] = zlb[nz + 1] + dz[nz + 1]
+    zlb[nz + 3] = zlb[nz + 1] + dz[nz + 1] * 2.0
+    dz[0] = dz[2]
+    dz[1] = dz[2]
+    dz[nz + 2] = dz[nz + 1]
+    dz[nz + 3] = dz[nz + 1]
+    return dz, zcc, zlb
+
+
+def geometry(cfg: Config) -> dict:
+    """kappa_pd, sigma_n{x,y,z}_pd (-1:nx+2,-1:ny+2,-1:nz+2) and dz_vec_pd (-1:nz+2)."""
+    NX, NY, NZ = cfg.nx + 4, cfg.ny + 4, cfg.nz + 4
+    dz, zcc, zlb = zgrid(cfg)
+    shp = (NX, NY, NZ)
+    kap = np.zeros(shp, order="F")
+    snx = np.zeros(shp, order="F")
+    sny = np.zeros(shp, order="F")
+    snz = np.zeros(shp, order="F")
+    if not cfg.latlon:
+        dx, dy = cfg.dx, cfg.dy
+        snz[:, :, :] = dy * dx
+        for kk in range(NZ):
+            snx[:, :, kk] = dz[kk] * dy
+            sny[:, :, kk] = dz[kk] * dx
+            kap[:, :, kk] = dx * dy * dz[kk]
+    else:
+        de, dn = cfg.de, cfg.dn
+        lat_cc = np.array([cfg.latLL + dn * float(j) - dn * 0.5 for j in range(-1, cfg.ny + 3)])
+        for kk in range(NZ):
+            r_1 = RAD_EARTH + zcc[kk] - 0.5 * dz[kk]
+            r_2 = RAD_EARTH + zcc[kk] + 0.5 * dz[kk]
+            rr_1 = r_1 * r_1
+            drr = r_2 * r_2 - r_1 * r_1
+            drrr = r_2 * r_2 * r_2 - r_1 * r_1 * r_1
+            for jj in range(NY):
+                phi_1 = DEG2RAD * (lat_cc[jj] - 0.5 * dn)
+                phi_2 = DEG2RAD * (lat_cc[jj] + 0.5 * dn)
+                theta_1 = 0.5 * PI - phi_1
+                theta_2 = 0.5 * PI - phi_2
+                del_theta = dn * DEG2RAD
+                del_costheta = math.cos(theta_2) - math.cos(theta_1)
+                del_lam = de * DEG2RAD
+                snx[:, jj, kk] = 0.5 * del_theta * drr
+                sny[:, jj, kk] = 0.5 * math.sin(theta_1) * del_lam * drr
+                snz[:, jj, kk] = rr_1 * del_lam * del_costheta
+                kap[:, jj, kk] = del_lam * drrr * del_costheta / 3.0
+    return dict(kappa=kap, sig_nx=snx, sig_ny=sny, sig_nz=snz, dz_vec=dz, z_cc=zcc, z_lb=zlb)
+
+
+def projected_dxdy(cfg: Config):
+    """dx, dy used by Adjust_DT on projected grids (lon/lat: Calc_Mesh.f90:143-149)."""
+    if not cfg.latlon:
+        return cfg.dx, cfg.dy
+    lat_top = cfg.latLL + cfg.dn * (cfg.ny + 1) - cfg.dn * 0.5
+    phi_bot = DEG2RAD * (cfg.latLL + cfg.dn * 1 - cfg.dn * 0.5 - cfg.dn * 0.5)
+    phi_top = DEG2RAD * (lat_top + cfg.dn * 0.5)
+    phi = max(abs(phi_bot), abs(phi_top))
+    return RAD_EARTH * cfg.de * DEG2RAD * math.cos(phi), RAD_EARTH * cfg.dn * DEG2RAD
+
+
+def diffusivity(cfg: Config):
+    """kx, ky, kz (0:nx+1,0:ny+1,0:nz+1) in km^2/h (Input_Data.f90:1799-1818)."""
+    k = cfg.diffusivity_m2s * M2PS_2_KM2PHR
+    shp = (cfg.nx + 2, cfg.ny + 2, cfg.nz + 2)
+    return (np.full(shp, k, order="F"), np.full(shp, k, order="F"), np.full(shp, k, order="F"))
+
+
+def fall_velocity(cfg: Config) -> np.ndarray:
+    """vf_pd(-1:nx+2,-1:ny+2,-1:nz+2,1:ns) = -v_s*3.6 (MesoInterpolater.f90:571-572)."""
+    vf = np.zeros((cfg.nx + 4, cfg.ny + 4, cfg.nz + 4, cfg.ns), order="F")
+    for g in range(cfg.ns):
+        vf[:, :, :, g] = (-1.0 * cfg.fall_mps[g]) * MPS_2_KMPHR
+    return vf
+
+
+# ---------------------------------------------------------------------------
+# synthetic met steps (FP32, m/s, interior nx*ny*nz, i fastest)
+# ---------------------------------------------------------------------------
+class MetSource:
+    """Deterministic generator of hourly FP32 met steps for a workload."""
+
+    def __init__(self, cfg: Config):
+        self.cfg = cfg
+        dz, zcc, _ = zgrid(cfg)
+        self.z = zcc[2:cfg.nz + 2]  # km at cell centres
+        if cfg.latlon:
+            self.lon = np.array([cfg.lonLL + cfg.de * (i + 1) - cfg.de * 0.5 for i in range(cfg.nx)])
+            self.lat = np.array([cfg.latLL + cfg.dn * (j + 1) - cfg.dn * 0.5 for j in range(cfg.ny)])
+        else:
+            self.lon = np.linspace(0.0, 180.0, cfg.nx)
+            self.lat = np.linspace(0.0, 90.0, cfg.ny)
+        self.steady = cfg.winds == "c1"
+
+    def step(self, hour: int):
+        """(vx, vy, vz) FP32 arrays of shape (nx, ny, nz), Fortran order."""
+        cfg = self.cfg
+        nx, ny, nz = cfg.nx, cfg.ny, cfg.nz
+        z = self.z[None, None, :]
+        if cfg.winds == "c1":
+            u = np.broadcast_to(10.0 + 0.5 * z, (nx, ny, nz))
+            v = np.full((nx, ny, nz), 2.0)
+            w = np.zeros((nx, ny, nz))
+        elif cfg.winds in ("c2", "c2p"):
+            lat = self.lat[None, :, None]
+            lon = self.lon[:, None, None]
+            ztop = 30.0
+            u = 40.0 * np.exp(-((lat - 45.0) / 10.0) ** 2) * np.sin(math.pi * z / ztop)
+            v = 5.0 * np.sin(2.0 * lon * DEG2RAD) * math.cos(2.0 * math.pi * hour / 24.0)
+            u = np.broadcast_to(u, (nx, ny, nz))
+            v = np.broadcast_to(v, (nx, ny, nz))
+            rng = np.random.default_rng(cfg.seed * 100003 + hour)
+            # 5% multiplicative noise, drawn in FP32 to keep generation cheap
+            u = u * (1.0 + 0.05 * rng.standard_normal((nx, ny, nz), dtype=np.float32))
+            v = v * (1.0 + 0.05 * rng.standard_normal((nx, ny, nz), dtype=np.float32))
+            w = np.zeros((nx, ny, nz))
+        else:  # 'random': smooth random field for small parity cases
+            rng = np.random.default_rng(cfg.seed * 7919 + hour)
+            x = np.linspace(0, 2 * math.pi, nx)[:, None, None]
+            y = np.linspace(0, 2 * math.pi, ny)[None, :, None]
+            zz = np.linspace(0, 1, nz)[None, None, :]
+            a = rng.uniform(-1, 1, 6)
+            u = 12.0 * (0.6 + a[0] * np.sin(x + a[1]) * np.cos(y) + 0.5 * zz)
+            v = 8.0 * (a[2] + a[3] * np.cos(x) * np.sin(y + a[4]) - 0.3 * zz)
+            w = 0.02 * a[5] * np.sin(x) * np.sin(y) * np.ones_like(zz)
+            u = u + 0.5 * rng.standard_normal((nx, ny, nz))
+            v = v + 0.5 * rng.standard_normal((nx, ny, nz))
+        f = lambda a: np.asfortranarray(np.asarray(a, dtype=np.float32).reshape(nx, ny, nz))
+        return f(u), f(v), f(w)
+
+
+# ---------------------------------------------------------------------------
+# source, src/Source.f90
+# ---------------------------------------------------------------------------
+def suzuki_column(cfg: Config) -> np.ndarray:
+    """NormSourceColumn(1, 1:nz+1) for one eruption (Calc_Normalized_SourceCol,
+    ZScaling_ID 0: s = z)."""
+    nz = cfg.nz
+    dz, zcc, zlb = zgrid(cfg)
+    s_lb = lambda k: zlb[k + 1]
+    s_cc = lambda k: zcc[k + 1]
+    ds = lambda k: dz[k + 1]
+    s_volcano = cfg.z_volcano
+    H = cfg.plume_km
+    kground, ktop = 1, 0
+    for k in range(1, nz + 1):
+        if s_volcano >= s_lb(k) and s_volcano < s_lb(k + 1):
+            kground = k
+        if H > s_lb(k) and H <= s_lb(k + 1):
+            ktop = k
+    sground = s_lb(kground)
+    Habove = H - sground
+    A = cfg.suzuki_a
+    sk = A / (1.0 - (A + 1.0) * math.exp(-A))
+    col = np.zeros(nz + 1)
+    for k in range(kground, ktop + 1):
+        top = min(s_cc(k) + 0.5 * ds(k), H)
+        bot = s_cc(k) - 0.5 * ds(k)
+        sc1 = (top - sground) / Habove
+        sc2 = (bot - sground) / Habove
+        c1 = 1.0 - sc1
+        c2 = 1.0 - sc2
+        f1 = 1.0 / A + c1
+        f2 = 1.0 / A + c2
+        col[k - 1] = sk * (f1 * math.exp(-1.0 * A * c1) - f2 * math.exp(-1.0 * A * c2))
+    return col / col.sum()
+
+
+def mass_flux_rate(cfg: Config) -> float:
+    """EruptivePulse_MassFluxRate (src/Source.f90:508-592), kg/h."""
+    return cfg.magma_density * cfg.volume_km3 * KM3_2_M3 / cfg.duration_h
+
+
+def pulse_fraction(cfg: Config, time: float, dt: float) -> float:
+    """dt_pulse_frac of CheckEruptivePulses (src/Source.f90:613-685), one pulse from t=0."""
+    t0, t1 = 0.0, cfg.duration_h
+    tstart, tend = time, time + dt
+    contributes = ((tstart >= t0 and tstart < t1) or (tend > t0 and tend <= t1)
+                   or (tstart < t0 and tend > t1))
+    if not contributes:
+        return 0.0
+    return (min(tend, t1) - max(tstart, t0)) / dt
+
+
+def source_flux(cfg: Config, norm_col: np.ndarray, kappa: np.ndarray, frac: float) -> np.ndarray:
+    """SourceNodeFlux(1:nz+1, 1:ns) (k fastest) of TephraSourceNodes, kg/km^3/h."""
+    nz, ns = cfg.nz, cfg.ns
+    mfr = mass_flux_rate(cfg)
+    flux = np.zeros((nz + 1, ns), order="F")
+    tfr = np.zeros(nz)
+    tfr[:] = 0.0 + mfr * frac * norm_col[:nz]
+    iv, jv = cfg.ivent, cfg.jvent
+    for k in range(1, nz + 1):
+        kap = kappa[iv + 1, jv + 1, k + 1]
+        for g in range(ns):
+            flux[k - 1, g] = cfg.bin_mass[g] * tfr[k - 1] / kap
+    return flux
+
+
+def source_vol_inc(cfg: Config, flux: np.ndarray, kappa: np.ndarray, dt: float) -> float:
+    """SourceVolInc (src/Source.f90:798-836), km^3 DRE."""
+    tmp = 0.0
+    iv, jv = cfg.ivent, cfg.jvent
+    for k in range(1, cfg.nz + 2):
+        for g in range(cfg.ns):
+            tmp = tmp + dt * flux[k - 1, g] * kappa[iv + 1, jv + 1, k + 1] / cfg.magma_density / KM3_2_M3
+    return tmp
