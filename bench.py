@@ -273,6 +273,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                                 device_id=torch.device("cuda", local_rank))
         comm = driver.Comm(device=torch.device("cuda", local_rank))
     cfg_g = syn.make_config(args.config)
+    if args.ny:
+        cfg_g.ny = args.ny
+        cfg_g.jvent = max(1, args.ny // 2)
     cfg = driver.shard_config(cfg_g, rank, world)
     geo = syn.geometry(cfg)
     gpu = Ash3dGPU(cfg, device=local_rank, geo=geo)
@@ -408,6 +411,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="C2", choices=sorted(WORKLOAD))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ny", type=int, default=0,
+                    help="run a y-slab of the workload with this many rows (profiling case)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
