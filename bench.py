@@ -276,6 +276,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     if args.ny:
         cfg_g.ny = args.ny
         cfg_g.jvent = max(1, args.ny // 2)
+    cfg_g.limiter = args.limiter
     cfg = driver.shard_config(cfg_g, rank, world)
     geo = syn.geometry(cfg)
     gpu = Ash3dGPU(cfg, device=local_rank, geo=geo)
@@ -411,6 +412,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="C2", choices=sorted(WORKLOAD))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--limiter", default="superbee",
+                    choices=["none", "laxwen", "bw", "fromm", "minmod", "superbee", "mc"],
+                    help="the reference's LIM_* build choice (default superbee)")
     ap.add_argument("--ny", type=int, default=0,
                     help="run a y-slab of the workload with this many rows (profiling case)")
     args = ap.parse_args()

@@ -224,6 +224,20 @@ int a3g_kernel_timing(a3g_ctx *ctx, int32_t enable);
  * ms[A3G_K_COUNT] total milliseconds, count[A3G_K_COUNT] launches. */
 int a3g_kernel_times(a3g_ctx *ctx, double *ms, uint64_t *count);
 
+/* ---- tuning (no counterpart in the reference) ---- */
+/* Selects the kernel variant of the advection sweep along dir (0 x, 1 y,
+ * 2 z): 0 marching threads, 1 blocks of 4 cells, 2 blocks of 8 cells.  All
+ * variants produce identical results; only their speed differs. */
+int a3g_set_variant(a3g_ctx *ctx, int32_t dir, int32_t variant);
+int a3g_get_variant(a3g_ctx *ctx, int32_t dir, int32_t *variant);
+
+/* ---- diagnostics (no counterpart in the reference) ---- */
+/* Checks the library's division against the IEEE division operator on n
+ * seeded operand pairs (mixed magnitudes, signs, powers of two, zeros) on
+ * the given device; *mismatches receives the number of differing quotients
+ * (0 is expected: the sweeps rely on bit-identical quotients). */
+int a3g_selftest_div(int device, uint64_t n, uint64_t seed, uint64_t *mismatches);
+
 #ifdef __cplusplus
 }
 #endif

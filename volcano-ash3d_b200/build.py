@@ -30,6 +30,7 @@ def needs_build() -> bool:
         return True
     t = OUT.stat().st_mtime
     deps = [HERE / "csrc" / s for s in SRCS] + [HERE / "csrc" / "a3g_internal.cuh",
+                                               HERE / "csrc" / "exact_div.cuh",
                                                HERE.parent / "include" / "ash3d_b200.h"]
     return any(d.stat().st_mtime > t for d in deps)
 

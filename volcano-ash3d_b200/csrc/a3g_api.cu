@@ -183,13 +183,18 @@ int a3g_create(const a3g_grid_desc *grid, const a3g_params *params, int device, 
   ctx->device = device;
   Layout &L = ctx->L;
   L.nx = grid->nx; L.ny = grid->ny; L.nz = grid->nz; L.ns = grid->ns;
-  L.P = ((long)grid->nx + 3) / 4 * 4;
+  L.P = ((long)grid->nx + 7) / 8 * 8;  // the x sweep stores 8 cells per thread
   L.PY = L.P * grid->ny;
   L.PG = L.PY * grid->nz;
   full_box(ctx);
   ctx->h_aloft.assign(grid->ns, 1);
   ctx->n_gs_aloft = grid->ns;
   ctx->last_bc = 0;
+  // fastest measured advection variants on B200 (x: marching rows; y, z:
+  // 4-cell blocks); a3g_set_variant overrides them
+  ctx->tune_advect[0] = 0;
+  ctx->tune_advect[1] = 1;
+  ctx->tune_advect[2] = 1;
   auto dmalloc = [&](void **p, size_t n) -> cudaError_t {
     cudaError_t e = cudaMalloc(p, n);
     if (e == cudaSuccess) { ctx->bytes += n; cudaMemsetAsync(*p, 0, n, ctx->stream); }
@@ -244,7 +249,7 @@ int a3g_destroy(a3g_ctx *ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   double *dptrs[] = {ctx->c0, ctx->c1, ctx->vx, ctx->vy, ctx->vz, ctx->out_yz1, ctx->out_yz2,
                      ctx->out_xz1, ctx->out_xz2, ctx->out_xy1, ctx->out_xy2, ctx->red_buf,
-                     ctx->src_buf, ctx->cn_buf, ctx->dz_vec};
+                     ctx->src_buf, ctx->cn_buf, ctx->dz_vec, ctx->dtv_buf};
   for (double *p : dptrs) if (p) cudaFree(p);
   for (double *p : ctx->geo_ptrs) if (p) cudaFree(p);
   if (ctx->met) cudaFree(ctx->met);
@@ -312,6 +317,18 @@ int a3g_set_geometry(a3g_ctx *ctx, const double *kappa_pd, const double *sigma_n
   const long n0 = ctx->grid.nx + 4, n1 = ctx->grid.ny + 4, n2 = ctx->grid.nz + 4;
   int rc;
   if ((rc = set_geo3(ctx, kappa_pd, n0, n1, n2, -1, &ctx->kappa, 0))) return rc;
+  {  // dt/kappa buffer with kappa's compressed layout
+    const long m0 = ctx->kappa.si ? n0 : 1;
+    const long m1 = ctx->kappa.sj ? n1 : 1;
+    const long m2 = ctx->kappa.sk ? n2 : 1;
+    ctx->kappa_len = (size_t)(m0 * m1 * m2);
+    if (ctx->dtv_buf) { cudaFree(ctx->dtv_buf); ctx->dtv_buf = nullptr; }
+    A3G_CUDA(cudaMalloc((void **)&ctx->dtv_buf, ctx->kappa_len * sizeof(double)));
+    ctx->bytes += ctx->kappa_len * sizeof(double);
+    ctx->dtv = ctx->kappa;
+    ctx->dtv.p = ctx->dtv_buf;
+    ctx->dtv_valid = false;
+  }
   if ((rc = set_geo3(ctx, sigma_nx_pd, n0, n1, n2, -1, &ctx->snx, 1))) return rc;
   if ((rc = set_geo3(ctx, sigma_ny_pd, n0, n1, n2, -1, &ctx->sny, 2))) return rc;
   if ((rc = set_geo3(ctx, sigma_nz_pd, n0, n1, n2, -1, &ctx->snz, 3))) return rc;
@@ -495,6 +512,7 @@ int a3g_step_prologue(a3g_ctx *ctx) {
 int a3g_set_dt(a3g_ctx *ctx, double dt) {
   CTX_CHECK(ctx);
   ctx->host_dt = dt;
+  ctx->dt_stamp++;
   A3G_CUDA(cudaMemcpyAsync(&ctx->sc->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   return A3G_OK;
 }
@@ -674,6 +692,7 @@ int a3g_adjust_dt(a3g_ctx *ctx, double time, double next_write_time, double simt
   if (ctx->prm.use_diffusion && !ctx->have_diffusivity) return fail(A3G_ERR_STATE, "diffusivity not set");
   int rc = launch_cfl(ctx, time, next_write_time, simtime);
   if (rc) return rc;
+  ctx->dt_stamp++;
   if ((rc = sync_scalars(ctx))) return rc;
   ctx->host_dt = ctx->h_sc->dt;
   if (dt_out) *dt_out = ctx->h_sc->dt;
@@ -701,6 +720,7 @@ int a3g_adjust_dt_from_maxima(a3g_ctx *ctx, const double *vmax3, int32_t n_gs_al
   A3G_CUDA(cudaMemcpyAsync(ctx->sc->vmax, v, sizeof(v), cudaMemcpyHostToDevice, ctx->stream));
   int rc = launch_dt_from_maxima(ctx, n_gs_aloft_total, time, next_write_time, simtime);
   if (rc) return rc;
+  ctx->dt_stamp++;
   if ((rc = sync_scalars(ctx))) return rc;
   ctx->host_dt = ctx->h_sc->dt;
   if (dt_out) *dt_out = ctx->h_sc->dt;
@@ -759,6 +779,19 @@ int a3g_kernel_times(a3g_ctx *ctx, double *ms, uint64_t *count) {
     ms[k] += t;
     count[k] += 1;
   }
+  return A3G_OK;
+}
+
+int a3g_set_variant(a3g_ctx *ctx, int32_t dir, int32_t variant) {
+  if (!ctx) return fail(A3G_ERR_ARG, "null context");
+  if (dir < 0 || dir > 2 || variant < 0 || variant > 2) return fail(A3G_ERR_ARG, "bad direction or variant");
+  ctx->tune_advect[dir] = variant;
+  return A3G_OK;
+}
+
+int a3g_get_variant(a3g_ctx *ctx, int32_t dir, int32_t *variant) {
+  if (!ctx || !variant || dir < 0 || dir > 2) return fail(A3G_ERR_ARG, "bad argument");
+  *variant = ctx->tune_advect[dir];
   return A3G_OK;
 }
 

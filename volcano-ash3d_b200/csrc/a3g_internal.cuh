@@ -3,7 +3,7 @@
 //
 // Device layout (chosen for the sweeps, not copied from the host):
 //   * concentration: interior cells only, [grain][k][j][i] with the x-row
-//     padded to a pitch P (a multiple of 4 doubles, 32-byte aligned rows).
+//     padded to a pitch P (a multiple of 8 doubles, 64-byte aligned rows).
 //     Ghost cells are never stored: every sweep generates the ghost values
 //     Set_BC would have written (zero / edge copy / periodic wrap) when it
 //     loads a row, which is exact because no ghost value survives from one
@@ -93,6 +93,11 @@ struct a3g_ctx {
   long met_n;               // nx*ny*nz
   double *geo_ptrs[8];      // compressed kappa,snx,sny,snz,kx,ky,kz,vf
   a3g::Geo3 kappa, snx, sny, snz, kx, ky, kz;
+  a3g::Geo3 dtv;            // dt/kappa of the current step (kappa's layout)
+  double *dtv_buf;
+  size_t kappa_len;
+  bool dtv_valid;
+  uint64_t dt_stamp, dtv_stamp;  // dt_stamp changes whenever dt may have changed
   a3g::Geo4 vf;
   double *dz_vec;           // (-1:nz+2) on device
   std::vector<double> h_dz; // host copy
@@ -122,6 +127,8 @@ struct a3g_ctx {
   double host_dt;
   uint64_t launches;
   size_t bytes;
+  // kernel variant per advection direction (0 march, 1 block V=4, 2 block V=8)
+  int tune_advect[3];
   // optional per-kernel timing (a3g_kernel_timing)
   bool timing;
   std::vector<cudaEvent_t> ev_pool;
@@ -168,6 +175,7 @@ int launch_interp_winds(a3g_ctx *ctx, double frac);
 int launch_source(a3g_ctx *ctx, int ivent, int jvent, double dt);
 int launch_zero_state(a3g_ctx *ctx);
 int check_device_error(a3g_ctx *ctx);
+int refresh_dtv(a3g_ctx *ctx);
 // per-kernel timing brackets (no-ops unless a3g_kernel_timing(ctx,1))
 void tbegin(a3g_ctx *ctx, int kind);
 void tend(a3g_ctx *ctx);

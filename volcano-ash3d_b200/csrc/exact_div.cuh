@@ -1,0 +1,75 @@
+// exact_div.cuh -- correctly rounded double division without a branchy
+// library call in the common case.
+//
+// The transport path needs quotients that are bit-identical to IEEE division
+// (the limiter's theta = dqu/dq, src/AdvectionHorz_DCU.f90:204, and the back
+// substitution of the tridiagonal solve).  Method (Markstein, "Computation of
+// elementary functions on the IBM RISC System/6000 processor", IBM J. R&D
+// 1990; also Muller et al., Handbook of Floating-Point Arithmetic, ch. 5):
+//   y  ~ 1/b from the hardware reciprocal approximation (PTX
+//        rcp.approx.ftz.f64), refined by two Newton-Raphson steps
+//        e = 1 - b*y, y = y + y*e (each one fused multiply-add);
+//   q  = a*y;  r = a - b*q (exact with an FMA);  q = q + r*y.
+// The result is then certified exactly: r = a - b*q is computed again with an
+// FMA (exact for a q within an ulp or two of a/b and operands far from the
+// underflow range), and q is accepted only if |r| < |b| * ulp(q)/2, i.e. the
+// true quotient lies strictly inside the rounding interval of q, and q is not
+// a power of two (whose rounding interval is asymmetric).  Everything else --
+// operands outside [2^-200, 2^200], a zero divisor, non-finite values, a
+// residual on or beyond the half-ulp bound -- falls back to the IEEE division
+// operator.  Both paths therefore return RN(a/b) exactly.
+#pragma once
+
+namespace a3g {
+
+__device__ __forceinline__ double rcp_approx(double b) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+  return y;
+}
+
+// True when |x| is zero or its binary exponent lies in [-200, 200].
+__device__ __forceinline__ bool in_fast_range(double x, bool allow_zero) {
+  const unsigned e = ((unsigned)__double2hiint(x) >> 20) & 0x7ffu;
+  return (e - 823u) <= 400u || (allow_zero && x == 0.0);
+}
+
+// Certifies q against a/b (see above); returns true if q == RN(a/b).
+__device__ __forceinline__ bool certified(double a, double b, double q) {
+  const double r = fma(-b, q, a);
+  const long long qb = __double_as_longlong(q);
+  const long long ex = qb & 0x7ff0000000000000LL;
+  const double half_ulp = __longlong_as_double(ex - (53LL << 52));  // 2^(e_q - 53)
+  const bool pow2 = (qb & 0x000fffffffffffffLL) == 0;
+  return fabs(r) < fabs(b) * half_ulp && !pow2;
+}
+
+// RN(a/b).
+__device__ __forceinline__ double div_rn(double a, double b) {
+  if (!(in_fast_range(b, false) && in_fast_range(a, true))) return a / b;
+  if (a == 0.0) return a / b;
+  double y = rcp_approx(b);
+  double e = fma(-b, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-b, y, 1.0);
+  y = fma(y, e, y);
+  double q = a * y;
+  const double r = fma(-b, q, a);
+  q = fma(r, y, q);
+  if (certified(a, b, q)) return q;
+  return a / b;
+}
+
+// RN(a/b) given y = RN(1/b) (precomputed once for a divisor shared by many
+// quotients, e.g. a tridiagonal pivot).
+__device__ __forceinline__ double div_rn_rcp(double a, double b, double y) {
+  if (!(in_fast_range(b, false) && in_fast_range(a, true))) return a / b;
+  if (a == 0.0) return a / b;
+  double q = a * y;
+  const double r = fma(-b, q, a);
+  q = fma(r, y, q);
+  if (certified(a, b, q)) return q;
+  return a / b;
+}
+
+}  // namespace a3g

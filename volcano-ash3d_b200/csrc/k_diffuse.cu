@@ -19,6 +19,7 @@
 // A line that would need a row interchange (or a zero pivot) raises
 // A3G_ERR_PIVOT instead of silently diverging from dgtsv.
 #include "a3g_internal.cuh"
+#include "exact_div.cuh"
 
 namespace a3g {
 
@@ -86,7 +87,9 @@ __global__ void __launch_bounds__(256) k_diff(Layout L, Box box, int periodic,
 // ---------------------------------------------------------------------------
 // Table fields, stored [field][position][line] so that neighbouring lines
 // (neighbouring threads) read neighbouring words.
-enum { CN_FACT = 0, CN_DP = 1, CN_DU = 2, CN_CL = 3, CN_CC = 4, CN_CR = 5, CN_NF = 6 };
+// CN_RDP holds RN(1/D'), so that the back substitution's quotients can be
+// formed by exact_div.cuh's certified path.
+enum { CN_FACT = 0, CN_DP = 1, CN_DU = 2, CN_CL = 3, CN_CC = 4, CN_CR = 5, CN_RDP = 6, CN_NF = 7 };
 
 struct LineMap {  // distinct-line indexing for one sweep direction
   int na, nb;     // extents of the two fixed indices (a fastest)
@@ -156,26 +159,23 @@ __global__ void k_cn_table(Layout L, Box box, double imp, LineMap map, Geo3 sig,
     tab[CN_CL * F + o] = (1.0 - imp) * Lf;
     tab[CN_CC * F + o] = 1.0 - (1.0 - imp) * Cf;
     tab[CN_CR * F + o] = (1.0 - imp) * Rf;
+    tab[CN_RDP * F + o] = 1.0 / Dp;
     dp_prev = Dp;
     du_prev = DU;
   }
   if (dp_prev == 0.0) raise_error(sc, A3G_ERR_PIVOT, ncells);
 }
 
-// Solve kernel: one thread per (line, grain).  Thread layout: x = lane index
-// along the first fixed index a (j for x-lines, i for y/z-lines), y = b,
-// z = grain.
+// Solve of one line (a, b) of grain g from the table.  The eliminated
+// right-hand side B' is written to the output line and read back by the back
+// substitution, which prefetches PF entries ahead (the loads cannot move
+// above the stores to the same line on their own).
 template <int DIR>
-__global__ void __launch_bounds__(128) k_cn_solve(Layout L, Box box, LineMap map,
-                                                  const double *__restrict__ cin,
-                                                  double *__restrict__ cout,
-                                                  const double *__restrict__ tab,
-                                                  const int32_t *__restrict__ aloft) {
-  const int a = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int b = blockIdx.y + 1;
-  const int g = blockIdx.z;
-  const int na = (DIR == 0) ? L.ny : L.nx;
-  if (a > na) return;
+__device__ __forceinline__ void cn_line(const Layout &L, const Box &box, const LineMap &map,
+                                        const double *__restrict__ cin, double *__restrict__ cout,
+                                        const double *__restrict__ tab,
+                                        const int32_t *__restrict__ aloft, int a, int b, int g) {
+  constexpr int PF = 4;
   const int n = (DIR == 0) ? L.nx : (DIR == 1) ? L.ny : L.nz;
   const int rmin = (DIR == 0) ? box.imin : (DIR == 1) ? box.jmin : box.kmin;
   const int rmax = (DIR == 0) ? box.imax : (DIR == 1) ? box.jmax : box.kmax;
@@ -203,32 +203,65 @@ __global__ void __launch_bounds__(128) k_cn_solve(Layout L, Box box, LineMap map
   for (int c = rmax + 1; c <= n; c++) x[(long)(c - 1) * st] = 0.0;
   const long U = map.U;
   const long F = (long)ncells * U;
-  const int u = map.u(a, b);
+  const double *t = tab + map.u(a, b);
+  const double *qq = q + (long)(rmin - 1) * st;  // cell rmin
+  double *xx = x + (long)(rmin - 1) * st;
   // forward elimination with the right-hand side built on the fly, :813-851
-  double qm = q[(long)(rmin - 1) * st];  // BC_left_t0 = q(rmin)
+  double qm = qq[0];  // BC_left_t0 = q(rmin)
   double qc = qm;
   double bp = 0.0;
-  for (int l = 1; l <= ncells; l++) {
-    const int c = rmin - 1 + l;
-    const double qp = (l < ncells) ? q[(long)c * st] : qc;  // BC_right_t0 = q(rmax)
-    const long o = (long)(l - 1) * U + u;
-    const double B = tab[CN_CL * F + o] * qm + tab[CN_CC * F + o] * qc + tab[CN_CR * F + o] * qp;
-    bp = (l == 1) ? B : B - tab[CN_FACT * F + o] * bp;
-    x[(long)(c - 1) * st] = bp;
+#pragma unroll 4
+  for (int l = 0; l < ncells; l++) {
+    const double qp = (l + 1 < ncells) ? qq[(long)(l + 1) * st] : qc;  // BC_right_t0 = q(rmax)
+    const long o = (long)l * U;
+    const double B = t[CN_CL * F + o] * qm + t[CN_CC * F + o] * qc + t[CN_CR * F + o] * qp;
+    bp = (l == 0) ? B : B - t[CN_FACT * F + o] * bp;
+    xx[(long)l * st] = bp;
     qm = qc;
     qc = qp;
   }
-  // back substitution
+  // back substitution with a PF-deep prefetch of B'
+  double ring[PF];
+#pragma unroll
+  for (int p = 0; p < PF; p++) ring[p] = (ncells - 1 - p >= 0) ? xx[(long)(ncells - 1 - p) * st] : 0.0;
   double xn = 0.0;
-  for (int l = ncells; l >= 1; l--) {
-    const int c = rmin - 1 + l;
-    const long o = (long)(l - 1) * U + u;
-    const double b2 = x[(long)(c - 1) * st];
-    const double v = (l == ncells) ? b2 / tab[CN_DP * F + o]
-                                   : (b2 - tab[CN_DU * F + o] * xn) / tab[CN_DP * F + o];
-    x[(long)(c - 1) * st] = v;
-    xn = v;
+  for (int l0 = ncells - 1; l0 >= 0; l0 -= PF) {
+#pragma unroll
+    for (int p = 0; p < PF; p++) {
+      const int l = l0 - p;
+      if (l >= 0) {
+        const double b2 = ring[p];
+        const int lp = l - PF;  // refill this slot for the next round
+        ring[p] = (lp >= 0) ? xx[(long)lp * st] : 0.0;
+        const long o = (long)l * U;
+        const double num = (l == ncells - 1) ? b2 : b2 - t[CN_DU * F + o] * xn;
+        const double v = div_rn_rcp(num, t[CN_DP * F + o], t[CN_RDP * F + o]);
+        xx[(long)l * st] = v;
+        xn = v;
+      }
+    }
   }
+}
+
+// Solve kernel: one thread per line (a, b, grain), lines enumerated with a
+// fastest so that a warp holds neighbouring lines (neighbouring i for y and
+// z lines: coalesced; neighbouring rows for x lines).
+template <int DIR>
+__global__ void __launch_bounds__(128) k_cn_solve(Layout L, Box box, LineMap map,
+                                                  const double *__restrict__ cin,
+                                                  double *__restrict__ cout,
+                                                  const double *__restrict__ tab,
+                                                  const int32_t *__restrict__ aloft) {
+  const int na = (DIR == 0) ? L.ny : L.nx;
+  const int nb = (DIR == 2) ? L.ny : L.nz;
+  const long nlines = (long)na * nb * L.ns;
+  const long w = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (w >= nlines) return;
+  const int a = (int)(w % na) + 1;
+  const long r = w / na;
+  const int b = (int)(r % nb) + 1;
+  const int g = (int)(r / nb);
+  cn_line<DIR>(L, box, map, cin, cout, tab, aloft, a, b, g);
 }
 
 // ---------------------------------------------------------------------------
@@ -295,10 +328,10 @@ static int launch_cn_dir(a3g_ctx *ctx) {
                                                                 ctx->kappa, kk, ctx->sc, ctx->cn_buf);
   tend(ctx);
   A3G_LAUNCH_CHECK(ctx);
-  dim3 grid((map.na + 127) / 128, map.nb, L.ns);
+  const long nlines = (long)map.na * map.nb * L.ns;
   tbegin(ctx, A3G_K_CN_SOLVE_X + DIR);
-  k_cn_solve<DIR><<<grid, 128, 0, ctx->stream>>>(L, box, map, ctx->c0, ctx->c1, ctx->cn_buf,
-                                                 ctx->aloft);
+  k_cn_solve<DIR><<<(unsigned)((nlines + 127) / 128), 128, 0, ctx->stream>>>(
+      L, box, map, ctx->c0, ctx->c1, ctx->cn_buf, ctx->aloft);
   tend(ctx);
   A3G_LAUNCH_CHECK(ctx);
   swap_levels(ctx);

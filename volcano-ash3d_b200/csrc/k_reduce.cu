@@ -12,6 +12,7 @@
 //  * met-step interpolation (src/MesoInterpolater.f90:207-223) and the vent
 //    column source insertion (src/Ash3d.F90:428-431).
 #include "a3g_internal.cuh"
+#include "exact_div.cuh"
 
 namespace a3g {
 
@@ -451,4 +452,62 @@ int launch_source(a3g_ctx *ctx, int ivent, int jvent, double dt) {
   return A3G_OK;
 }
 
+// ---------------------------------------------------------------------------
+// self-test of exact_div.cuh against the IEEE division operator
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t mix64(uint64_t x) {  // splitmix64 finaliser
+  x += 0x9E3779B97F4A7C15ULL;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBULL;
+  return x ^ (x >> 31);
+}
+
+__device__ double test_operand(uint64_t h) {
+  const int kind = (int)(h & 15);
+  const double sgn = (h & 16) ? -1.0 : 1.0;
+  const uint64_t m = (h >> 12) & 0x000fffffffffffffULL;
+  int e;
+  if (kind < 8) e = (int)((h >> 5) & 63) - 32;          // moderate magnitudes
+  else if (kind < 12) e = (int)((h >> 5) & 1023) - 512;  // wide range (fallbacks)
+  else if (kind < 14) e = (int)((h >> 5) & 15) - 8;
+  else e = (int)((h >> 5) & 7) - 4;
+  double v = __longlong_as_double((long long)(((uint64_t)(1023 + e) << 52) | (kind == 14 ? 0 : m)));
+  if (kind == 15) v = (double)((h >> 20) & 255) - 128.0;  // small integers, zeros, exact ratios
+  return sgn * v;
+}
+
+__global__ void k_selftest_div(uint64_t n, uint64_t seed, unsigned long long *bad) {
+  unsigned long long local = 0;
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
+    const double a = test_operand(mix64(seed ^ (2 * t)));
+    const double b = test_operand(mix64(seed ^ (2 * t + 1)));
+    if (b == 0.0) continue;
+    const double q1 = div_rn(a, b), q2 = a / b;
+    const double y = 1.0 / b;
+    const double q3 = div_rn_rcp(a, b, y);
+    const bool same1 = __double_as_longlong(q1) == __double_as_longlong(q2) || (q1 != q1 && q2 != q2);
+    const bool same3 = __double_as_longlong(q3) == __double_as_longlong(q2) || (q3 != q3 && q2 != q2);
+    local += (same1 ? 0 : 1) + (same3 ? 0 : 1);
+  }
+  if (local) atomicAdd(bad, local);
+}
+
 }  // namespace a3g
+
+extern "C" int a3g_selftest_div(int device, uint64_t n, uint64_t seed, uint64_t *mismatches) {
+  if (!mismatches) { a3g::set_error("null mismatches"); return A3G_ERR_ARG; }
+  A3G_CUDA(cudaSetDevice(device));
+  unsigned long long *d = nullptr;
+  A3G_CUDA(cudaMalloc((void **)&d, sizeof(*d)));
+  cudaError_t e = cudaMemset(d, 0, sizeof(*d));
+  if (e == cudaSuccess) {
+    a3g::k_selftest_div<<<148 * 8, 256>>>(n, seed, d);
+    e = cudaGetLastError();
+  }
+  unsigned long long h = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&h, d, sizeof(h), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return a3g::cuda_fail(e, "a3g_selftest_div");
+  *mismatches = h;
+  return A3G_OK;
+}

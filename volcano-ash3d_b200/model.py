@@ -81,6 +81,9 @@ class Ash3dGPU:
         check(self.lib.a3g_kernel_times(self.ctx, dptr(ms), cnt))
         return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(_lib.KERNEL_CLASSES)}
 
+    def set_variant(self, direction: int, variant: int):
+        check(self.lib.a3g_set_variant(self.ctx, direction, variant))
+
     def kernel_launches(self) -> int:
         n = C.c_uint64()
         check(self.lib.a3g_kernel_launches(self.ctx, C.byref(n)))

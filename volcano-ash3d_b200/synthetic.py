@@ -131,6 +131,15 @@ def make_config(name: str) -> Config:
                       fall_mps=(0.1, 1.0), bin_mass=(0.5, 0.5), plume_km=5.0, volume_km3=1.0e-3,
                       duration_h=1.0, use_cn=True, sim_hours=2.0, winds="random", seed=15,
                       fast_subgrid=True)
+    if name == "tiny_wide":  # rows longer than one x segment (1024 cells)
+        return Config("tiny_wide", 1100, 6, 5, 2, dx=2.0, dy=5.0, dz=0.5, ivent=550, jvent=3,
+                      fall_mps=(0.1, 1.0), bin_mass=(0.5, 0.5), plume_km=2.0, volume_km3=1.0e-3,
+                      duration_h=1.0, use_cn=True, sim_hours=1.0, winds="random", seed=16)
+    if name == "tiny_tall":  # y and z lines longer than one march segment (96 cells)
+        return Config("tiny_tall", 20, 200, 110, 3, dx=5.0, dy=2.0, dz=0.1, ivent=10, jvent=100,
+                      fall_mps=(0.05, 0.4, 1.5), bin_mass=(0.3, 0.3, 0.4), plume_km=8.0,
+                      volume_km3=1.0e-3, duration_h=1.0, use_cn=True, sim_hours=1.0,
+                      winds="random", seed=17)
     raise KeyError(name)
 
 
