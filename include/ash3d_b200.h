@@ -231,6 +231,29 @@ int a3g_kernel_times(a3g_ctx *ctx, double *ms, uint64_t *count);
 int a3g_set_variant(a3g_ctx *ctx, int32_t dir, int32_t variant);
 int a3g_get_variant(a3g_ctx *ctx, int32_t dir, int32_t *variant);
 
+/* ---- allocation-free entry point (no counterpart in the reference) ---- */
+/* Per-grain airborne mass sum(c*kappa) (the mass_aloft of Calc_AshVol_Aloft,
+ * src/Output_Vars.f90:1255-1293) for callers that cannot allocate device
+ * memory at the time of the call: hosts that reserve all GPU memory at
+ * start-up, hosts that pass buffers from their own memory manager, or code
+ * running where allocation calls are not allowed (such as a host function
+ * enqueued on a stream).  It calls no allocation routine: its partial sums
+ * live in a fixed device array of the library (64 grains x 296 blocks x 2
+ * doubles, about 296 KiB per device, held until the process exits).
+ *   conc:  device array [ns][nz][ny][row_pitch] (i fastest, interior cells)
+ *   kappa: device array [nz][ny][nx] (interior cell volumes)
+ *   mass_out: device array [ns] (written)
+ *   stream: a cudaStream_t, or NULL for the default stream; the call is
+ *           asynchronous on it.
+ * ns above 64 is rejected with A3G_ERR_ARG.  The first call on a device looks
+ * up the array's device address with that device current; make that first
+ * call before any stream capture.  All calls share the array and it keeps
+ * the last call's contents (nothing in it needs to start at zero); calls
+ * whose kernels overlap on the same device race on it. */
+int a3g_mass_aloft_noalloc(int device, const double *conc, const double *kappa, int32_t nx,
+                           int32_t ny, int32_t nz, int32_t ns, int64_t row_pitch,
+                           double *mass_out, void *stream);
+
 /* ---- diagnostics (no counterpart in the reference) ---- */
 /* Checks the library's division against the IEEE division operator on n
  * seeded operand pairs (mixed magnitudes, signs, powers of two, zeros) on

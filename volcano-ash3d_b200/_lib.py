@@ -36,7 +36,7 @@ EXPORTED = [
     "a3g_get_minmax_index", "a3g_set_subgrid", "a3g_get_subgrid", "a3g_step",
     "a3g_kernel_launches", "a3g_get_stream", "a3g_kernel_timing", "a3g_kernel_times",
     "a3g_cfl_maxima", "a3g_adjust_dt_from_maxima", "a3g_selftest_div", "a3g_set_variant",
-    "a3g_get_variant",
+    "a3g_get_variant", "a3g_mass_aloft_noalloc",
 ]
 KERNEL_CLASSES = ["advect_x", "advect_y", "advect_z", "diff_x", "diff_y", "diff_z", "cn_table",
                   "cn_solve_x", "cn_solve_y", "cn_solve_z", "cfl", "totals", "winds", "other"]
@@ -114,6 +114,8 @@ def load(path: os.PathLike | str | None = None) -> C.CDLL:
         "a3g_cfl_maxima": (C.c_int, [P, D]),
         "a3g_set_variant": (C.c_int, [P, C.c_int32, C.c_int32]),
         "a3g_get_variant": (C.c_int, [P, C.c_int32, C.POINTER(C.c_int32)]),
+        "a3g_mass_aloft_noalloc": (C.c_int, [C.c_int, D, D, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                             C.c_int64, D, C.c_void_p]),
         "a3g_selftest_div": (C.c_int, [C.c_int, C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)]),
         "a3g_adjust_dt_from_maxima": (C.c_int, [P, D, C.c_int32, C.c_double, C.c_double, C.c_double, D]),
         "a3g_get_minmax_index": (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, I]),

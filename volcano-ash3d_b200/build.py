@@ -14,7 +14,7 @@ import subprocess
 import sys
 
 HERE = pathlib.Path(__file__).resolve().parent
-SRCS = ["a3g_api.cu", "k_advect.cu", "k_diffuse.cu", "k_reduce.cu"]
+SRCS = ["a3g_api.cu", "k_advect.cu", "k_diffuse.cu", "k_reduce.cu", "a3g_noalloc.cu"]
 OUT = HERE / "libash3d_b200.so"
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "--fmad=false", "-std=c++17",
               "-lineinfo", "-Xcompiler", "-fPIC", "-shared"]
