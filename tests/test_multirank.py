@@ -1,0 +1,107 @@
+"""Grain-sharded runs over torch.distributed (gloo, world size 2, CPU).
+
+The multi-GPU path shards the grain bins; each rank runs the full transport
+step on its bins, and the ranks exchange only the CFL maxima (all-reduce MAX)
+and the totals (all-reduce SUM).  These tests run that host logic with the
+oracle as each rank's model, so they need no GPU: the sharded run must give
+the single-process run's dt sequence bitwise, each rank's concentration must
+equal the matching grains of the single-process field bitwise, and the summed
+totals must agree to 1e-13.
+"""
+import os
+import pathlib
+import socket
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = pathlib.Path(__file__).resolve().parent.parent
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank: int, world: int, port: int, cfg_name: str, steps: int, out_dir: str):
+    sys.path.insert(0, str(ROOT / "tests"))
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        import conftest
+        import ash3d_oracle as orc
+        mod = conftest._load_pkg()
+        pkg, syn = mod.driver, mod.synthetic
+        gcfg = syn.make_config(cfg_name)
+        cfg = pkg.split_grains(gcfg, rank, world)
+        model = orc.OracleModel(cfg, threads=1)
+        st = pkg.run(model, cfg, max_steps=steps, comm=pkg.Comm(), n_gs_aloft_total=gcfg.ns)
+        hist = np.array([[r.time, r.dt, r.aloft, r.dep, r.outflow, r.tot] for r in st.history])
+        np.savez(os.path.join(out_dir, f"rank{rank}.npz"), hist=hist, conc=model.interior(),
+                 dep=model.outflows()["deposit"])
+    finally:
+        dist.destroy_process_group()
+
+
+def _sharded(cfg_name: str, world: int, steps: int, tmp_path):
+    import torch.multiprocessing as mp
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, cfg_name, steps, str(tmp_path)))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=240)
+    for p in procs:
+        if p.is_alive():
+            p.kill()
+            p.join()
+        assert p.exitcode == 0, f"rank process exit code {p.exitcode}"
+    return [np.load(tmp_path / f"rank{r}.npz") for r in range(world)]
+
+
+@pytest.mark.parametrize("cfg_name,steps", [("tiny_proj", 12), ("tiny_latlon", 8)])
+def test_grain_sharded_matches_single(pkg, oracle_mod, cfg_name, steps, tmp_path):
+    syn, drv = pkg.synthetic, pkg.driver
+    gcfg = syn.make_config(cfg_name)
+    world = 2
+    ranks = _sharded(cfg_name, world, steps, tmp_path)
+
+    ref = oracle_mod.OracleModel(gcfg, threads=1)
+    st = drv.run(ref, gcfg, max_steps=steps)
+    ref_hist = np.array([[r.time, r.dt, r.aloft, r.dep, r.outflow, r.tot] for r in st.history])
+    ref_c = ref.interior()
+    ref_dep = ref.outflows()["deposit"]
+
+    for r in range(world):
+        h = ranks[r]["hist"]
+        assert h.shape == ref_hist.shape
+        # identical dt sequence and clock on every rank (bitwise)
+        assert np.array_equal(h[:, :2], ref_hist[:, :2])
+        lo, hi = drv.grain_range(gcfg.ns, r, world)
+        assert np.array_equal(ranks[r]["conc"], ref_c[..., lo:hi])
+        assert np.array_equal(ranks[r]["dep"], ref_dep[..., lo:hi])
+        # totals are all-reduced: every rank holds the global sums
+        np.testing.assert_allclose(h[:, 2:], ref_hist[:, 2:], rtol=1e-13, atol=1e-300)
+
+
+def test_split_grains_partition(pkg):
+    syn, drv = pkg.synthetic, pkg.driver
+    cfg = syn.make_config("C2")
+    for world in (1, 2, 3, 4, 7, 10):
+        got = []
+        for r in range(world):
+            c = drv.split_grains(cfg, r, world)
+            lo, hi = drv.grain_range(cfg.ns, r, world)
+            assert c.ns == hi - lo and c.fall_mps == cfg.fall_mps[lo:hi]
+            got.extend(c.fall_mps)
+        assert tuple(got) == cfg.fall_mps
+    with pytest.raises(ValueError):
+        drv.split_grains(cfg, 0, 11)

@@ -91,6 +91,32 @@ def shard_config(cfg: syn.Config, rank: int, world: int) -> syn.Config:
     return c
 
 
+def split_grains(cfg: syn.Config, rank: int, world: int) -> syn.Config:
+    """Strong split of one run's grain bins over ``world`` ranks: rank r keeps
+    a contiguous block of bins (the first ``ns % world`` ranks one more), with
+    the global run's fall speeds and mass fractions unchanged, so the union of
+    the ranks' fields is the single-process run's field."""
+    if world == 1:
+        return cfg
+    if cfg.ns < world:
+        raise ValueError(f"{cfg.ns} grain bins cannot be split over {world} ranks")
+    base, extra = divmod(cfg.ns, world)
+    lo = rank * base + min(rank, extra)
+    n = base + (1 if rank < extra else 0)
+    c = dataclasses.replace(cfg)
+    c.ns = n
+    c.fall_mps = tuple(cfg.fall_mps[lo:lo + n])
+    c.bin_mass = tuple(cfg.bin_mass[lo:lo + n])
+    return c
+
+
+def grain_range(ns: int, rank: int, world: int) -> tuple[int, int]:
+    """[lo, hi) of the global grain bins that split_grains gives ``rank``."""
+    base, extra = divmod(ns, world)
+    lo = rank * base + min(rank, extra)
+    return lo, lo + base + (1 if rank < extra else 0)
+
+
 def step(model, st: RunState, simtime: float | None = None, totals: bool = True,
          comm: Comm | None = None, n_gs_aloft_total: int | None = None) -> StepRecord:
     """Advances the model by one reference time step."""
@@ -133,10 +159,14 @@ def step(model, st: RunState, simtime: float | None = None, totals: bool = True,
 
 
 def run(model, cfg: syn.Config, max_steps: int | None = None, sim_hours: float | None = None,
-        geo: dict | None = None, totals: bool = True) -> RunState:
-    """Runs until sim_hours (or max_steps) like the reference's stop test 2."""
+        geo: dict | None = None, totals: bool = True, comm: Comm | None = None,
+        n_gs_aloft_total: int | None = None) -> RunState:
+    """Runs until sim_hours (or max_steps) like the reference's stop test 2.
+    With ``comm`` (a grain-sharded run), dt comes from the all-reduced CFL
+    maxima and the totals are summed over ranks; every rank takes the same
+    number of steps because every rank gets the same dt."""
     st = new_state(cfg, geo)
     simtime = cfg.sim_hours if sim_hours is None else sim_hours
     while st.time < simtime and (max_steps is None or st.itime < max_steps):
-        step(model, st, simtime, totals)
+        step(model, st, simtime, totals, comm, n_gs_aloft_total)
     return st

@@ -1,0 +1,391 @@
+!##############################################################################
+!
+! ash3d_b200_shim.f90 -- ISO_C_BINDING drop-in for Ash3d's transport path.
+!
+! Build Ash3d with USEPOINTERS=T (src/makefile:80) so that c_loc() of the
+! module arrays is legal, compile this file in place of
+!   src/AdvectionHorz.f90, src/AdvectionHorz_DCU.f90,
+!   src/AdvectionVert_DCU.f90, src/Diffusion.F90, src/Set_BC.f90,
+!   src/Adjust_dt.f90, src/TimeStepTotals.f90
+! and link libash3d_b200.so.  Ash3d.F90 keeps calling the same names with the
+! same arguments:
+!   Set_BC(bc_code)            src/Set_BC.f90:15
+!   AdvectHorz(itoggle)        src/AdvectionHorz.f90:47
+!   AdvectVert                 src/AdvectionVert_DCU.f90:64
+!   DiffuseHorz(i), DiffuseVert  src/Diffusion.F90:151,232
+!   Adjust_DT(mesostep)        src/Adjust_dt.f90:19
+!   TimeStepTotals(itime)      src/TimeStepTotals.f90:17
+! A nonzero status from the library is reported on errlog and ends the run
+! with "stop 1", the reference's error convention (e.g. src/Set_BC.f90:119-123).
+!
+! The concentration lives on the GPU between calls.  B200_Download copies it
+! back into concen_pd(:,:,:,:,ts0) (and the outflow/deposit arrays) before
+! the host reads them: before Gen_Output_Vars/output_results and restart
+! writes.  B200_Upload sends a host-modified field back (restart loads).
+! This file is written against the reference's module interfaces and is not
+! compiled in this repository's test suite (no Fortran compiler in the image).
+!##############################################################################
+
+      module B200_Transport
+
+      use iso_c_binding
+
+      implicit none
+
+      private
+      public B200_Init, B200_Finalize, B200_Upload, B200_Download, B200_Check, &
+             B200_StepPrologue, B200_AddSource, B200_SetWinds, B200_SetMetSteps, &
+             B200_InterpWinds, b200_ctx
+
+      type, bind(C) :: a3g_grid_desc
+        integer(c_int32_t) :: nx, ny, nz, ns
+        integer(c_int32_t) :: periodic, latlon
+        real(c_double)     :: dx, dy
+      end type a3g_grid_desc
+
+      type, bind(C) :: a3g_params
+        integer(c_int32_t) :: limiter, use_cn, use_diffusion, fast_subgrid, nocycle, zscaling_id
+        real(c_double)     :: cfl, dt_min, dt_max, imp_fac, imp_dt_fac, eps_thresh, eps_small
+        real(c_double)     :: cloudcon_grid_thresh, magma_density
+      end type a3g_params
+
+      type(c_ptr), save :: b200_ctx = c_null_ptr
+
+      interface
+        subroutine a3g_default_params(p) bind(C, name="a3g_default_params")
+          import :: a3g_params
+          type(a3g_params), intent(out) :: p
+        end subroutine
+        function a3g_last_error() bind(C, name="a3g_last_error") result(msg)
+          import :: c_ptr
+          type(c_ptr) :: msg
+        end function
+        integer(c_int) function a3g_create(grid, prm, device, ctx) bind(C, name="a3g_create")
+          import :: a3g_grid_desc, a3g_params, c_int, c_ptr
+          type(a3g_grid_desc), intent(in) :: grid
+          type(a3g_params), intent(in) :: prm
+          integer(c_int), value :: device
+          type(c_ptr), intent(out) :: ctx
+        end function
+        integer(c_int) function a3g_destroy(ctx) bind(C, name="a3g_destroy")
+          import :: c_int, c_ptr
+          type(c_ptr), value :: ctx
+        end function
+        integer(c_int) function a3g_set_geometry(ctx, kap, snx, sny, snz, dz) bind(C, name="a3g_set_geometry")
+          import :: c_int, c_ptr
+          type(c_ptr), value :: ctx, kap, snx, sny, snz, dz
+        end function
+        integer(c_int) function a3g_set_diffusivity(ctx, kx, ky, kz) bind(C, name="a3g_set_diffusivity")
+          import :: c_int, c_ptr
+          type(c_ptr), value :: ctx, kx, ky, kz
+        end function
+        integer(c_int) function a3g_set_fall_velocity(ctx, vf) bind(C, name="a3g_set_fall_velocity")
+          import :: c_int, c_ptr
+          type(c_ptr), value :: ctx, vf
+        end function
+        integer(c_int) function a3g_set_aloft(ctx, aloft) bind(C, name="a3g_set_aloft")
+          import :: c_int, c_ptr
+          type(c_ptr), value :: ctx, aloft
+        end function
+        integer(c_int) function a3g_set_winds(ctx, vx, vy, vz) bind(C, name="a3g_set_winds")
+          import :: c_int, c_ptr
+          type(c_ptr), value :: ctx, vx, vy, vz
+        end function
+        integer(c_int) function a3g_set_met_steps(ctx, xl, yl, zl, xn, yn, zn) bind(C, name="a3g_set_met_steps")
+          import :: c_int, c_ptr
+          type(c_ptr), value :: ctx, xl, yl, zl, xn, yn, zn
+        end function
+        integer(c_int) function a3g_interp_winds(ctx, frac) bind(C, name="a3g_interp_winds")
+          import :: c_int, c_ptr, c_double
+          type(c_ptr), value :: ctx
+          real(c_double), value :: frac
+        end function
+        integer(c_int) function a3g_upload_concen(ctx, c) bind(C, name="a3g_upload_concen")
+          import :: c_int, c_ptr
+          type(c_ptr), value :: ctx, c
+        end function
+        integer(c_int) function a3g_download_concen(ctx, c) bind(C, name="a3g_download_concen")
+          import :: c_int, c_ptr
+          type(c_ptr), value :: ctx, c
+        end function
+        integer(c_int) function a3g_upload_outflow(ctx, a, b, c, d, e, f) bind(C, name="a3g_upload_outflow")
+          import :: c_int, c_ptr
+          type(c_ptr), value :: ctx, a, b, c, d, e, f
+        end function
+        integer(c_int) function a3g_download_outflow(ctx, a, b, c, d, e, f, dep) &
+            bind(C, name="a3g_download_outflow")
+          import :: c_int, c_ptr
+          type(c_ptr), value :: ctx, a, b, c, d, e, f, dep
+        end function
+        integer(c_int) function a3g_step_prologue(ctx) bind(C, name="a3g_step_prologue")
+          import :: c_int, c_ptr
+          type(c_ptr), value :: ctx
+        end function
+        integer(c_int) function a3g_set_dt(ctx, dt) bind(C, name="a3g_set_dt")
+          import :: c_int, c_ptr, c_double
+          type(c_ptr), value :: ctx
+          real(c_double), value :: dt
+        end function
+        integer(c_int) function a3g_add_source_column(ctx, iv, jv, flux, dt) bind(C, name="a3g_add_source_column")
+          import :: c_int, c_int32_t, c_ptr, c_double
+          type(c_ptr), value :: ctx, flux
+          integer(c_int32_t), value :: iv, jv
+          real(c_double), value :: dt
+        end function
+        integer(c_int) function a3g_set_bc(ctx, code) bind(C, name="a3g_set_bc")
+          import :: c_int, c_int32_t, c_ptr
+          type(c_ptr), value :: ctx
+          integer(c_int32_t), value :: code
+        end function
+        integer(c_int) function a3g_advect_horz(ctx, itoggle, iv, jv, kv) bind(C, name="a3g_advect_horz")
+          import :: c_int, c_int32_t, c_ptr
+          type(c_ptr), value :: ctx
+          integer(c_int32_t), value :: itoggle, iv, jv, kv
+        end function
+        integer(c_int) function a3g_advect_vert(ctx) bind(C, name="a3g_advect_vert")
+          import :: c_int, c_ptr
+          type(c_ptr), value :: ctx
+        end function
+        integer(c_int) function a3g_diffuse_horz(ctx, itime) bind(C, name="a3g_diffuse_horz")
+          import :: c_int, c_int32_t, c_ptr
+          type(c_ptr), value :: ctx
+          integer(c_int32_t), value :: itime
+        end function
+        integer(c_int) function a3g_diffuse_vert(ctx) bind(C, name="a3g_diffuse_vert")
+          import :: c_int, c_ptr
+          type(c_ptr), value :: ctx
+        end function
+        integer(c_int) function a3g_adjust_dt(ctx, time, nwt, simtime, dt) bind(C, name="a3g_adjust_dt")
+          import :: c_int, c_ptr, c_double
+          type(c_ptr), value :: ctx
+          real(c_double), value :: time, nwt, simtime
+          real(c_double), intent(out) :: dt
+        end function
+        integer(c_int) function a3g_timestep_totals(ctx, out4, mass) bind(C, name="a3g_timestep_totals")
+          import :: c_int, c_ptr
+          type(c_ptr), value :: ctx, out4, mass
+        end function
+        integer(c_int) function a3g_get_subgrid(ctx, box) bind(C, name="a3g_get_subgrid")
+          import :: c_int, c_ptr
+          type(c_ptr), value :: ctx, box
+        end function
+      end interface
+
+      contains
+
+      !------------------------------------------------------------------------
+      ! Maps a nonzero library status to the reference's errlog + stop 1.
+      subroutine B200_Check(rc, where)
+        use io_units
+        integer(c_int), intent(in) :: rc
+        character(len=*), intent(in) :: where
+        character(kind=c_char), pointer :: msg(:)
+        integer :: n
+        if (rc .eq. 0) return
+        call c_f_pointer(a3g_last_error(), msg, [512])
+        n = 0
+        do while (n .lt. 512)
+          if (msg(n+1) .eq. c_null_char) exit
+          n = n + 1
+        enddo
+        do io=1,2;if(VB(io).le.verbosity_error)then
+          write(errlog(io),*)"ERROR (B200) in ", where, ": status ", rc, " ", msg(1:n)
+        endif;enddo
+        stop 1
+      end subroutine B200_Check
+
+      !------------------------------------------------------------------------
+      ! After alloc_arrays, calc_mesh_params and Allocate_Diff (src/Ash3d.F90:230-240).
+      subroutine B200_Init(device)
+        use global_param, only : CFL, DT_MIN, DT_MAX, useDiffusion, useCN, EPS_THRESH, EPS_SMALL
+        use mesh,         only : nxmax, nymax, nzmax, nsmax, IsPeriodic, IsLatLon, dx, dy, &
+                                 kappa_pd, sigma_nx_pd, sigma_ny_pd, sigma_nz_pd, dz_vec_pd, ZScaling_ID
+        use solution,     only : vf_pd
+        use Diffusion,    only : kx, ky, kz, Imp_fac, Imp_DT_fac
+        use Output_Vars,  only : CLOUDCON_GRID_THRESH
+        use Tephra,       only : MagmaDensity
+        integer, intent(in) :: device
+        type(a3g_grid_desc) :: g
+        type(a3g_params) :: p
+        g%nx = nxmax; g%ny = nymax; g%nz = nzmax; g%ns = nsmax
+        g%periodic = merge(1, 0, IsPeriodic); g%latlon = merge(1, 0, IsLatLon)
+        g%dx = dx; g%dy = dy
+        call a3g_default_params(p)
+        p%use_cn = merge(1, 0, useCN)
+        p%use_diffusion = merge(1, 0, useDiffusion)
+#ifdef FAST_SUBGRID
+        p%fast_subgrid = 1
+#endif
+        p%zscaling_id = ZScaling_ID
+        p%cfl = CFL; p%dt_min = DT_MIN; p%dt_max = DT_MAX
+        p%imp_fac = Imp_fac; p%imp_dt_fac = Imp_DT_fac; p%eps_thresh = EPS_THRESH
+        p%eps_small = EPS_SMALL; p%cloudcon_grid_thresh = CLOUDCON_GRID_THRESH
+        p%magma_density = MagmaDensity
+        call B200_Check(a3g_create(g, p, int(device, c_int), b200_ctx), "a3g_create")
+        call B200_Check(a3g_set_geometry(b200_ctx, c_loc(kappa_pd), c_loc(sigma_nx_pd), &
+                        c_loc(sigma_ny_pd), c_loc(sigma_nz_pd), c_loc(dz_vec_pd)), "a3g_set_geometry")
+        call B200_Check(a3g_set_diffusivity(b200_ctx, c_loc(kx), c_loc(ky), c_loc(kz)), "a3g_set_diffusivity")
+        call B200_Check(a3g_set_fall_velocity(b200_ctx, c_loc(vf_pd)), "a3g_set_fall_velocity")
+      end subroutine B200_Init
+
+      subroutine B200_Finalize
+        integer(c_int) :: rc
+        rc = a3g_destroy(b200_ctx)
+        b200_ctx = c_null_ptr
+      end subroutine B200_Finalize
+
+      ! concen_pd(:,:,:,:,ts0) and the outflow accumulators -> device
+      subroutine B200_Upload
+        use mesh,     only : ts0
+        use solution, only : concen_pd, outflow_yz1_pd, outflow_yz2_pd, outflow_xz1_pd, &
+                             outflow_xz2_pd, outflow_xy1_pd, outflow_xy2_pd
+        call B200_Check(a3g_upload_concen(b200_ctx, c_loc(concen_pd(-1,-1,-1,1,ts0))), "a3g_upload_concen")
+        call B200_Check(a3g_upload_outflow(b200_ctx, c_loc(outflow_yz1_pd), c_loc(outflow_yz2_pd), &
+                        c_loc(outflow_xz1_pd), c_loc(outflow_xz2_pd), c_loc(outflow_xy1_pd), &
+                        c_loc(outflow_xy2_pd)), "a3g_upload_outflow")
+      end subroutine B200_Upload
+
+      ! device -> concen_pd(ts0) and ts1 (the state after the step), outflows, deposit
+      subroutine B200_Download
+        use mesh,     only : ts0, ts1
+        use solution, only : concen_pd, outflow_yz1_pd, outflow_yz2_pd, outflow_xz1_pd, &
+                             outflow_xz2_pd, outflow_xy1_pd, outflow_xy2_pd, DepositGranularity
+        call B200_Check(a3g_download_concen(b200_ctx, c_loc(concen_pd(-1,-1,-1,1,ts1))), "a3g_download_concen")
+        concen_pd(:,:,:,:,ts0) = concen_pd(:,:,:,:,ts1)
+        call B200_Check(a3g_download_outflow(b200_ctx, c_loc(outflow_yz1_pd), c_loc(outflow_yz2_pd), &
+                        c_loc(outflow_xz1_pd), c_loc(outflow_xz2_pd), c_loc(outflow_xy1_pd), &
+                        c_loc(outflow_xy2_pd), c_loc(DepositGranularity)), "a3g_download_outflow")
+      end subroutine B200_Download
+
+      ! replaces the two full-array copies of src/Ash3d.F90:376-378
+      subroutine B200_StepPrologue
+        call B200_Check(a3g_step_prologue(b200_ctx), "a3g_step_prologue")
+      end subroutine B200_StepPrologue
+
+      ! replaces the vent-column update of src/Ash3d.F90:428-431
+      subroutine B200_AddSource
+        use mesh,      only : ivent, jvent
+        use Source,    only : SourceNodeFlux
+        use time_data, only : dt
+        call B200_Check(a3g_add_source_column(b200_ctx, int(ivent, c_int32_t), int(jvent, c_int32_t), &
+                        c_loc(SourceNodeFlux), real(dt, c_double)), "a3g_add_source_column")
+      end subroutine B200_AddSource
+
+      ! host-interpolated FP64 winds (MesoInterpolater left unchanged)
+      subroutine B200_SetWinds
+        use solution, only : vx_pd, vy_pd, vz_pd
+        call B200_Check(a3g_set_winds(b200_ctx, c_loc(vx_pd), c_loc(vy_pd), c_loc(vz_pd)), "a3g_set_winds")
+      end subroutine B200_SetWinds
+
+      ! device interpolation: upload the bracketing FP32 met steps once per met step ...
+      subroutine B200_SetMetSteps
+        use wind_grid, only : vx_meso_last_step_sp, vy_meso_last_step_sp, vz_meso_last_step_sp, &
+                              vx_meso_next_step_sp, vy_meso_next_step_sp, vz_meso_next_step_sp
+        call B200_Check(a3g_set_met_steps(b200_ctx, c_loc(vx_meso_last_step_sp), c_loc(vy_meso_last_step_sp), &
+                        c_loc(vz_meso_last_step_sp), c_loc(vx_meso_next_step_sp), &
+                        c_loc(vy_meso_next_step_sp), c_loc(vz_meso_next_step_sp)), "a3g_set_met_steps")
+      end subroutine B200_SetMetSteps
+
+      ! ... and interpolate on the device every step (src/MesoInterpolater.f90:207-223)
+      subroutine B200_InterpWinds(frac)
+        real(kind=8), intent(in) :: frac
+        call B200_Check(a3g_interp_winds(b200_ctx, real(frac, c_double)), "a3g_interp_winds")
+      end subroutine B200_InterpWinds
+
+      end module B200_Transport
+
+!##############################################################################
+! Drop-in replacements with the reference's names and signatures
+!##############################################################################
+
+      module AdvectionHorz
+      use iso_c_binding
+      use B200_Transport
+      implicit none
+      private
+      public AdvectHorz
+      contains
+      subroutine AdvectHorz(itoggle)
+        use mesh, only : ivent, jvent, kvent
+        integer, intent(in) :: itoggle
+        call B200_Check(a3g_advect_horz(b200_ctx, int(itoggle, c_int32_t), int(ivent, c_int32_t), &
+                        int(jvent, c_int32_t), int(kvent, c_int32_t)), "AdvectHorz")
+      end subroutine AdvectHorz
+      end module AdvectionHorz
+
+      module AdvectionVert_DCU
+      use iso_c_binding
+      use B200_Transport
+      implicit none
+      private
+      public AdvectVert
+      contains
+      subroutine AdvectVert
+        call B200_Check(a3g_advect_vert(b200_ctx), "AdvectVert")
+      end subroutine AdvectVert
+      end module AdvectionVert_DCU
+
+      module Diffusion
+      use iso_c_binding
+      use B200_Transport
+      implicit none
+      private
+      public Allocate_Diff, Deallocate_Diff, DiffuseHorz, DiffuseVert
+      real(kind=8), public :: diffusivity_horz, diffusivity_vert
+      real(kind=8), public :: Imp_fac = 0.5d0
+      real(kind=8), public :: Imp_DT_fac = 4.0d0
+      real(kind=8), dimension(:,:,:), pointer, public :: kx => null(), ky => null(), kz => null()
+      contains
+      subroutine Allocate_Diff   ! src/Diffusion.F90:83-104
+        use mesh, only : nxmax, nymax, nzmax
+        if(.not.associated(kx))allocate(kx(0:nxmax+1,0:nymax+1,0:nzmax+1)); kx = diffusivity_horz
+        if(.not.associated(ky))allocate(ky(0:nxmax+1,0:nymax+1,0:nzmax+1)); ky = diffusivity_horz
+        if(.not.associated(kz))allocate(kz(0:nxmax+1,0:nymax+1,0:nzmax+1)); kz = diffusivity_vert
+      end subroutine Allocate_Diff
+      subroutine Deallocate_Diff
+        if(associated(kx)) deallocate(kx)
+        if(associated(ky)) deallocate(ky)
+        if(associated(kz)) deallocate(kz)
+      end subroutine Deallocate_Diff
+      subroutine DiffuseHorz(i)
+        integer :: i
+        call B200_Check(a3g_diffuse_horz(b200_ctx, int(i, c_int32_t)), "DiffuseHorz")
+      end subroutine DiffuseHorz
+      subroutine DiffuseVert
+        call B200_Check(a3g_diffuse_vert(b200_ctx), "DiffuseVert")
+      end subroutine DiffuseVert
+      end module Diffusion
+
+      subroutine Set_BC(bc_code)
+        use iso_c_binding
+        use B200_Transport
+        integer, intent(in) :: bc_code
+        call B200_Check(a3g_set_bc(b200_ctx, int(bc_code, c_int32_t)), "Set_BC")
+      end subroutine Set_BC
+
+      subroutine Adjust_DT(mesostep)
+        use iso_c_binding
+        use B200_Transport
+        use io_data,   only : NextWriteTime
+        use time_data, only : time, dt, dt_ip, dt_meso_next, Simtime_in_hours
+        logical, intent(in), optional :: mesostep
+        real(c_double) :: dtn
+        ! FAST_DT's met-step estimate (mesostep=.true.) uses the same device maxima
+        call B200_Check(a3g_adjust_dt(b200_ctx, real(time, c_double), real(NextWriteTime, c_double), &
+                        real(Simtime_in_hours, c_double), dtn), "Adjust_DT")
+        dt = dtn
+        dt_ip = dtn
+        if (present(mesostep)) then
+          if (mesostep) dt_meso_next = dt
+        endif
+      end subroutine Adjust_DT
+
+      subroutine TimeStepTotals(itime)
+        use iso_c_binding
+        use B200_Transport
+        use solution, only : aloft_vol, dep_vol, outflow_vol, tot_vol, mass_aloft
+        integer, intent(in) :: itime
+        real(c_double), target :: out4(4)
+        call B200_Check(a3g_timestep_totals(b200_ctx, c_loc(out4), c_loc(mass_aloft)), "TimeStepTotals")
+        aloft_vol = out4(1); dep_vol = out4(2); outflow_vol = out4(3); tot_vol = out4(4)
+      end subroutine TimeStepTotals
