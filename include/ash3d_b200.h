@@ -225,9 +225,11 @@ int a3g_kernel_timing(a3g_ctx *ctx, int32_t enable);
 int a3g_kernel_times(a3g_ctx *ctx, double *ms, uint64_t *count);
 
 /* ---- tuning (no counterpart in the reference) ---- */
-/* Selects the kernel variant of the advection sweep along dir (0 x, 1 y,
- * 2 z): 0 marching threads, 1 blocks of 4 cells, 2 blocks of 8 cells.  All
- * variants produce identical results; only their speed differs. */
+/* Selects a kernel variant.  dir 0, 1, 2: the advection sweep along x, y, z,
+ * variant 0 marching threads, 1 blocks of 4 cells, 2 blocks of 8 cells.
+ * dir 3: the Crank-Nicolson x solve, variant 0 warp-tiled (default), 1 one
+ * thread per line.  All variants produce identical results; only their speed
+ * differs. */
 int a3g_set_variant(a3g_ctx *ctx, int32_t dir, int32_t variant);
 int a3g_get_variant(a3g_ctx *ctx, int32_t dir, int32_t *variant);
 

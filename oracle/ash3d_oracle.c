@@ -953,3 +953,337 @@ void orc_prune_gs(orc_state *s, double airborne_thresh) {
   }
   s->n_gs_aloft = naloft;
 }
+
+/* ======================================================================== */
+/* Discrete adjoint of the transport step (no counterpart in the reference). */
+/*                                                                          */
+/* Each sweep is piecewise linear in the concentration: with the limiter    */
+/* branches fixed by the state the sweep was applied to, the limited slope   */
+/* ldq is a*dq + b*dqu (a, b constants of the branch), so the sweep is a     */
+/* linear map J(c) and these routines apply its transpose J(c)^T to lam (the */
+/* adjoint of the sweep's output), in place.  They are written as the        */
+/* reverse of the forward statements (hand reverse mode): the forward state  */
+/* must be in concen(:,:,:,:,ts0) (the sweep's input), the box must be the   */
+/* full grid (the subgrid box depends on the state), and lam has the shape   */
+/* of one concentration level (ghosts ignored, left zero).  Ghost values     */
+/* written by Set_BC(1) are zero (their adjoint is dropped) except x-        */
+/* periodic wraps, whose adjoint goes back to the wrapped cells; Neumann     */
+/* ghosts of the diffusion sweeps go back to the edge cells.  Grains that    */
+/* are not aloft are zeroed by every sweep, so their adjoint is zero.        */
+/* ======================================================================== */
+
+/* Coefficients of the frozen limiter branch: d(ldq) = a*d(dq) + b*d(dqu).    */
+/* Ties between branches follow the forward fmx/fmn selection.               */
+void orc_lim_coef(int lim, double dq, double dqu, double eps, double *a, double *b) {
+  if (lim == ORC_LIM_LAXWEN) { *a = 1.0; *b = 0.0; return; }
+  if (lim == ORC_LIM_BW) { *a = 0.0; *b = 1.0; return; }
+  const int clamp = fabs(dqu) > 3.0 * fabs(dq) || fabs(dq) < eps;
+  const double th = clamp ? copysign(3.0, dqu * dq) : dqu / dq;
+  double phi, dphi;
+  switch (lim) {
+    case ORC_LIM_FROMM:
+      phi = 0.5 * (1.0 + th); dphi = 0.5; break;
+    case ORC_LIM_MINMOD: {
+      double m = fmn(1.0, th), dm = (1.0 < th) ? 0.0 : 1.0;
+      phi = fmx(0.0, m); dphi = (0.0 > m) ? 0.0 : dm; break;
+    }
+    case ORC_LIM_MC: {
+      double m1 = fmn((1.0 + th) / 2.0, 2.0), dm1 = ((1.0 + th) / 2.0 < 2.0) ? 0.5 : 0.0;
+      double m2 = fmn(m1, 2.0 * th), dm2 = (m1 < 2.0 * th) ? dm1 : 2.0;
+      phi = fmx(0.0, m2); dphi = (0.0 > m2) ? 0.0 : dm2; break;
+    }
+    case ORC_LIM_SUPERBEE:
+    default: {
+      double m1 = fmn(1.0, 2.0 * th), dm1 = (1.0 < 2.0 * th) ? 0.0 : 2.0;
+      double a1 = fmx(0.0, m1), da1 = (0.0 > m1) ? 0.0 : dm1;
+      double m2 = fmn(2.0, th), dm2 = (2.0 < th) ? 0.0 : 1.0;
+      phi = fmx(a1, m2); dphi = (a1 > m2) ? da1 : dm2; break;
+    }
+  }
+  if (clamp) dphi = 0.0;
+  *a = phi - th * dphi;
+  *b = dphi;
+}
+
+/* Reverse of dcu_row: lu[i] (i = rmin-1..rmax+1) is the adjoint of upd[i];
+ * adds the adjoint of q[i] (i = rmin-2..rmax+2) into lq.  r->q, vel, sig,
+ * kap hold the forward row. */
+static void adj_dcu_row(const orc_state *s, row_scratch *r, int len, int rmin, int rmax,
+                        const double *lu, double *lq) {
+  const double dt = s->dt, eps = s->eps_thresh;
+  double *q = r->q, *vel = r->vel, *sig = r->sig, *kap = r->kap;
+  double *dtv = r->dtv, *usig = r->usig, *dq = r->dq;
+  double *lfsl = r->fsl, *lfsr = r->fsr, *lfss = r->fss, *ldq = r->upd;  /* reused as adjoints */
+  for (int i = rmin - 2; i <= rmax + 2; i++) dtv[i] = dt / kap[i];
+  for (int i = -1; i <= len + 2; i++) usig[i] = 0.0;
+  for (int I = rmin - 1; I <= rmax + 1; I++) usig[I] = 0.5 * (vel[I - 1] + vel[I]) * sig[I];
+  for (int I = rmin - 1; I <= rmax + 2; I++) dq[I] = q[I] - q[I - 1];
+  for (int I = rmin - 1; I <= rmax + 2; I++) { lfsl[I] = 0.0; lfsr[I] = 0.0; lfss[I] = 0.0; ldq[I] = 0.0; }
+  /* upd[i] = -(dtv[i]*(fsl[i+1] + fsr[i] + fss[i+1] - fss[i])) */
+  for (int i = rmin - 1; i <= rmax + 1; i++) {
+    const double t = -(dtv[i] * lu[i]);
+    lfsl[i + 1] += t; lfsr[i] += t; lfss[i + 1] += t; lfss[i] -= t;
+  }
+  /* fsr[I] = max(0,u)dq[I] + q[I]divu_m; fsl[I] = min(0,u)dq[I] + q[I-1]divu_p */
+  for (int I = rmin - 1; I <= rmax + 1; I++) {
+    const double divu_p = fmx(0.0, usig[I]) - fmx(0.0, usig[I - 1]);
+    const double divu_m = fmn(0.0, usig[I + 1]) - fmn(0.0, usig[I]);
+    ldq[I] += fmx(0.0, usig[I]) * lfsr[I] + fmn(0.0, usig[I]) * lfsl[I];
+    lq[I] += divu_m * lfsr[I];
+    lq[I - 1] += divu_p * lfsl[I];
+  }
+  /* fss[I] = w*(a*dq[I] + b*dqu) */
+  if (s->limiter != ORC_LIM_NONE) {
+    for (int I = rmin; I <= rmax + 1; I++) {
+      if (!s->nocycle && fabs(dq[I]) <= eps) continue;
+      const int up = usig[I] > 0.0 ? I - 1 : I + 1;
+      double a, b;
+      orc_lim_coef(s->limiter, dq[I], dq[up], eps, &a, &b);
+      const double aus = fabs(usig[I]);
+      const double w = 0.5 * aus * (1.0 - dtv[I] * aus);
+      ldq[I] += w * a * lfss[I];
+      ldq[up] += w * b * lfss[I];
+    }
+  }
+  /* dq[I] = q[I] - q[I-1] */
+  for (int I = rmin - 1; I <= rmax + 2; I++) { lq[I] += ldq[I]; lq[I - 1] -= ldq[I]; }
+}
+
+static size_t lv(const orc_state *s, int i, int j, int k, int n) { return c5(s, i, j, k, n, 0); }
+
+void orc_adj_advect_x(orc_state *s, double *lam) {
+  orc_set_bc(s, 1);
+  const int rmin = s->imin, rmax = s->imax, nx = s->nx;
+  const int nth = orc_get_threads();
+  for (int n = 1; n <= s->ns; n++) {
+    if (!s->is_aloft[n - 1]) {
+      for (int k = 1; k <= s->nz; k++) for (int j = 1; j <= s->ny; j++) for (int i = 1; i <= nx; i++)
+        lam[lv(s, i, j, k, n)] = 0.0;
+      continue;
+    }
+#pragma omp parallel num_threads(nth)
+    {
+      row_scratch r; row_alloc(&r, nx);
+      double *lu = (double *)calloc(nx + 6, sizeof(double)) + 2;
+      double *lq = (double *)calloc(nx + 6, sizeof(double)) + 2;
+#pragma omp for collapse(2) schedule(static)
+      for (int k = s->kmin; k <= s->kmax; k++)
+        for (int j = s->jmin; j <= s->jmax; j++) {
+          for (int i = rmin - 2; i <= rmax + 2; i++) {
+            r.q[i] = s->concen[c5(s, i, j, k, n, 0)];
+            r.vel[i] = s->vx[i3(s, i, j, k)];
+            r.sig[i] = s->sig_nx[i3(s, i, j, k)];
+            r.kap[i] = s->kappa[i3(s, i, j, k)];
+            lq[i] = 0.0;
+          }
+          lu[rmin - 1] = 0.0; lu[rmax + 1] = 0.0;  /* outflows are not observed */
+          for (int i = rmin; i <= rmax; i++) lu[i] = lam[lv(s, i, j, k, n)];
+          adj_dcu_row(s, &r, nx, rmin, rmax, lu, lq);
+          for (int i = rmin; i <= rmax; i++) lq[i] += lu[i];  /* out = q + upd */
+          if (s->periodic) {  /* Set_BC(1) wraps */
+            lq[nx - 1] += lq[-1]; lq[nx] += lq[0]; lq[1] += lq[nx + 1]; lq[2] += lq[nx + 2];
+          }
+          for (int i = 1; i <= nx; i++) lam[lv(s, i, j, k, n)] = lq[i];
+        }
+      free(r.mem); free(lu - 2); free(lq - 2);
+    }
+  }
+}
+
+void orc_adj_advect_y(orc_state *s, double *lam) {
+  orc_set_bc(s, 1);
+  const int rmin = s->jmin, rmax = s->jmax, ny = s->ny;
+  const int nth = orc_get_threads();
+  for (int n = 1; n <= s->ns; n++) {
+    if (!s->is_aloft[n - 1]) {
+      for (int k = 1; k <= s->nz; k++) for (int j = 1; j <= ny; j++) for (int i = 1; i <= s->nx; i++)
+        lam[lv(s, i, j, k, n)] = 0.0;
+      continue;
+    }
+#pragma omp parallel num_threads(nth)
+    {
+      row_scratch r; row_alloc(&r, ny);
+      double *lu = (double *)calloc(ny + 6, sizeof(double)) + 2;
+      double *lq = (double *)calloc(ny + 6, sizeof(double)) + 2;
+#pragma omp for collapse(2) schedule(static)
+      for (int k = s->kmin; k <= s->kmax; k++)
+        for (int i = s->imin; i <= s->imax; i++) {
+          for (int j = rmin - 2; j <= rmax + 2; j++) {
+            r.q[j] = s->concen[c5(s, i, j, k, n, 0)];
+            r.vel[j] = s->vy[i3(s, i, j, k)];
+            r.sig[j] = s->sig_ny[i3(s, i, j, k)];
+            r.kap[j] = s->kappa[i3(s, i, j, k)];
+            lq[j] = 0.0;
+          }
+          lu[rmin - 1] = 0.0; lu[rmax + 1] = 0.0;
+          for (int j = rmin; j <= rmax; j++) lu[j] = lam[lv(s, i, j, k, n)];
+          adj_dcu_row(s, &r, ny, rmin, rmax, lu, lq);
+          for (int j = rmin; j <= rmax; j++) lq[j] += lu[j];
+          for (int j = 1; j <= ny; j++) lam[lv(s, i, j, k, n)] = lq[j];
+        }
+      free(r.mem); free(lu - 2); free(lq - 2);
+    }
+  }
+}
+
+/* lam_dep: adjoint of DepositGranularity = outflow_xy1 (nx,ny,ns), which
+ * accumulates upd(0) of every z column (src/AdvectionVert_DCU.f90:306-308,321);
+ * NULL for none. */
+void orc_adj_advect_z(orc_state *s, double *lam, const double *lam_dep) {
+  orc_set_bc(s, 1);
+  const int rmin = s->kmin, rmax = s->kmax, nz = s->nz;
+  const int nth = orc_get_threads();
+  for (int n = 1; n <= s->ns; n++) {
+    if (!s->is_aloft[n - 1]) {
+      for (int k = 1; k <= nz; k++) for (int j = 1; j <= s->ny; j++) for (int i = 1; i <= s->nx; i++)
+        lam[lv(s, i, j, k, n)] = 0.0;
+      continue;
+    }
+#pragma omp parallel num_threads(nth)
+    {
+      row_scratch r; row_alloc(&r, nz);
+      double *lu = (double *)calloc(nz + 6, sizeof(double)) + 2;
+      double *lq = (double *)calloc(nz + 6, sizeof(double)) + 2;
+#pragma omp for collapse(2) schedule(static)
+      for (int j = s->jmin; j <= s->jmax; j++)
+        for (int i = s->imin; i <= s->imax; i++) {
+          for (int k = rmin - 2; k <= rmax + 2; k++) {
+            r.q[k] = s->concen[c5(s, i, j, k, n, 0)];
+            r.vel[k] = s->vz[i3(s, i, j, k)] + s->vh[i3(s, i, j, k)] + s->vf[v4(s, i, j, k, n)];
+            r.sig[k] = s->sig_nz[i3(s, i, j, k)];
+            r.kap[k] = s->kappa[i3(s, i, j, k)];
+            lq[k] = 0.0;
+          }
+          lu[rmin - 1] = (lam_dep && rmin == 1) ? lam_dep[dep(s, i, j, n)] : 0.0;
+          lu[rmax + 1] = 0.0;
+          for (int k = rmin; k <= rmax; k++) lu[k] = lam[lv(s, i, j, k, n)];
+          adj_dcu_row(s, &r, nz, rmin, rmax, lu, lq);
+          for (int k = rmin; k <= rmax; k++) lq[k] += lu[k];
+          for (int k = 1; k <= nz; k++) lam[lv(s, i, j, k, n)] = lq[k];
+        }
+      free(r.mem); free(lu - 2); free(lq - 2);
+    }
+  }
+}
+
+/* Explicit diffusion: out[l] = q[l] + cR_l (q[l+1]-q[l]) - cL_l (q[l]-q[l-1])
+ * with cR_l = dt*kdsR*(sig[l+1]/kap[l]), cL_l = dt*kdsL*(sig[l]/kap[l]) and
+ * Neumann ghosts (periodic in x). */
+static void adj_diff_row(double dt, int n, int periodic, const double *kap, const double *sig,
+                         const double *kk, const double *lo, double *lq) {
+  for (int l = 0; l <= n + 1; l++) lq[l] = 0.0;
+  for (int l = 1; l <= n; l++) {
+    const double dsR = 2.0 * sig[l + 1] / (kap[l] + kap[l + 1]);
+    const double kdsR = 0.5 * (kk[l] + kk[l + 1]) * dsR;
+    const double dsL = 2.0 * sig[l] / (kap[l - 1] + kap[l]);
+    const double kdsL = 0.5 * (kk[l - 1] + kk[l]) * dsL;
+    const double cR = dt * kdsR * (sig[l + 1] / kap[l]);
+    const double cL = dt * kdsL * (sig[l] / kap[l]);
+    lq[l] += lo[l] - cR * lo[l] - cL * lo[l];
+    lq[l + 1] += cR * lo[l];
+    lq[l - 1] += cL * lo[l];
+  }
+  if (periodic) { lq[n] += lq[0]; lq[1] += lq[n + 1]; }
+  else { lq[1] += lq[0]; lq[n] += lq[n + 1]; }
+}
+
+static void adj_diff_dir(orc_state *s, double *lam, int dir) {
+  const int nx = s->nx, ny = s->ny, nz = s->nz;
+  const int n = dir == 0 ? nx : dir == 1 ? ny : nz;
+  const int na = dir == 0 ? ny : nx, nb = dir == 2 ? ny : nz;
+  double *buf = (double *)calloc(6 * (size_t)(n + 4), sizeof(double));
+  double *kap = buf + 1, *sig = kap + (n + 4), *kk = sig + (n + 4), *lo = kk + (n + 4), *lq = lo + (n + 4);
+  for (int g = 1; g <= s->ns; g++)
+    for (int b = 1; b <= nb; b++)
+      for (int a = 1; a <= na; a++) {
+        for (int l = 0; l <= n + 1; l++) {
+          const int i = dir == 0 ? l : a, j = dir == 1 ? l : (dir == 0 ? a : b), k = dir == 2 ? l : b;
+          kap[l] = s->kappa[i3(s, i, j, k)];
+          sig[l] = (dir == 0 ? s->sig_nx : dir == 1 ? s->sig_ny : s->sig_nz)[i3(s, i, j, k)];
+          kk[l] = (dir == 0 ? s->kx : dir == 1 ? s->ky : s->kz)[k3(s, i, j, k)];
+          lo[l] = (l >= 1 && l <= n && s->is_aloft[g - 1]) ? lam[lv(s, i, j, k, g)] : 0.0;
+        }
+        adj_diff_row(s->dt, n, dir == 0 && s->periodic, kap, sig, kk, lo, lq);
+        for (int l = 1; l <= n; l++) {
+          const int i = dir == 0 ? l : a, j = dir == 1 ? l : (dir == 0 ? a : b), k = dir == 2 ? l : b;
+          lam[lv(s, i, j, k, g)] = lq[l];
+        }
+      }
+  free(buf);
+}
+
+/* Crank-Nicolson: out = M^-1 N q with M = (DL, D, DU) and N the explicit
+ * half (Neumann rows).  Adjoint: solve M^T y = lam (dgtsv on the transposed
+ * diagonals), then lam_q = N^T y. */
+static void adj_cn_dir(orc_state *s, double *lam, int dir) {
+  const int nx = s->nx, ny = s->ny, nz = s->nz;
+  const int n = dir == 0 ? nx : dir == 1 ? ny : nz;
+  if (n <= 1) return;  /* the forward sweep leaves ts0 unchanged (:770) */
+  const int na = dir == 0 ? ny : nx, nb = dir == 2 ? ny : nz;
+  const double dt = s->dt, imp = s->imp_fac;
+  double *buf = (double *)calloc(12 * (size_t)(n + 4), sizeof(double));
+  double *kap = buf + 1, *sig = kap + (n + 4), *kk = sig + (n + 4);
+  double *DL = kk + (n + 4), *D = DL + (n + 4), *DU = D + (n + 4);
+  double *CL = DU + (n + 4), *CC = CL + (n + 4), *CR = CC + (n + 4), *y = CR + (n + 4);
+  double *lq = y + (n + 4);
+  for (int g = 1; g <= s->ns; g++)
+    for (int b = 1; b <= nb; b++)
+      for (int a = 1; a <= na; a++) {
+        for (int l = 0; l <= n + 1; l++) {
+          const int i = dir == 0 ? l : a, j = dir == 1 ? l : (dir == 0 ? a : b), k = dir == 2 ? l : b;
+          kap[l] = s->kappa[i3(s, i, j, k)];
+          sig[l] = (dir == 0 ? s->sig_nx : dir == 1 ? s->sig_ny : s->sig_nz)[i3(s, i, j, k)];
+          kk[l] = (dir == 0 ? s->kx : dir == 1 ? s->ky : s->kz)[k3(s, i, j, k)];
+        }
+        for (int l = 1; l <= n; l++) {
+          const double vavgL = 0.5 * (kap[l - 1] + kap[l]), kavgL = 0.5 * (kk[l - 1] + kk[l]);
+          const double kdsL = kavgL * (sig[l] / vavgL);
+          const double vavgR = 0.5 * (kap[l] + kap[l + 1]), kavgR = 0.5 * (kk[l] + kk[l + 1]);
+          const double kdsR = kavgR * (sig[l + 1] / vavgR);
+          const double Lf = dt * kdsL * sig[l] / kap[l], Rf = dt * kdsR * sig[l + 1] / kap[l];
+          const double Cf = Lf + Rf;
+          const int r = l - 1;
+          D[r] = 1.0 + imp * Cf - (l == 1 ? imp * Lf : 0.0) - (l == n ? imp * Rf : 0.0);
+          if (l < n) DU[r] = -(imp * Rf);   /* M(r, r+1) */
+          if (l > 1) DL[r - 1] = -(imp * Lf);  /* M(r, r-1) */
+          CL[r] = (1.0 - imp) * Lf; CC[r] = 1.0 - (1.0 - imp) * Cf; CR[r] = (1.0 - imp) * Rf;
+        }
+        for (int l = 1; l <= n; l++) {
+          const int i = dir == 0 ? l : a, j = dir == 1 ? l : (dir == 0 ? a : b), k = dir == 2 ? l : b;
+          y[l - 1] = s->is_aloft[g - 1] ? lam[lv(s, i, j, k, g)] : 0.0;
+        }
+        /* M^T: sub-diagonal DU, super-diagonal DL (dgtsv overwrites copies) */
+        {
+          double *dl2 = (double *)malloc(sizeof(double) * 3 * (size_t)n);
+          double *d2 = dl2 + n, *du2 = d2 + n;
+          for (int r = 0; r < n - 1; r++) { dl2[r] = DU[r]; du2[r] = DL[r]; }
+          for (int r = 0; r < n; r++) d2[r] = D[r];
+          (void)orc_dgtsv(n, dl2, d2, du2, y);
+          free(dl2);
+        }
+        /* N: row 0 = (CL0+CC0) q0 + CR0 q1; row n-1 = CL q(n-2) + (CC+CR) q(n-1) */
+        for (int r = 0; r < n; r++) lq[r] = 0.0;
+        for (int r = 0; r < n; r++) {
+          const int rm = r > 0 ? r - 1 : 0, rp = r < n - 1 ? r + 1 : n - 1;
+          lq[rm] += CL[r] * y[r];
+          lq[r] += CC[r] * y[r];
+          lq[rp] += CR[r] * y[r];
+        }
+        for (int l = 1; l <= n; l++) {
+          const int i = dir == 0 ? l : a, j = dir == 1 ? l : (dir == 0 ? a : b), k = dir == 2 ? l : b;
+          lam[lv(s, i, j, k, g)] = s->is_aloft[g - 1] ? lq[l - 1] : 0.0;
+        }
+      }
+  free(buf);
+}
+
+void orc_adj_diffuse_horz(orc_state *s, double *lam, int itime) {
+  /* forward: even x then y, odd y then x (src/Diffusion.F90:186-214) */
+  const int first = (itime % 2 == 0) ? 1 : 0, second = 1 - first;  /* reverse order */
+  if (s->use_cn) { adj_cn_dir(s, lam, first); adj_cn_dir(s, lam, second); }
+  else { adj_diff_dir(s, lam, first); adj_diff_dir(s, lam, second); }
+}
+
+void orc_adj_diffuse_vert(orc_state *s, double *lam) {
+  if (s->use_cn) adj_cn_dir(s, lam, 2); else adj_diff_dir(s, lam, 2);
+}

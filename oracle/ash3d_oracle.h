@@ -128,6 +128,17 @@ void orc_prune_gs(orc_state *s, double airborne_thresh);
  * published algorithm: Gaussian elimination with partial pivoting of a
  * tridiagonal matrix, then back substitution).  Returns LAPACK's INFO. */
 int  orc_dgtsv(int n, double *dl, double *d, double *du, double *b);
+/* Discrete adjoint (no counterpart in the reference).  Each routine applies
+ * the transpose of one sweep's Jacobian, with the limiter branches fixed by
+ * the forward state in concen(:,:,:,:,ts0), to lam (one level, shaped like
+ * concen(:,:,:,:,ts0)) in place.  Full box only.  lam_dep: adjoint of
+ * DepositGranularity (nx,ny,ns) or NULL. */
+void orc_lim_coef(int lim, double dq, double dqu, double eps, double *a, double *b);
+void orc_adj_advect_x(orc_state *s, double *lam);
+void orc_adj_advect_y(orc_state *s, double *lam);
+void orc_adj_advect_z(orc_state *s, double *lam, const double *lam_dep);
+void orc_adj_diffuse_horz(orc_state *s, double *lam, int itime);
+void orc_adj_diffuse_vert(orc_state *s, double *lam);
 /* OpenMP thread count for the advection rows (<=0: runtime default). */
 void orc_set_threads(int n);
 int  orc_get_threads(void);

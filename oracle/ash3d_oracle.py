@@ -83,6 +83,9 @@ def load() -> C.CDLL:
             ("orc_prune_gs", None, [S, C.c_double]),
             ("orc_dgtsv", C.c_int, [C.c_int, D, D, D, D]),
             ("orc_set_threads", None, [C.c_int]), ("orc_get_threads", C.c_int, []),
+            ("orc_adj_advect_x", None, [S, D]), ("orc_adj_advect_y", None, [S, D]),
+            ("orc_adj_advect_z", None, [S, D, D]),
+            ("orc_adj_diffuse_horz", None, [S, D, C.c_int]), ("orc_adj_diffuse_vert", None, [S, D]),
         ]:
             fn = getattr(lib, name)
             fn.restype = res
@@ -256,6 +259,50 @@ class OracleModel:
 
     def prune_gs(self, thresh=1.0e-3):
         self.lib.orc_prune_gs(self.ps, thresh)
+
+    # --- discrete adjoint (no counterpart in the reference) ------------------
+    # lam arrays are interior-shaped (nx, ny, nz, ns); each call applies the
+    # transpose of one sweep, linearised at the state now in ts0.
+    def _lam_in(self, lam):
+        c = self.cfg
+        w = np.zeros(self.concen.shape[:4], order="F")
+        w[2:c.nx + 2, 2:c.ny + 2, 2:c.nz + 2, :] = lam
+        return w
+
+    def _lam_out(self, w):
+        c = self.cfg
+        return w[2:c.nx + 2, 2:c.ny + 2, 2:c.nz + 2, :].copy(order="F")
+
+    def adj_advect_x(self, lam):
+        w = self._lam_in(lam)
+        self.lib.orc_adj_advect_x(self.ps, _d(w))
+        return self._lam_out(w)
+
+    def adj_advect_y(self, lam):
+        w = self._lam_in(lam)
+        self.lib.orc_adj_advect_y(self.ps, _d(w))
+        return self._lam_out(w)
+
+    def adj_advect_z(self, lam, lam_dep=None):
+        w = self._lam_in(lam)
+        ld = None if lam_dep is None else np.asfortranarray(lam_dep, dtype=np.float64)
+        self.lib.orc_adj_advect_z(self.ps, _d(w), None if ld is None else _d(ld))
+        return self._lam_out(w)
+
+    def adj_diffuse_horz(self, lam, itime):
+        w = self._lam_in(lam)
+        self.lib.orc_adj_diffuse_horz(self.ps, _d(w), itime)
+        return self._lam_out(w)
+
+    def adj_diffuse_vert(self, lam):
+        w = self._lam_in(lam)
+        self.lib.orc_adj_diffuse_vert(self.ps, _d(w))
+        return self._lam_out(w)
+
+    def zero_outflows(self):
+        for a in (self.out_yz1, self.out_yz2, self.out_xz1, self.out_xz2, self.out_xy1, self.out_xy2,
+                  self.deposit):
+            a[...] = 0.0
 
     # --- state access --------------------------------------------------------
     def interior(self):

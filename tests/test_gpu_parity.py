@@ -14,7 +14,7 @@ from gpu_common import pair, prime, random_state
 pytestmark = pytest.mark.gpu
 
 CONFIGS = ["tiny_proj", "tiny_cn", "tiny_latlon", "tiny_periodic", "tiny_subgrid", "tiny_wide",
-           "tiny_tall"]
+           "tiny_tall", "tiny_stretch"]
 OPS = ["advect_x", "advect_y", "AdvectVert", "DiffuseHorz_even", "DiffuseHorz_odd", "DiffuseVert"]
 
 
@@ -39,16 +39,28 @@ def _assert_outflows_equal(gpu, ref):
         assert np.array_equal(og[key], orf[key]), key
 
 
+ADVECTION = ("advect_x", "advect_y", "AdvectVert")
+
+
 def _variants(op):
-    return (0, 1, 2) if op in ("advect_x", "advect_y", "AdvectVert") else (0,)
+    # advection: march / block-4 / block-8; horizontal diffusion: the CN x
+    # solve warp-tiled / one thread per line
+    return (0, 1, 2) if op in ADVECTION else (0, 1) if op.startswith("DiffuseHorz") else (0,)
+
+
+def _set_variant(gpu, op, variant):
+    if op in ADVECTION:
+        for d in range(3):
+            gpu.set_variant(d, variant)
+    else:
+        gpu.set_variant(3, variant)
 
 
 @pytest.mark.parametrize("name", CONFIGS)
 @pytest.mark.parametrize("op,variant", [(o, v) for o in OPS for v in _variants(o)])
 def test_single_operator_bitwise(name, op, variant):
     cfg, gpu, ref = pair(name)
-    for d in range(3):
-        gpu.set_variant(d, variant)
+    _set_variant(gpu, op, variant)
     box = None
     if cfg.fast_subgrid:  # a strict sub-box: cells outside it must come back as zero
         box = (4, cfg.nx - 5, 3, cfg.ny - 4, 2, cfg.nz - 3)
@@ -107,6 +119,7 @@ def test_run_bitwise(name, variant):
     cfg, gpu, ref = pair(name)
     for d in range(3):
         gpu.set_variant(d, variant)
+    gpu.set_variant(3, variant % 2)
     sg = driver.run(gpu, cfg, max_steps=16)
     sr = driver.run(ref, cfg, max_steps=16)
     assert [h.dt for h in sg.history] == [h.dt for h in sr.history]

@@ -129,6 +129,7 @@ struct a3g_ctx {
   size_t bytes;
   // kernel variant per advection direction (0 march, 1 block V=4, 2 block V=8)
   int tune_advect[3];
+  int tune_cn_x;            // CN x solve: 0 warp-tiled, 1 one thread per line
   // optional per-kernel timing (a3g_kernel_timing)
   bool timing;
   std::vector<cudaEvent_t> ev_pool;

@@ -91,18 +91,54 @@ __global__ void __launch_bounds__(256) k_diff(Layout L, Box box, int periodic,
 // formed by exact_div.cuh's certified path.
 enum { CN_FACT = 0, CN_DP = 1, CN_DU = 2, CN_CL = 3, CN_CC = 4, CN_CR = 5, CN_RDP = 6, CN_NF = 7 };
 
+// Constant runs.  Along a line whose geometry and diffusivity do not change
+// (every x line of a lon/lat grid, every line of a projected grid with
+// uniform spacing) the interior rows of the matrix are identical, and the
+// elimination factors of dgtsv settle to a fixed point after a few rows, so
+// the table rows become bit-identical.  Per distinct line the table keeps the
+// run [lo, hi] of identical rows that ends at the last interior row
+// (hi = ncells-2): row lo is stored, rows lo+1..hi are not, and readers take
+// them from registers.  The values are the same bits either way.  The run
+// bounds follow the CN_NF fields: [2][U] doubles holding lo and hi.
+struct CnRun {
+  int lo, hi;
+  double v[CN_NF];
+};
+
+__device__ __forceinline__ void cn_load_run(const double *__restrict__ t, long F, long U,
+                                            const double *__restrict__ runs, long u, CnRun &R) {
+  R.lo = (int)runs[u];
+  R.hi = (int)runs[U + u];
+#pragma unroll
+  for (int f = 0; f < CN_NF; f++) R.v[f] = t[f * F + (long)R.lo * U];
+}
+
+// Field f of row l: from the run registers inside (lo, hi], else from the table.
+__device__ __forceinline__ double cn_coef(const double *__restrict__ t, long F, long U, const CnRun &R,
+                                          int f, int l) {
+  return (l > R.lo && l <= R.hi) ? R.v[f] : t[f * F + (long)l * U];
+}
+
 struct LineMap {  // distinct-line indexing for one sweep direction
   int na, nb;     // extents of the two fixed indices (a fastest)
   int da, db;     // 1 if the coefficients vary with a / b
   int U;          // number of distinct lines
-  __device__ __forceinline__ int u(int a, int b) const {
+  __host__ __device__ __forceinline__ int u(int a, int b) const {
     return (da ? a - 1 : 0) + (da ? na : 1) * (db ? b - 1 : 0);
   }
 };
 
+__device__ __forceinline__ bool same_bits(double a, double b) {
+  return __double_as_longlong(a) == __double_as_longlong(b);
+}
+
+// Only the x tables (read by the warp-tiled x solve) leave their final run
+// unstored; the y and z tables are written in full, because their solves
+// read every row.
 template <int DIR>
 __global__ void k_cn_table(Layout L, Box box, double imp, LineMap map, Geo3 sig, Geo3 kap, Geo3 kk,
                            DevScalars *sc, double *__restrict__ tab) {
+  constexpr bool COMPRESS = (DIR == 0);
   const int u = blockIdx.x * blockDim.x + threadIdx.x;
   if (u >= map.U) return;
   // representative fixed indices of this distinct line
@@ -119,10 +155,82 @@ __global__ void k_cn_table(Layout L, Box box, double imp, LineMap map, Geo3 sig,
   };
   const double dt = sc->dt;
   const long U = map.U;
+  const long F = (long)ncells * U;
+  auto put = [&](int l, const double *v) {
+#pragma unroll
+    for (int f = 0; f < CN_NF; f++) tab[f * F + (long)l * U + u] = v[f];
+  };
   double dp_prev = 0.0, du_prev = 0.0;
-  for (int l = 1; l <= ncells; l++) {
-    const int c = rmin - 1 + l;
+  double rv[CN_NF];   // first row of the current run
+  int s = 0;          // index of that row
+  bool cont = false;  // row l-1 repeated row l-2
+  double pin[8];      // inputs of row l-1
+  for (int l = 0; l < ncells - 1; l++) {
+    const int c = rmin + l;
+    const double in[8] = {G(kap, c - 1), G(kap, c), G(kap, c + 1), G(kk, c - 1),
+                          G(kk, c),      G(kk, c + 1), G(sig, c),   G(sig, c + 1)};
+    bool same_in = l >= 2;
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+      if (l >= 2) same_in = same_in && same_bits(in[e], pin[e]);
+      pin[e] = in[e];
+    }
+    // an interior row with the inputs and the carried (D', DU) of its
+    // predecessor repeats it: nothing to compute or store
+    if (cont && same_in) {
+      if (!COMPRESS) put(l, rv);
+      continue;
+    }
     // :794-801 and :809-811
+    const double vavgL = 0.5 * (in[0] + in[1]);
+    const double kavgL = 0.5 * (in[3] + in[4]);
+    const double dsL = in[6] / vavgL;
+    const double kdsL = kavgL * dsL;
+    const double vavgR = 0.5 * (in[1] + in[2]);
+    const double kavgR = 0.5 * (in[4] + in[5]);
+    const double dsR = in[7] / vavgR;
+    const double kdsR = kavgR * dsR;
+    const double Lf = dt * kdsL * in[6] / in[1];
+    const double Rf = dt * kdsR * in[7] / in[1];
+    const double Cf = Lf + Rf;
+    double D, DU = 0.0;
+    if (l == 0) {
+      D = 1.0 + imp * Cf - imp * Lf;
+      DU = -(imp * Rf);
+    } else {
+      D = 1.0 + imp * Cf;
+      DU = -(imp * Rf);
+    }
+    double fact = 0.0, Dp = D;
+    if (l > 0) {
+      const double DL = -(imp * Lf);  // DL_d(l-1)
+      if (!(fabs(dp_prev) >= fabs(DL)) || dp_prev == 0.0) raise_error(sc, A3G_ERR_PIVOT, l + 1);
+      fact = DL / dp_prev;
+      Dp = D - fact * du_prev;
+    }
+    const double v[CN_NF] = {fact, Dp, DU, (1.0 - imp) * Lf, 1.0 - (1.0 - imp) * Cf, (1.0 - imp) * Rf,
+                             1.0 / Dp};
+    bool same = l >= 1;
+#pragma unroll
+    for (int f = 0; f < CN_NF; f++) same = same && same_bits(v[f], rv[f]);
+    cont = same;
+    dp_prev = Dp;
+    du_prev = DU;
+    if (same) {
+      if (!COMPRESS) put(l, rv);
+      continue;
+    }
+    if (COMPRESS)
+      for (int m = s + 1; m < l; m++) put(m, rv);  // materialise the finished run
+    put(l, v);
+#pragma unroll
+    for (int f = 0; f < CN_NF; f++) rv[f] = v[f];
+    s = l;
+  }
+  // last row (always distinct: DU = 0); the run ending at ncells-2 stays unstored
+  {
+    const int l = ncells - 1;
+    const int c = rmin + l;
     const double vavgL = 0.5 * (G(kap, c - 1) + G(kap, c));
     const double kavgL = 0.5 * (G(kk, c - 1) + G(kk, c));
     const double dsL = G(sig, c) / vavgL;
@@ -134,38 +242,20 @@ __global__ void k_cn_table(Layout L, Box box, double imp, LineMap map, Geo3 sig,
     const double Lf = dt * kdsL * G(sig, c) / G(kap, c);
     const double Rf = dt * kdsR * G(sig, c + 1) / G(kap, c);
     const double Cf = Lf + Rf;
-    double D, DU = 0.0;
-    if (l == 1) {
-      D = 1.0 + imp * Cf - imp * Lf;
-      DU = -(imp * Rf);
-    } else if (l < ncells) {
-      D = 1.0 + imp * Cf;
-      DU = -(imp * Rf);
-    } else {
-      D = 1.0 + imp * Cf - imp * Rf;
-    }
-    double fact = 0.0, Dp = D;
-    if (l > 1) {
-      const double DL = -(imp * Lf);  // DL_d(l-1)
-      if (!(fabs(dp_prev) >= fabs(DL)) || dp_prev == 0.0) raise_error(sc, A3G_ERR_PIVOT, l);
-      fact = DL / dp_prev;
-      Dp = D - fact * du_prev;
-    }
-    const long o = (long)(l - 1) * U + u;
-    const long F = (long)ncells * U;
-    tab[CN_FACT * F + o] = fact;
-    tab[CN_DP * F + o] = Dp;
-    tab[CN_DU * F + o] = DU;
-    tab[CN_CL * F + o] = (1.0 - imp) * Lf;
-    tab[CN_CC * F + o] = 1.0 - (1.0 - imp) * Cf;
-    tab[CN_CR * F + o] = (1.0 - imp) * Rf;
-    tab[CN_RDP * F + o] = 1.0 / Dp;
-    dp_prev = Dp;
-    du_prev = DU;
+    const double D = 1.0 + imp * Cf - imp * Rf;
+    const double DL = -(imp * Lf);
+    if (!(fabs(dp_prev) >= fabs(DL)) || dp_prev == 0.0) raise_error(sc, A3G_ERR_PIVOT, l + 1);
+    const double fact = DL / dp_prev;
+    const double Dp = D - fact * du_prev;
+    if (Dp == 0.0) raise_error(sc, A3G_ERR_PIVOT, ncells);
+    const double v[CN_NF] = {fact, Dp, 0.0, (1.0 - imp) * Lf, 1.0 - (1.0 - imp) * Cf, (1.0 - imp) * Rf,
+                             1.0 / Dp};
+    put(l, v);
+    double *runs = tab + CN_NF * F;
+    runs[u] = (double)s;
+    runs[U + u] = (double)(ncells - 2);
   }
-  if (dp_prev == 0.0) raise_error(sc, A3G_ERR_PIVOT, ncells);
 }
-
 // Solve of one line (a, b) of grain g from the table.  The eliminated
 // right-hand side B' is written to the output line and read back by the back
 // substitution, which prefetches PF entries ahead (the loads cannot move
@@ -203,7 +293,13 @@ __device__ __forceinline__ void cn_line(const Layout &L, const Box &box, const L
   for (int c = rmax + 1; c <= n; c++) x[(long)(c - 1) * st] = 0.0;
   const long U = map.U;
   const long F = (long)ncells * U;
-  const double *t = tab + map.u(a, b);
+  const long u = map.u(a, b);
+  const double *t = tab + u;
+  CnRun R;
+  if (DIR == 0) cn_load_run(t, F, U, tab + CN_NF * F, u, R);
+  auto co = [&](int f, int l) {  // the y and z tables are stored in full
+    return (DIR == 0) ? cn_coef(t, F, U, R, f, l) : t[f * F + (long)l * U];
+  };
   const double *qq = q + (long)(rmin - 1) * st;  // cell rmin
   double *xx = x + (long)(rmin - 1) * st;
   // forward elimination with the right-hand side built on the fly, :813-851
@@ -213,9 +309,9 @@ __device__ __forceinline__ void cn_line(const Layout &L, const Box &box, const L
 #pragma unroll 4
   for (int l = 0; l < ncells; l++) {
     const double qp = (l + 1 < ncells) ? qq[(long)(l + 1) * st] : qc;  // BC_right_t0 = q(rmax)
-    const long o = (long)l * U;
-    const double B = t[CN_CL * F + o] * qm + t[CN_CC * F + o] * qc + t[CN_CR * F + o] * qp;
-    bp = (l == 0) ? B : B - t[CN_FACT * F + o] * bp;
+    const double B = co(CN_CL, l) * qm + co(CN_CC, l) * qc +
+                     co(CN_CR, l) * qp;
+    bp = (l == 0) ? B : B - co(CN_FACT, l) * bp;
     xx[(long)l * st] = bp;
     qm = qc;
     qc = qp;
@@ -233,9 +329,8 @@ __device__ __forceinline__ void cn_line(const Layout &L, const Box &box, const L
         const double b2 = ring[p];
         const int lp = l - PF;  // refill this slot for the next round
         ring[p] = (lp >= 0) ? xx[(long)lp * st] : 0.0;
-        const long o = (long)l * U;
-        const double num = (l == ncells - 1) ? b2 : b2 - t[CN_DU * F + o] * xn;
-        const double v = div_rn_rcp(num, t[CN_DP * F + o], t[CN_RDP * F + o]);
+        const double num = (l == ncells - 1) ? b2 : b2 - co(CN_DU, l) * xn;
+        const double v = div_rn_rcp(num, co(CN_DP, l), co(CN_RDP, l));
         xx[(long)l * st] = v;
         xn = v;
       }
@@ -245,7 +340,7 @@ __device__ __forceinline__ void cn_line(const Layout &L, const Box &box, const L
 
 // Solve kernel: one thread per line (a, b, grain), lines enumerated with a
 // fastest so that a warp holds neighbouring lines (neighbouring i for y and
-// z lines: coalesced; neighbouring rows for x lines).
+// z lines: coalesced loads and stores).
 template <int DIR>
 __global__ void __launch_bounds__(128) k_cn_solve(Layout L, Box box, LineMap map,
                                                   const double *__restrict__ cin,
@@ -262,6 +357,185 @@ __global__ void __launch_bounds__(128) k_cn_solve(Layout L, Box box, LineMap map
   const int b = (int)(r % nb) + 1;
   const int g = (int)(r / nb);
   cn_line<DIR>(L, box, map, cin, cout, tab, aloft, a, b, g);
+}
+
+// x lines, warp-tiled.  A warp owns 32 consecutive x rows (row r =
+// (g*nz + k-1)*ny + j-1 starts at r*P) and walks them in chunks of 32 cells
+// through a shared-memory tile: every global load and store of the
+// concentration is a coalesced 256-byte row segment, and each lane then runs
+// its own row's recurrence out of the tile.
+//   pass 1 (forward): the elimination of B' over the whole row, keeping only
+//     B' at the last cell of every chunk (a checkpoint, parked in the output
+//     row at that cell);
+//   pass 2 (backward, last chunk first): reload the chunk, recompute its B'
+//     from the checkpoint of the previous chunk (same operations, same bits),
+//     back-substitute, store the chunk.
+// Against writing B' out and reading it back this moves one read of the
+// input in place of a write and a read of B'.
+constexpr int XT_WARPS = 4;
+constexpr int XT_S = 35;  // tile row stride in doubles: 34 columns, odd stride
+
+__global__ void __launch_bounds__(128, 5) k_cn_solve_xt(Layout L, Box box, LineMap map,
+                                                     const double *__restrict__ cin,
+                                                     double *__restrict__ cout,
+                                                     const double *__restrict__ tab,
+                                                     const int32_t *__restrict__ aloft) {
+  __shared__ double sh[XT_WARPS][32 * XT_S];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double *tile = sh[w];
+  const long nrows = (long)L.ny * L.nz * L.ns;
+  const long r0 = ((long)blockIdx.x * XT_WARPS + w) * 32;
+  if (r0 >= nrows) return;  // uniform over the warp
+  const long r = r0 + lane;
+  const bool valid = r < nrows;
+  const long rc = valid ? r : nrows - 1;
+  const int j = (int)(rc % L.ny) + 1;
+  const long t1 = rc / L.ny;
+  const int k = (int)(t1 % L.nz) + 1;
+  const int g = (int)(t1 / L.nz);
+  const bool active =
+      valid && j >= box.jmin && j <= box.jmax && k >= box.kmin && k <= box.kmax && aloft[g] != 0;
+  const unsigned amask = __ballot_sync(0xffffffffu, active);
+  const int nvalid = (int)((nrows - r0) < 32 ? (nrows - r0) : 32);
+  const int rmin = box.imin, rmax = box.imax;
+  const int ncells = rmax - rmin + 1;
+  const long P = L.P;
+  if (valid) {  // cells outside [rmin, rmax] (FAST_SUBGRID box)
+    double *xr = cout + r * P;
+    for (int c = 1; c < rmin; c++) xr[c - 1] = 0.0;
+    for (int c = rmax + 1; c <= L.nx; c++) xr[c - 1] = 0.0;
+  }
+  const double *q0 = cin + r0 * P + (rmin - 1);  // row r0, cell rmin
+  double *x0 = cout + r0 * P + (rmin - 1);
+  const double *qown = q0 + (long)lane * P;
+  double *xown = x0 + (long)lane * P;
+  const long U = map.U;
+  const long F = (long)ncells * U;
+  const long u = map.u(j, k);
+  const double *t = tab + u;
+  CnRun R;
+  cn_load_run(t, F, U, tab + CN_NF * F, u, R);
+  double *tr = tile + lane * XT_S;  // this lane's row of the tile
+  const int nch = (ncells + 31) >> 5;
+
+  // tile columns: 0 = cell l0-1, 1..32 = cells l0..l0+31, 33 = cell l0+32
+  auto load_tile = [&](int l0, int cnt) {
+#pragma unroll
+    for (int h = 0; h < 32; h += 8) {
+      double v[8];
+#pragma unroll
+      for (int e = 0; e < 8; e++) {
+        const int row = h + e;
+        v[e] = (row < nvalid && lane < cnt) ? q0[(long)row * P + l0 + lane] : 0.0;
+      }
+#pragma unroll
+      for (int e = 0; e < 8; e++) tile[(h + e) * XT_S + 1 + lane] = v[e];
+    }
+    tr[0] = (valid && l0 > 0) ? qown[l0 - 1] : 0.0;
+    tr[33] = (valid && l0 + 32 < ncells) ? qown[l0 + 32] : 0.0;
+    __syncwarp();
+  };
+
+  // A chunk whose rows all lie inside every lane's constant run (rows
+  // lo_w+1 .. ncells-2, lo_w the warp's largest lo) takes its coefficients
+  // from registers with no per-row test: the fast path.
+  int lo_w = R.lo;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) lo_w = max(lo_w, __shfl_xor_sync(0xffffffffu, lo_w, o));
+  auto fast_chunk = [&](int l0, int cnt) { return cnt == 32 && l0 > lo_w && l0 + 31 <= ncells - 2; };
+  const double fCL = R.v[CN_CL], fCC = R.v[CN_CC], fCR = R.v[CN_CR], fFA = R.v[CN_FACT];
+  const double fDU = R.v[CN_DU], fDP = R.v[CN_DP], fRD = R.v[CN_RDP];
+
+  // pass 1: forward elimination, checkpoints only (:813-851 and dgtsv)
+  double qm = 0.0, qc = 0.0, bp = 0.0;
+  for (int ch = 0; ch < nch; ch++) {
+    const int l0 = ch << 5;
+    const int cnt = (ncells - l0) < 32 ? (ncells - l0) : 32;
+    load_tile(l0, cnt);
+    if (ch == 0) {
+      qm = tr[1];  // BC_left_t0 = q(rmin)
+      qc = qm;
+    }
+    if (fast_chunk(l0, cnt)) {  // rows l0..l0+31 < ncells-1: qp always from the tile
+#pragma unroll 8
+      for (int c = 0; c < 32; c++) {
+        const double qp = tr[c + 2];
+        const double B = fCL * qm + fCC * qc + fCR * qp;
+        bp = B - fFA * bp;
+        qm = qc;
+        qc = qp;
+      }
+      if (valid && ch + 1 < nch) xown[l0 + 31] = bp;
+      __syncwarp();
+      continue;
+    }
+    for (int c = 0; c < cnt; c++) {
+      const int l = l0 + c;
+      const double qp = (l + 1 < ncells) ? tr[c + 2] : qc;  // BC_right_t0 = q(rmax)
+      const double B = cn_coef(t, F, U, R, CN_CL, l) * qm + cn_coef(t, F, U, R, CN_CC, l) * qc +
+                       cn_coef(t, F, U, R, CN_CR, l) * qp;
+      bp = (l == 0) ? B : B - cn_coef(t, F, U, R, CN_FACT, l) * bp;
+      qm = qc;
+      qc = qp;
+    }
+    if (valid && ch + 1 < nch) xown[l0 + 31] = bp;  // checkpoint B'(l0+31)
+    __syncwarp();
+  }
+
+  // pass 2: per chunk, last first: recompute B', back-substitute, store
+  double xn = 0.0;
+  for (int ch = nch - 1; ch >= 0; ch--) {
+    const int l0 = ch << 5;
+    const int cnt = (ncells - l0) < 32 ? (ncells - l0) : 32;
+    load_tile(l0, cnt);
+    double bq = (valid && ch > 0) ? xown[l0 - 1] : 0.0;
+    double qm2 = (ch == 0) ? tr[1] : tr[0];
+    double qc2 = tr[1];
+    if (fast_chunk(l0, cnt)) {
+#pragma unroll 8
+      for (int c = 0; c < 32; c++) {
+        const double qp = tr[c + 2];
+        const double B = fCL * qm2 + fCC * qc2 + fCR * qp;
+        bq = B - fFA * bq;
+        tr[c + 1] = bq;
+        qm2 = qc2;
+        qc2 = qp;
+      }
+#pragma unroll 8
+      for (int c = 31; c >= 0; c--) {
+        const double num = tr[c + 1] - fDU * xn;
+        const double v = div_rn_rcp(num, fDP, fRD);
+        tr[c + 1] = v;
+        xn = v;
+      }
+    } else {
+    for (int c = 0; c < cnt; c++) {
+      const int l = l0 + c;
+      const double qp = (l + 1 < ncells) ? tr[c + 2] : qc2;
+      const double B = cn_coef(t, F, U, R, CN_CL, l) * qm2 + cn_coef(t, F, U, R, CN_CC, l) * qc2 +
+                       cn_coef(t, F, U, R, CN_CR, l) * qp;
+      bq = (l == 0) ? B : B - cn_coef(t, F, U, R, CN_FACT, l) * bq;
+      tr[c + 1] = bq;
+      qm2 = qc2;
+      qc2 = qp;
+    }
+    for (int c = cnt - 1; c >= 0; c--) {
+      const int l = l0 + c;
+      const double b2 = tr[c + 1];
+      const double num = (l == ncells - 1) ? b2 : b2 - cn_coef(t, F, U, R, CN_DU, l) * xn;
+      const double v = div_rn_rcp(num, cn_coef(t, F, U, R, CN_DP, l), cn_coef(t, F, U, R, CN_RDP, l));
+      tr[c + 1] = v;
+      xn = v;
+    }
+    }
+    __syncwarp();
+#pragma unroll 8
+    for (int row = 0; row < 32; row++) {
+      if (row < nvalid && lane < cnt)
+        x0[(long)row * P + l0 + lane] = ((amask >> row) & 1u) ? tile[row * XT_S + 1 + lane] : 0.0;
+    }
+    __syncwarp();
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -300,7 +574,8 @@ size_t cn_table_doubles(const a3g_ctx *ctx, int dir) {
   const bool da = varies(ctx->kappa, ia) || varies(sig, ia) || varies(kk, ia);
   const bool db = varies(ctx->kappa, ib) || varies(sig, ib) || varies(kk, ib);
   const size_t n = (dir == 0) ? L.nx : (dir == 1) ? L.ny : L.nz;
-  return (size_t)CN_NF * n * (size_t)(da ? na : 1) * (size_t)(db ? nb : 1);
+  const size_t U = (size_t)(da ? na : 1) * (size_t)(db ? nb : 1);
+  return (size_t)CN_NF * n * U + 2 * U;
 }
 
 template <int DIR>
@@ -330,8 +605,14 @@ static int launch_cn_dir(a3g_ctx *ctx) {
   A3G_LAUNCH_CHECK(ctx);
   const long nlines = (long)map.na * map.nb * L.ns;
   tbegin(ctx, A3G_K_CN_SOLVE_X + DIR);
-  k_cn_solve<DIR><<<(unsigned)((nlines + 127) / 128), 128, 0, ctx->stream>>>(
-      L, box, map, ctx->c0, ctx->c1, ctx->cn_buf, ctx->aloft);
+  if (DIR == 0 && ctx->tune_cn_x == 0) {
+    const long nwarps = (nlines + 31) / 32;
+    k_cn_solve_xt<<<(unsigned)((nwarps + XT_WARPS - 1) / XT_WARPS), 32 * XT_WARPS, 0, ctx->stream>>>(
+        L, box, map, ctx->c0, ctx->c1, ctx->cn_buf, ctx->aloft);
+  } else {
+    k_cn_solve<DIR><<<(unsigned)((nlines + 127) / 128), 128, 0, ctx->stream>>>(
+        L, box, map, ctx->c0, ctx->c1, ctx->cn_buf, ctx->aloft);
+  }
   tend(ctx);
   A3G_LAUNCH_CHECK(ctx);
   swap_levels(ctx);

@@ -52,6 +52,7 @@ class Config:
     xLL: float = 0.0
     yLL: float = 0.0
     dz: float = 0.5          # km
+    dz_profile: tuple = ()   # per-level thicknesses (km), overriding dz when given
     ivent: int = 1
     jvent: int = 1
     z_volcano: float = 0.0   # vent elevation (km)
@@ -140,6 +141,12 @@ def make_config(name: str) -> Config:
                       fall_mps=(0.05, 0.4, 1.5), bin_mass=(0.3, 0.3, 0.4), plume_km=8.0,
                       volume_km3=1.0e-3, duration_h=1.0, use_cn=True, sim_hours=1.0,
                       winds="random", seed=17)
+    if name == "tiny_stretch":  # lon/lat CN, x lines of 3 tiles, dz changing part-way up
+        return Config("tiny_stretch", 75, 10, 24, 2, latlon=True, de=0.5, dn=0.5, lonLL=20.0,
+                      latLL=40.0, dz=0.3, dz_profile=(0.3,) * 10 + (0.45,) * 8 + (0.7,) * 6,
+                      ivent=37, jvent=5, fall_mps=(0.2, 1.2), bin_mass=(0.5, 0.5), plume_km=5.0,
+                      volume_km3=1.0e-3, duration_h=1.0, use_cn=True, sim_hours=1.0,
+                      winds="random", seed=18)
     raise KeyError(name)
 
 
@@ -148,7 +155,11 @@ def make_config(name: str) -> Config:
 # ---------------------------------------------------------------------------
 def zgrid(cfg: Config):
     nz = cfg.nz
-    z_vec_init = np.array([cfg.dz * k for k in range(nz + 1)], dtype=np.float64)  # Input_Data.f90:1579
+    if cfg.dz_profile:  # a stretched column: level tops from the listed thicknesses
+        assert len(cfg.dz_profile) == nz
+        z_vec_init = np.concatenate([[0.0], np.cumsum(np.asarray(cfg.dz_profile, dtype=np.float64))])
+    else:
+        z_vec_init = np.array([cfg.dz * k for k in range(nz + 1)], dtype=np.float64)  # Input_Data.f90:1579
     dz = np.zeros(nz + 4)          # index k+1 for k=-1..nz+2
     zcc = np.zeros(nz + 4)
     zlb = np.zeros(nz + 4)
