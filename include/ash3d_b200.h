@@ -215,7 +215,8 @@ int a3g_get_stream(a3g_ctx *ctx, void **stream);
 #define A3G_K_TOTALS     11
 #define A3G_K_WINDS      12
 #define A3G_K_OTHER      13
-#define A3G_K_COUNT      14
+#define A3G_K_ADJOINT    14
+#define A3G_K_COUNT      15
 /* Starts (enable=1) or stops per-kernel CUDA-event timing; starting clears
  * the accumulators.  Timing brackets every launch with two events on the
  * context's stream. */
@@ -232,6 +233,54 @@ int a3g_kernel_times(a3g_ctx *ctx, double *ms, uint64_t *count);
  * differs. */
 int a3g_set_variant(a3g_ctx *ctx, int32_t dir, int32_t variant);
 int a3g_get_variant(a3g_ctx *ctx, int32_t dir, int32_t *variant);
+
+/* ---- discrete adjoint (no counterpart in the reference) ----
+ * Reverse mode of the transport step for source inversion.  Every sweep is
+ * piecewise linear in the concentration; with the limiter branches fixed by
+ * the state the sweep was applied to it is a linear map J, and these calls
+ * apply J^T to the adjoint field lam kept on the device.  They need the full
+ * box (fast_subgrid off: the subgrid box depends on the state) and leave the
+ * forward state and the outflow accumulators untouched.  dt and the winds
+ * must be those of the forward step (a3g_set_dt / a3g_set_winds or
+ * a3g_interp_winds). */
+/* Allocates lam, the deposit adjoint and the step's stage buffers (4 levels
+ * plus one face); lam starts at zero. */
+int a3g_adj_enable(a3g_ctx *ctx);
+int a3g_adj_zero(a3g_ctx *ctx);
+/* lam in the layout of concen_pd(:,:,:,:,ts0) (ghost values ignored on
+ * upload, left untouched on download). */
+int a3g_adj_set_lambda(a3g_ctx *ctx, const double *lam);
+int a3g_adj_get_lambda(a3g_ctx *ctx, double *lam);
+/* adjoint of DepositGranularity (nx,ny,ns), the bottom outflow of AdvectVert */
+int a3g_adj_set_lambda_dep(a3g_ctx *ctx, const double *lam_dep);
+int a3g_adj_get_lambda_dep(a3g_ctx *ctx, double *lam_dep);
+/* One sweep's transpose, linearised at the current state (the sweep's
+ * input): lam <- J^T lam.  a3g_adj_advect_vert also adds the deposit
+ * adjoint's contribution.  a3g_adj_diffuse_horz(itime) reverses
+ * DiffuseHorz(itime)'s order of x and y. */
+int a3g_adj_advect_x(a3g_ctx *ctx);
+int a3g_adj_advect_y(a3g_ctx *ctx);
+int a3g_adj_advect_vert(a3g_ctx *ctx);
+int a3g_adj_diffuse_horz(a3g_ctx *ctx, int32_t itime);
+int a3g_adj_diffuse_vert(a3g_ctx *ctx);
+/* The whole transport step itime (Set_BC(1), AdvectHorz(itime), AdvectVert,
+ * Set_BC(2), DiffuseHorz(itime), DiffuseVert) in reverse, with the state
+ * after the step's source insertion in the context.  The step's
+ * intermediate states are recomputed on the device. */
+int a3g_adj_step(a3g_ctx *ctx, int32_t itime);
+/* lam at the vent column, (nz+1) x ns with k fastest (the layout of the
+ * source flux): the adjoint of the source insertion before dt/kappa. */
+int a3g_adj_vent_column(a3g_ctx *ctx, int32_t ivent, int32_t jvent, double *out);
+/* Unmasked column load (CloudLoad of src/Output_Vars.f90:1061-1069,
+ * tonnes/km^2) of the current state, (nx,ny); and lam += H^T w for a
+ * weight w (nx,ny), H that column load. */
+int a3g_cloud_load(a3g_ctx *ctx, double *out);
+int a3g_adj_add_cloud_load(a3g_ctx *ctx, const double *w);
+/* Device-resident copies of the concentration (checkpoints of the forward
+ * run for the reverse sweep). */
+int a3g_snapshot_alloc(a3g_ctx *ctx, int32_t nslots);
+int a3g_snapshot_save(a3g_ctx *ctx, int32_t slot);
+int a3g_snapshot_load(a3g_ctx *ctx, int32_t slot);
 
 /* ---- allocation-free entry point (no counterpart in the reference) ---- */
 /* Per-grain airborne mass sum(c*kappa) (the mass_aloft of Calc_AshVol_Aloft,

@@ -299,6 +299,94 @@ class OracleModel:
         self.lib.orc_adj_diffuse_vert(self.ps, _d(w))
         return self._lam_out(w)
 
+    # stateful form (the GPU model's interface): lam kept here
+    def adj_enable(self):
+        if getattr(self, "lam", None) is None:
+            self.adj_zero()
+
+    def adj_zero(self):
+        c = self.cfg
+        self.lam = np.zeros((c.nx, c.ny, c.nz, c.ns), order="F")
+        self.lam_dep = np.zeros((c.nx, c.ny, c.ns), order="F")
+
+    def set_lambda(self, lam):
+        self.adj_enable()
+        self.lam = np.asfortranarray(lam, dtype=np.float64).copy(order="F")
+
+    def get_lambda(self):
+        return self.lam.copy(order="F")
+
+    def set_lambda_dep(self, lam_dep):
+        self.adj_enable()
+        c = self.cfg
+        self.lam_dep = np.zeros((c.nx, c.ny, c.ns), order="F") if lam_dep is None else \
+            np.asfortranarray(lam_dep, dtype=np.float64).copy(order="F")
+
+    def get_lambda_dep(self):
+        return self.lam_dep.copy(order="F")
+
+    def adj_step(self, itime):
+        """Reverse of one transport step; ts0 holds the state after the
+        step's source insertion and is left unchanged."""
+        a = self.interior()
+        keep = [x.copy() for x in (self.out_yz1, self.out_yz2, self.out_xz1, self.out_xz2,
+                                   self.out_xy1, self.out_xy2, self.deposit)]
+        even = itime % 2 == 0
+        self.set_interior(a)
+        (self.advect_y if even else self.advect_x)()
+        b = self.interior()
+        (self.advect_x if even else self.advect_y)()
+        cst = self.interior()
+        for dst, src in zip((self.out_yz1, self.out_yz2, self.out_xz1, self.out_xz2, self.out_xy1,
+                             self.out_xy2, self.deposit), keep):
+            dst[...] = src
+        lam = self.lam
+        if self.cfg.use_diffusion:
+            lam = self.adj_diffuse_vert(lam)
+            lam = self.adj_diffuse_horz(lam, itime)
+        self.set_interior(cst)
+        lam = self.adj_advect_z(lam, self.lam_dep)
+        self.set_interior(b)
+        lam = (self.adj_advect_x if even else self.adj_advect_y)(lam)
+        self.set_interior(a)
+        lam = (self.adj_advect_y if even else self.adj_advect_x)(lam)
+        self.lam = lam
+
+    def adj_vent_column(self):
+        c = self.cfg
+        out = np.zeros((c.nz + 1, c.ns), order="F")
+        out[:c.nz, :] = self.lam[c.ivent - 1, c.jvent - 1, :, :]
+        return out
+
+    def cloud_load(self):
+        """Unmasked CloudLoad (src/Output_Vars.f90:1061-1069), same order."""
+        c = self.cfg
+        q = self.interior()
+        load = np.zeros((c.nx, c.ny))
+        for k in range(c.nz):
+            s = np.zeros((c.nx, c.ny))
+            for g in range(c.ns):
+                s = s + q[:, :, k, g]
+            load = load + s * self.dz_vec[k + 2] / 1.0e3
+        return load
+
+    def adj_add_cloud_load(self, w):
+        c = self.cfg
+        for k in range(c.nz):
+            add = w * self.dz_vec[k + 2] / 1.0e3
+            for g in range(c.ns):
+                self.lam[:, :, k, g] = self.lam[:, :, k, g] + add
+
+    def snapshot_alloc(self, n):
+        if not hasattr(self, "_snaps"):
+            self._snaps = {}
+
+    def snapshot_save(self, slot):
+        self._snaps[slot] = self.interior()
+
+    def snapshot_load(self, slot):
+        self.set_interior(self._snaps[slot])
+
     def zero_outflows(self):
         for a in (self.out_yz1, self.out_yz2, self.out_xz1, self.out_xz2, self.out_xy1, self.out_xy2,
                   self.deposit):

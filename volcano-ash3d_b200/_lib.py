@@ -37,9 +37,15 @@ EXPORTED = [
     "a3g_kernel_launches", "a3g_get_stream", "a3g_kernel_timing", "a3g_kernel_times",
     "a3g_cfl_maxima", "a3g_adjust_dt_from_maxima", "a3g_selftest_div", "a3g_set_variant",
     "a3g_get_variant", "a3g_mass_aloft_noalloc",
+    "a3g_adj_enable", "a3g_adj_zero", "a3g_adj_set_lambda", "a3g_adj_get_lambda",
+    "a3g_adj_set_lambda_dep", "a3g_adj_get_lambda_dep", "a3g_adj_advect_x", "a3g_adj_advect_y",
+    "a3g_adj_advect_vert", "a3g_adj_diffuse_horz", "a3g_adj_diffuse_vert", "a3g_adj_step",
+    "a3g_adj_vent_column", "a3g_cloud_load", "a3g_adj_add_cloud_load", "a3g_snapshot_alloc",
+    "a3g_snapshot_save", "a3g_snapshot_load",
 ]
 KERNEL_CLASSES = ["advect_x", "advect_y", "advect_z", "diff_x", "diff_y", "diff_z", "cn_table",
-                  "cn_solve_x", "cn_solve_y", "cn_solve_z", "cfl", "totals", "winds", "other"]
+                  "cn_solve_x", "cn_solve_y", "cn_solve_z", "cfl", "totals", "winds", "other",
+                  "adjoint"]
 
 
 class A3GError(RuntimeError):
@@ -126,6 +132,16 @@ def load(path: os.PathLike | str | None = None) -> C.CDLL:
         "a3g_get_stream": (C.c_int, [P, C.POINTER(C.c_void_p)]),
         "a3g_kernel_timing": (C.c_int, [P, C.c_int32]),
         "a3g_kernel_times": (C.c_int, [P, D, C.POINTER(C.c_uint64)]),
+        "a3g_adj_enable": (C.c_int, [P]), "a3g_adj_zero": (C.c_int, [P]),
+        "a3g_adj_set_lambda": (C.c_int, [P, D]), "a3g_adj_get_lambda": (C.c_int, [P, D]),
+        "a3g_adj_set_lambda_dep": (C.c_int, [P, D]), "a3g_adj_get_lambda_dep": (C.c_int, [P, D]),
+        "a3g_adj_advect_x": (C.c_int, [P]), "a3g_adj_advect_y": (C.c_int, [P]),
+        "a3g_adj_advect_vert": (C.c_int, [P]), "a3g_adj_diffuse_horz": (C.c_int, [P, C.c_int32]),
+        "a3g_adj_diffuse_vert": (C.c_int, [P]), "a3g_adj_step": (C.c_int, [P, C.c_int32]),
+        "a3g_adj_vent_column": (C.c_int, [P, C.c_int32, C.c_int32, D]),
+        "a3g_cloud_load": (C.c_int, [P, D]), "a3g_adj_add_cloud_load": (C.c_int, [P, D]),
+        "a3g_snapshot_alloc": (C.c_int, [P, C.c_int32]), "a3g_snapshot_save": (C.c_int, [P, C.c_int32]),
+        "a3g_snapshot_load": (C.c_int, [P, C.c_int32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -1,6 +1,7 @@
 // a3g_api.cu -- the C-ABI (include/ash3d_b200.h): context lifetime, data
 // movement between the Fortran-layout host arrays and the device layout,
 // and the per-step entry points that mirror the reference subroutines.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -263,6 +264,10 @@ int a3g_destroy(a3g_ctx *ctx) {
   if (ctx->h_tot) cudaFreeHost(ctx->h_tot);
   if (ctx->src_event) cudaEventDestroy(ctx->src_event);
   for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
+  double *aptrs[] = {ctx->lam0, ctx->lam1, ctx->lam_dep, ctx->stage1, ctx->stage2, ctx->adj_face,
+                     ctx->obs_buf};
+  for (double *p : aptrs) if (p) cudaFree(p);
+  for (double *p : ctx->snaps) if (p) cudaFree(p);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return A3G_OK;
@@ -801,6 +806,251 @@ int a3g_get_variant(a3g_ctx *ctx, int32_t dir, int32_t *variant) {
 int a3g_kernel_launches(a3g_ctx *ctx, uint64_t *count) {
   if (!ctx || !count) return fail(A3G_ERR_ARG, "null argument");
   *count = ctx->launches;
+  return A3G_OK;
+}
+
+// ---------------------------------------------------------------------------
+// discrete adjoint
+// ---------------------------------------------------------------------------
+static size_t level_bytes(const a3g_ctx *ctx) { return sizeof(double) * ctx->L.PG * ctx->L.ns; }
+
+static int adj_ready(a3g_ctx *ctx) {
+  if (!ctx->lam0) return fail(A3G_ERR_STATE, "a3g_adj_enable has not been called");
+  if (ctx->prm.fast_subgrid) return fail(A3G_ERR_UNSUPPORTED, "the adjoint needs fast_subgrid off");
+  int rc = ready(ctx);
+  if (rc) return rc;
+  full_box(ctx);
+  return A3G_OK;
+}
+
+static void swap_lam(a3g_ctx *ctx) {
+  double *t = ctx->lam0;
+  ctx->lam0 = ctx->lam1;
+  ctx->lam1 = t;
+}
+
+int a3g_adj_enable(a3g_ctx *ctx) {
+  CTX_CHECK(ctx);
+  if (ctx->lam0) return a3g_adj_zero(ctx);
+  const size_t lev = level_bytes(ctx);
+  const int nx = ctx->grid.nx, ny = ctx->grid.ny, nz = ctx->grid.nz, ns = ctx->grid.ns;
+  const size_t face = sizeof(double) * (size_t)ns *
+                      (size_t)std::max(std::max((long)ny * nz, (long)nx * nz), (long)nx * ny);
+  const size_t obs = sizeof(double) * std::max((size_t)nx * ny, (size_t)(nz + 1) * ns);
+  double **bufs[] = {&ctx->lam0, &ctx->lam1, &ctx->stage1, &ctx->stage2};
+  for (double **b : bufs) {
+    if (cudaMalloc((void **)b, lev) != cudaSuccess) return fail(A3G_ERR_NOMEM, "adjoint level allocation failed");
+    ctx->bytes += lev;
+  }
+  if (cudaMalloc((void **)&ctx->lam_dep, sizeof(double) * (size_t)nx * ny * ns) != cudaSuccess ||
+      cudaMalloc((void **)&ctx->adj_face, face) != cudaSuccess ||
+      cudaMalloc((void **)&ctx->obs_buf, obs) != cudaSuccess)
+    return fail(A3G_ERR_NOMEM, "adjoint buffer allocation failed");
+  ctx->bytes += sizeof(double) * (size_t)nx * ny * ns + face + obs;
+  return a3g_adj_zero(ctx);
+}
+
+int a3g_adj_zero(a3g_ctx *ctx) {
+  CTX_CHECK(ctx);
+  if (!ctx->lam0) return fail(A3G_ERR_STATE, "a3g_adj_enable has not been called");
+  A3G_CUDA(cudaMemsetAsync(ctx->lam0, 0, level_bytes(ctx), ctx->stream));
+  A3G_CUDA(cudaMemsetAsync(ctx->lam1, 0, level_bytes(ctx), ctx->stream));
+  A3G_CUDA(cudaMemsetAsync(ctx->lam_dep, 0,
+                           sizeof(double) * (size_t)ctx->grid.nx * ctx->grid.ny * ctx->grid.ns, ctx->stream));
+  return A3G_OK;
+}
+
+int a3g_adj_set_lambda(a3g_ctx *ctx, const double *lam) {
+  CTX_CHECK(ctx);
+  if (!lam) return fail(A3G_ERR_ARG, "null lam");
+  if (!ctx->lam0) return fail(A3G_ERR_STATE, "a3g_adj_enable has not been called");
+  const int nx = ctx->grid.nx, ny = ctx->grid.ny, nz = ctx->grid.nz;
+  A3G_CUDA(cudaMemsetAsync(ctx->lam0, 0, level_bytes(ctx), ctx->stream));
+  int rc = copy_level(ctx, const_cast<double *>(lam), ctx->lam0, true, nx + 4, ny + 4, nz + 4, 2, nx, ny, nz,
+                      ctx->grid.ns, ctx->L.P, ctx->L.PY, ctx->L.PG);
+  if (rc) return rc;
+  A3G_CUDA(cudaStreamSynchronize(ctx->stream));
+  return A3G_OK;
+}
+
+int a3g_adj_get_lambda(a3g_ctx *ctx, double *lam) {
+  CTX_CHECK(ctx);
+  if (!lam) return fail(A3G_ERR_ARG, "null lam");
+  if (!ctx->lam0) return fail(A3G_ERR_STATE, "a3g_adj_enable has not been called");
+  const int nx = ctx->grid.nx, ny = ctx->grid.ny, nz = ctx->grid.nz;
+  int rc = copy_level(ctx, lam, ctx->lam0, false, nx + 4, ny + 4, nz + 4, 2, nx, ny, nz, ctx->grid.ns,
+                      ctx->L.P, ctx->L.PY, ctx->L.PG);
+  if (rc) return rc;
+  return sync_scalars(ctx);
+}
+
+int a3g_adj_set_lambda_dep(a3g_ctx *ctx, const double *lam_dep) {
+  CTX_CHECK(ctx);
+  if (!lam_dep) return fail(A3G_ERR_ARG, "null lam_dep");
+  if (!ctx->lam0) return fail(A3G_ERR_STATE, "a3g_adj_enable has not been called");
+  A3G_CUDA(cudaMemcpyAsync(ctx->lam_dep, lam_dep, sizeof(double) * (size_t)ctx->grid.nx * ctx->grid.ny * ctx->grid.ns,
+                           cudaMemcpyHostToDevice, ctx->stream));
+  A3G_CUDA(cudaStreamSynchronize(ctx->stream));
+  return A3G_OK;
+}
+
+int a3g_adj_get_lambda_dep(a3g_ctx *ctx, double *lam_dep) {
+  CTX_CHECK(ctx);
+  if (!lam_dep) return fail(A3G_ERR_ARG, "null lam_dep");
+  if (!ctx->lam0) return fail(A3G_ERR_STATE, "a3g_adj_enable has not been called");
+  A3G_CUDA(cudaMemcpyAsync(lam_dep, ctx->lam_dep, sizeof(double) * (size_t)ctx->grid.nx * ctx->grid.ny * ctx->grid.ns,
+                           cudaMemcpyDeviceToHost, ctx->stream));
+  return sync_scalars(ctx);
+}
+
+static int adj_advect_dir(a3g_ctx *ctx, int dir, const double *state) {
+  int rc = launch_adj_advect(ctx, dir, state, ctx->lam0, ctx->lam1, dir == 2 ? ctx->lam_dep : nullptr);
+  if (rc) return rc;
+  swap_lam(ctx);
+  return A3G_OK;
+}
+
+static int adj_diffuse_dir(a3g_ctx *ctx, int dir) {
+  int rc = launch_adj_diffuse(ctx, dir, ctx->lam0, ctx->lam1);
+  if (rc) return rc;
+  swap_lam(ctx);
+  return A3G_OK;
+}
+
+int a3g_adj_advect_x(a3g_ctx *ctx) {
+  CTX_CHECK(ctx);
+  int rc = adj_ready(ctx);
+  return rc ? rc : adj_advect_dir(ctx, 0, ctx->c0);
+}
+
+int a3g_adj_advect_y(a3g_ctx *ctx) {
+  CTX_CHECK(ctx);
+  int rc = adj_ready(ctx);
+  return rc ? rc : adj_advect_dir(ctx, 1, ctx->c0);
+}
+
+int a3g_adj_advect_vert(a3g_ctx *ctx) {
+  CTX_CHECK(ctx);
+  int rc = adj_ready(ctx);
+  return rc ? rc : adj_advect_dir(ctx, 2, ctx->c0);
+}
+
+int a3g_adj_diffuse_horz(a3g_ctx *ctx, int32_t itime) {
+  CTX_CHECK(ctx);
+  int rc = adj_ready(ctx);
+  if (rc) return rc;
+  if (!ctx->have_diffusivity) return fail(A3G_ERR_STATE, "diffusivity not set");
+  // DiffuseHorz: even x then y, odd y then x (src/Diffusion.F90:186-214)
+  const int first = (itime % 2 == 0) ? 0 : 1;
+  if ((rc = adj_diffuse_dir(ctx, 1 - first))) return rc;
+  return adj_diffuse_dir(ctx, first);
+}
+
+int a3g_adj_diffuse_vert(a3g_ctx *ctx) {
+  CTX_CHECK(ctx);
+  int rc = adj_ready(ctx);
+  if (rc) return rc;
+  if (!ctx->have_diffusivity) return fail(A3G_ERR_STATE, "diffusivity not set");
+  return adj_diffuse_dir(ctx, 2);
+}
+
+int a3g_adj_step(a3g_ctx *ctx, int32_t itime) {
+  CTX_CHECK(ctx);
+  int rc = adj_ready(ctx);
+  if (rc) return rc;
+  if (ctx->prm.use_diffusion && !ctx->have_diffusivity) return fail(A3G_ERR_STATE, "diffusivity not set");
+  // Recompute the states entering the second horizontal sweep and the
+  // vertical sweep, keeping the forward state and accumulators intact: the
+  // recomputed sweeps write into the stage buffers and add their outflow
+  // updates to a scratch face.
+  double *keep_c0 = ctx->c0, *keep_c1 = ctx->c1;
+  double *outs[6] = {ctx->out_yz1, ctx->out_yz2, ctx->out_xz1, ctx->out_xz2, ctx->out_xy1, ctx->out_xy2};
+  ctx->out_yz1 = ctx->out_yz2 = ctx->out_xz1 = ctx->out_xz2 = ctx->out_xy1 = ctx->out_xy2 = ctx->adj_face;
+  const int first = (itime % 2 == 0) ? 1 : 0;  // AdvectHorz: even y then x, odd x then y
+  ctx->c1 = ctx->stage1;
+  rc = (first == 0) ? launch_advect_x(ctx) : launch_advect_y(ctx);  // c0 := stage1 (state b)
+  if (!rc) {
+    ctx->c1 = ctx->stage2;
+    rc = (first == 0) ? launch_advect_y(ctx) : launch_advect_x(ctx);  // c0 := stage2 (state c)
+  }
+  ctx->out_yz1 = outs[0]; ctx->out_yz2 = outs[1]; ctx->out_xz1 = outs[2];
+  ctx->out_xz2 = outs[3]; ctx->out_xy1 = outs[4]; ctx->out_xy2 = outs[5];
+  ctx->c0 = keep_c0;
+  ctx->c1 = keep_c1;
+  if (rc) return rc;
+  if (ctx->prm.use_diffusion) {
+    if ((rc = adj_diffuse_dir(ctx, 2))) return rc;  // DiffuseVert^T
+    const int dfirst = (itime % 2 == 0) ? 0 : 1;     // DiffuseHorz: even x then y
+    if ((rc = adj_diffuse_dir(ctx, 1 - dfirst))) return rc;
+    if ((rc = adj_diffuse_dir(ctx, dfirst))) return rc;
+  }
+  if ((rc = adj_advect_dir(ctx, 2, ctx->stage2))) return rc;         // AdvectVert^T at state c
+  if ((rc = adj_advect_dir(ctx, 1 - first, ctx->stage1))) return rc; // second horizontal sweep at b
+  return adj_advect_dir(ctx, first, ctx->c0);                        // first horizontal sweep at a
+}
+
+int a3g_adj_vent_column(a3g_ctx *ctx, int32_t ivent, int32_t jvent, double *out) {
+  CTX_CHECK(ctx);
+  if (!out) return fail(A3G_ERR_ARG, "null out");
+  if (!ctx->lam0) return fail(A3G_ERR_STATE, "a3g_adj_enable has not been called");
+  if (ivent < 1 || ivent > ctx->grid.nx || jvent < 1 || jvent > ctx->grid.ny)
+    return fail(A3G_ERR_ARG, "vent outside the grid");
+  int rc = launch_vent_column(ctx, ivent, jvent, ctx->lam0, ctx->obs_buf);
+  if (rc) return rc;
+  A3G_CUDA(cudaMemcpyAsync(out, ctx->obs_buf, sizeof(double) * (size_t)(ctx->grid.nz + 1) * ctx->grid.ns,
+                           cudaMemcpyDeviceToHost, ctx->stream));
+  return sync_scalars(ctx);
+}
+
+int a3g_cloud_load(a3g_ctx *ctx, double *out) {
+  CTX_CHECK(ctx);
+  if (!out) return fail(A3G_ERR_ARG, "null out");
+  if (!ctx->obs_buf) return fail(A3G_ERR_STATE, "a3g_adj_enable has not been called");
+  if (!ctx->have_geometry) return fail(A3G_ERR_STATE, "geometry not set");
+  int rc = launch_cloud_load(ctx, ctx->c0, ctx->obs_buf);
+  if (rc) return rc;
+  A3G_CUDA(cudaMemcpyAsync(out, ctx->obs_buf, sizeof(double) * (size_t)ctx->grid.nx * ctx->grid.ny,
+                           cudaMemcpyDeviceToHost, ctx->stream));
+  return sync_scalars(ctx);
+}
+
+int a3g_adj_add_cloud_load(a3g_ctx *ctx, const double *w) {
+  CTX_CHECK(ctx);
+  if (!w) return fail(A3G_ERR_ARG, "null w");
+  if (!ctx->lam0) return fail(A3G_ERR_STATE, "a3g_adj_enable has not been called");
+  A3G_CUDA(cudaMemcpyAsync(ctx->obs_buf, w, sizeof(double) * (size_t)ctx->grid.nx * ctx->grid.ny,
+                           cudaMemcpyHostToDevice, ctx->stream));
+  int rc = launch_adj_cloud_load(ctx, ctx->obs_buf, ctx->lam0);
+  if (rc) return rc;
+  A3G_CUDA(cudaStreamSynchronize(ctx->stream));  // w may be reused by the caller
+  return A3G_OK;
+}
+
+int a3g_snapshot_alloc(a3g_ctx *ctx, int32_t nslots) {
+  CTX_CHECK(ctx);
+  if (nslots < 0) return fail(A3G_ERR_ARG, "negative slot count");
+  while ((int)ctx->snaps.size() < nslots) {
+    double *p = nullptr;
+    if (cudaMalloc((void **)&p, level_bytes(ctx)) != cudaSuccess)
+      return fail(A3G_ERR_NOMEM, "snapshot allocation failed");
+    ctx->bytes += level_bytes(ctx);
+    ctx->snaps.push_back(p);
+  }
+  return A3G_OK;
+}
+
+int a3g_snapshot_save(a3g_ctx *ctx, int32_t slot) {
+  CTX_CHECK(ctx);
+  if (slot < 0 || slot >= (int)ctx->snaps.size()) return fail(A3G_ERR_ARG, "snapshot slot out of range");
+  A3G_CUDA(cudaMemcpyAsync(ctx->snaps[slot], ctx->c0, level_bytes(ctx), cudaMemcpyDeviceToDevice, ctx->stream));
+  return A3G_OK;
+}
+
+int a3g_snapshot_load(a3g_ctx *ctx, int32_t slot) {
+  CTX_CHECK(ctx);
+  if (slot < 0 || slot >= (int)ctx->snaps.size()) return fail(A3G_ERR_ARG, "snapshot slot out of range");
+  A3G_CUDA(cudaMemcpyAsync(ctx->c0, ctx->snaps[slot], level_bytes(ctx), cudaMemcpyDeviceToDevice, ctx->stream));
+  ctx->ts1_zeroed = false;  // a restored state survives the next prologue
   return A3G_OK;
 }
 

@@ -130,6 +130,13 @@ struct a3g_ctx {
   // kernel variant per advection direction (0 march, 1 block V=4, 2 block V=8)
   int tune_advect[3];
   int tune_cn_x;            // CN x solve: 0 warp-tiled, 1 one thread per line
+  // discrete adjoint (a3g_adj_*)
+  double *lam0, *lam1;      // lam and its scratch level
+  double *lam_dep;          // adjoint of DepositGranularity (ns,ny,nx)
+  double *stage1, *stage2;  // recomputed states inside a step
+  double *adj_face;         // sink for outflow updates of recomputed sweeps
+  double *obs_buf;          // (nx*ny) or ((nz+1)*ns), whichever is larger
+  std::vector<double *> snaps;
   // optional per-kernel timing (a3g_kernel_timing)
   bool timing;
   std::vector<cudaEvent_t> ev_pool;
@@ -176,6 +183,12 @@ int launch_interp_winds(a3g_ctx *ctx, double frac);
 int launch_source(a3g_ctx *ctx, int ivent, int jvent, double dt);
 int launch_zero_state(a3g_ctx *ctx);
 int check_device_error(a3g_ctx *ctx);
+int launch_adj_advect(a3g_ctx *ctx, int dir, const double *cq, const double *lin, double *lout,
+                      const double *lam_lo);
+int launch_adj_diffuse(a3g_ctx *ctx, int dir, const double *lin, double *lout);
+int launch_cloud_load(a3g_ctx *ctx, const double *c, double *out);
+int launch_adj_cloud_load(a3g_ctx *ctx, const double *w, double *lam);
+int launch_vent_column(a3g_ctx *ctx, int ivent, int jvent, const double *lam, double *out);
 int refresh_dtv(a3g_ctx *ctx);
 // per-kernel timing brackets (no-ops unless a3g_kernel_timing(ctx,1))
 void tbegin(a3g_ctx *ctx, int kind);

@@ -712,4 +712,221 @@ int launch_advect_z(a3g_ctx *ctx) {
   return A3G_OK;
 }
 
+// ===========================================================================
+// Discrete adjoint of one advection sweep (no counterpart in the reference).
+//
+// With the limiter branches fixed by the sweep's input state q, the limited
+// slope is ldq = a*dq + b*dqu, so the sweep is linear; this kernel applies
+// its transpose to lam (the adjoint of the sweep's output).  It is a gather:
+// one thread per cell-grain, lanes along x in every direction (coalesced),
+// each thread re-deriving the four interfaces m-1..m+2 that its cell feeds
+// (limiter branch, flux-area terms) from q, winds and geometry.  With t(i) =
+// -dt/kappa(i)*lam_u(i) (lam_u = lam inside the line, the deposit adjoint
+// at the z bottom outflow, 0 at the other outflows):
+//   lam_fsr(I) = t(I), lam_fsl(I) = t(I-1), lam_fss(I) = t(I-1) - t(I)
+//   e(J) = 0.5|us|(1 - dtv|us|) * lam_fss(J)       (active fss interfaces)
+//   lam_dq(I) = max(0,us)lam_fsr(I) + min(0,us)lam_fsl(I) + a(I)e(I)
+//               + b(I+1)e(I+1) [us(I+1) > 0] + b(I-1)e(I-1) [us(I-1) <= 0]
+//   lam_q(m)  = lam(m) + divu_m(m)lam_fsr(m) + divu_p(m+1)lam_fsl(m+1)
+//               + lam_dq(m) - lam_dq(m+1)
+// Ghost cells of Set_BC(1) are zero (their adjoint is dropped) except x-
+// periodic wraps, whose adjoint is added back to the wrapped cells.  Full box
+// only (the subgrid box depends on the state).
+// ===========================================================================
+
+// d(ldq) = a*d(dq) + b*d(dqu) on the branch the forward limiter takes.
+template <int LIM>
+__device__ __forceinline__ void lim_coef(double dq, double dqu, double eps, double &a, double &b) {
+  if (LIM == A3G_LIM_LAXWEN) { a = 1.0; b = 0.0; return; }
+  if (LIM == A3G_LIM_BW) { a = 0.0; b = 1.0; return; }
+  const bool clamp = fabs(dqu) > 3.0 * fabs(dq) || fabs(dq) < eps;
+  const double th = clamp ? copysign(3.0, dqu * dq) : div_rn(dqu, dq);
+  double phi, dphi;
+  if (LIM == A3G_LIM_FROMM) {
+    phi = 0.5 * (1.0 + th); dphi = 0.5;
+  } else if (LIM == A3G_LIM_MINMOD) {
+    const double m = fmn(1.0, th), dm = (1.0 < th) ? 0.0 : 1.0;
+    phi = fmx(0.0, m); dphi = (0.0 > m) ? 0.0 : dm;
+  } else if (LIM == A3G_LIM_MC) {
+    const double m1 = fmn((1.0 + th) / 2.0, 2.0), dm1 = ((1.0 + th) / 2.0 < 2.0) ? 0.5 : 0.0;
+    const double m2 = fmn(m1, 2.0 * th), dm2 = (m1 < 2.0 * th) ? dm1 : 2.0;
+    phi = fmx(0.0, m2); dphi = (0.0 > m2) ? 0.0 : dm2;
+  } else {  // superbee
+    const double m1 = fmn(1.0, 2.0 * th), dm1 = (1.0 < 2.0 * th) ? 0.0 : 2.0;
+    const double a1 = fmx(0.0, m1), da1 = (0.0 > m1) ? 0.0 : dm1;
+    const double m2 = fmn(2.0, th), dm2 = (2.0 < th) ? 0.0 : 1.0;
+    phi = fmx(a1, m2); dphi = (a1 > m2) ? da1 : dm2;
+  }
+  if (clamp) dphi = 0.0;
+  a = phi - th * dphi;
+  b = dphi;
+}
+
+template <int DIR, int LIM, bool PER>
+__global__ void __launch_bounds__(256) k_adj_advect(Layout L, int nocycle, double eps,
+                                                    const double *__restrict__ cq,
+                                                    const double *__restrict__ lin,
+                                                    double *__restrict__ lout,
+                                                    const double *__restrict__ vel, Geo4 vf, Geo3 sig,
+                                                    Geo3 dtvt, const int32_t *__restrict__ aloft,
+                                                    const double *__restrict__ lam_lo) {
+  const int i = blockIdx.x * 32 + threadIdx.x + 1;
+  const int j = blockIdx.y * 8 + threadIdx.y + 1;
+  const int k = (int)(blockIdx.z % L.nz) + 1;
+  const int g = (int)(blockIdx.z / L.nz);
+  if (i > L.nx || j > L.ny) return;
+  const long cell = L.cell(i, j, k);
+  const long gb = (long)g * L.PG;
+  if (!aloft[g]) {
+    lout[gb + cell] = 0.0;
+    return;
+  }
+  const int n = (DIR == 0) ? L.nx : (DIR == 1) ? L.ny : L.nz;
+  const int m = (DIR == 0) ? i : (DIR == 1) ? j : k;
+  const long st = (DIR == 0) ? 1 : (DIR == 1) ? L.P : L.PY;
+  const long lb = cell - (long)(m - 1) * st;  // sweep index 1 of this line
+  const int la = (DIR == 0) ? j : i, lo_ = (DIR == 2) ? j : k;
+  const LineGeo gsig = line_of<DIR>(sig, la, lo_);
+  const LineGeo gdtv = line_of<DIR>(dtvt, la, lo_);
+  const double *pq = cq + gb + lb;
+  const double *pl = lin + gb + lb;
+  const double *pv = vel + lb;
+  const double *pvf = vf.p + (long)(i + 1) * vf.si + (long)(j + 1) * vf.sj + (long)g * vf.sg;
+  auto wrap = [&](int c) { return c < 1 ? c + n : (c > n ? c - n : c); };
+  auto Q = [&](int c) -> double {
+    if (c < -1 || c > n + 2) return 0.0;
+    if (c >= 1 && c <= n) return pq[(long)(c - 1) * st];
+    return PER ? pq[(long)(wrap(c) - 1) * st] : 0.0;
+  };
+  auto V = [&](int c) -> double {
+    const int cl = PER ? wrap(c) : (c < 1 ? 1 : (c > n ? n : c));
+    double v = pv[(long)(cl - 1) * st];
+    if (DIR == 2) v = v + pvf[(long)(cl + 1) * vf.sk];
+    return v;
+  };
+  auto US = [&](int I) -> double {  // usig(I), zero outside [0, n+1]
+    if (I < 0 || I > n + 1) return 0.0;
+    return 0.5 * (V(I - 1) + V(I)) * gsig.at(I);
+  };
+  auto T = [&](int c) -> double {  // t(c) = -dtv(c)*lam_u(c)
+    if (c < 0 || c > n + 1) return 0.0;
+    double lu = 0.0;
+    if (c >= 1 && c <= n) lu = pl[(long)(c - 1) * st];
+    else if (c == 0 && lam_lo) lu = lam_lo[(long)g * L.nx * L.ny + (long)(j - 1) * L.nx + (i - 1)];
+    return -(gdtv.at(c) * lu);
+  };
+  auto DQ = [&](int I) -> double { return (I < 0 || I > n + 2) ? 0.0 : Q(I) - Q(I - 1); };
+  // lam_q at sweep index c (an interior cell or a ghost)
+  auto lam_at = [&](int c) -> double {
+    double us[6], tt[5], dq[6];
+#pragma unroll
+    for (int d = 0; d < 6; d++) us[d] = US(c - 2 + d);  // us(c-2 .. c+3)
+#pragma unroll
+    for (int d = 0; d < 5; d++) tt[d] = T(c - 2 + d);   // t(c-2 .. c+2)
+#pragma unroll
+    for (int d = 0; d < 6; d++) dq[d] = DQ(c - 2 + d);  // dq(c-2 .. c+3)
+    // interfaces J = c-1 .. c+2 (index r = J-c+1): a*e, b*e, upwind side
+    double ea[4], eb[4];
+    bool up[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const int J = c - 1 + r;
+      const double u = us[r + 1];
+      up[r] = u > 0.0;
+      ea[r] = 0.0;
+      eb[r] = 0.0;
+      if (LIM != A3G_LIM_NONE && J >= 1 && J <= n + 1) {
+        const double dqJ = dq[r + 1];
+        if (nocycle || !(fabs(dqJ) <= eps)) {
+          const double aus = fabs(u);
+          const double w = 0.5 * aus * (1.0 - gdtv.at(J) * aus);
+          const double e = w * (tt[r] - tt[r + 1]);  // t(J-1) - t(J)
+          double a, b;
+          lim_coef<LIM>(dqJ, up[r] ? dq[r] : dq[r + 2], eps, a, b);
+          ea[r] = a * e;
+          eb[r] = b * e;
+        }
+      }
+    }
+    // lam_dq(c) (r = 1) and lam_dq(c+1) (r = 2)
+    double ldq[2];
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      const int I = c + s, r = 1 + s;
+      double v = 0.0;
+      if (I >= 0 && I <= n + 2) {
+        const double u = us[r + 1];
+        const double lfsr = tt[r + 1];                          // t(I)
+        const double lfsl = (I <= n + 1) ? tt[r] : 0.0;         // t(I-1)
+        v = dmx(0.0, u) * lfsr + dmn(0.0, u) * lfsl + ea[r];
+        if (up[r + 1]) v = v + eb[r + 1];
+        if (!up[r - 1]) v = v + eb[r - 1];
+      }
+      ldq[s] = v;
+    }
+    double lam = (c >= 1 && c <= n) ? pl[(long)(c - 1) * st] : 0.0;
+    if (c >= 0 && c <= n + 1) {  // divu_m(c)*lam_fsr(c)
+      const double divm = dmn(0.0, us[3]) - dmn(0.0, us[2]);
+      lam = lam + divm * tt[2];
+    }
+    if (c + 1 >= 0 && c + 1 <= n + 1) {  // divu_p(c+1)*lam_fsl(c+1)
+      const double divp = dmx(0.0, us[3]) - dmx(0.0, us[2]);
+      lam = lam + divp * tt[2];
+    }
+    return lam + ldq[0] - ldq[1];
+  };
+  double lam = lam_at(m);
+  if (PER) {
+    if (m <= 2) lam = lam + lam_at(m + n);
+    if (m >= n - 1) lam = lam + lam_at(m - n);
+  }
+  lout[gb + cell] = lam;
+}
+
+template <int DIR, int LIM>
+static void launch_adj_dir_lim(a3g_ctx *ctx, const double *cq, const double *lin, double *lout,
+                               const double *lam_lo) {
+  const Layout &L = ctx->L;
+  dim3 grid((L.nx + 31) / 32, (L.ny + 7) / 8, L.nz * L.ns);
+  const bool per = (DIR == 0) && ctx->grid.periodic;
+  const double *vel = (DIR == 0) ? ctx->vx : (DIR == 1) ? ctx->vy : ctx->vz;
+  const Geo3 &sig = (DIR == 0) ? ctx->snx : (DIR == 1) ? ctx->sny : ctx->snz;
+  if (per)
+    k_adj_advect<DIR, LIM, true><<<grid, dim3(32, 8), 0, ctx->stream>>>(
+        L, ctx->prm.nocycle, ctx->prm.eps_thresh, cq, lin, lout, vel, ctx->vf, sig, ctx->dtv, ctx->aloft,
+        lam_lo);
+  else
+    k_adj_advect<DIR, LIM, false><<<grid, dim3(32, 8), 0, ctx->stream>>>(
+        L, ctx->prm.nocycle, ctx->prm.eps_thresh, cq, lin, lout, vel, ctx->vf, sig, ctx->dtv, ctx->aloft,
+        lam_lo);
+}
+
+template <int DIR>
+static void launch_adj_dir(a3g_ctx *ctx, const double *cq, const double *lin, double *lout,
+                           const double *lam_lo) {
+  switch (ctx->prm.limiter) {
+    case A3G_LIM_NONE: launch_adj_dir_lim<DIR, A3G_LIM_NONE>(ctx, cq, lin, lout, lam_lo); break;
+    case A3G_LIM_LAXWEN: launch_adj_dir_lim<DIR, A3G_LIM_LAXWEN>(ctx, cq, lin, lout, lam_lo); break;
+    case A3G_LIM_BW: launch_adj_dir_lim<DIR, A3G_LIM_BW>(ctx, cq, lin, lout, lam_lo); break;
+    case A3G_LIM_FROMM: launch_adj_dir_lim<DIR, A3G_LIM_FROMM>(ctx, cq, lin, lout, lam_lo); break;
+    case A3G_LIM_MINMOD: launch_adj_dir_lim<DIR, A3G_LIM_MINMOD>(ctx, cq, lin, lout, lam_lo); break;
+    case A3G_LIM_MC: launch_adj_dir_lim<DIR, A3G_LIM_MC>(ctx, cq, lin, lout, lam_lo); break;
+    default: launch_adj_dir_lim<DIR, A3G_LIM_SUPERBEE>(ctx, cq, lin, lout, lam_lo); break;
+  }
+}
+
+// lam_out <- J(cq)^T lam_in for the advection sweep along dir (0 x, 1 y, 2 z).
+int launch_adj_advect(a3g_ctx *ctx, int dir, const double *cq, const double *lin, double *lout,
+                      const double *lam_lo) {
+  int rc = refresh_dtv(ctx);
+  if (rc) return rc;
+  tbegin(ctx, A3G_K_ADJOINT);
+  if (dir == 0) launch_adj_dir<0>(ctx, cq, lin, lout, nullptr);
+  else if (dir == 1) launch_adj_dir<1>(ctx, cq, lin, lout, nullptr);
+  else launch_adj_dir<2>(ctx, cq, lin, lout, lam_lo);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  return A3G_OK;
+}
+
 }  // namespace a3g

@@ -624,4 +624,180 @@ int launch_diffcn_x(a3g_ctx *ctx) { return launch_cn_dir<0>(ctx); }
 int launch_diffcn_y(a3g_ctx *ctx) { return launch_cn_dir<1>(ctx); }
 int launch_diffcn_z(a3g_ctx *ctx) { return launch_cn_dir<2>(ctx); }
 
+// ===========================================================================
+// Discrete adjoint of the diffusion sweeps (no counterpart in the reference).
+// Both sweeps are linear; full box only.
+// ===========================================================================
+// Explicit: out(l) = q(l) + cR(l)(q(l+1)-q(l)) - cL(l)(q(l)-q(l-1)) with the
+// Neumann ghosts (periodic in x); the transpose gathers, per cell m,
+//   lam_q(m) = lam(m)(1 - cR(m) - cL(m)) + cR(m-1)lam(m-1) + cL(m+1)lam(m+1)
+// and folds the ghost terms back: cL(1)lam(1) into cell 1 and cR(n)lam(n)
+// into cell n (Neumann), or into cells n and 1 (periodic).
+template <int DIR>
+__global__ void __launch_bounds__(256) k_adj_diff(Layout L, int periodic, const double *__restrict__ lin,
+                                                  double *__restrict__ lout, Geo3 sig, Geo3 kap, Geo3 kk,
+                                                  const int32_t *__restrict__ aloft,
+                                                  const DevScalars *__restrict__ sc) {
+  const int i = blockIdx.x * 32 + threadIdx.x + 1;
+  const int j = blockIdx.y * 8 + threadIdx.y + 1;
+  const int k = blockIdx.z + 1;
+  if (i > L.nx || j > L.ny) return;
+  const int n = (DIR == 0) ? L.nx : (DIR == 1) ? L.ny : L.nz;
+  const int l = (DIR == 0) ? i : (DIR == 1) ? j : k;
+  const long st = (DIR == 0) ? 1 : (DIR == 1) ? L.P : L.PY;
+  const long cell = L.cell(i, j, k);
+  auto G = [&](const Geo3 &a, int m) {
+    return (DIR == 0) ? a.at(m, j, k) : (DIR == 1) ? a.at(i, m, k) : a.at(i, j, m);
+  };
+  const double dt = sc->dt;
+  auto cR = [&](int m) {
+    const double dsR = 2.0 * G(sig, m + 1) / (G(kap, m) + G(kap, m + 1));
+    return dt * (0.5 * (G(kk, m) + G(kk, m + 1)) * dsR) * (G(sig, m + 1) / G(kap, m));
+  };
+  auto cL = [&](int m) {
+    const double dsL = 2.0 * G(sig, m) / (G(kap, m - 1) + G(kap, m));
+    return dt * (0.5 * (G(kk, m - 1) + G(kk, m)) * dsL) * (G(sig, m) / G(kap, m));
+  };
+  const bool per = DIR == 0 && periodic;
+  const double cRl = cR(l), cLl = cL(l);
+  const double cRm = (l > 1) ? cR(l - 1) : 0.0, cLp = (l < n) ? cL(l + 1) : 0.0;
+  const double cRn = (l == 1 && per) ? cR(n) : 0.0, cL1 = (l == n && per) ? cL(1) : 0.0;
+  for (int g = 0; g < L.ns; g++) {
+    const long a = (long)g * L.PG + cell;
+    if (!aloft[g]) { lout[a] = 0.0; continue; }
+    const double lm = lin[a];
+    double v = lm - cRl * lm - cLl * lm;
+    if (l > 1) v = v + cRm * lin[a - st];
+    if (l < n) v = v + cLp * lin[a + st];
+    if (!per) {
+      if (l == 1) v = v + cLl * lm;
+      if (l == n) v = v + cRl * lm;
+    } else {
+      if (l == 1) v = v + cRn * lin[a + (long)(n - 1) * st];
+      if (l == n) v = v + cL1 * lin[a - (long)(n - 1) * st];
+    }
+    lout[a] = v;
+  }
+}
+
+// Crank-Nicolson: out = M^-1 N q.  With dgtsv's factors M = L U (L unit
+// lower with multipliers fact(r), U upper with D'(r), DU(r)), the adjoint
+// solves U^T z = lam (forward), L^T y = z (backward), then applies N^T:
+//   lam_q(r) = CC(r)y(r) + CR(r-1)y(r-1) + CL(r+1)y(r+1)
+// plus CL(0)y(0) in row 0 and CR(n-1)y(n-1) in the last row (the Neumann
+// columns of N).  One thread per line; z is parked in the output line.
+template <int DIR>
+__global__ void __launch_bounds__(128) k_adj_cn(Layout L, LineMap map, const double *__restrict__ lin,
+                                                double *__restrict__ lout, const double *__restrict__ tab,
+                                                const int32_t *__restrict__ aloft) {
+  const int na = (DIR == 0) ? L.ny : L.nx;
+  const int nb = (DIR == 2) ? L.ny : L.nz;
+  const long nlines = (long)na * nb * L.ns;
+  const long w = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (w >= nlines) return;
+  const int a = (int)(w % na) + 1;
+  const long r0 = w / na;
+  const int b = (int)(r0 % nb) + 1;
+  const int g = (int)(r0 / nb);
+  const int n = (DIR == 0) ? L.nx : (DIR == 1) ? L.ny : L.nz;
+  long base, st;
+  if (DIR == 0) { base = L.cell(1, a, b); st = 1; }
+  else if (DIR == 1) { base = L.cell(a, 1, b); st = L.P; }
+  else { base = L.cell(a, b, 1); st = L.PY; }
+  base += (long)g * L.PG;
+  const double *li = lin + base;
+  double *lo = lout + base;
+  if (!aloft[g]) {
+    for (int r = 0; r < n; r++) lo[(long)r * st] = 0.0;
+    return;
+  }
+  const long U = map.U;
+  const long F = (long)n * U;
+  const long u = map.u(a, b);
+  const double *t = tab + u;
+  CnRun R;
+  if (DIR == 0) cn_load_run(t, F, U, tab + CN_NF * F, u, R);
+  auto co = [&](int f, int l) { return (DIR == 0) ? cn_coef(t, F, U, R, f, l) : t[f * F + (long)l * U]; };
+  // U^T z = lam
+  double zp = 0.0;
+  for (int r = 0; r < n; r++) {
+    const double rhs = (r == 0) ? li[0] : li[(long)r * st] - co(CN_DU, r - 1) * zp;
+    zp = rhs / co(CN_DP, r);
+    lo[(long)r * st] = zp;
+  }
+  // L^T y = z, with lam_q(r+1) emitted as soon as y(r) is known
+  double y2 = 0.0;                 // y(r+2)
+  double y1 = lo[(long)(n - 1) * st];  // y(n-1) = z(n-1)
+  for (int r = n - 2; r >= -1; r--) {
+    double y0 = 0.0;
+    if (r >= 0) y0 = lo[(long)r * st] - co(CN_FACT, r + 1) * y1;
+    const int q = r + 1;  // finished row
+    double v = co(CN_CC, q) * y1;
+    if (q > 0) v = v + co(CN_CR, q - 1) * y0;
+    if (q < n - 1) v = v + co(CN_CL, q + 1) * y2;
+    if (q == 0) v = v + co(CN_CL, 0) * y1;
+    if (q == n - 1) v = v + co(CN_CR, n - 1) * y1;
+    lo[(long)q * st] = v;
+    y2 = y1;
+    y1 = y0;
+  }
+}
+
+template <int DIR>
+static int launch_adj_diff_dir(a3g_ctx *ctx, const double *lin, double *lout) {
+  const Layout &L = ctx->L;
+  const Geo3 &sig = (DIR == 0) ? ctx->snx : (DIR == 1) ? ctx->sny : ctx->snz;
+  const Geo3 &kk = (DIR == 0) ? ctx->kx : (DIR == 1) ? ctx->ky : ctx->kz;
+  dim3 grid((L.nx + 31) / 32, (L.ny + 7) / 8, L.nz);
+  tbegin(ctx, A3G_K_ADJOINT);
+  k_adj_diff<DIR><<<grid, dim3(32, 8), 0, ctx->stream>>>(L, ctx->grid.periodic, lin, lout, sig, ctx->kappa,
+                                                         kk, ctx->aloft, ctx->sc);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  return A3G_OK;
+}
+
+template <int DIR>
+static int launch_adj_cn_dir(a3g_ctx *ctx, const double *lin, double *lout) {
+  const Layout &L = ctx->L;
+  const int n = (DIR == 0) ? L.nx : (DIR == 1) ? L.ny : L.nz;
+  if (n <= 1) {  // the forward sweep leaves ts0 unchanged (:770)
+    A3G_CUDA(cudaMemcpyAsync(lout, lin, sizeof(double) * L.PG * L.ns, cudaMemcpyDeviceToDevice,
+                             ctx->stream));
+    return A3G_OK;
+  }
+  const Geo3 &sig = (DIR == 0) ? ctx->snx : (DIR == 1) ? ctx->sny : ctx->snz;
+  const Geo3 &kk = (DIR == 0) ? ctx->kx : (DIR == 1) ? ctx->ky : ctx->kz;
+  const int ia = (DIR == 0) ? 1 : 0, ib = (DIR == 2) ? 1 : 2;
+  LineMap map;
+  map.na = (DIR == 0) ? L.ny : L.nx;
+  map.nb = (DIR == 2) ? L.ny : L.nz;
+  map.da = varies(ctx->kappa, ia) || varies(sig, ia) || varies(kk, ia);
+  map.db = varies(ctx->kappa, ib) || varies(sig, ib) || varies(kk, ib);
+  map.U = (map.da ? map.na : 1) * (map.db ? map.nb : 1);
+  tbegin(ctx, A3G_K_ADJOINT);
+  k_cn_table<DIR><<<(map.U + 127) / 128, 128, 0, ctx->stream>>>(L, ctx->box, ctx->prm.imp_fac, map, sig,
+                                                                ctx->kappa, kk, ctx->sc, ctx->cn_buf);
+  A3G_LAUNCH_CHECK(ctx);
+  const long nlines = (long)map.na * map.nb * L.ns;
+  k_adj_cn<DIR><<<(unsigned)((nlines + 127) / 128), 128, 0, ctx->stream>>>(L, map, lin, lout, ctx->cn_buf,
+                                                                           ctx->aloft);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  return A3G_OK;
+}
+
+// lam_out <- D^T lam_in for the diffusion sweep along dir (explicit or CN
+// as the context is configured).  Full box.
+int launch_adj_diffuse(a3g_ctx *ctx, int dir, const double *lin, double *lout) {
+  if (ctx->prm.use_cn) {
+    if (dir == 0) return launch_adj_cn_dir<0>(ctx, lin, lout);
+    if (dir == 1) return launch_adj_cn_dir<1>(ctx, lin, lout);
+    return launch_adj_cn_dir<2>(ctx, lin, lout);
+  }
+  if (dir == 0) return launch_adj_diff_dir<0>(ctx, lin, lout);
+  if (dir == 1) return launch_adj_diff_dir<1>(ctx, lin, lout);
+  return launch_adj_diff_dir<2>(ctx, lin, lout);
+}
+
 }  // namespace a3g

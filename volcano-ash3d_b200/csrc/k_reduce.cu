@@ -453,6 +453,74 @@ int launch_source(a3g_ctx *ctx, int ivent, int jvent, double dt) {
 }
 
 // ---------------------------------------------------------------------------
+// observation operators for the adjoint (no counterpart in the reference's
+// transport path; the column load is Gen_Output_Vars' CloudLoad)
+// ---------------------------------------------------------------------------
+// CloudLoad(i,j) = sum_k sum_g c(i,j,k,g) * dz(k) / 1e3 (tonnes/km^2), in the
+// order of src/Output_Vars.f90:1061-1069, without the cloud mask.
+__global__ void k_cloud_load(Layout L, const double *__restrict__ c, const double *__restrict__ dz_vec,
+                             double *__restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y + 1;
+  if (i > L.nx) return;
+  double load = 0.0;
+  for (int k = 1; k <= L.nz; k++) {
+    double s = 0.0;
+    for (int g = 0; g < L.ns; g++) s = s + c[(long)g * L.PG + L.cell(i, j, k)];
+    load = load + s * dz_vec[k + 1] / 1.0e3;
+  }
+  out[(long)(j - 1) * L.nx + (i - 1)] = load;
+}
+
+// lam(i,j,k,g) += w(i,j) * dz(k) / 1e3: the transpose of the column load.
+__global__ void k_adj_cloud_load(Layout L, const double *__restrict__ w, const double *__restrict__ dz_vec,
+                                 double *__restrict__ lam) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y + 1;
+  const int kg = blockIdx.z;
+  if (i > L.nx) return;
+  const int k = kg % L.nz + 1, g = kg / L.nz;
+  const long a = (long)g * L.PG + L.cell(i, j, k);
+  lam[a] = lam[a] + w[(long)(j - 1) * L.nx + (i - 1)] * dz_vec[k + 1] / 1.0e3;
+}
+
+// lam at the vent column, (nz+1) x ns with k fastest (row nz+1, the ghost
+// that Set_BC(1) zeroes, is 0): the adjoint of the source insertion.
+__global__ void k_vent_column(Layout L, int ivent, int jvent, const double *__restrict__ lam,
+                              double *__restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (L.nz + 1) * L.ns) return;
+  const int k = t % (L.nz + 1) + 1, g = t / (L.nz + 1);
+  out[t] = (k <= L.nz) ? lam[(long)g * L.PG + L.cell(ivent, jvent, k)] : 0.0;
+}
+
+int launch_cloud_load(a3g_ctx *ctx, const double *c, double *out) {
+  const Layout &L = ctx->L;
+  tbegin(ctx, A3G_K_ADJOINT);
+  k_cloud_load<<<dim3((L.nx + 127) / 128, L.ny), 128, 0, ctx->stream>>>(L, c, ctx->dz_vec, out);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  return A3G_OK;
+}
+
+int launch_adj_cloud_load(a3g_ctx *ctx, const double *w, double *lam) {
+  const Layout &L = ctx->L;
+  tbegin(ctx, A3G_K_ADJOINT);
+  k_adj_cloud_load<<<dim3((L.nx + 127) / 128, L.ny, L.nz * L.ns), 128, 0, ctx->stream>>>(L, w, ctx->dz_vec,
+                                                                                        lam);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  return A3G_OK;
+}
+
+int launch_vent_column(a3g_ctx *ctx, int ivent, int jvent, const double *lam, double *out) {
+  const int n = (ctx->L.nz + 1) * ctx->L.ns;
+  k_vent_column<<<(n + 127) / 128, 128, 0, ctx->stream>>>(ctx->L, ivent, jvent, lam, out);
+  A3G_LAUNCH_CHECK(ctx);
+  return A3G_OK;
+}
+
+// ---------------------------------------------------------------------------
 // self-test of exact_div.cuh against the IEEE division operator
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint64_t mix64(uint64_t x) {  // splitmix64 finaliser

@@ -175,6 +175,95 @@ class Ash3dGPU:
         f = np.asarray(flags, dtype=np.int32)
         check(self.lib.a3g_set_aloft(self.ctx, iptr(f)))
 
+    # --- discrete adjoint (no counterpart in the reference) ------------------
+    # Stateful calls keep lam on the device (adj_step, adj_add_cloud_load,
+    # adj_vent_column); the adj_<sweep>(lam) helpers upload lam, apply one
+    # sweep's transpose at the current state and return the result.
+    def adj_enable(self):
+        if not getattr(self, "_adj_on", False):
+            check(self.lib.a3g_adj_enable(self.ctx))
+            self._adj_on = True
+
+    def adj_zero(self):
+        self.adj_enable()
+        check(self.lib.a3g_adj_zero(self.ctx))
+
+    def set_lambda(self, lam: np.ndarray):
+        self.adj_enable()
+        c = self.cfg
+        lv = np.zeros((c.nx + 4, c.ny + 4, c.nz + 4, c.ns), order="F")
+        lv[2:c.nx + 2, 2:c.ny + 2, 2:c.nz + 2, :] = lam
+        check(self.lib.a3g_adj_set_lambda(self.ctx, dptr(lv)))
+
+    def get_lambda(self) -> np.ndarray:
+        c = self.cfg
+        lv = np.zeros((c.nx + 4, c.ny + 4, c.nz + 4, c.ns), order="F")
+        check(self.lib.a3g_adj_get_lambda(self.ctx, dptr(lv)))
+        return lv[2:c.nx + 2, 2:c.ny + 2, 2:c.nz + 2, :].copy(order="F")
+
+    def set_lambda_dep(self, lam_dep):
+        self.adj_enable()
+        c = self.cfg
+        ld = np.zeros((c.nx, c.ny, c.ns), order="F") if lam_dep is None else \
+            np.asfortranarray(lam_dep, dtype=np.float64)
+        check(self.lib.a3g_adj_set_lambda_dep(self.ctx, dptr(ld)))
+
+    def get_lambda_dep(self) -> np.ndarray:
+        c = self.cfg
+        ld = np.zeros((c.nx, c.ny, c.ns), order="F")
+        check(self.lib.a3g_adj_get_lambda_dep(self.ctx, dptr(ld)))
+        return ld
+
+    def _adj1(self, fn, lam, *args):
+        self.set_lambda(lam)
+        check(fn(self.ctx, *args))
+        return self.get_lambda()
+
+    def adj_advect_x(self, lam):
+        return self._adj1(self.lib.a3g_adj_advect_x, lam)
+
+    def adj_advect_y(self, lam):
+        return self._adj1(self.lib.a3g_adj_advect_y, lam)
+
+    def adj_advect_z(self, lam, lam_dep=None):
+        self.set_lambda_dep(lam_dep)
+        return self._adj1(self.lib.a3g_adj_advect_vert, lam)
+
+    def adj_diffuse_horz(self, lam, itime):
+        return self._adj1(self.lib.a3g_adj_diffuse_horz, lam, itime)
+
+    def adj_diffuse_vert(self, lam):
+        return self._adj1(self.lib.a3g_adj_diffuse_vert, lam)
+
+    def adj_step(self, itime: int):
+        check(self.lib.a3g_adj_step(self.ctx, itime))
+
+    def adj_vent_column(self) -> np.ndarray:
+        c = self.cfg
+        out = np.zeros((c.nz + 1, c.ns), order="F")
+        check(self.lib.a3g_adj_vent_column(self.ctx, c.ivent, c.jvent, dptr(out)))
+        return out
+
+    def cloud_load(self) -> np.ndarray:
+        self.adj_enable()
+        c = self.cfg
+        out = np.zeros((c.nx, c.ny), order="F")
+        check(self.lib.a3g_cloud_load(self.ctx, dptr(out)))
+        return out
+
+    def adj_add_cloud_load(self, w: np.ndarray):
+        wf = np.asfortranarray(w, dtype=np.float64)
+        check(self.lib.a3g_adj_add_cloud_load(self.ctx, dptr(wf)))
+
+    def snapshot_alloc(self, n: int):
+        check(self.lib.a3g_snapshot_alloc(self.ctx, n))
+
+    def snapshot_save(self, slot: int):
+        check(self.lib.a3g_snapshot_save(self.ctx, slot))
+
+    def snapshot_load(self, slot: int):
+        check(self.lib.a3g_snapshot_load(self.ctx, slot))
+
     # --- state access --------------------------------------------------------
     def upload_level(self, level: np.ndarray):
         lv = np.asfortranarray(level, dtype=np.float64)
