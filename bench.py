@@ -148,7 +148,7 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-# algorithmic bytes per launch, per kernel class (see DESIGN.md roofline)
+# algorithmic bytes per launch, per kernel class
 # ---------------------------------------------------------------------------
 def algorithmic_bytes(cfg, kclass: str) -> float:
     cells = cfg.nx * cfg.ny * cfg.nz
@@ -404,6 +404,66 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         dist.destroy_process_group()
 
 
+def run_adjoint(args):
+    """Source inversion on C4 (projected 200x200x50, 6 grains, 24 h, explicit
+    diffusion): control = mass rate per (level, hour, grain) = 7200
+    parameters; observations = hourly column loads of a seeded truth (the
+    prior times a lognormal sigma=0.5 perturbation) with 5% noise.  Times one
+    forward run and one checkpointed gradient (K=32) through the public API,
+    host loop included, and checks the gradient against central differences
+    on --fd seeded active parameters."""
+    import torch
+    from volcano_ash3d_b200 import adjoint as adj
+    from volcano_ash3d_b200.model import Ash3dGPU
+    cfg = syn.make_config("C4")
+    inv = adj.SourceInversion(cfg, hours=int(cfg.sim_hours))
+    gpu = Ash3dGPU(cfg)
+    p_true = inv.prior(seed=4, lognormal_sigma=0.5, active_hours=inv.hours)
+    _, loads, logs, _ = inv.forward(gpu, p_true)
+    obs = {h: loads[h] * (1 + 0.05 * np.random.default_rng(100 + h).standard_normal(loads[h].shape))
+           for h in loads}
+    p = inv.prior(active_hours=inv.hours)
+    inv.forward(gpu, p, obs)  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    J, _, logs, _ = inv.forward(gpu, p, obs)
+    gpu.sync()
+    t_fwd = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    J2, grad = inv.gradient(gpu, p, obs, K=32)
+    gpu.sync()
+    t_grad = time.perf_counter() - t0
+    steps = len(logs)
+    fd = None
+    if args.fd:
+        rng = np.random.default_rng(7)
+        active = np.argwhere(p > 0)
+        errs = []
+        for _ in range(args.fd):
+            i = tuple(int(v) for v in active[rng.integers(0, len(active))])
+            h = 1e-4 * p[i]
+            pp, pm = p.copy(), p.copy()
+            pp[i] += h
+            pm[i] -= h
+            d = (inv.forward(gpu, pp, obs)[0] - inv.forward(gpu, pm, obs)[0]) / (2 * h)
+            errs.append(abs(grad[i] - d) / max(abs(d), 1e-300))
+        fd = {"params": args.fd, "step": "1e-4 of the component", "max_rel_err": float(max(errs)),
+              "median_rel_err": float(np.median(errs))}
+    line = {
+        "metric": "C4 source-inversion gradient wall time", "value": t_grad, "unit": "s",
+        "higher_is_better": False, "n_gpus": 1, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "C4: " + WORKLOAD["C4"] + ", 24 h, 7200 controls, hourly column loads",
+                   "grid": [cfg.nx, cfg.ny, cfg.nz], "grains": cfg.ns, "steps": steps,
+                   "checkpoint_every": 32},
+        "forward_s": t_fwd, "adjoint_forward_ratio": t_grad / t_fwd, "J": J2,
+        "forward_cell_grain_steps_per_s": cfg.cell_grains * steps / t_fwd,
+        "gradient_norm": float(np.linalg.norm(grad)), "fd_check": fd,
+        "gpu_launches": int(gpu.kernel_launches()),
+    }
+    print(json.dumps(line), flush=True)
+    gpu.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -417,6 +477,10 @@ def main():
                     help="the reference's LIM_* build choice (default superbee)")
     ap.add_argument("--ny", type=int, default=0,
                     help="run a y-slab of the workload with this many rows (profiling case)")
+    ap.add_argument("--adjoint", action="store_true",
+                    help="time the C4 source-inversion gradient instead of the forward step")
+    ap.add_argument("--fd", type=int, default=0,
+                    help="with --adjoint: central-difference checks on this many parameters")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -425,6 +489,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.adjoint:
+        run_adjoint(args)
         return
     run_ours(args, rank, world, local_rank)
 

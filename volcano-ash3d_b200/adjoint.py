@@ -54,16 +54,19 @@ class SourceInversion:
     def shape(self):
         return (self.cfg.nz, self.hours, self.cfg.ns)
 
-    def prior(self, seed: int = 0, lognormal_sigma: float = 0.0) -> np.ndarray:
+    def prior(self, seed: int = 0, lognormal_sigma: float = 0.0,
+              active_hours: float | None = None) -> np.ndarray:
         """Mass rate (kg/h) per level, hour, grain: the reference's Suzuki
         column for the configuration's plume, times the grain mass fraction,
-        for the hours of the eruption; optionally perturbed lognormally."""
+        for the hours of the eruption (active_hours, default the
+        configuration's duration); optionally perturbed lognormally."""
         cfg = self.cfg
         col = syn.suzuki_column(cfg)[:cfg.nz]
         rate = syn.mass_flux_rate(cfg)
+        active = cfg.duration_h if active_hours is None else active_hours
         p = np.zeros(self.shape)
         for h in range(self.hours):
-            if h < cfg.duration_h:
+            if h < active:
                 for g in range(cfg.ns):
                     p[:, h, g] = rate * cfg.bin_mass[g] * col
         if lognormal_sigma > 0.0:
