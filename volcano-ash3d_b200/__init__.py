@@ -13,7 +13,7 @@ Python modules:
   ``synthetic``  grids, geometry, met steps and source for the named workloads
   ``build``      the nvcc recipe (sm_100a)
 """
-from . import adjoint, driver, synthetic  # noqa: F401
+from . import adjoint, driver, ensemble, synthetic  # noqa: F401
 from ._lib import A3GError  # noqa: F401
 
 
