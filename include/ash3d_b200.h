@@ -177,7 +177,9 @@ int a3g_adjust_dt_from_maxima(a3g_ctx *ctx, const double *vmax3, int32_t n_gs_al
                               double *dt_out);
 /* TimeStepTotals sums, src/TimeStepTotals.f90:57-66 with Calc_AshVol_Aloft/
  * Deposit/Outflow (src/Output_Vars.f90:1255-1459).  out4 = {aloft_vol,
- * dep_vol, outflow_vol, tot_vol} (km^3 DRE); mass_aloft (ns, kg) may be NULL. */
+ * dep_vol, outflow_vol, tot_vol} (km^3 DRE); mass_aloft (ns, kg) may be NULL.
+ * Returns A3G_ERR_NONFINITE (the values still written) when a total is NaN or
+ * infinite, which the reference would carry on with silently. */
 int a3g_timestep_totals(a3g_ctx *ctx, double *out4, double *mass_aloft);
 /* get_minmax_index, src/Calc_Mesh.f90:432-542: box = {imin,imax,jmin,jmax,kmin,kmax}. */
 int a3g_get_minmax_index(a3g_ctx *ctx, int32_t ivent, int32_t jvent, int32_t kvent,

@@ -2,6 +2,7 @@
 // movement between the Fortran-layout host arrays and the device layout,
 // and the per-step entry points that mirror the reference subroutines.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -739,7 +740,12 @@ int a3g_timestep_totals(a3g_ctx *ctx, double *out4, double *mass_aloft) {
   if (!ctx->have_geometry) return fail(A3G_ERR_STATE, "geometry not set");
   int rc = launch_totals(ctx, out4, mass_aloft);
   if (rc) return rc;
-  return sync_scalars(ctx);
+  if ((rc = sync_scalars(ctx))) return rc;
+  // The reference carries a NaN on silently (its mass-conservation stop
+  // test compares false); the totals are still written, but the caller is told.
+  for (int q = 0; q < 4; q++)
+    if (!std::isfinite(out4[q])) return fail(A3G_ERR_NONFINITE, "non-finite mass total (NaN/Inf in the state)");
+  return A3G_OK;
 }
 
 int a3g_step(a3g_ctx *ctx, int32_t itime, int32_t ivent, int32_t jvent, int32_t kvent, const double *flux) {

@@ -94,7 +94,10 @@ def make_config(name: str) -> Config:
                       volume_km3=1.0e-2, duration_h=3.0, diffusivity_m2s=500.0, use_cn=False,
                       sim_hours=6.0, winds="c1", seed=1)
     if name == "C2":
-        return Config("C2", 720, 360, 60, 10, latlon=True, de=0.25, dn=0.25, lonLL=0.0, latLL=0.0,
+        # 5 S - 85 N: a top boundary on the pole itself gives the pole interface
+        # zero area and the ghost cells beyond it negative volume, so the CN
+        # coefficient of the last row is 0/0 in the reference's formulas.
+        return Config("C2", 720, 360, 60, 10, latlon=True, de=0.25, dn=0.25, lonLL=0.0, latLL=-5.0,
                       dz=0.5, ivent=360, jvent=180, fall_mps=_logspace(1e-3, 3.0, 10),
                       bin_mass=(0.1,) * 10, plume_km=15.0, volume_km3=1.0e-2, duration_h=3.0,
                       diffusivity_m2s=500.0, use_cn=True, sim_hours=24.0, winds="c2", seed=2)
