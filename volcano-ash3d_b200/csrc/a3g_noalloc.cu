@@ -57,11 +57,9 @@ __global__ void __launch_bounds__(256) k_mass_partial(const double *__restrict__
   const long n = (long)nx * ny * nz;
   const double *cg = conc + (long)g * pitch * ny * nz;
   DDn acc = {0.0, 0.0};
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
-    const long i = t % nx;
-    const long r = t / nx;  // (k-1)*ny + (j-1)
-    acc = add(acc, cg[r * pitch + i] * kappa[t]);
-  }
+  const long nrow = n / nx;  // rows (j,k), r = (k-1)*ny + (j-1)
+  for (long r = blockIdx.x; r < nrow; r += gridDim.x)
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) acc = add(acc, cg[r * pitch + i] * kappa[r * nx + i]);
   for (int o = 16; o > 0; o >>= 1) {
     DDn other;
     other.hi = __shfl_xor_sync(0xffffffffu, acc.hi, o);

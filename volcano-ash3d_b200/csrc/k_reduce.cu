@@ -44,33 +44,46 @@ __global__ void __launch_bounds__(256) k_cfl(Layout L, int latlon, const double 
                                              const double *__restrict__ vz, Geo4 vf, Geo3 snx,
                                              Geo3 sny, Geo3 kap, const double *__restrict__ dz_vec,
                                              DevScalars *sc) {
-  const long ncell = (long)L.nx * L.ny * L.nz;
-  double m0 = 0.0, m1 = 0.0, m2 = 0.0;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < ncell; t += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(t % L.nx) + 1;
-    const long r = t / L.nx;
-    const int j = (int)(r % L.ny) + 1;
-    const int k = (int)(r / L.ny) + 1;
-    const long c = L.cell(i, j, k);
-    const double ax = fabs(vx[c]), ay = fabs(vy[c]);
-    double t1, t2;
-    if (latlon) {
-      const double kp = kap.at(i, j, k);
-      t1 = ax * fmn(snx.at(i, j, k), snx.at(i + 1, j, k)) / kp;
-      t2 = ay * fmn(sny.at(i, j, k), sny.at(i, j + 1, k)) / kp;
-    } else {
-      t1 = ax;
-      t2 = ay;
-    }
-    double vfm = 0.0;
+  // block-strided rows (j,k), threads along i (a maximum does not depend on
+  // the visiting order)
+  const int nrow = L.ny * L.nz;
+  const bool vf_const = vf.si == 0 && vf.sj == 0 && vf.sk == 0;  // per-grain settling speeds
+  double vf0 = 0.0;
+  if (vf_const)
     for (int g = 0; g < L.ns; g++) {
-      const double a = fabs(vf.at(i, j, k, g));
-      if (g == 0 || a > vfm) vfm = a;
+      const double a = fabs(vf.at(1, 1, 1, g));
+      if (g == 0 || a > vf0) vf0 = a;
     }
-    const double t3 = (fabs(vz[c]) + vfm) / dz_vec[k + 1];
-    if (t1 > m0) m0 = t1;
-    if (t2 > m1) m1 = t2;
-    if (t3 > m2) m2 = t3;
+  double m0 = 0.0, m1 = 0.0, m2 = 0.0;
+  for (int r = blockIdx.x; r < nrow; r += gridDim.x) {
+    const int j = r % L.ny + 1, k = r / L.ny + 1;
+    const double rdz = dz_vec[k + 1];
+    const long rb = L.cell(1, j, k);
+    for (int i = threadIdx.x + 1; i <= L.nx; i += blockDim.x) {
+      const long c = rb + (i - 1);
+      const double ax = fabs(vx[c]), ay = fabs(vy[c]);
+      double t1, t2;
+      if (latlon) {
+        const double kp = kap.at(i, j, k);
+        t1 = ax * fmn(snx.at(i, j, k), snx.at(i + 1, j, k)) / kp;
+        t2 = ay * fmn(sny.at(i, j, k), sny.at(i, j + 1, k)) / kp;
+      } else {
+        t1 = ax;
+        t2 = ay;
+      }
+      double vfm = vf0;
+      if (!vf_const) {
+        vfm = 0.0;
+        for (int g = 0; g < L.ns; g++) {
+          const double a = fabs(vf.at(i, j, k, g));
+          if (g == 0 || a > vfm) vfm = a;
+        }
+      }
+      const double t3 = (fabs(vz[c]) + vfm) / rdz;
+      if (t1 > m0) m0 = t1;
+      if (t2 > m1) m1 = t2;
+      if (t3 > m2) m2 = t3;
+    }
   }
   m0 = warp_max(m0);
   m1 = warp_max(m1);
@@ -274,15 +287,19 @@ __global__ void __launch_bounds__(256) k_totals(Layout L, const double *__restri
     case 2: case 3: n = (long)L.ny * L.nz; break;
     default: n = (long)L.nx * L.nz; break;
   }
+  if (job == 0) {  // airborne mass: block-strided rows (j,k), threads along i
+    const double *cg = c + (long)g * L.PG;
+    const int nrow = L.ny * L.nz;
+    for (int r = blockIdx.x; r < nrow; r += gridDim.x) {
+      const int j = r % L.ny + 1, k = r / L.ny + 1;
+      const double *row = cg + (long)r * L.P;
+      for (int i = threadIdx.x; i < L.nx; i += blockDim.x) acc = dd_add(acc, row[i] * kap.at(i + 1, j, k));
+    }
+    n = 0;
+  }
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
     double v;
-    if (job == 0) {
-      const int i = (int)(t % L.nx) + 1;
-      const long r = t / L.nx;
-      const int j = (int)(r % L.ny) + 1;
-      const int k = (int)(r / L.ny) + 1;
-      v = c[(long)g * L.PG + L.cell(i, j, k)] * kap.at(i, j, k);
-    } else if (job == 1 || job == 6) {
+    if (job == 1 || job == 6) {
       const int i = (int)(t % L.nx) + 1, j = (int)(t / L.nx) + 1;
       const double *a = (job == 1) ? xy1 : xy2;
       v = a[(long)g * L.nx * L.ny + t] * kap.at(i, j, job == 1 ? 0 : L.nz + 1);
