@@ -488,8 +488,8 @@ def run_ensemble(args):
                    "steps_total": int(sum(r.steps for r in con))},
         "speedup_vs_sequential": t_seq / t_con, "sequential_s": t_seq, "concurrent_s": t_con,
         "sequential_value": work / t_seq, "autotune_s": t_tune,
-        "variants": {str(k): sum(1 for v in e.variants if v.get(k) is not None and v[k] == 0)
-                     for k in range(4)},
+        "members_choosing_variant_0": {str(k): sum(1 for v in e.variants if v.get(k) == 0)
+                                       for k in range(5)},
     }
     print(json.dumps(line), flush=True)
 

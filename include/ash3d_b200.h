@@ -231,8 +231,9 @@ int a3g_kernel_times(a3g_ctx *ctx, double *ms, uint64_t *count);
 /* Selects a kernel variant.  dir 0, 1, 2: the advection sweep along x, y, z,
  * variant 0 marching threads, 1 blocks of 4 cells, 2 blocks of 8 cells.
  * dir 3: the Crank-Nicolson x solve, variant 0 warp-tiled (default), 1 one
- * thread per line.  All variants produce identical results; only their speed
- * differs. */
+ * thread per line.  dir 4: the Crank-Nicolson y and z solves, variant 0 one
+ * grain per thread, 1 two grains of a line per thread (default), 2 four.  All variants
+ * produce identical results; only their speed differs. */
 int a3g_set_variant(a3g_ctx *ctx, int32_t dir, int32_t variant);
 int a3g_get_variant(a3g_ctx *ctx, int32_t dir, int32_t *variant);
 

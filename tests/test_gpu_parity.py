@@ -43,9 +43,10 @@ ADVECTION = ("advect_x", "advect_y", "AdvectVert")
 
 
 def _variants(op):
-    # advection: march / block-4 / block-8; horizontal diffusion: the CN x
-    # solve warp-tiled / one thread per line
-    return (0, 1, 2) if op in ADVECTION else (0, 1) if op.startswith("DiffuseHorz") else (0,)
+    # advection: march / block-4 / block-8; diffusion: the CN x solve
+    # warp-tiled / one thread per line and the y, z solves one / two grains
+    # per thread
+    return (0, 1, 2) if op in ADVECTION else (0, 1, 2)
 
 
 def _set_variant(gpu, op, variant):
@@ -53,7 +54,8 @@ def _set_variant(gpu, op, variant):
         for d in range(3):
             gpu.set_variant(d, variant)
     else:
-        gpu.set_variant(3, variant)
+        gpu.set_variant(3, variant % 2)
+        gpu.set_variant(4, variant)
 
 
 @pytest.mark.parametrize("name", CONFIGS)
@@ -120,6 +122,7 @@ def test_run_bitwise(name, variant):
     for d in range(3):
         gpu.set_variant(d, variant)
     gpu.set_variant(3, variant % 2)
+    gpu.set_variant(4, variant)
     sg = driver.run(gpu, cfg, max_steps=16)
     sr = driver.run(ref, cfg, max_steps=16)
     assert [h.dt for h in sg.history] == [h.dt for h in sr.history]

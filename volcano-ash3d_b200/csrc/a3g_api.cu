@@ -198,6 +198,7 @@ int a3g_create(const a3g_grid_desc *grid, const a3g_params *params, int device, 
   ctx->tune_advect[1] = 0;
   ctx->tune_advect[2] = 1;
   ctx->tune_cn_x = 0;
+  ctx->tune_cn_yz = 1;
   auto dmalloc = [&](void **p, size_t n) -> cudaError_t {
     cudaError_t e = cudaMalloc(p, n);
     if (e == cudaSuccess) { ctx->bytes += n; cudaMemsetAsync(*p, 0, n, ctx->stream); }
@@ -796,16 +797,17 @@ int a3g_kernel_times(a3g_ctx *ctx, double *ms, uint64_t *count) {
 
 int a3g_set_variant(a3g_ctx *ctx, int32_t dir, int32_t variant) {
   if (!ctx) return fail(A3G_ERR_ARG, "null context");
-  if (dir < 0 || dir > 3 || variant < 0 || variant > (dir == 3 ? 1 : 2))
+  if (dir < 0 || dir > 4 || variant < 0 || variant > (dir == 3 ? 1 : 2))
     return fail(A3G_ERR_ARG, "bad direction or variant");
   if (dir == 3) ctx->tune_cn_x = variant;
+  else if (dir == 4) ctx->tune_cn_yz = variant;
   else ctx->tune_advect[dir] = variant;
   return A3G_OK;
 }
 
 int a3g_get_variant(a3g_ctx *ctx, int32_t dir, int32_t *variant) {
-  if (!ctx || !variant || dir < 0 || dir > 3) return fail(A3G_ERR_ARG, "bad argument");
-  *variant = (dir == 3) ? ctx->tune_cn_x : ctx->tune_advect[dir];
+  if (!ctx || !variant || dir < 0 || dir > 4) return fail(A3G_ERR_ARG, "bad argument");
+  *variant = (dir == 3) ? ctx->tune_cn_x : (dir == 4) ? ctx->tune_cn_yz : ctx->tune_advect[dir];
   return A3G_OK;
 }
 

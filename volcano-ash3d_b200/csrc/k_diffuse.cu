@@ -338,6 +338,123 @@ __device__ __forceinline__ void cn_line(const Layout &L, const Box &box, const L
   }
 }
 
+// y and z lines, GC grains of one line per thread: the factor-table row is
+// the same for every grain, so its loads are shared, and the GC recurrences
+// are independent chains the scheduler interleaves.  Same operations per
+// grain as cn_line.
+template <int DIR, int GC>
+__device__ __forceinline__ void cn_line_gc(const Layout &L, const Box &box, const LineMap &map,
+                                           const double *__restrict__ cin, double *__restrict__ cout,
+                                           const double *__restrict__ tab,
+                                           const int32_t *__restrict__ aloft, int a, int b, int g0) {
+  constexpr int PF = 4;
+  const int n = (DIR == 1) ? L.ny : L.nz;
+  const int rmin = (DIR == 1) ? box.jmin : box.kmin;
+  const int rmax = (DIR == 1) ? box.jmax : box.kmax;
+  const int ncells = rmax - rmin + 1;
+  bool active;
+  long base, st;
+  if (DIR == 1) {
+    active = a >= box.imin && a <= box.imax && b >= box.kmin && b <= box.kmax;
+    base = L.cell(a, 1, b); st = L.P;
+  } else {
+    active = a >= box.imin && a <= box.imax && b >= box.jmin && b <= box.jmax;
+    base = L.cell(a, b, 1); st = L.PY;
+  }
+  const double *q[GC];
+  double *x[GC];
+  bool on[GC], any = false;
+#pragma unroll
+  for (int u = 0; u < GC; u++) {
+    const int g = g0 + u < L.ns ? g0 + u : L.ns - 1;
+    q[u] = cin + base + (long)g * L.PG;
+    x[u] = cout + base + (long)g * L.PG;
+    on[u] = g0 + u < L.ns && active && aloft[g] != 0;
+    any = any || on[u];
+    if (g0 + u < L.ns && !on[u])
+      for (int c = 1; c <= n; c++) x[u][(long)(c - 1) * st] = 0.0;
+    else if (on[u]) {
+      for (int c = 1; c < rmin; c++) x[u][(long)(c - 1) * st] = 0.0;
+      for (int c = rmax + 1; c <= n; c++) x[u][(long)(c - 1) * st] = 0.0;
+    }
+  }
+  if (!any) return;
+  const long U = map.U;
+  const long F = (long)ncells * U;
+  const double *t = tab + map.u(a, b);
+  auto co = [&](int f, int l) { return t[f * F + (long)l * U]; };
+  const long off = (long)(rmin - 1) * st;
+  // forward elimination with the right-hand side built on the fly, :813-851
+  double qm[GC], qc[GC], bp[GC];
+#pragma unroll
+  for (int u = 0; u < GC; u++) {
+    qm[u] = on[u] ? q[u][off] : 0.0;  // BC_left_t0 = q(rmin)
+    qc[u] = qm[u];
+    bp[u] = 0.0;
+  }
+#pragma unroll 4
+  for (int l = 0; l < ncells; l++) {
+    const double cl = co(CN_CL, l), cc = co(CN_CC, l), cr = co(CN_CR, l), fa = co(CN_FACT, l);
+#pragma unroll
+    for (int u = 0; u < GC; u++) {
+      const double qp = (l + 1 < ncells) ? (on[u] ? q[u][off + (long)(l + 1) * st] : 0.0) : qc[u];
+      const double B = cl * qm[u] + cc * qc[u] + cr * qp;
+      bp[u] = (l == 0) ? B : B - fa * bp[u];
+      if (on[u]) x[u][off + (long)l * st] = bp[u];
+      qm[u] = qc[u];
+      qc[u] = qp;
+    }
+  }
+  // back substitution with a PF-deep prefetch of B'
+  double ring[GC][PF];
+#pragma unroll
+  for (int u = 0; u < GC; u++)
+#pragma unroll
+    for (int p = 0; p < PF; p++)
+      ring[u][p] = (on[u] && ncells - 1 - p >= 0) ? x[u][off + (long)(ncells - 1 - p) * st] : 0.0;
+  double xn[GC];
+#pragma unroll
+  for (int u = 0; u < GC; u++) xn[u] = 0.0;
+  for (int l0 = ncells - 1; l0 >= 0; l0 -= PF) {
+#pragma unroll
+    for (int p = 0; p < PF; p++) {
+      const int l = l0 - p;
+      if (l >= 0) {
+        const int lp = l - PF;
+        const double du = co(CN_DU, l), dp = co(CN_DP, l), rd = co(CN_RDP, l);
+#pragma unroll
+        for (int u = 0; u < GC; u++) {
+          const double b2 = ring[u][p];
+          ring[u][p] = (on[u] && lp >= 0) ? x[u][off + (long)lp * st] : 0.0;
+          const double num = (l == ncells - 1) ? b2 : b2 - du * xn[u];
+          const double v = div_rn_rcp(num, dp, rd);
+          if (on[u]) x[u][off + (long)l * st] = v;
+          xn[u] = v;
+        }
+      }
+    }
+  }
+}
+
+template <int DIR, int GC>
+__global__ void __launch_bounds__(128) k_cn_solve_gc(Layout L, Box box, LineMap map,
+                                                     const double *__restrict__ cin,
+                                                     double *__restrict__ cout,
+                                                     const double *__restrict__ tab,
+                                                     const int32_t *__restrict__ aloft) {
+  const int na = L.nx;
+  const int nb = (DIR == 2) ? L.ny : L.nz;
+  const int ngr = (L.ns + GC - 1) / GC;
+  const long nlines = (long)na * nb * ngr;
+  const long w = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (w >= nlines) return;
+  const int a = (int)(w % na) + 1;
+  const long r = w / na;
+  const int b = (int)(r % nb) + 1;
+  const int gg = (int)(r / nb);
+  cn_line_gc<DIR, GC>(L, box, map, cin, cout, tab, aloft, a, b, gg * GC);
+}
+
 // Solve kernel: one thread per line (a, b, grain), lines enumerated with a
 // fastest so that a warp holds neighbouring lines (neighbouring i for y and
 // z lines: coalesced loads and stores).
@@ -608,6 +725,14 @@ static int launch_cn_dir(a3g_ctx *ctx) {
   if (DIR == 0 && ctx->tune_cn_x == 0) {
     const long nwarps = (nlines + 31) / 32;
     k_cn_solve_xt<<<(unsigned)((nwarps + XT_WARPS - 1) / XT_WARPS), 32 * XT_WARPS, 0, ctx->stream>>>(
+        L, box, map, ctx->c0, ctx->c1, ctx->cn_buf, ctx->aloft);
+  } else if (DIR != 0 && ctx->tune_cn_yz == 1 && L.ns >= 2) {
+    const long nl2 = (long)map.na * map.nb * ((L.ns + 1) / 2);
+    k_cn_solve_gc<DIR == 0 ? 1 : DIR, 2><<<(unsigned)((nl2 + 127) / 128), 128, 0, ctx->stream>>>(
+        L, box, map, ctx->c0, ctx->c1, ctx->cn_buf, ctx->aloft);
+  } else if (DIR != 0 && ctx->tune_cn_yz == 2 && L.ns >= 2) {
+    const long nl4 = (long)map.na * map.nb * ((L.ns + 3) / 4);
+    k_cn_solve_gc<DIR == 0 ? 1 : DIR, 4><<<(unsigned)((nl4 + 127) / 128), 128, 0, ctx->stream>>>(
         L, box, map, ctx->c0, ctx->c1, ctx->cn_buf, ctx->aloft);
   } else {
     k_cn_solve<DIR><<<(unsigned)((nlines + 127) / 128), 128, 0, ctx->stream>>>(

@@ -47,8 +47,9 @@ def c3_members(n: int = 64, seed: int = 3, hours: float = 12.0) -> list[syn.Conf
 
 
 def autotune(cfg: syn.Config, device: int = 0, steps: int = 2) -> dict:
-    """{direction: variant} for directions 0..2 (advection) and 3 (CN x
-    solve), timed with the per-kernel CUDA events on a scratch context."""
+    """{direction: variant} for directions 0..2 (advection), 3 (CN x solve)
+    and 4 (CN y and z solves), timed with the per-kernel CUDA events on a
+    scratch context."""
     from .model import Ash3dGPU
     m = Ash3dGPU(cfg, device=device)
     rng = np.random.default_rng(0)
@@ -57,9 +58,10 @@ def autotune(cfg: syn.Config, device: int = 0, steps: int = 2) -> dict:
     far = 1.0e9  # never clip dt to the end of the run while timing
     driver.step(m, st, simtime=far, totals=False)
     choice = {}
-    keys = {0: "advect_x", 1: "advect_y", 2: "advect_z", 3: "cn_solve_x"}
-    for d, options in ((0, (0, 1, 2)), (1, (0, 1, 2)), (2, (0, 1, 2)), (3, (0, 1))):
-        if d == 3 and not cfg.use_cn:
+    keys = {0: ("advect_x",), 1: ("advect_y",), 2: ("advect_z",), 3: ("cn_solve_x",),
+            4: ("cn_solve_y", "cn_solve_z")}
+    for d, options in ((0, (0, 1, 2)), (1, (0, 1, 2)), (2, (0, 1, 2)), (3, (0, 1)), (4, (0, 1, 2))):
+        if d >= 3 and not cfg.use_cn:
             continue
         best, best_ms = None, None
         for v in options:
@@ -67,7 +69,8 @@ def autotune(cfg: syn.Config, device: int = 0, steps: int = 2) -> dict:
             m.kernel_timing(True)
             for _ in range(steps):
                 driver.step(m, st, simtime=far, totals=False)
-            ms = m.kernel_times()[keys[d]][0]
+            kt = m.kernel_times()
+            ms = sum(kt[k][0] for k in keys[d])
             m.kernel_timing(False)
             if best_ms is None or ms < best_ms:
                 best, best_ms = v, ms
