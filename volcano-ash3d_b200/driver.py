@@ -117,11 +117,24 @@ def grain_range(ns: int, rank: int, world: int) -> tuple[int, int]:
     return lo, lo + base + (1 if rank < extra else 0)
 
 
+def next_write_time(write_times, time: float) -> float:
+    """NextWriteTime: the first output time still ahead (Output_Results.f90:
+    183-189), or 1/EPS_SMALL once none is left."""
+    for t in write_times or ():
+        if t > time + 1.0e-5:  # within DT_MIN of it: that output is done
+            return float(t)
+    return 1.0 / 1.0e-6
+
+
 def step(model, st: RunState, simtime: float | None = None, totals: bool = True,
-         comm: Comm | None = None, n_gs_aloft_total: int | None = None) -> StepRecord:
-    """Advances the model by one reference time step."""
+         comm: Comm | None = None, n_gs_aloft_total: int | None = None,
+         write_times=None) -> StepRecord:
+    """Advances the model by one reference time step.  dt is clipped to the
+    next of write_times (the control file's output times), when given, and to
+    simtime."""
     cfg = st.cfg
     simtime = cfg.sim_hours if simtime is None else simtime
+    nwt = next_write_time(write_times, st.time) if write_times is not None else simtime
     st.itime += 1
     model.step_prologue()
     h = int(math.floor(st.time))
@@ -130,10 +143,10 @@ def step(model, st: RunState, simtime: float | None = None, totals: bool = True,
         st.hour = h
     model.interp_winds(st.time - h)
     if comm is None:
-        dt = model.Adjust_DT(st.time, simtime, simtime)
+        dt = model.Adjust_DT(st.time, nwt, simtime)
     else:
         vmax = comm.max(model.cfl_maxima())
-        dt = model.adjust_dt_from_maxima(vmax, n_gs_aloft_total, st.time, simtime, simtime)
+        dt = model.adjust_dt_from_maxima(vmax, n_gs_aloft_total, st.time, nwt, simtime)
     frac = syn.pulse_fraction(cfg, st.time, dt)
     if frac > 0.0:
         flux = syn.source_flux(cfg, st.norm_col, st.kappa, frac)

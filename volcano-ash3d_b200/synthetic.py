@@ -68,7 +68,9 @@ class Config:
     limiter: str = "superbee"
     cfl: float = 0.8
     sim_hours: float = 6.0
-    winds: str = "c1"        # 'c1' steady shear, 'c2' jet + wave + noise, 'random'
+    winds: str = "c1"        # 'c1' steady shear, 'c2' jet + wave + noise, 'random', 'const', 'sounding'
+    wind_uv: tuple = (0.0, 0.0)   # 'const': uniform (u, v) in m/s
+    sounding: tuple = ()     # 'sounding': ((z_m, u_mps, v_mps), ...) of a 1-D wind profile
     seed: int = 1
     fast_subgrid: bool = False
     magma_density: float = 2500.0
@@ -290,6 +292,20 @@ class MetSource:
             # 5% multiplicative noise, drawn in FP32 to keep generation cheap
             u = u * (1.0 + 0.05 * rng.standard_normal((nx, ny, nz), dtype=np.float32))
             v = v * (1.0 + 0.05 * rng.standard_normal((nx, ny, nz), dtype=np.float32))
+            w = np.zeros((nx, ny, nz))
+        elif cfg.winds == "const":
+            u = np.full((nx, ny, nz), np.float32(cfg.wind_uv[0]))
+            v = np.full((nx, ny, nz), np.float32(cfg.wind_uv[1]))
+            w = np.zeros((nx, ny, nz))
+        elif cfg.winds == "sounding":
+            # a 1-D profile (heights in m) at the cell centres: linear in height
+            # between its levels, the top level's value above it (the
+            # iHeightHandler = 2 rule of the control file), FP32 as met data are
+            zs = np.array([p[0] for p in cfg.sounding], dtype=np.float64) / 1000.0
+            us = np.array([p[1] for p in cfg.sounding], dtype=np.float64)
+            vs = np.array([p[2] for p in cfg.sounding], dtype=np.float64)
+            u = np.broadcast_to(np.interp(self.z, zs, us).astype(np.float32), (nx, ny, nz))
+            v = np.broadcast_to(np.interp(self.z, zs, vs).astype(np.float32), (nx, ny, nz))
             w = np.zeros((nx, ny, nz))
         else:  # 'random': smooth random field for small parity cases
             rng = np.random.default_rng(cfg.seed * 7919 + hour)
