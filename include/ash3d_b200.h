@@ -229,13 +229,35 @@ int a3g_kernel_times(a3g_ctx *ctx, double *ms, uint64_t *count);
 
 /* ---- tuning (no counterpart in the reference) ---- */
 /* Selects a kernel variant.  dir 0, 1, 2: the advection sweep along x, y, z,
- * variant 0 marching threads, 1 blocks of 4 cells, 2 blocks of 8 cells.
+ * variant 0 marching threads, 1 blocks of 4 cells, 2 blocks of 8 cells, and
+ * for x only 3, warps marching 32 rows through shared-memory tiles.
  * dir 3: the Crank-Nicolson x solve, variant 0 warp-tiled (default), 1 one
  * thread per line.  dir 4: the Crank-Nicolson y and z solves, variant 0 one
  * grain per thread, 1 two grains of a line per thread (default), 2 four.  All variants
  * produce identical results; only their speed differs. */
 int a3g_set_variant(a3g_ctx *ctx, int32_t dir, int32_t variant);
 int a3g_get_variant(a3g_ctx *ctx, int32_t dir, int32_t *variant);
+
+/* ---- output products (Gen_Output_Vars, src/Output_Vars.f90:1192-1240) ----
+ * The 2-D products the reference writes at output and log steps, computed
+ * on the device from the current state: ConcentrationCalculator (column
+ * cloud load in t/km2 masked below CLOUDLOAD_THRESH, cloud top and bottom
+ * heights from CLOUDCON_THRESH, peak concentration in mg/m3, the cloud mask;
+ * :1026-1123), AshThicknessCalculator (deposit thickness in mm from
+ * DepositGranularity and its mask; :855-895), CloudAreaCalculator (:1138-1177)
+ * and the arrival-time marks (:1226-1236), which persist in the context.
+ * z_cc: z_cc_pd(1:nz) (km).  Defaults: CLOUDCON_THRESH 1e-3 kg/km3,
+ * CLOUDLOAD_THRESH 0.2 t/km2, DEPO_THRESH 0.01 mm, DepositDensity 1000 kg/m3. */
+int a3g_set_output_params(a3g_ctx *ctx, const double *z_cc, double cloudcon_thresh,
+                          double cloudload_thresh, double depo_thresh, double deposit_density);
+/* Arrival times back to "not arrived" (-1). */
+int a3g_output_reset(a3g_ctx *ctx);
+/* All 2-D arrays (nx,ny), i fastest; any output may be NULL.  areas =
+ * {CloudArea, DepositAreaCovered, CloudLoadArea(1:5)} (km2), summed in the
+ * reference's loop order over the current subgrid box. */
+int a3g_output_vars(a3g_ctx *ctx, double time, double *cloud_load, double *max_height,
+                    double *min_height, double *max_conc, int32_t *mask_cloud, double *dep_thick,
+                    int32_t *mask_dep, double *cloud_arrival, double *dep_arrival, double *areas);
 
 /* ---- discrete adjoint (no counterpart in the reference) ----
  * Reverse mode of the transport step for source inversion.  Every sweep is

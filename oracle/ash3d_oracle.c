@@ -1287,3 +1287,84 @@ void orc_adj_diffuse_horz(orc_state *s, double *lam, int itime) {
 void orc_adj_diffuse_vert(orc_state *s, double *lam) {
   if (s->use_cn) adj_cn_dir(s, lam, 2); else adj_diff_dir(s, lam, 2);
 }
+
+/* ======================================================================== */
+/* Output products of Gen_Output_Vars (src/Output_Vars.f90:1192-1240):       */
+/* ConcentrationCalculator (:1026-1123), AshThicknessCalculator (:855-895),  */
+/* CloudAreaCalculator (:1138-1177) and the arrival-time marks (:1226-1236). */
+/* 2-D arrays are (nx,ny), i fastest; z_cc holds z_cc_pd(1:nz).              */
+/* areas = {CloudArea, DepositAreaCovered, CloudLoadArea(1:5)}.              */
+/* ======================================================================== */
+void orc_output_vars(orc_state *s, const double *z_cc, double cloudcon_thresh,
+                     double cloudload_thresh, double depo_thresh, double deposit_density,
+                     double time, double *cloud_load, double *max_height, double *min_height,
+                     double *max_conc, int32_t *mask_cloud, double *dep_thick, int32_t *mask_dep,
+                     double *cloud_arrival, double *dep_arrival, double *areas) {
+  const int nx = s->nx, ny = s->ny, nz = s->nz, ns = s->ns;
+  const double *dz = s->dz_vec + 1; /* dz[k] = dz_vec_pd(k) */
+  double *tc = (double *)calloc((size_t)nz + 1, sizeof(double));
+  /* AshThicknessCalculator */
+  double dep_area = 0.0;
+  for (int i = 1; i <= nx; i++)
+    for (int j = 1; j <= ny; j++) {
+      const size_t o = (size_t)(i - 1) + (size_t)nx * (j - 1);
+      double sg = 0.0;
+      for (int n = 1; n <= ns; n++) sg = sg + s->deposit[dep(s, i, j, n)];
+      dep_thick[o] = sg * dz[1] / 1.0e6 / deposit_density * 1.0e3;
+      mask_dep[o] = dep_thick[o] > depo_thresh;
+      if (mask_dep[o]) dep_area = dep_area + s->sig_nz[i3(s, i, j, 1)];
+    }
+  /* ConcentrationCalculator */
+  for (int i = 1; i <= nx; i++)
+    for (int j = 1; j <= ny; j++) {
+      const size_t o = (size_t)(i - 1) + (size_t)nx * (j - 1);
+      cloud_load[o] = 0.0; max_conc[o] = 0.0; max_height[o] = 0.0; min_height[o] = 100.0;
+      mask_cloud[o] = 0;
+    }
+  double cloud_area = 0.0;
+  if (ns > 0)
+    for (int i = s->imin; i <= s->imax; i++)
+      for (int j = s->jmin; j <= s->jmax; j++) {
+        const size_t o = (size_t)(i - 1) + (size_t)nx * (j - 1);
+        for (int k = 1; k <= nz; k++) {
+          double sg = 0.0;
+          for (int n = 1; n <= ns; n++) sg = sg + s->concen[c5(s, i, j, k, n, 0)];
+          cloud_load[o] = cloud_load[o] + sg * dz[k] / 1.0e3;
+          tc[k] = sg;
+          if (tc[k] >= cloudcon_thresh) max_height[o] = z_cc[k - 1] + 0.5 * dz[k];
+        }
+        for (int k = nz; k >= 1; k--)
+          if (tc[k] <= cloudcon_thresh) min_height[o] = z_cc[k - 1] - 0.5 * dz[k];
+        double mx = tc[1];
+        for (int k = 2; k <= nz; k++) mx = fmx(mx, tc[k]);
+        mask_cloud[o] = cloud_load[o] >= cloudload_thresh;
+        if (mask_cloud[o]) {
+          if (min_height[o] < 0.0 && max_height[o] > 0.0) min_height[o] = 0.0;
+          min_height[o] = fmn(max_height[o], min_height[o]);
+          cloud_area = cloud_area + s->sig_nz[i3(s, i, j, 1)];
+          max_conc[o] = mx * 1.0e6 / 1.0e9;
+        } else {
+          cloud_load[o] = 0.0; max_conc[o] = 0.0; max_height[o] = 0.0; min_height[o] = 0.0;
+        }
+      }
+  /* CloudAreaCalculator */
+  static const double load_val[5] = {0.24, 1.0, 2.0, 4.0, 6.0};
+  double la[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  if (ns > 0)
+    for (int i = s->imin; i <= s->imax; i++)
+      for (int j = s->jmin; j <= s->jmax; j++) {
+        const double cell = s->sig_nz[i3(s, i, j, 1)];
+        const size_t o = (size_t)(i - 1) + (size_t)nx * (j - 1);
+        for (int k = 0; k < 5; k++)
+          if (cloud_load[o] > load_val[k]) la[k] = la[k] + cell;
+      }
+  /* arrival times */
+  for (size_t o = 0; o < (size_t)nx * ny; o++) {
+    if (mask_dep[o] && dep_arrival[o] < 0.0) dep_arrival[o] = time;
+    if (mask_cloud[o] && cloud_arrival[o] < 0.0) cloud_arrival[o] = time;
+  }
+  areas[0] = cloud_area;
+  areas[1] = dep_area;
+  for (int k = 0; k < 5; k++) areas[2 + k] = la[k];
+  free(tc);
+}

@@ -146,6 +146,17 @@ void orc_adj_advect_y(orc_state *s, double *lam);
 void orc_adj_advect_z(orc_state *s, double *lam, const double *lam_dep);
 void orc_adj_diffuse_horz(orc_state *s, double *lam, int itime);
 void orc_adj_diffuse_vert(orc_state *s, double *lam);
+/* Output products of Gen_Output_Vars (src/Output_Vars.f90:1192-1240):
+ * cloud load (masked), cloud top/bottom, maximum concentration (mg/m3), cloud
+ * and deposit masks, deposit thickness (mm), the arrival-time marks (arrays
+ * start at -1 and keep the first time a mask holds) and areas = {CloudArea,
+ * DepositAreaCovered, CloudLoadArea(1:5)}.  2-D arrays (nx,ny), i fastest;
+ * z_cc = z_cc_pd(1:nz). */
+void orc_output_vars(orc_state *s, const double *z_cc, double cloudcon_thresh,
+                     double cloudload_thresh, double depo_thresh, double deposit_density,
+                     double time, double *cloud_load, double *max_height, double *min_height,
+                     double *max_conc, int32_t *mask_cloud, double *dep_thick, int32_t *mask_dep,
+                     double *cloud_arrival, double *dep_arrival, double *areas);
 /* OpenMP thread count for the advection rows (<=0: runtime default). */
 void orc_set_threads(int n);
 int  orc_get_threads(void);

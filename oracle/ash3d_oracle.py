@@ -86,6 +86,8 @@ def load() -> C.CDLL:
             ("orc_adj_advect_x", None, [S, D]), ("orc_adj_advect_y", None, [S, D]),
             ("orc_adj_advect_z", None, [S, D, D]),
             ("orc_adj_diffuse_horz", None, [S, D, C.c_int]), ("orc_adj_diffuse_vert", None, [S, D]),
+            ("orc_output_vars", None, [S, D, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                                       D, D, D, D, C.POINTER(C.c_int32), D, C.POINTER(C.c_int32), D, D, D]),
         ]:
             fn = getattr(lib, name)
             fn.restype = res
@@ -386,6 +388,39 @@ class OracleModel:
 
     def snapshot_load(self, slot):
         self.set_interior(self._snaps[slot])
+
+    # --- output products (Gen_Output_Vars) ----------------------------------
+    OUTPUT_DEFAULTS = dict(cloudcon_thresh=1.0e-3, cloudload_thresh=0.2, depo_thresh=1.0e-2,
+                           deposit_density=1000.0)
+
+    def output_reset(self):
+        c = self.cfg
+        self._arr_cloud = np.full((c.nx, c.ny), -1.0, order="F")
+        self._arr_dep = np.full((c.nx, c.ny), -1.0, order="F")
+
+    def output_vars(self, time, **thresholds):
+        """Gen_Output_Vars products of the current state (dict of arrays)."""
+        c = self.cfg
+        t = dict(self.OUTPUT_DEFAULTS, **thresholds)
+        if getattr(self, "_arr_cloud", None) is None:
+            self.output_reset()
+        _, zcc, _ = self.syn.zgrid(c)
+        z_cc = np.ascontiguousarray(zcc[2:c.nz + 2])
+        f = lambda: np.zeros((c.nx, c.ny), order="F")
+        out = dict(cloud_load=f(), max_height=f(), min_height=f(), max_conc=f(), dep_thick=f())
+        mc = np.zeros((c.nx, c.ny), dtype=np.int32, order="F")
+        md = np.zeros((c.nx, c.ny), dtype=np.int32, order="F")
+        areas = np.zeros(7)
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+        self.lib.orc_output_vars(self.ps, _d(z_cc), t["cloudcon_thresh"], t["cloudload_thresh"],
+                                 t["depo_thresh"], t["deposit_density"], time,
+                                 _d(out["cloud_load"]), _d(out["max_height"]), _d(out["min_height"]),
+                                 _d(out["max_conc"]), ip(mc), _d(out["dep_thick"]), ip(md),
+                                 _d(self._arr_cloud), _d(self._arr_dep), _d(areas))
+        out.update(mask_cloud=mc.astype(bool), mask_dep=md.astype(bool),
+                   cloud_arrival=self._arr_cloud.copy(), dep_arrival=self._arr_dep.copy(),
+                   cloud_area=areas[0], dep_area=areas[1], cloud_load_area=areas[2:].copy())
+        return out
 
     def zero_outflows(self):
         for a in (self.out_yz1, self.out_yz2, self.out_xz1, self.out_xz2, self.out_xy1, self.out_xy2,

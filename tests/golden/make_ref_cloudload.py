@@ -1,8 +1,9 @@
 """Builds tests/golden/ref_cloudload.json from the reference's own regression
 tests (tests/test_01, tests/test_02 of the Ash3d source tree): the control
 parameters this restatement needs, read from the control file and the 1-D
-wind sounding, and the golden CloudLoad outputs (ESRI ASCII grids of the
-reference binary at 2 h and 4 h), kept as their nonzero cells.
+wind sounding, and the golden output grids of the reference binary (ESRI
+ASCII): CloudLoad, CloudHeight and CloudConcentration at 2 h and 4 h and
+CloudArrivalTime, each kept as its nonzero cells (fill values included).
 
     python tests/golden/make_ref_cloudload.py [path/to/Ash3d/source/tree]
 
@@ -55,7 +56,7 @@ def sounding(path):
 
 
 def cloudload(path):
-    """CloudLoad grid as [i][j] (j from the south), nonzero cells only."""
+    """A 2-D output grid as [i][j] (j from the south), nonzero cells only."""
     head = dict(ln.split()[:2] for ln in path.read_text().splitlines()[:2])
     nx, ny = int(head["NCOLS"]), int(head["NROWS"])
     g = np.loadtxt(path, skiprows=6).reshape(ny, nx)[::-1, :].T
@@ -70,7 +71,12 @@ def main(root):
         t = root / "tests" / test
         out[test] = {"control": control(t / inp), "sounding": sounding(t / "Hanford_Ncol_N.txt"),
                      "cloudload": {h: cloudload(t / "output" / f"CloudLoad_{float(h):06.2f}hrs.dat")
-                                   for h in ("2.0", "4.0")}}
+                                   for h in ("2.0", "4.0")},
+                     "cloudheight": {h: cloudload(t / "output" / f"CloudHeight_{float(h):06.2f}hrs.dat")
+                                     for h in ("2.0", "4.0")},
+                     "cloudconc": {h: cloudload(t / "output" / f"CloudConcentration_{float(h):06.2f}hrs.dat")
+                                   for h in ("2.0", "4.0")},
+                     "cloudarrival": cloudload(t / "output" / "CloudArrivalTime.dat")}
     (HERE / "ref_cloudload.json").write_text(json.dumps(out, separators=(",", ":")))
 
 

@@ -1,25 +1,28 @@
-"""The transport path against the reference program's own regression
-outputs (its tests/test_01 and tests/test_02; fixture built by
-tests/golden/make_ref_cloudload.py from the control files, the wind
-soundings and the golden CloudLoad grids).
+"""The transport path and its output products against the reference
+program's own regression outputs (its tests/test_01 and tests/test_02;
+fixture built by tests/golden/make_ref_cloudload.py from the control files,
+the wind soundings and the golden CloudLoad, CloudHeight, CloudConcentration
+and CloudArrivalTime grids).
 
 Each case is rerun from its control file's values: 50x50 cells of 2 km, dz
 1 km up to ZPADDING (1.3) times the plume height, one Suzuki (k=4) pulse of
 0.16 km3 DRE to 18 km over 1 h, one tracer bin (v_s = 0), superbee, explicit
 diffusion (the build the goldens come from), FAST_SUBGRID on (the default
-build), output times 2 h and 4 h clipping dt.  The unmasked column load is
-masked below CLOUDLOAD_THRESH = 0.2 t/km2 (src/Output_Vars.f90:114,
-1089-1111) and compared with the reference's check, L2 error / (nx*ny)
-(src/tools/Ash3d_ASCII_check.f90:213-229).
+build), output times 2 h and 4 h clipping dt, and Gen_Output_Vars after every
+step (log_step = 1).  Each grid is compared with the reference's own check,
+L2 error / (nx*ny) (src/tools/Ash3d_ASCII_check.f90:213-229).
 
-test_02 (uniform 1 m/s wind, 500 m2/s diffusion) matches to 2e-4 against the
-reference's tolerance of 0.1, within the FP32 rounding of the golden files.
-test_01 (a rotating 1-D sounding, no diffusion) reaches 0.038 / 0.088
-against the reference's 0.01: the sounding is spread onto the grid by
-MetReader, a library outside the reference tree, whose interpolation is
-restated here as linear in height with the top value held above the last
-level (iHeightHandler = 2).  Its bound here is 0.15, and the cloud's centroid
-and spread (first and second moments) match to 3e-5 relative.
+test_02 (uniform 1 m/s wind, 500 m2/s diffusion) matches every grid: cloud
+load to 2e-4 against the reference's tolerance of 0.1 (the FP32 rounding of
+the golden files), cloud height and arrival times exactly, concentration to
+2e-5.  test_01 (a rotating 1-D sounding, no diffusion) matches cloud height
+exactly and arrival times to 4e-5 (the reference's bound is 0.01); its cloud
+load and concentration reach 0.04-0.09 against 0.01: the sounding is spread
+onto the grid by MetReader, a library outside the reference tree, whose
+interpolation is restated here as linear in height with the top value held
+above the last level (iHeightHandler = 2).  Their bound here is 0.15, and the
+cloud's centroid and spread (first and second moments) match to 3e-5
+relative.
 """
 import json
 import math
@@ -33,7 +36,7 @@ from volcano_ash3d_b200 import driver
 from volcano_ash3d_b200 import synthetic as syn
 
 FIX = json.loads((pathlib.Path(__file__).resolve().parent / "golden" / "ref_cloudload.json").read_text())
-ZPADDING, CLOUDLOAD_THRESH = 1.3, 0.2
+ZPADDING = 1.3
 
 
 def config(test: str) -> syn.Config:
@@ -48,9 +51,9 @@ def config(test: str) -> syn.Config:
                       fast_subgrid=True)
 
 
-def golden(test: str, hour: str, nx: int, ny: int) -> np.ndarray:
+def grid(test: str, key: str, hour, nx: int, ny: int) -> np.ndarray:
     g = np.zeros((nx, ny))
-    for i, j, v in FIX[test]["cloudload"][hour]:
+    for i, j, v in (FIX[test][key][hour] if hour else FIX[test][key]):
         g[i, j] = v
     return g
 
@@ -65,29 +68,45 @@ def moments(a: np.ndarray, dx: float):
 
 
 def rerun(model, cfg):
-    """(hour, masked cloud load) at the control file's output times."""
+    """Output products at the control file's output times and the final
+    cloud arrival times."""
     st = driver.new_state(cfg)
-    out = {}
-    while st.time < 4.0 - 1e-9:
+    model.output_reset()
+    out, last = {}, None
+    while st.time < cfg.sim_hours - 1e-9:
         driver.step(model, st, simtime=cfg.sim_hours, totals=False, write_times=[2.0, 4.0])
+        last = model.output_vars(st.time)
         for h in ("2.0", "4.0"):
             if abs(st.time - float(h)) < 1e-5:
-                load = model.cloud_load()
-                load[load < CLOUDLOAD_THRESH] = 0.0
-                out[h] = load
+                out[h] = last
+    out["arrival"] = np.where(last["cloud_arrival"] >= 0.0, last["cloud_arrival"], -9999.0)
     return out
 
 
-def check(test, loads, cfg):
-    for h, load in loads.items():
-        g = golden(test, h, cfg.nx, cfg.ny)
-        l2 = math.sqrt(((load - g) ** 2).sum()) / cfg.nx / cfg.ny
+def check(test, res, cfg):
+    """CloudLoad, CloudHeight (MaxHeight where the cloud mask holds, else
+    -9999, src/Output_Results.f90:219-228), CloudConcentration and
+    CloudArrivalTime against the golden grids."""
+    nx, ny = cfg.nx, cfg.ny
+    l2 = lambda a, b: math.sqrt(((a - b) ** 2).sum()) / nx / ny
+    for h in ("2.0", "4.0"):
+        o = res[h]
+        load, gl = o["cloud_load"], grid(test, "cloudload", h, nx, ny)
+        height = np.where(o["mask_cloud"], o["max_height"], -9999.0)
+        gh = grid(test, "cloudheight", h, nx, ny)
+        gc = grid(test, "cloudconc", h, nx, ny)
+        assert l2(height, gh) == 0.0, (h, "height", l2(height, gh))
         if test == "test_02":
-            assert l2 < 1e-3, (h, l2)  # the reference's own bound is 0.1
-            assert np.abs(load - g).max() <= 1e-6 * g.max()  # the golden files' FP32 rounding
+            assert l2(load, gl) < 1e-3, (h, l2(load, gl))  # the reference's own bound is 0.1
+            assert np.abs(load - gl).max() <= 1e-6 * gl.max()  # the golden files' FP32 rounding
+            assert l2(o["max_conc"], gc) < 1e-4, (h, "conc", l2(o["max_conc"], gc))
         else:
-            assert l2 < 0.15, (h, l2)
-            np.testing.assert_allclose(moments(load, cfg.dx), moments(g, cfg.dx), rtol=3e-5)
+            assert l2(load, gl) < 0.15, (h, l2(load, gl))
+            assert l2(o["max_conc"], gc) < 0.15, (h, "conc", l2(o["max_conc"], gc))
+            np.testing.assert_allclose(moments(load, cfg.dx), moments(gl, cfg.dx), rtol=3e-5)
+    ga = grid(test, "cloudarrival", None, nx, ny)
+    tol = 1e-9 if test == "test_02" else 0.01  # test_01: the reference's bound
+    assert l2(res["arrival"], ga) < tol, ("arrival", l2(res["arrival"], ga))
 
 
 @pytest.mark.parametrize("test", ["test_02", "test_01"])
@@ -102,9 +121,14 @@ def test_gpu_reproduces_reference_goldens(test):
     from volcano_ash3d_b200.model import Ash3dGPU
     cfg = config(test)
     gpu = Ash3dGPU(cfg)
-    loads = rerun(gpu, cfg)
-    check(test, loads, cfg)
+    res = rerun(gpu, cfg)
+    check(test, res, cfg)
     ref = rerun(orc.OracleModel(cfg, threads=1), cfg)
-    for h in loads:  # and bit for bit the oracle's own rerun
-        assert np.array_equal(loads[h], ref[h])
+    for h in ("2.0", "4.0"):  # and bit for bit the oracle's own rerun
+        for key in ("cloud_load", "max_height", "min_height", "max_conc", "mask_cloud", "dep_thick"):
+            assert np.array_equal(res[h][key], ref[h][key]), (h, key)
+        assert res[h]["cloud_area"] == ref[h]["cloud_area"]
+        assert res[h]["dep_area"] == ref[h]["dep_area"]
+        assert np.array_equal(res[h]["cloud_load_area"], ref[h]["cloud_load_area"])
+    assert np.array_equal(res["arrival"], ref["arrival"])
     gpu.close()

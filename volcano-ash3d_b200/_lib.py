@@ -41,7 +41,8 @@ EXPORTED = [
     "a3g_adj_set_lambda_dep", "a3g_adj_get_lambda_dep", "a3g_adj_advect_x", "a3g_adj_advect_y",
     "a3g_adj_advect_vert", "a3g_adj_diffuse_horz", "a3g_adj_diffuse_vert", "a3g_adj_step",
     "a3g_adj_vent_column", "a3g_cloud_load", "a3g_adj_add_cloud_load", "a3g_snapshot_alloc",
-    "a3g_snapshot_save", "a3g_snapshot_load",
+    "a3g_snapshot_save", "a3g_snapshot_load", "a3g_set_output_params", "a3g_output_reset",
+    "a3g_output_vars",
 ]
 KERNEL_CLASSES = ["advect_x", "advect_y", "advect_z", "diff_x", "diff_y", "diff_z", "cn_table",
                   "cn_solve_x", "cn_solve_y", "cn_solve_z", "cfl", "totals", "winds", "other",
@@ -142,6 +143,9 @@ def load(path: os.PathLike | str | None = None) -> C.CDLL:
         "a3g_cloud_load": (C.c_int, [P, D]), "a3g_adj_add_cloud_load": (C.c_int, [P, D]),
         "a3g_snapshot_alloc": (C.c_int, [P, C.c_int32]), "a3g_snapshot_save": (C.c_int, [P, C.c_int32]),
         "a3g_snapshot_load": (C.c_int, [P, C.c_int32]),
+        "a3g_set_output_params": (C.c_int, [P, D, C.c_double, C.c_double, C.c_double, C.c_double]),
+        "a3g_output_reset": (C.c_int, [P]),
+        "a3g_output_vars": (C.c_int, [P, C.c_double, D, D, D, D, I, D, I, D, D, D]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -198,6 +198,10 @@ int a3g_create(const a3g_grid_desc *grid, const a3g_params *params, int device, 
   ctx->tune_advect[1] = 0;
   ctx->tune_advect[2] = 1;
   ctx->tune_cn_x = 0;
+  ctx->ov_cloudcon = 1.0e-3;   // CLOUDCON_THRESH, src/Output_Vars.f90:119
+  ctx->ov_cloudload = 2.0e-1;  // CLOUDLOAD_THRESH, :114
+  ctx->ov_depo = 1.0e-2;       // DEPO_THRESH, :113
+  ctx->ov_density = 1000.0;    // DepositDensity, src/Tephra.f90:55
   ctx->tune_cn_yz = 1;
   auto dmalloc = [&](void **p, size_t n) -> cudaError_t {
     cudaError_t e = cudaMalloc(p, n);
@@ -267,7 +271,7 @@ int a3g_destroy(a3g_ctx *ctx) {
   if (ctx->src_event) cudaEventDestroy(ctx->src_event);
   for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
   double *aptrs[] = {ctx->lam0, ctx->lam1, ctx->lam_dep, ctx->stage1, ctx->stage2, ctx->adj_face,
-                     ctx->obs_buf};
+                     ctx->obs_buf, ctx->ov_buf, ctx->ov_zcc};
   for (double *p : aptrs) if (p) cudaFree(p);
   for (double *p : ctx->snaps) if (p) cudaFree(p);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -341,6 +345,12 @@ int a3g_set_geometry(a3g_ctx *ctx, const double *kappa_pd, const double *sigma_n
   if ((rc = set_geo3(ctx, sigma_ny_pd, n0, n1, n2, -1, &ctx->sny, 2))) return rc;
   if ((rc = set_geo3(ctx, sigma_nz_pd, n0, n1, n2, -1, &ctx->snz, 3))) return rc;
   ctx->h_dz.assign(dz_vec_pd, dz_vec_pd + n2);
+  // sigma_nz_pd(1:nx,1:ny,1): the cell areas the output products sum
+  ctx->h_area.resize((size_t)ctx->grid.nx * ctx->grid.ny);
+  for (int j = 1; j <= ctx->grid.ny; j++)
+    for (int i = 1; i <= ctx->grid.nx; i++)
+      ctx->h_area[(size_t)(i - 1) + (size_t)ctx->grid.nx * (j - 1)] =
+          sigma_nz_pd[(size_t)(i + 1) + (size_t)n0 * ((size_t)(j + 1) + (size_t)n1 * 2)];
   if (ctx->dz_vec) { cudaFree(ctx->dz_vec); ctx->dz_vec = nullptr; }
   if ((rc = upload_vec(ctx, ctx->h_dz, &ctx->dz_vec))) return rc;
   ctx->have_geometry = true;
@@ -797,7 +807,7 @@ int a3g_kernel_times(a3g_ctx *ctx, double *ms, uint64_t *count) {
 
 int a3g_set_variant(a3g_ctx *ctx, int32_t dir, int32_t variant) {
   if (!ctx) return fail(A3G_ERR_ARG, "null context");
-  if (dir < 0 || dir > 4 || variant < 0 || variant > (dir == 3 ? 1 : 2))
+  if (dir < 0 || dir > 4 || variant < 0 || variant > (dir == 0 ? 3 : dir == 3 ? 1 : 2))
     return fail(A3G_ERR_ARG, "bad direction or variant");
   if (dir == 3) ctx->tune_cn_x = variant;
   else if (dir == 4) ctx->tune_cn_yz = variant;
@@ -1059,6 +1069,105 @@ int a3g_snapshot_load(a3g_ctx *ctx, int32_t slot) {
   if (slot < 0 || slot >= (int)ctx->snaps.size()) return fail(A3G_ERR_ARG, "snapshot slot out of range");
   A3G_CUDA(cudaMemcpyAsync(ctx->c0, ctx->snaps[slot], level_bytes(ctx), cudaMemcpyDeviceToDevice, ctx->stream));
   ctx->ts1_zeroed = false;  // a restored state survives the next prologue
+  return A3G_OK;
+}
+
+// ---------------------------------------------------------------------------
+// output products (Gen_Output_Vars)
+// ---------------------------------------------------------------------------
+int a3g_set_output_params(a3g_ctx *ctx, const double *z_cc, double cloudcon_thresh, double cloudload_thresh,
+                          double depo_thresh, double deposit_density) {
+  CTX_CHECK(ctx);
+  if (!z_cc) return fail(A3G_ERR_ARG, "null z_cc");
+  if (!(deposit_density > 0.0)) return fail(A3G_ERR_ARG, "deposit density must be positive");
+  if (!ctx->ov_zcc) {
+    A3G_CUDA(cudaMalloc((void **)&ctx->ov_zcc, sizeof(double) * ctx->grid.nz));
+    ctx->bytes += sizeof(double) * ctx->grid.nz;
+  }
+  A3G_CUDA(cudaMemcpyAsync(ctx->ov_zcc, z_cc, sizeof(double) * ctx->grid.nz, cudaMemcpyHostToDevice, ctx->stream));
+  A3G_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->ov_cloudcon = cloudcon_thresh;
+  ctx->ov_cloudload = cloudload_thresh;
+  ctx->ov_depo = depo_thresh;
+  ctx->ov_density = deposit_density;
+  return A3G_OK;
+}
+
+static int ensure_ov(a3g_ctx *ctx) {
+  if (ctx->ov_buf) return A3G_OK;
+  const size_t n = (size_t)ctx->grid.nx * ctx->grid.ny;
+  // 5 double planes, 2 int planes (as doubles' room), 2 arrival planes
+  const size_t bytes = sizeof(double) * n * 9;
+  if (cudaMalloc((void **)&ctx->ov_buf, bytes) != cudaSuccess) return fail(A3G_ERR_NOMEM, "output buffers");
+  ctx->bytes += bytes;
+  return a3g_output_reset(ctx);
+}
+
+int a3g_output_reset(a3g_ctx *ctx) {
+  CTX_CHECK(ctx);
+  if (!ctx->ov_buf) return ensure_ov(ctx);
+  const size_t n = (size_t)ctx->grid.nx * ctx->grid.ny;
+  std::vector<double> neg(2 * n, -1.0);
+  A3G_CUDA(cudaMemcpyAsync(ctx->ov_buf + 7 * n, neg.data(), sizeof(double) * 2 * n, cudaMemcpyHostToDevice,
+                           ctx->stream));
+  A3G_CUDA(cudaStreamSynchronize(ctx->stream));
+  return A3G_OK;
+}
+
+int a3g_output_vars(a3g_ctx *ctx, double time, double *cloud_load, double *max_height, double *min_height,
+                    double *max_conc, int32_t *mask_cloud, double *dep_thick, int32_t *mask_dep,
+                    double *cloud_arrival, double *dep_arrival, double *areas) {
+  CTX_CHECK(ctx);
+  if (!ctx->have_geometry) return fail(A3G_ERR_STATE, "geometry not set");
+  if (!ctx->ov_zcc) return fail(A3G_ERR_STATE, "a3g_set_output_params has not been called");
+  int rc = ensure_ov(ctx);
+  if (rc) return rc;
+  const int nx = ctx->grid.nx, ny = ctx->grid.ny;
+  const size_t n = (size_t)nx * ny;
+  double *b = ctx->ov_buf;
+  int32_t *mc = reinterpret_cast<int32_t *>(b + 5 * n);
+  int32_t *md = mc + n;
+  if ((rc = launch_output_vars(ctx, time, b, b + n, b + 2 * n, b + 3 * n, mc, b + 4 * n, md, b + 7 * n,
+                               b + 8 * n)))
+    return rc;
+  // the host needs the loads and masks for the areas (sequential sums, reference order)
+  std::vector<double> h_load(n), h_dep(n);
+  std::vector<int32_t> h_mc(n), h_md(n);
+  A3G_CUDA(cudaMemcpyAsync(h_load.data(), b, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  A3G_CUDA(cudaMemcpyAsync(h_mc.data(), mc, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  A3G_CUDA(cudaMemcpyAsync(h_md.data(), md, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  double *outs[] = {max_height, min_height, max_conc, dep_thick};
+  for (int q = 0; q < 4; q++)
+    if (outs[q])
+      A3G_CUDA(cudaMemcpyAsync(outs[q], b + (q + 1) * n, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  if (cloud_arrival)
+    A3G_CUDA(cudaMemcpyAsync(cloud_arrival, b + 7 * n, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  if (dep_arrival)
+    A3G_CUDA(cudaMemcpyAsync(dep_arrival, b + 8 * n, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  if ((rc = sync_scalars(ctx))) return rc;
+  if (cloud_load) std::memcpy(cloud_load, h_load.data(), sizeof(double) * n);
+  if (mask_cloud) std::memcpy(mask_cloud, h_mc.data(), sizeof(int32_t) * n);
+  if (mask_dep) std::memcpy(mask_dep, h_md.data(), sizeof(int32_t) * n);
+  if (areas) {
+    // DepositAreaCovered (:881-889), CloudArea (:1101), CloudLoadArea (:1157-1170)
+    const Box &bx = ctx->box;
+    auto o = [&](int i, int j) { return (size_t)(i - 1) + (size_t)nx * (j - 1); };
+    double dep_area = 0.0, cloud_area = 0.0, la[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    static const double load_val[5] = {0.24, 1.0, 2.0, 4.0, 6.0};
+    for (int i = 1; i <= nx; i++)
+      for (int j = 1; j <= ny; j++)
+        if (h_md[o(i, j)]) dep_area = dep_area + ctx->h_area[o(i, j)];
+    for (int i = bx.imin; i <= bx.imax; i++)
+      for (int j = bx.jmin; j <= bx.jmax; j++)
+        if (h_mc[o(i, j)]) cloud_area = cloud_area + ctx->h_area[o(i, j)];
+    for (int i = bx.imin; i <= bx.imax; i++)
+      for (int j = bx.jmin; j <= bx.jmax; j++)
+        for (int k = 0; k < 5; k++)
+          if (h_load[o(i, j)] > load_val[k]) la[k] = la[k] + ctx->h_area[o(i, j)];
+    areas[0] = cloud_area;
+    areas[1] = dep_area;
+    for (int k = 0; k < 5; k++) areas[2 + k] = la[k];
+  }
   return A3G_OK;
 }
 

@@ -138,6 +138,11 @@ struct a3g_ctx {
   double *adj_face;         // sink for outflow updates of recomputed sweeps
   double *obs_buf;          // (nx*ny) or ((nz+1)*ns), whichever is larger
   std::vector<double *> snaps;
+  // output products (a3g_output_vars): 9 (nx*ny) planes, z_cc, parameters
+  double *ov_buf;
+  double *ov_zcc;
+  double ov_cloudcon, ov_cloudload, ov_depo, ov_density;
+  std::vector<double> h_area;  // sigma_nz_pd(1:nx,1:ny,1)
   // optional per-kernel timing (a3g_kernel_timing)
   bool timing;
   std::vector<cudaEvent_t> ev_pool;
@@ -190,6 +195,8 @@ int launch_adj_diffuse(a3g_ctx *ctx, int dir, const double *lin, double *lout);
 int launch_cloud_load(a3g_ctx *ctx, const double *c, double *out);
 int launch_adj_cloud_load(a3g_ctx *ctx, const double *w, double *lam);
 int launch_vent_column(a3g_ctx *ctx, int ivent, int jvent, const double *lam, double *out);
+int launch_output_vars(a3g_ctx *ctx, double time, double *load, double *maxh, double *minh, double *maxc,
+                       int32_t *mcl, double *dthick, int32_t *mdep, double *carr, double *darr);
 int refresh_dtv(a3g_ctx *ctx);
 // per-kernel timing brackets (no-ops unless a3g_kernel_timing(ctx,1))
 void tbegin(a3g_ctx *ctx, int kind);

@@ -586,6 +586,190 @@ __global__ void __launch_bounds__(128) k_advect_block(Layout L, Box box, int noc
 }
 
 // ---------------------------------------------------------------------------
+// Warp-tiled x sweep.  A warp owns 32 x rows (row r = (g*nz + k-1)*ny + j-1
+// starts at r*P; its winds at (r mod ny*nz)*P) and marches them side by side,
+// one lane per row, over the whole row.  The leading-edge values of each
+// step (q and the wind at cell c+2) come from shared-memory tiles of XA_TW
+// columns that the warp fills with coalesced row segments, and the updated
+// cells go out through a third tile the same way, so no lane touches global
+// memory row-wise in the interior.  The arithmetic of a step is the march's
+// (make_iface, iface_grain, cell_update in the same order), so the results
+// are the same bits.  No lane returns early: lanes of rows past the end, of
+// rows outside the box or of grains not aloft take part in the tile traffic
+// and write zeros (or nothing past the last row).
+// ---------------------------------------------------------------------------
+constexpr int XA_TW = 16;        // tile width (cells)
+constexpr int XA_S = XA_TW + 1;  // tile row stride (odd: conflict-free per-lane reads)
+constexpr int XA_WARPS = 2;
+
+template <int LIM, bool PER>
+__global__ void __launch_bounds__(32 * XA_WARPS) k_advect_xt(Layout L, Box box, int nocycle, double eps,
+                                                           const double *__restrict__ cin,
+                                                           double *__restrict__ cout,
+                                                           const double *__restrict__ vel, Geo3 sig,
+                                                           Geo3 dtvt, const int32_t *__restrict__ aloft,
+                                                           double *__restrict__ out1,
+                                                           double *__restrict__ out2) {
+  __shared__ double tq[XA_WARPS][32 * XA_S], tv[XA_WARPS][32 * XA_S], to[XA_WARPS][32 * XA_S];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const long nrows = (long)L.ny * L.nz * L.ns;
+  const long r0 = ((long)blockIdx.x * XA_WARPS + w) * 32;
+  if (r0 >= nrows) return;  // uniform over the warp
+  double *const sq = tq[w], *const sv = tv[w], *const so = to[w];
+  const long plane = (long)L.ny * L.nz;
+  const long r = r0 + lane;
+  const bool valid = r < nrows;
+  const long rc = valid ? r : nrows - 1;
+  const int j = (int)(rc % L.ny) + 1;
+  const int k = (int)((rc / L.ny) % L.nz) + 1;
+  const int g = (int)(rc / plane);
+  const int n = L.nx;
+  const int rmin = box.imin, rmax = box.imax;
+  const bool lane_active = j >= box.jmin && j <= box.jmax && k >= box.kmin && k <= box.kmax;
+  const bool al = valid && lane_active && aloft[g] != 0;
+  const long P = L.P;
+  const double *pq = cin + rc * P;          // own row
+  const double *pv = vel + (rc % plane) * P;
+  const LineGeo gsig = line_of<0>(sig, j, k);
+  const LineGeo gdtv = line_of<0>(dtvt, j, k);
+  const bool out_lo = !PER && rmin == 1;
+  const bool out_hi = !PER && rmax == n;
+  const int ctop = rmax + 1;
+  const long oo = (long)g * L.ny * L.nz + (long)(k - 1) * L.ny + (j - 1);
+  auto wrap = [&](int c) { return c < 1 ? c + n : (c > n ? c - n : c); };
+  // ghost-aware values of cell c of a row (Set_BC(1): zero concentration,
+  // edge or periodic winds); cells beyond the reach of any step give 0
+  auto qval = [&](const double *row, int c) -> double {
+    if (c < rmin - 2 || c > rmax + 2 || c < -1 || c > n + 2) return 0.0;
+    if (c >= 1 && c <= n) return row[c - 1];
+    return PER ? row[wrap(c) - 1] : 0.0;
+  };
+  auto vval = [&](const double *row, int c) -> double {
+    if (c < -1 || c > n + 2) return 0.0;
+    const int cl = PER ? wrap(c) : (c < 1 ? 1 : (c > n ? n : c));
+    return row[cl - 1];
+  };
+  // tile of cells t0 .. t0+XA_TW-1 for the warp's 32 rows
+  auto load_tiles = [&](int t0) {
+#pragma unroll 4
+    for (int it = 0; it < 32 * XA_TW / 32; it++) {
+      const int row = it * (32 / XA_TW) + lane / XA_TW, col = lane % XA_TW;
+      const long rr = r0 + row;
+      double a = 0.0, b = 0.0;
+      if (rr < nrows) {
+        a = qval(cin + rr * P, t0 + col);
+        b = vval(vel + (rr % plane) * P, t0 + col);
+      }
+      sq[row * XA_S + col] = a;
+      sv[row * XA_S + col] = b;
+    }
+    __syncwarp();
+  };
+  // output tile of cells o0 .. o0+XA_TW-1 (only cells 1..n are stored)
+  auto flush = [&](int o0) {
+    __syncwarp();
+#pragma unroll 4
+    for (int it = 0; it < 32 * XA_TW / 32; it++) {
+      const int row = it * (32 / XA_TW) + lane / XA_TW, col = lane % XA_TW;
+      const long rr = r0 + row;
+      const int c = o0 + col;
+      if (rr < nrows && c >= 1 && c <= n) cout[rr * P + (c - 1)] = so[row * XA_S + col];
+    }
+    __syncwarp();
+  };
+  auto fs_ok = [&](int I) { return I >= rmin - 1 && I <= rmax + 1; };
+  auto fss_ok = [&](int I) { return I >= rmin && I <= rmax + 1; };
+  const int cs = out_lo ? 0 : 1;
+  const int ce = out_hi ? n + 1 : n;
+
+  // ---- prologue at cell cs: interface cs, window q(cs), q(cs+1) ----
+  double q0, q1, d0, d1, fss0, fsr0, usA, usB, vB;
+  double dtv0 = gdtv.at(cs);
+  {
+    const double vm2 = vval(pv, cs - 2), vm1 = vval(pv, cs - 1), v0 = vval(pv, cs), v1 = vval(pv, cs + 1);
+    const double sm1 = fs_ok(cs - 1) ? gsig.at(cs - 1) : 0.0;
+    const double s0_ = fs_ok(cs) ? gsig.at(cs) : 0.0;
+    const double s1_ = fs_ok(cs + 1) ? gsig.at(cs + 1) : 0.0;
+    const double usm1 = fs_ok(cs - 1) ? 0.5 * (vm2 + vm1) * sm1 : 0.0;
+    usA = fs_ok(cs) ? 0.5 * (vm1 + v0) * s0_ : 0.0;
+    usB = fs_ok(cs + 1) ? 0.5 * (v0 + v1) * s1_ : 0.0;
+    vB = v1;
+    const double qm2 = qval(pq, cs - 2), qm1 = qval(pq, cs - 1);
+    q0 = qval(pq, cs);
+    q1 = qval(pq, cs + 1);
+    const double dm = qm1 - qm2;
+    d0 = q0 - qm1;
+    d1 = q1 - q0;
+    const Iface f = make_iface(usm1, usA, usB, dtv0, fss_ok(cs), fs_ok(cs));
+    double fsl_unused;
+    iface_grain<LIM>(f, dm, d0, d1, qm1, q0, eps, nocycle, fss0, fsr0, fsl_unused);
+  }
+  // steps that need no range checks: c >= rmin, c+2 <= min(n, rmax+1)
+  const int fa = max(cs, rmin), fb = min(ce, min(rmax - 1, n - 2));
+  int t0 = cs + 2;  // q/vel tile holds cells t0 .. t0+XA_TW-1 (the c+2 of steps c)
+  load_tiles(t0);
+  int o0 = 1;       // output tile holds cells o0 .. o0+XA_TW-1
+  for (int c = cs; c <= ce; c++) {
+    if (c + 2 >= t0 + XA_TW) {  // uniform: every lane is at the same c
+      t0 += XA_TW;
+      __syncwarp();
+      load_tiles(t0);
+    }
+    const int ti = lane * XA_S + (c + 2 - t0);
+    const double q2 = sq[ti], vn = sv[ti];
+    const int I = c + 1;
+    const bool fast = c >= fa && c <= fb;
+    const bool fsok2 = fast || fs_ok(c + 2);
+    const double sI2 = fsok2 ? gsig.at(c + 2) : 0.0;
+    const double dtv1 = gdtv.at(I);
+    const double usC = fsok2 ? 0.5 * (vB + vn) * sI2 : 0.0;
+    vB = vn;
+    const Iface f = make_iface(usA, usB, usC, dtv1, fast || fss_ok(I), fast || fs_ok(I));
+    usA = usB;
+    usB = usC;
+    const double d2 = q2 - q1;
+    double fss1, fsr1, fsl1;
+    iface_grain<LIM>(f, d0, d1, d2, q0, q1, eps, nocycle, fss1, fsr1, fsl1);
+    const double upd = cell_update(dtv0, fsl1, fsr0, fss1, fss0);
+    if (c >= 1 && c <= n) {
+      const bool inbox = c >= rmin && c <= rmax;
+      so[lane * XA_S + (c - o0)] = (al && inbox) ? q0 + upd : 0.0;
+      if (c == o0 + XA_TW - 1 || c == n) {
+        flush(o0);
+        o0 += XA_TW;
+      }
+    }
+    if (al) {
+      if (out_lo && c == 0) out1[oo] += upd;
+      if (out_hi && c == ctop) out2[oo] += upd;
+    }
+    fss0 = fss1;
+    fsr0 = fsr1;
+    q0 = q1;
+    q1 = q2;
+    d0 = d1;
+    d1 = d2;
+    dtv0 = dtv1;
+  }
+}
+
+template <int LIM>
+static void launch_advect_xt(a3g_ctx *ctx) {
+  const Layout &L = ctx->L;
+  const long nrows = (long)L.ny * L.nz * L.ns;
+  const long nwarps = (nrows + 31) / 32;
+  const unsigned blocks = (unsigned)((nwarps + XA_WARPS - 1) / XA_WARPS);
+  if (ctx->grid.periodic)
+    k_advect_xt<LIM, true><<<blocks, 32 * XA_WARPS, 0, ctx->stream>>>(
+        L, ctx->box, ctx->prm.nocycle, ctx->prm.eps_thresh, ctx->c0, ctx->c1, ctx->vx, ctx->snx, ctx->dtv,
+        ctx->aloft, ctx->out_yz1, ctx->out_yz2);
+  else
+    k_advect_xt<LIM, false><<<blocks, 32 * XA_WARPS, 0, ctx->stream>>>(
+        L, ctx->box, ctx->prm.nocycle, ctx->prm.eps_thresh, ctx->c0, ctx->c1, ctx->vx, ctx->snx, ctx->dtv,
+        ctx->aloft, ctx->out_yz1, ctx->out_yz2);
+}
+
+// ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
 template <int DIR, int LIM, int GC, bool PER>
@@ -627,6 +811,10 @@ template <int DIR, int LIM>
 static void launch_dir_lim(a3g_ctx *ctx) {
   const bool per = (DIR == 0) && ctx->grid.periodic;
   const int variant = ctx->tune_advect[DIR];
+  if (DIR == 0 && variant == 3) {
+    launch_advect_xt<LIM>(ctx);
+    return;
+  }
   if (variant == 1) {
     if (per) launch_block_v<DIR, LIM, 4, true>(ctx);
     else launch_block_v<DIR, LIM, 4, false>(ctx);

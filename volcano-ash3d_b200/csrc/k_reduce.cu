@@ -538,6 +538,75 @@ int launch_vent_column(a3g_ctx *ctx, int ivent, int jvent, const double *lam, do
 }
 
 // ---------------------------------------------------------------------------
+// output products of Gen_Output_Vars, one thread per column (i,j), in the
+// reference's order: ConcentrationCalculator (src/Output_Vars.f90:1026-1123),
+// AshThicknessCalculator (:855-895), the arrival-time marks (:1226-1236).
+// ---------------------------------------------------------------------------
+__global__ void k_output_vars(Layout L, Box box, const double *__restrict__ c, const double *__restrict__ dz_vec,
+                              const double *__restrict__ zcc, const double *__restrict__ dep, double cloudcon,
+                              double cloudload_th, double depo_th, double density, double time,
+                              double *__restrict__ load, double *__restrict__ maxh, double *__restrict__ minh,
+                              double *__restrict__ maxc, int32_t *__restrict__ mcl, double *__restrict__ dthick,
+                              int32_t *__restrict__ mdep, double *__restrict__ carr, double *__restrict__ darr) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y + 1;
+  if (i > L.nx) return;
+  const long o = (long)(j - 1) * L.nx + (i - 1);
+  const long plane = (long)L.nx * L.ny;
+  // deposit thickness (mm) from DepositGranularity
+  double sg = 0.0;
+  for (int g = 0; g < L.ns; g++) sg = sg + dep[(long)g * plane + o];
+  const double th = sg * dz_vec[2] / 1.0e6 / density * 1.0e3;
+  const bool md = th > depo_th;
+  dthick[o] = th;
+  mdep[o] = md;
+  double ld = 0.0, mh = 0.0, nh = 100.0, mx = 0.0;
+  bool mc = false;
+  if (L.ns > 0 && i >= box.imin && i <= box.imax && j >= box.jmin && j <= box.jmax) {
+    auto tc = [&](int k) {
+      double s = 0.0;
+      for (int g = 0; g < L.ns; g++) s = s + c[(long)g * L.PG + L.cell(i, j, k)];
+      return s;
+    };
+    for (int k = 1; k <= L.nz; k++) {
+      const double t = tc(k);
+      ld = ld + t * dz_vec[k + 1] / 1.0e3;
+      if (t >= cloudcon) mh = zcc[k - 1] + 0.5 * dz_vec[k + 1];
+      mx = (k == 1) ? t : fmx(mx, t);
+    }
+    for (int k = L.nz; k >= 1; k--)
+      if (tc(k) <= cloudcon) nh = zcc[k - 1] - 0.5 * dz_vec[k + 1];
+    mc = ld >= cloudload_th;
+    if (mc) {
+      if (nh < 0.0 && mh > 0.0) nh = 0.0;
+      nh = fmn(mh, nh);
+      mx = mx * 1.0e6 / 1.0e9;
+    } else {
+      ld = 0.0; mx = 0.0; mh = 0.0; nh = 0.0;
+    }
+  }
+  load[o] = ld;
+  maxh[o] = mh;
+  minh[o] = nh;
+  maxc[o] = mx;
+  mcl[o] = mc;
+  if (md && darr[o] < 0.0) darr[o] = time;
+  if (mc && carr[o] < 0.0) carr[o] = time;
+}
+
+int launch_output_vars(a3g_ctx *ctx, double time, double *load, double *maxh, double *minh, double *maxc,
+                       int32_t *mcl, double *dthick, int32_t *mdep, double *carr, double *darr) {
+  const Layout &L = ctx->L;
+  tbegin(ctx, A3G_K_OTHER);
+  k_output_vars<<<dim3((L.nx + 127) / 128, L.ny), 128, 0, ctx->stream>>>(
+      L, ctx->box, ctx->c0, ctx->dz_vec, ctx->ov_zcc, ctx->out_xy1, ctx->ov_cloudcon, ctx->ov_cloudload,
+      ctx->ov_depo, ctx->ov_density, time, load, maxh, minh, maxc, mcl, dthick, mdep, carr, darr);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  return A3G_OK;
+}
+
+// ---------------------------------------------------------------------------
 // self-test of exact_div.cuh against the IEEE division operator
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint64_t mix64(uint64_t x) {  // splitmix64 finaliser

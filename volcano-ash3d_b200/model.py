@@ -264,6 +264,43 @@ class Ash3dGPU:
     def snapshot_load(self, slot: int):
         check(self.lib.a3g_snapshot_load(self.ctx, slot))
 
+    # --- output products (Gen_Output_Vars) ----------------------------------
+    OUTPUT_DEFAULTS = dict(cloudcon_thresh=1.0e-3, cloudload_thresh=0.2, depo_thresh=1.0e-2,
+                           deposit_density=1000.0)
+
+    def set_output_params(self, **thresholds):
+        c = self.cfg
+        t = dict(self.OUTPUT_DEFAULTS, **thresholds)
+        _, zcc, _ = syn.zgrid(c)
+        z = np.ascontiguousarray(zcc[2:c.nz + 2])
+        check(self.lib.a3g_set_output_params(self.ctx, dptr(z), t["cloudcon_thresh"], t["cloudload_thresh"],
+                                             t["depo_thresh"], t["deposit_density"]))
+        self._ov_params = True
+
+    def output_reset(self):
+        if not getattr(self, "_ov_params", False):
+            self.set_output_params()
+        check(self.lib.a3g_output_reset(self.ctx))
+
+    def output_vars(self, time: float) -> dict:
+        """Gen_Output_Vars products of the current state (dict of arrays)."""
+        if not getattr(self, "_ov_params", False):
+            self.set_output_params()
+        c = self.cfg
+        f = lambda: np.zeros((c.nx, c.ny), order="F")
+        out = dict(cloud_load=f(), max_height=f(), min_height=f(), max_conc=f(), dep_thick=f(),
+                   cloud_arrival=f(), dep_arrival=f())
+        mc = np.zeros((c.nx, c.ny), dtype=np.int32, order="F")
+        md = np.zeros((c.nx, c.ny), dtype=np.int32, order="F")
+        areas = np.zeros(7)
+        check(self.lib.a3g_output_vars(self.ctx, time, dptr(out["cloud_load"]), dptr(out["max_height"]),
+                                       dptr(out["min_height"]), dptr(out["max_conc"]), iptr(mc),
+                                       dptr(out["dep_thick"]), iptr(md), dptr(out["cloud_arrival"]),
+                                       dptr(out["dep_arrival"]), dptr(areas)))
+        out.update(mask_cloud=mc.astype(bool), mask_dep=md.astype(bool), cloud_area=areas[0],
+                   dep_area=areas[1], cloud_load_area=areas[2:].copy())
+        return out
+
     # --- state access --------------------------------------------------------
     def upload_level(self, level: np.ndarray):
         lv = np.asfortranarray(level, dtype=np.float64)
