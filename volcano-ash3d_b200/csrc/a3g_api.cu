@@ -195,7 +195,7 @@ int a3g_create(const a3g_grid_desc *grid, const a3g_params *params, int device, 
   // fastest measured advection variants on B200 (x: marching rows; y, z:
   // 4-cell blocks); a3g_set_variant overrides them
   ctx->tune_advect[0] = 0;
-  ctx->tune_advect[1] = 0;
+  ctx->tune_advect[1] = 1;
   ctx->tune_advect[2] = 1;
   ctx->tune_cn_x = 0;
   ctx->ov_cloudcon = 1.0e-3;   // CLOUDCON_THRESH, src/Output_Vars.f90:119
