@@ -437,11 +437,11 @@ __device__ __forceinline__ void cn_line_gc(const Layout &L, const Box &box, cons
 }
 
 template <int DIR, int GC>
-__global__ void __launch_bounds__(128) k_cn_solve_gc(Layout L, Box box, LineMap map,
-                                                     const double *__restrict__ cin,
-                                                     double *__restrict__ cout,
-                                                     const double *__restrict__ tab,
-                                                     const int32_t *__restrict__ aloft) {
+__device__ __forceinline__ void cn_solve_gc_thread(const Layout &L, const Box &box, const LineMap &map,
+                                                   const double *__restrict__ cin,
+                                                   double *__restrict__ cout,
+                                                   const double *__restrict__ tab,
+                                                   const int32_t *__restrict__ aloft) {
   const int na = L.nx;
   const int nb = (DIR == 2) ? L.ny : L.nz;
   const int ngr = (L.ns + GC - 1) / GC;
@@ -453,6 +453,41 @@ __global__ void __launch_bounds__(128) k_cn_solve_gc(Layout L, Box box, LineMap 
   const int b = (int)(r % nb) + 1;
   const int gg = (int)(r / nb);
   cn_line_gc<DIR, GC>(L, box, map, cin, cout, tab, aloft, a, b, gg * GC);
+}
+
+// z lines: unconstrained registers (64-96, no spills) measured fastest; an
+// 8-blocks-per-SM bound slowed the C2 z solve 1.29 -> 1.37 ms on B200.
+template <int DIR, int GC>
+__global__ void __launch_bounds__(128) k_cn_solve_gc(Layout L, Box box, LineMap map,
+                                                     const double *__restrict__ cin,
+                                                     double *__restrict__ cout,
+                                                     const double *__restrict__ tab,
+                                                     const int32_t *__restrict__ aloft) {
+  cn_solve_gc_thread<DIR, GC>(L, box, map, cin, cout, tab, aloft);
+}
+
+// y lines: 12 blocks of 128 per SM (at most 40 registers, some spilled to
+// L1) hide the strided dependent loads better (C2 1.76 -> 1.62 ms on B200).
+template <int GC>
+__global__ void __launch_bounds__(128, 12) k_cn_solve_gc_y(Layout L, Box box, LineMap map,
+                                                           const double *__restrict__ cin,
+                                                           double *__restrict__ cout,
+                                                           const double *__restrict__ tab,
+                                                           const int32_t *__restrict__ aloft) {
+  cn_solve_gc_thread<1, GC>(L, box, map, cin, cout, tab, aloft);
+}
+
+template <int DIR, int GC>
+static void launch_cn_solve_gc(a3g_ctx *ctx, const LineMap &map) {
+  const Layout &L = ctx->L;
+  const long n = (long)map.na * map.nb * ((L.ns + GC - 1) / GC);
+  const unsigned grid = (unsigned)((n + 127) / 128);
+  if constexpr (DIR == 1)
+    k_cn_solve_gc_y<GC><<<grid, 128, 0, ctx->stream>>>(L, ctx->box, map, ctx->c0, ctx->c1, ctx->cn_buf,
+                                                       ctx->aloft);
+  else
+    k_cn_solve_gc<DIR, GC><<<grid, 128, 0, ctx->stream>>>(L, ctx->box, map, ctx->c0, ctx->c1, ctx->cn_buf,
+                                                          ctx->aloft);
 }
 
 // Solve kernel: one thread per line (a, b, grain), lines enumerated with a
@@ -727,13 +762,9 @@ static int launch_cn_dir(a3g_ctx *ctx) {
     k_cn_solve_xt<<<(unsigned)((nwarps + XT_WARPS - 1) / XT_WARPS), 32 * XT_WARPS, 0, ctx->stream>>>(
         L, box, map, ctx->c0, ctx->c1, ctx->cn_buf, ctx->aloft);
   } else if (DIR != 0 && ctx->tune_cn_yz == 1 && L.ns >= 2) {
-    const long nl2 = (long)map.na * map.nb * ((L.ns + 1) / 2);
-    k_cn_solve_gc<DIR == 0 ? 1 : DIR, 2><<<(unsigned)((nl2 + 127) / 128), 128, 0, ctx->stream>>>(
-        L, box, map, ctx->c0, ctx->c1, ctx->cn_buf, ctx->aloft);
+    launch_cn_solve_gc<DIR == 0 ? 1 : DIR, 2>(ctx, map);
   } else if (DIR != 0 && ctx->tune_cn_yz == 2 && L.ns >= 2) {
-    const long nl4 = (long)map.na * map.nb * ((L.ns + 3) / 4);
-    k_cn_solve_gc<DIR == 0 ? 1 : DIR, 4><<<(unsigned)((nl4 + 127) / 128), 128, 0, ctx->stream>>>(
-        L, box, map, ctx->c0, ctx->c1, ctx->cn_buf, ctx->aloft);
+    launch_cn_solve_gc<DIR == 0 ? 1 : DIR, 4>(ctx, map);
   } else {
     k_cn_solve<DIR><<<(unsigned)((nlines + 127) / 128), 128, 0, ctx->stream>>>(
         L, box, map, ctx->c0, ctx->c1, ctx->cn_buf, ctx->aloft);
