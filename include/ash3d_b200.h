@@ -72,7 +72,7 @@ typedef struct a3g_params {
   int32_t use_diffusion;    /* useDiffusion */
   int32_t fast_subgrid;     /* FAST_SUBGRID */
   int32_t nocycle;          /* NOCYCLE */
-  int32_t zscaling_id;      /* ZScaling_ID; only 0 and 1 are implemented */
+  int32_t zscaling_id;      /* ZScaling_ID 0 (s = z), 1 (shifted), 2 (scaled, advect_sigma) */
   double cfl;               /* CFL (0.8) */
   double dt_min, dt_max;    /* DT_MIN, DT_MAX (hours) */
   double imp_fac;           /* Imp_fac (0.5) */
@@ -123,6 +123,25 @@ int a3g_set_met_steps(a3g_ctx *ctx, const float *vx_last, const float *vy_last,
 /* Device form of src/MesoInterpolater.f90:207-223:
  * v = (dble(last) + dble(next-last)*frac)*3.6 */
 int a3g_interp_winds(a3g_ctx *ctx, double interval_frac);
+
+/* ---- terrain (useTopo; src/Topography.f90) ---- */
+/* Binds the topography terms of the step: dhdx_comp, dhdy_comp, DelDxonD_cc,
+ * DelDyonD_cc (-1:nx+2,-1:ny+2, as Calc_FDGrad_Topo leaves them,
+ * src/Topography.f90:2471-2536), s_cc_pd (-1:nz+2) and Ztop (km).  From
+ * then on every a3g_set_winds / a3g_interp_winds also forms vh on the device
+ * (Calc_Vmod_Topo, src/Topography.f90:2138-2166, which the reference calls
+ * right after MesoInterpolater, src/Ash3d.F90:398), and the z sweep uses
+ * vz+vh+vf (src/AdvectionVert_DCU.f90:172-174).  vh is zero on the ghost
+ * levels, where the reference's vx_pd and vy_pd are never written.  With
+ * ZScaling_ID 2 the x and y sweeps add the DelD*onD_cc terms
+ * (src/AdvectionHorz_DCU.f90:163-166,251-257) and AdvectVert runs
+ * advect_sigma (:341-564, the same line update as advect_z); the scaled
+ * kappa_pd and sigma_n{x,y}_pd of calc_s_mesh (src/Calc_Mesh.f90:316-328)
+ * come in through a3g_set_geometry.  ZScaling_ID 0 makes vh zero.  The
+ * adjoint (a3g_adj_*) returns A3G_ERR_UNSUPPORTED once terrain is bound. */
+int a3g_set_topo(a3g_ctx *ctx, const double *dhdx_comp, const double *dhdy_comp,
+                 const double *deldx_on_d, const double *deldy_on_d, const double *s_cc_pd,
+                 double ztop);
 
 /* ---- concentration state ---- */
 /* Uploads/downloads the interior of one level (ghosts of the download are

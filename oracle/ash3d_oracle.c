@@ -47,6 +47,9 @@ static inline size_t dep(const orc_state *s, int i, int j, int n) {
 }
 
 /* Fortran MAX/MIN of two reals (no NaNs reach these). */
+static inline size_t d2(const orc_state *s, int i, int j) { /* (-1:nx+2,-1:ny+2) */
+  return (size_t)(i + 1) + (size_t)(s->nx + 4) * (size_t)(j + 1);
+}
 static inline double fmx(double a, double b) { return a > b ? a : b; }
 static inline double fmn(double a, double b) { return a < b ? a : b; }
 
@@ -171,25 +174,27 @@ int orc_set_bc(orc_state *s, int code) {
 /* One DCU row: the body shared by advect_x/y/z                              */
 /* src/AdvectionHorz_DCU.f90:153-281 (identical in :485-533 and              */
 /* src/AdvectionVert_DCU.f90:183-298).  All arrays are indexed -1..len+2     */
-/* through pointers offset by one element; the topography term (:251-257)    */
-/* is identically zero for ZScaling_ID 0/1 and is not restated.              */
+/* through pointers offset by one element.  The topography term (:251-257)   */
+/* is added when topo is set (ZScaling_ID 2, DelDonD_cc of :163-166 in       */
+/* r->deld); for ZScaling_ID 0/1 DelDonD_cc is 0 and the term is not        */
+/* restated.                                                                */
 /* ======================================================================== */
 typedef struct {
-  double *q, *vel, *sig, *kap, *dtv, *usig, *dq, *fss, *fsl, *fsr, *upd;
+  double *q, *vel, *sig, *kap, *dtv, *usig, *dq, *fss, *fsl, *fsr, *upd, *deld;
   double *mem;
 } row_scratch;
 
 static void row_alloc(row_scratch *r, int len) {
   size_t m = (size_t)len + 4;
-  r->mem = (double *)calloc(11 * m, sizeof(double));
+  r->mem = (double *)calloc(12 * m, sizeof(double));
   double *p = r->mem;
   r->q = p + 1; p += m;  r->vel = p + 1; p += m; r->sig = p + 1; p += m;
   r->kap = p + 1; p += m; r->dtv = p + 1; p += m; r->usig = p + 1; p += m;
   r->dq = p + 1; p += m;  r->fss = p + 1; p += m; r->fsl = p + 1; p += m;
-  r->fsr = p + 1; p += m; r->upd = p + 1;
+  r->fsr = p + 1; p += m; r->upd = p + 1; p += m; r->deld = p + 1;
 }
 
-static void dcu_row(const orc_state *s, row_scratch *r, int len, int rmin, int rmax) {
+static void dcu_row(const orc_state *s, row_scratch *r, int len, int rmin, int rmax, int topo) {
   const double dt = s->dt, eps = s->eps_thresh;
   double *q = r->q, *vel = r->vel, *sig = r->sig, *kap = r->kap;
   double *dtv = r->dtv, *usig = r->usig, *dq = r->dq, *fss = r->fss;
@@ -237,6 +242,11 @@ static void dcu_row(const orc_state *s, row_scratch *r, int len, int rmin, int r
     double divu_m = fmn(0.0, usig[I + 1]) - fmn(0.0, usig[I]);
     fsr[I] = fsr[I] + q[I] * divu_m;
     fsl[I] = fsl[I] + q[I - 1] * divu_p;
+    if (topo) {                                                                 /* :251-257 */
+      const double *dd = r->deld;
+      fsr[I] = fsr[I] + 0.5 * vel[I] * (sig[I] + sig[I + 1]) * q[I] * dd[I];
+      fsl[I] = fsl[I] - 0.5 * vel[I - 1] * (sig[I - 1] + sig[I]) * q[I - 1] * dd[I - 1];
+    }
   }
   for (int i = rmin - 1; i <= rmax + 1; i++)                                  /* :264-281 */
     upd[i] = -(dtv[i] * (fsl[i + 1] + fsr[i] + fss[i + 1] - fss[i]));
@@ -261,6 +271,7 @@ static int max3(int a, int b, int c) { int m = a > b ? a : b; return m > c ? m :
 void orc_advect_x(orc_state *s) {
   orc_set_bc(s, 1);                                                           /* :115 */
   const int rmin = s->imin, rmax = s->imax, nx = s->nx;
+  const int topo = s->use_topo && s->zscaling_id == 2;
   zero_level(s, 1);                                                           /* :122 */
   const int nth = orc_get_threads();
   for (int n = 1; n <= s->ns; n++) {
@@ -277,7 +288,10 @@ void orc_advect_x(orc_state *s) {
             r.sig[i] = s->sig_nx[i3(s, i, j, k)];
             r.kap[i] = s->kappa[i3(s, i, j, k)];
           }
-          dcu_row(s, &r, nx, rmin, rmax);
+          if (topo)                                                           /* :163-166 */
+            for (int i = rmin - 2; i <= rmax + 2; i++)
+              r.deld[i] = (i >= rmin - 1 && i <= rmax + 1) ? s->deldx[d2(s, i, j)] : 0.0;
+          dcu_row(s, &r, nx, rmin, rmax, topo);
           for (int i = rmin; i <= rmax; i++)                                  /* :285-287 */
             s->concen[c5(s, i, j, k, n, 1)] = s->concen[c5(s, i, j, k, n, 0)] + r.upd[i];
           if (rmin == 1 && !s->periodic) s->outflow_yz1[oyz(s, j, k, n)] += r.upd[0];
@@ -293,6 +307,7 @@ void orc_advect_x(orc_state *s) {
 void orc_advect_y(orc_state *s) {
   orc_set_bc(s, 1);
   const int rmin = s->jmin, rmax = s->jmax, ny = s->ny;
+  const int topo = s->use_topo && s->zscaling_id == 2;
   zero_level(s, 1);
   const int nth = orc_get_threads();
   for (int n = 1; n <= s->ns; n++) {
@@ -309,7 +324,10 @@ void orc_advect_y(orc_state *s) {
             r.sig[j] = s->sig_ny[i3(s, i, j, k)];
             r.kap[j] = s->kappa[i3(s, i, j, k)];
           }
-          dcu_row(s, &r, ny, rmin, rmax);
+          if (topo)                                                           /* :414-417 */
+            for (int j = rmin - 2; j <= rmax + 2; j++)
+              r.deld[j] = (j >= rmin - 1 && j <= rmax + 1) ? s->deldy[d2(s, i, j)] : 0.0;
+          dcu_row(s, &r, ny, rmin, rmax, topo);
           for (int j = rmin; j <= rmax; j++)
             s->concen[c5(s, i, j, k, n, 1)] = s->concen[c5(s, i, j, k, n, 0)] + r.upd[j];
           if (rmin == 1) s->outflow_xz1[oxz(s, i, k, n)] += r.upd[0];          /* :540-545 */
@@ -342,7 +360,7 @@ void orc_advect_z(orc_state *s) {
             r.sig[k] = s->sig_nz[i3(s, i, j, k)];
             r.kap[k] = s->kappa[i3(s, i, j, k)];
           }
-          dcu_row(s, &r, nz, rmin, rmax);
+          dcu_row(s, &r, nz, rmin, rmax, 0);
           for (int k = rmin; k <= rmax; k++)
             s->concen[c5(s, i, j, k, n, 1)] = s->concen[c5(s, i, j, k, n, 0)] + r.upd[k];
           if (rmin == 1) s->outflow_xy1[oxy(s, i, j, n)] += r.upd[0];          /* :306-308 */
@@ -410,7 +428,24 @@ int orc_advect_horz(orc_state *s, int itoggle, int ivent, int jvent, int kvent) 
 }
 
 /* AdvectVert, src/AdvectionVert_DCU.f90:64-82 */
-void orc_advect_vert(orc_state *s) { orc_advect_z(s); }
+void orc_advect_vert(orc_state *s) { orc_advect_z(s); }  /* advect_sigma == advect_z */
+
+/* Calc_Vmod_Topo, src/Topography.f90:2138-2166 (every i, j, k of vh_pd). */
+void orc_calc_vmod_topo(orc_state *s) {
+  const int nx = s->nx, ny = s->ny, nz = s->nz;
+  for (int k = -1; k <= nz + 2; k++)
+    for (int j = -1; j <= ny + 2; j++)
+      for (int i = -1; i <= nx + 2; i++) {
+        const size_t m = i3(s, i, j, k);
+        if (!s->use_topo || s->zscaling_id == 0) {
+          s->vh[m] = 0.0;
+        } else {
+          const double g = s->vx[m] * s->dhdx[d2(s, i, j)] + s->vy[m] * s->dhdy[d2(s, i, j)];
+          if (s->zscaling_id == 1) s->vh[m] = -1.0 * g;
+          else s->vh[m] = (s->s_cc[k + 1] / s->ztop - 1.0) * g;
+        }
+      }
+}
 
 /* ======================================================================== */
 /* Explicit diffusion, src/Diffusion.F90:266-650                             */

@@ -76,11 +76,18 @@ typedef struct orc_state {
   double *deposit;
   int32_t *is_aloft;
   double *mass_aloft;
+  /* Terrain (src/Topography.f90): ZScaling_ID, useTopo, Ztop (km) and, when
+   * use_topo, dhdx_comp, dhdy_comp, DelDxonD_cc, DelDyonD_cc (-1:nx+2,
+   * -1:ny+2) and s_cc_pd (-1:nz+2). */
+  int32_t zscaling_id, use_topo;
+  double ztop;
+  double *dhdx, *dhdy, *deldx, *deldy, *s_cc;
 } orc_state;
 
 /* Set_BC(bc_code), src/Set_BC.f90:15-126.  Returns 1 for an unknown code. */
 int  orc_set_bc(orc_state *s, int code);
-/* advect_x / advect_y, src/AdvectionHorz_DCU.f90:68-305 / 322-556. */
+/* advect_x / advect_y, src/AdvectionHorz_DCU.f90:68-305 / 322-556 (with
+ * the DelD*onD_cc topography terms of :163-166,251-257 when ZScaling_ID 2). */
 void orc_advect_x(orc_state *s);
 void orc_advect_y(orc_state *s);
 /* advect_z, src/AdvectionVert_DCU.f90:100-323. */
@@ -88,8 +95,13 @@ void orc_advect_z(orc_state *s);
 /* AdvectHorz(itoggle), src/AdvectionHorz.f90:47-85 (get_minmax_index when
  * fast_subgrid, else the full box).  Returns nonzero on kmax<kmin. */
 int  orc_advect_horz(orc_state *s, int itoggle, int ivent, int jvent, int kvent);
-/* AdvectVert, src/AdvectionVert_DCU.f90:64-82 (ZScaling_ID 0/1 path). */
+/* AdvectVert, src/AdvectionVert_DCU.f90:64-82.  ZScaling_ID 2 selects
+ * advect_sigma (:341-564), whose body is advect_z's line for line. */
 void orc_advect_vert(orc_state *s);
+/* Calc_Vmod_Topo, src/Topography.f90:2138-2166: vh over the whole ghosted
+ * array from the current vx, vy (ZScaling_ID 1: -(vx*dhdx + vy*dhdy);
+ * 2: (s_cc/Ztop - 1)*(vx*dhdx + vy*dhdy); 0: 0). */
+void orc_calc_vmod_topo(orc_state *s);
 /* diff_x/diff_y/diff_z, src/Diffusion.F90:266-650. */
 void orc_diff_x(orc_state *s);
 void orc_diff_y(orc_state *s);

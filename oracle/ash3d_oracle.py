@@ -50,7 +50,9 @@ class OrcState(C.Structure):
         "concen", "vx", "vy", "vz", "vh", "vf", "kappa", "sig_nx", "sig_ny", "sig_nz", "dz_vec",
         "kx", "ky", "kz", "outflow_yz1", "outflow_yz2", "outflow_xz1", "outflow_xz2",
         "outflow_xy1", "outflow_xy2", "deposit")] + [
-        ("is_aloft", C.POINTER(C.c_int32)), ("mass_aloft", C.POINTER(C.c_double))]
+        ("is_aloft", C.POINTER(C.c_int32)), ("mass_aloft", C.POINTER(C.c_double)),
+        ("zscaling_id", C.c_int32), ("use_topo", C.c_int32), ("ztop", C.c_double)] + [
+        (n, C.POINTER(C.c_double)) for n in ("dhdx", "dhdy", "deldx", "deldy", "s_cc")]
 
 
 _lib = None
@@ -68,7 +70,7 @@ def load() -> C.CDLL:
             ("orc_set_bc", C.c_int, [S, C.c_int]),
             ("orc_advect_x", None, [S]), ("orc_advect_y", None, [S]), ("orc_advect_z", None, [S]),
             ("orc_advect_horz", C.c_int, [S, C.c_int, C.c_int, C.c_int, C.c_int]),
-            ("orc_advect_vert", None, [S]),
+            ("orc_advect_vert", None, [S]), ("orc_calc_vmod_topo", None, [S]),
             ("orc_diff_x", None, [S]), ("orc_diff_y", None, [S]), ("orc_diff_z", None, [S]),
             ("orc_diffcn_x", None, [S]), ("orc_diffcn_y", None, [S]), ("orc_diffcn_z", None, [S]),
             ("orc_diffuse_horz", None, [S, C.c_int]), ("orc_diffuse_vert", None, [S]),
@@ -172,8 +174,12 @@ class OracleModel:
                           ("deposit", self.deposit), ("mass_aloft", self.mass_aloft)]:
             setattr(s, name, _d(arr))
         s.is_aloft = self.is_aloft.ctypes.data_as(C.POINTER(C.c_int32))
+        s.zscaling_id, s.use_topo, s.ztop = int(cfg.zscaling_id), 0, 0.0
         self.s = s
         self.ps = C.byref(s)
+        self._topo = None
+        if syn.use_topo(cfg):
+            self.set_topo(**syn.topo_fields(cfg))
 
     # --- routines with the reference names ---------------------------------
     def Set_BC(self, code):
@@ -249,11 +255,31 @@ class OracleModel:
     def interp_winds(self, frac):
         m = self._met
         self.lib.orc_interp_winds(self.ps, _f(m[0]), _f(m[3]), _f(m[1]), _f(m[4]), _f(m[2]), _f(m[5]), frac)
+        if self.s.use_topo:  # Ash3d.F90:398, right after MesoInterpolater
+            self.lib.orc_calc_vmod_topo(self.ps)
 
     def set_winds(self, vx, vy, vz):
         self.vx[...] = vx
         self.vy[...] = vy
         self.vz[...] = vz
+        if self.s.use_topo:
+            self.lib.orc_calc_vmod_topo(self.ps)
+
+    def set_topo(self, dhdx, dhdy, deldx, deldy, s_cc, ztop):
+        """useTopo: dhdx_comp, dhdy_comp, DelDxonD_cc, DelDyonD_cc
+        (-1:nx+2,-1:ny+2), s_cc_pd (-1:nz+2), Ztop (km).  vh is recomputed
+        after every wind update (Calc_Vmod_Topo)."""
+        c = self.cfg
+        a2 = [np.asfortranarray(a, dtype=np.float64) for a in (dhdx, dhdy, deldx, deldy)]
+        for a in a2:
+            assert a.shape == (c.nx + 4, c.ny + 4)
+        sc = np.ascontiguousarray(s_cc, dtype=np.float64)
+        assert sc.shape == (c.nz + 4,)
+        self._topo = (*a2, sc)
+        s = self.s
+        s.dhdx, s.dhdy, s.deldx, s.deldy, s.s_cc = [_d(a) for a in self._topo]
+        s.ztop, s.use_topo = float(ztop), 1
+        self.lib.orc_calc_vmod_topo(self.ps)
 
     def set_aloft(self, flags):
         self.is_aloft[:] = np.asarray(flags, dtype=np.int32)

@@ -167,8 +167,8 @@ int a3g_create(const a3g_grid_desc *grid, const a3g_params *params, int device, 
   if (grid->nx < 1 || grid->ny < 1 || grid->nz < 1 || grid->ns < 1)
     return fail(A3G_ERR_ARG, "grid extents must be >= 1");
   if (grid->periodic && grid->nx < 2) return fail(A3G_ERR_ARG, "periodic grid needs nx >= 2");
-  if (params->zscaling_id != 0 && params->zscaling_id != 1)
-    return fail(A3G_ERR_UNSUPPORTED, "ZScaling_ID 2 (advect_sigma) is not implemented");
+  if (params->zscaling_id < 0 || params->zscaling_id > 2)
+    return fail(A3G_ERR_ARG, "ZScaling_ID must be 0, 1 or 2");
   if (params->limiter < A3G_LIM_NONE || params->limiter > A3G_LIM_MC)
     return fail(A3G_ERR_ARG, "unknown limiter");
   if (!(params->dt_min > 0.0) || !(params->dt_max >= params->dt_min))
@@ -271,7 +271,7 @@ int a3g_destroy(a3g_ctx *ctx) {
   if (ctx->src_event) cudaEventDestroy(ctx->src_event);
   for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
   double *aptrs[] = {ctx->lam0, ctx->lam1, ctx->lam_dep, ctx->stage1, ctx->stage2, ctx->adj_face,
-                     ctx->obs_buf, ctx->ov_buf, ctx->ov_zcc};
+                     ctx->obs_buf, ctx->ov_buf, ctx->ov_zcc, ctx->topo_buf, ctx->vzh};
   for (double *p : aptrs) if (p) cudaFree(p);
   for (double *p : ctx->snaps) if (p) cudaFree(p);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -414,6 +414,10 @@ int a3g_set_winds(a3g_ctx *ctx, const double *vx_pd, const double *vy_pd, const 
                         L.nx, L.ny, L.nz, 1, L.P, L.PY, L.PG);
     if (rc) return rc;
   }
+  if (ctx->topo_on) {
+    int rc = launch_vmod_topo(ctx);
+    if (rc) return rc;
+  }
   A3G_CUDA(cudaStreamSynchronize(ctx->stream));
   ctx->have_winds = true;
   return A3G_OK;
@@ -441,8 +445,49 @@ int a3g_interp_winds(a3g_ctx *ctx, double interval_frac) {
   CTX_CHECK(ctx);
   if (!ctx->met) return fail(A3G_ERR_STATE, "a3g_set_met_steps has not been called");
   int rc = launch_interp_winds(ctx, interval_frac);
+  if (!rc && ctx->topo_on) rc = launch_vmod_topo(ctx);  // Calc_Vmod_Topo, src/Ash3d.F90:398
   if (!rc) ctx->have_winds = true;
   return rc;
+}
+
+int a3g_set_topo(a3g_ctx *ctx, const double *dhdx_comp, const double *dhdy_comp, const double *deldx_on_d,
+                 const double *deldy_on_d, const double *s_cc_pd, double ztop) {
+  CTX_CHECK(ctx);
+  const int z = ctx->prm.zscaling_id;
+  const long nx = ctx->grid.nx, ny = ctx->grid.ny, nz = ctx->grid.nz;
+  const long n2 = (nx + 4) * (ny + 4);
+  if (!dhdx_comp || !dhdy_comp) return fail(A3G_ERR_ARG, "null topography gradient");
+  if (z == 2 && (!deldx_on_d || !deldy_on_d || !s_cc_pd)) return fail(A3G_ERR_ARG, "ZScaling_ID 2 needs DelD*onD_cc and s_cc_pd");
+  if (z == 2 && !(ztop > 0.0)) return fail(A3G_ERR_ARG, "Ztop must be positive");
+  // per-level factor of vh (src/Topography.f90:2151-2163), in the
+  // reference's operations: -1.0 for ZScaling_ID 1, s_cc/Ztop - 1.0 for 2
+  std::vector<double> h(4 * n2 + nz, 0.0);
+  std::memcpy(h.data(), dhdx_comp, sizeof(double) * n2);
+  std::memcpy(h.data() + n2, dhdy_comp, sizeof(double) * n2);
+  if (deldx_on_d) std::memcpy(h.data() + 2 * n2, deldx_on_d, sizeof(double) * n2);
+  if (deldy_on_d) std::memcpy(h.data() + 3 * n2, deldy_on_d, sizeof(double) * n2);
+  for (long k = 1; k <= nz; k++)
+    h[4 * n2 + k - 1] = (z == 1) ? -1.0 : (z == 2) ? (s_cc_pd[k + 1] / ztop - 1.0) : 0.0;
+  if (!ctx->topo_buf) {
+    if (cudaMalloc((void **)&ctx->topo_buf, sizeof(double) * h.size()) != cudaSuccess)
+      return fail(A3G_ERR_NOMEM, "topography allocation failed");
+    ctx->bytes += sizeof(double) * h.size();
+  }
+  if (!ctx->vzh) {
+    const size_t w3 = (size_t)ctx->L.PG * sizeof(double);
+    if (cudaMalloc((void **)&ctx->vzh, w3) != cudaSuccess) return fail(A3G_ERR_NOMEM, "vz+vh allocation failed");
+    ctx->bytes += w3;
+    A3G_CUDA(cudaMemsetAsync(ctx->vzh, 0, w3, ctx->stream));
+  }
+  A3G_CUDA(cudaMemcpyAsync(ctx->topo_buf, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice,
+                           ctx->stream));
+  ctx->topo_on = true;
+  if (ctx->have_winds) {
+    int rc = launch_vmod_topo(ctx);
+    if (rc) return rc;
+  }
+  A3G_CUDA(cudaStreamSynchronize(ctx->stream));
+  return A3G_OK;
 }
 
 int a3g_upload_concen(a3g_ctx *ctx, const double *concen_level) {
@@ -835,6 +880,7 @@ static size_t level_bytes(const a3g_ctx *ctx) { return sizeof(double) * ctx->L.P
 static int adj_ready(a3g_ctx *ctx) {
   if (!ctx->lam0) return fail(A3G_ERR_STATE, "a3g_adj_enable has not been called");
   if (ctx->prm.fast_subgrid) return fail(A3G_ERR_UNSUPPORTED, "the adjoint needs fast_subgrid off");
+  if (ctx->topo_on) return fail(A3G_ERR_UNSUPPORTED, "the adjoint does not cover the terrain terms");
   int rc = ready(ctx);
   if (rc) return rc;
   full_box(ctx);

@@ -143,6 +143,12 @@ struct a3g_ctx {
   double *ov_zcc;
   double ov_cloudcon, ov_cloudload, ov_depo, ov_density;
   std::vector<double> h_area;  // sigma_nz_pd(1:nx,1:ny,1)
+  // terrain (a3g_set_topo): dhdx, dhdy, DelDxonD, DelDyonD ((nx+4)*(ny+4) each,
+  // ghosted, i fastest) and the per-level factor of vh (nz); vzh = vz + vh on
+  // the interior, the vertical wind of the z sweep
+  bool topo_on;
+  double *topo_buf;
+  double *vzh;
   // optional per-kernel timing (a3g_kernel_timing)
   bool timing;
   std::vector<cudaEvent_t> ev_pool;
@@ -186,6 +192,7 @@ int launch_dt_from_maxima(a3g_ctx *ctx, int n_gs_aloft, double time, double next
 int launch_totals(a3g_ctx *ctx, double *out4, double *mass_aloft);
 int launch_plane_flags(a3g_ctx *ctx);
 int launch_interp_winds(a3g_ctx *ctx, double frac);
+int launch_vmod_topo(a3g_ctx *ctx);
 int launch_source(a3g_ctx *ctx, int ivent, int jvent, double dt);
 int launch_zero_state(a3g_ctx *ctx);
 int check_device_error(a3g_ctx *ctx);

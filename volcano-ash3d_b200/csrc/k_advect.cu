@@ -138,11 +138,13 @@ __device__ __forceinline__ LineGeo line_of(const Geo3 &g, int a, int o) {
 struct CkT { static constexpr bool value = true; };     // step with range checks
 struct FastT { static constexpr bool value = false; };  // interior step
 
-template <int DIR, int LIM, int GC, bool PER>
+template <int DIR, int LIM, int GC, bool PER, bool TOPO>
 __global__ void __launch_bounds__(128, 1) k_advect_march(Layout L, Box box, int nocycle, double eps, int seg,
                                                       int ngroups, const double *__restrict__ cin,
                                                       double *__restrict__ cout,
-                                                      const double *__restrict__ vel, Geo4 vf, Geo3 sig,
+                                                      const double *__restrict__ vel,
+                                                      const double *__restrict__ vghost,
+                                                      const double *__restrict__ deld, Geo4 vf, Geo3 sig,
                                                       Geo3 dtvt, const int32_t *__restrict__ aloft,
                                                       DevScalars *sc, double *__restrict__ out1,
                                                       double *__restrict__ out2) {
@@ -193,6 +195,13 @@ __global__ void __launch_bounds__(128, 1) k_advect_march(Layout L, Box box, int 
   const LineGeo gsig = line_of<DIR>(sig, a, o);
   const LineGeo gdtv = line_of<DIR>(dtvt, a, o);  // dt/kappa of this step
   const double *pv = vel + base;
+  const double *pvg = vghost + base;  // ghost levels of z: plain vz (no vh)
+  // DelDonD_cc(c) of this line (ZScaling_ID 2, :163-166; 0 outside
+  // rmin-1..rmax+1): x row (j = a) at (c+1) + (a+1)*(nx+4), y column (i = a)
+  // at (a+1) + (c+1)*(nx+4)
+  const long dst = (DIR == 0) ? 1 : (long)(L.nx + 4);
+  const double *pd = TOPO ? ((DIR == 0) ? deld + 1 + (long)(a + 1) * (L.nx + 4) : deld + (a + 1) + (L.nx + 4))
+                          : nullptr;
   // top-outflow cell: n+1 for x and y; update_cc(ncells+1) for z (:309-311)
   const int ctop = (DIR == 2) ? ncells + 1 : rmax + 1;
   if (DIR == 2 && rmax == n && ctop < rmin - 1) raise_error(sc, A3G_ERR_UNSUPPORTED, 311);
@@ -213,7 +222,11 @@ __global__ void __launch_bounds__(128, 1) k_advect_march(Layout L, Box box, int 
   };
   auto vload = [&](int c) -> double {
     const int cl = PER ? wrap(c) : (c < 1 ? 1 : (c > n ? n : c));
-    return pv[(long)(cl - 1) * st];
+    const double *src = (DIR == 2 && (c < 1 || c > n)) ? pvg : pv;
+    return src[(long)(cl - 1) * st];
+  };
+  auto dload = [&](int c) -> double {
+    return (c >= rmin - 1 && c <= rmax + 1) ? pd[(long)c * dst] : 0.0;
   };
   auto vfload = [&](int q, int c) -> double {
     const int cl = c < 1 ? 1 : (c > n ? n : c);
@@ -226,6 +239,10 @@ __global__ void __launch_bounds__(128, 1) k_advect_march(Layout L, Box box, int 
   double q0[GC], q1[GC], d0[GC], d1[GC], fss0[GC], fsr0[GC];
   double usA[NU], usB[NU], vB[NU];  // us(c), us(c+1), vel(c+1) (+vf for z)
   double dtv0 = gdtv.at(cs);
+  // topography term T(c) = 0.5*vel(c)*(sig(c)+sig(c+1))*q(c)*DelDonD(c) of
+  // :251-257 (fs_r(I) += T(I), fs_l(I) -= T(I-1)): tp = T(c) per grain,
+  // sB = sig(c+1) unmasked
+  double tp[GC], sB = 0.0;
   {
     const double vm2 = vload(cs - 2), vm1 = vload(cs - 1), v0 = vload(cs), v1 = vload(cs + 1);
     const double sm1 = fs_ok(cs - 1) ? gsig.at(cs - 1) : 0.0;
@@ -258,7 +275,13 @@ __global__ void __launch_bounds__(128, 1) k_advect_march(Layout L, Box box, int 
       const Iface f = make_iface(usm1[u], usA[u], usB[u], dtv0, fss_ok(cs), fs_ok(cs));
       double fsl_unused;
       iface_grain<LIM>(f, dm, d0[q], d1[q], qm1, q0[q], eps, nocycle, fss0[q], fsr0[q], fsl_unused);
+      if (TOPO) {
+        const double t0 = (((0.5 * v0) * (gsig.at(cs) + gsig.at(cs + 1))) * q0[q]) * dload(cs);
+        if (fs_ok(cs)) fsr0[q] = fsr0[q] + t0;
+        tp[q] = t0;
+      }
     }
+    if (TOPO) sB = gsig.at(cs + 1);
   }
 
   // ---- one march step: interface c+1 and the update of cell c -------------
@@ -275,6 +298,8 @@ __global__ void __launch_bounds__(128, 1) k_advect_march(Layout L, Box box, int 
     const double sI2 = fsok2 ? sI2raw : 0.0;
     const bool own = CK ? (c >= s0 && c <= s1) : true;
     const bool inbox = CK ? (c >= rmin && c <= rmax) : true;
+    const double vc1 = vB[0];                     // vel(c+1) (x, y)
+    const double dcur = TOPO ? dload(I) : 0.0;    // DelDonD(c+1)
     Iface f[NU];
 #pragma unroll
     for (int u = 0; u < NU; u++) {
@@ -293,6 +318,14 @@ __global__ void __launch_bounds__(128, 1) k_advect_march(Layout L, Box box, int 
       double fss1, fsr1, fsl1;
       iface_grain<LIM>(f[(DIR == 2) ? q : 0], d0[q], d1[q], d2, q0[q], q1[q], eps, nocycle, fss1, fsr1,
                        fsl1);
+      if (TOPO) {
+        const double t1 = (((0.5 * vc1) * (sB + sI2raw)) * q1[q]) * dcur;
+        if (fsok1) {
+          fsr1 = fsr1 + t1;
+          fsl1 = fsl1 - tp[q];
+        }
+        tp[q] = t1;
+      }
       const double upd = cell_update(dtv0, fsl1, fsr0[q], fss1, fss0[q]);
       if (gval[q]) {
         if (own) po[q][(long)(c - 1) * st] = (gal[q] && inbox) ? q0[q] + upd : 0.0;
@@ -309,6 +342,7 @@ __global__ void __launch_bounds__(128, 1) k_advect_march(Layout L, Box box, int 
       d1[q] = d2;
     }
     dtv0 = dtv1;
+    if (TOPO) sB = sI2raw;
   };
   auto checked_step = [&](int c) {
     double q2v[GC], vf2[NU];
@@ -316,7 +350,8 @@ __global__ void __launch_bounds__(128, 1) k_advect_march(Layout L, Box box, int 
     for (int q = 0; q < GC; q++) q2v[q] = qload(q, c + 2);
 #pragma unroll
     for (int u = 0; u < NU; u++) vf2[u] = (DIR == 2) ? vfload(u, c + 2) : 0.0;
-    const double sraw = fs_ok(c + 2) ? gsig.at(c + 2) : 0.0;
+    // unmasked for the topography term (sigma is ghosted to n+2)
+    const double sraw = (TOPO ? (c + 2 <= n + 2) : fs_ok(c + 2)) ? gsig.at(c + 2) : 0.0;
     step(c, CkT{}, q2v, vload(c + 2), sraw, gdtv.at(c + 1), vf2);
   };
   // cells whose step needs no range checks: c >= rmin, c+2 <= min(n, rmax+1)
@@ -410,7 +445,8 @@ __device__ __forceinline__ double fss_select(double dqm, double dq, double dqp, 
 template <int DIR, int LIM, int V, bool PER, bool CK>
 __device__ __forceinline__ void block_body(const Layout &L, const Box &box, int nocycle, double eps,
                                            const double *__restrict__ line, double *__restrict__ oline,
-                                           long st, const double *__restrict__ pv, const double *pvf,
+                                           long st, const double *__restrict__ pv,
+                                           const double *__restrict__ pvg, const double *pvf,
                                            long vfs, const LineGeo &gsig, const LineGeo &gdtv, int c0,
                                            int n, bool lane_active, bool al, double *o1, double *o2,
                                            DevScalars *sc) {
@@ -444,7 +480,7 @@ __device__ __forceinline__ void block_body(const Layout &L, const Box &box, int 
         }
         w[m] = q;
         const int cl = PER ? wrap(c) : (c < 1 ? 1 : (c > n ? n : c));
-        vw[m] = pv[(long)(cl - 1) * st];
+        vw[m] = ((DIR == 2 && (c < 1 || c > n)) ? pvg : pv)[(long)(cl - 1) * st];
       } else {
         w[m] = line[(long)(c - 1) * st];
         vw[m] = pv[(long)(c - 1) * st];
@@ -532,7 +568,8 @@ template <int DIR, int LIM, int V, bool PER>
 __global__ void __launch_bounds__(128, 7) k_advect_block(Layout L, Box box, int nocycle, double eps, int nblk,
                                                       const double *__restrict__ cin,
                                                       double *__restrict__ cout,
-                                                      const double *__restrict__ vel, Geo4 vf, Geo3 sig,
+                                                      const double *__restrict__ vel,
+                                                      const double *__restrict__ vghost, Geo4 vf, Geo3 sig,
                                                       Geo3 dtvt, const int32_t *__restrict__ aloft,
                                                       DevScalars *sc, double *__restrict__ out1,
                                                       double *__restrict__ out2) {
@@ -569,6 +606,7 @@ __global__ void __launch_bounds__(128, 7) k_advect_block(Layout L, Box box, int 
   }
   const double *line = cin + (long)g * L.PG + base;
   const double *pv = vel + base;
+  const double *pvg = vghost + base;
   const double *pvf = vf.p + (long)(((DIR == 0) ? 0 : a) + 1) * vf.si +
                       (long)(((DIR == 2) ? o : 0) + 1) * vf.sj + (long)g * vf.sg;
   const LineGeo gsig = line_of<DIR>(sig, a, o);
@@ -580,11 +618,11 @@ __global__ void __launch_bounds__(128, 7) k_advect_block(Layout L, Box box, int 
   const long oo = (long)g * na * nother + (long)(o - 1) * na + (a - 1);
   const bool fast = c0 >= 3 && c0 >= rmin && c0 + V <= rmax && c0 + V <= n - 1;
   if (fast)
-    block_body<DIR, LIM, V, PER, false>(L, box, nocycle, eps, line, oline, st, pv, pvf, vf.sk, gsig, gdtv, c0,
-                                        n, lane_active, al, out1 + oo, out2 + oo, sc);
+    block_body<DIR, LIM, V, PER, false>(L, box, nocycle, eps, line, oline, st, pv, pvg, pvf, vf.sk, gsig, gdtv,
+                                        c0, n, lane_active, al, out1 + oo, out2 + oo, sc);
   else
-    block_body<DIR, LIM, V, PER, true>(L, box, nocycle, eps, line, oline, st, pv, pvf, vf.sk, gsig, gdtv, c0, n,
-                                       lane_active, al, out1 + oo, out2 + oo, sc);
+    block_body<DIR, LIM, V, PER, true>(L, box, nocycle, eps, line, oline, st, pv, pvg, pvf, vf.sk, gsig, gdtv,
+                                       c0, n, lane_active, al, out1 + oo, out2 + oo, sc);
 }
 
 // ---------------------------------------------------------------------------
@@ -774,7 +812,15 @@ static void launch_advect_xt(a3g_ctx *ctx) {
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
-template <int DIR, int LIM, int GC, bool PER>
+// the vertical wind of the z sweep: vz + vh once terrain is bound
+static inline const double *dir_vel(a3g_ctx *ctx, int dir) {
+  return (dir == 0) ? ctx->vx : (dir == 1) ? ctx->vy : (ctx->topo_on ? ctx->vzh : ctx->vz);
+}
+static inline const double *dir_vghost(a3g_ctx *ctx, int dir) {
+  return (dir == 0) ? ctx->vx : (dir == 1) ? ctx->vy : ctx->vz;
+}
+
+template <int DIR, int LIM, int GC, bool PER, bool TOPO = false>
 static void launch_march_gc(a3g_ctx *ctx) {
   const Layout &L = ctx->L;
   const int n = (DIR == 0) ? L.nx : (DIR == 1) ? L.ny : L.nz;
@@ -785,9 +831,11 @@ static void launch_march_gc(a3g_ctx *ctx) {
   const int seg = (n + nseg - 1) / nseg;
   const int ngroups = (L.ns + GC - 1) / GC;
   dim3 grid(((na + 31) / 32) * ngroups, (nother + 3) / 4, (n + seg - 1) / seg);
-  k_advect_march<DIR, LIM, GC, PER><<<grid, dim3(32, 4), 0, ctx->stream>>>(
+  const long n2 = (long)(L.nx + 4) * (L.ny + 4);
+  const double *deld = TOPO ? ctx->topo_buf + ((DIR == 0) ? 2 : 3) * n2 : nullptr;
+  k_advect_march<DIR, LIM, GC, PER, TOPO><<<grid, dim3(32, 4), 0, ctx->stream>>>(
       L, ctx->box, ctx->prm.nocycle, ctx->prm.eps_thresh, seg, ngroups, ctx->c0, ctx->c1,
-      (DIR == 0) ? ctx->vx : (DIR == 1) ? ctx->vy : ctx->vz, ctx->vf,
+      dir_vel(ctx, DIR), dir_vghost(ctx, DIR), deld, ctx->vf,
       (DIR == 0) ? ctx->snx : (DIR == 1) ? ctx->sny : ctx->snz, ctx->dtv, ctx->aloft, ctx->sc,
       (DIR == 0) ? ctx->out_yz1 : (DIR == 1) ? ctx->out_xz1 : ctx->out_xy1,
       (DIR == 0) ? ctx->out_yz2 : (DIR == 1) ? ctx->out_xz2 : ctx->out_xy2);
@@ -803,7 +851,7 @@ static void launch_block_v(a3g_ctx *ctx) {
   else grid = dim3((L.nx + 31) / 32, (nblk * ((DIR == 1) ? L.nz : L.ny) + 3) / 4, L.ns);
   k_advect_block<DIR, LIM, V, PER><<<grid, dim3(32, 4), 0, ctx->stream>>>(
       L, ctx->box, ctx->prm.nocycle, ctx->prm.eps_thresh, nblk, ctx->c0, ctx->c1,
-      (DIR == 0) ? ctx->vx : (DIR == 1) ? ctx->vy : ctx->vz, ctx->vf,
+      dir_vel(ctx, DIR), dir_vghost(ctx, DIR), ctx->vf,
       (DIR == 0) ? ctx->snx : (DIR == 1) ? ctx->sny : ctx->snz, ctx->dtv, ctx->aloft, ctx->sc,
       (DIR == 0) ? ctx->out_yz1 : (DIR == 1) ? ctx->out_xz1 : ctx->out_xy1,
       (DIR == 0) ? ctx->out_yz2 : (DIR == 1) ? ctx->out_xz2 : ctx->out_xy2);
@@ -813,6 +861,22 @@ template <int DIR, int LIM>
 static void launch_dir_lim(a3g_ctx *ctx) {
   const bool per = (DIR == 0) && ctx->grid.periodic;
   const int variant = ctx->tune_advect[DIR];
+  if constexpr (DIR != 2) {
+    // ZScaling_ID 2: the DelD*onD_cc terms live in the marching kernel only
+    if (ctx->topo_on && ctx->prm.zscaling_id == 2) {
+      const bool g2 = ctx->L.ns >= 2;
+      if constexpr (DIR == 0) {
+        if (per) {
+          if (g2) launch_march_gc<DIR, LIM, 2, true, true>(ctx);
+          else launch_march_gc<DIR, LIM, 1, true, true>(ctx);
+          return;
+        }
+      }
+      if (g2) launch_march_gc<DIR, LIM, 2, false, true>(ctx);
+      else launch_march_gc<DIR, LIM, 1, false, true>(ctx);
+      return;
+    }
+  }
   if (DIR == 0 && variant == 3) {
     launch_advect_xt<LIM>(ctx);
     return;

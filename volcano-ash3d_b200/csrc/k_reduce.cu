@@ -451,6 +451,42 @@ int launch_interp_winds(a3g_ctx *ctx, double frac) {
   return A3G_OK;
 }
 
+// Calc_Vmod_Topo (src/Topography.f90:2138-2166) on the interior, fused with
+// the sum the z sweep needs: vzh = vz + vh, vh = f(k)*(vx*dhdx + vy*dhdy)
+// with f = -1.0 (ZScaling_ID 1) or s_cc(k)/Ztop - 1.0 (2), precomputed on the
+// host in those operations.  The ghost levels keep plain vz (vh is zero
+// there in the reference: vx_pd and vy_pd are never written at ghost k).
+__global__ void __launch_bounds__(256) k_vmod_topo(Layout L, const double *__restrict__ topo,
+                                                   const double *__restrict__ vx,
+                                                   const double *__restrict__ vy,
+                                                   const double *__restrict__ vz,
+                                                   double *__restrict__ vzh) {
+  const long n = (long)L.nx * L.ny * L.nz;
+  const long n2 = (long)(L.nx + 4) * (L.ny + 4);
+  const double *dhdx = topo, *dhdy = topo + n2, *fac = topo + 4 * n2;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % L.nx) + 1;
+    const long r = t / L.nx;
+    const int j = (int)(r % L.ny) + 1;
+    const int k = (int)(r / L.ny) + 1;
+    const long c = L.cell(i, j, k);
+    const long m = (long)(i + 1) + (long)(L.nx + 4) * (j + 1);
+    const double vh = fac[k - 1] * (vx[c] * dhdx[m] + vy[c] * dhdy[m]);
+    vzh[c] = vz[c] + vh;
+  }
+}
+
+int launch_vmod_topo(a3g_ctx *ctx) {
+  const long n = (long)ctx->L.nx * ctx->L.ny * ctx->L.nz;
+  int blocks = (int)((n + 255) / 256);
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  tbegin(ctx, A3G_K_WINDS);
+  k_vmod_topo<<<blocks, 256, 0, ctx->stream>>>(ctx->L, ctx->topo_buf, ctx->vx, ctx->vy, ctx->vz, ctx->vzh);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  return A3G_OK;
+}
+
 __global__ void k_source(Layout L, int ivent, int jvent, const double *__restrict__ flux, double dt,
                          double *__restrict__ c) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;  // (k-1) + nz*g

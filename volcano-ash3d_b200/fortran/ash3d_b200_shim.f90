@@ -35,7 +35,7 @@
       private
       public B200_Init, B200_Finalize, B200_Upload, B200_Download, B200_Check, &
              B200_StepPrologue, B200_AddSource, B200_SetWinds, B200_SetMetSteps, &
-             B200_InterpWinds, b200_ctx
+             B200_InterpWinds, B200_SetTopo, b200_ctx
 
       type, bind(C) :: a3g_grid_desc
         integer(c_int32_t) :: nx, ny, nz, ns
@@ -99,6 +99,11 @@
           import :: c_int, c_ptr, c_double
           type(c_ptr), value :: ctx
           real(c_double), value :: frac
+        end function
+        integer(c_int) function a3g_set_topo(ctx, dhdx, dhdy, ddx, ddy, scc, ztop) bind(C, name="a3g_set_topo")
+          import :: c_int, c_ptr, c_double
+          type(c_ptr), value :: ctx, dhdx, dhdy, ddx, ddy, scc
+          real(c_double), value :: ztop
         end function
         integer(c_int) function a3g_upload_concen(ctx, c) bind(C, name="a3g_upload_concen")
           import :: c_int, c_ptr
@@ -195,7 +200,9 @@
       end subroutine B200_Check
 
       !------------------------------------------------------------------------
-      ! After alloc_arrays, calc_mesh_params and Allocate_Diff (src/Ash3d.F90:230-240).
+      ! After alloc_arrays, calc_mesh_params, Get_Topo, calc_s_mesh (so that the
+      ! ZScaling_ID 2 geometry is the scaled one) and Allocate_Diff
+      ! (src/Ash3d.F90:230-240).
       subroutine B200_Init(device)
         use global_param, only : CFL, DT_MIN, DT_MAX, useDiffusion, useCN, EPS_THRESH, EPS_SMALL
         use mesh,         only : nxmax, nymax, nzmax, nsmax, IsPeriodic, IsLatLon, dx, dy, &
@@ -291,6 +298,18 @@
         real(kind=8), intent(in) :: frac
         call B200_Check(a3g_interp_winds(b200_ctx, real(frac, c_double)), "a3g_interp_winds")
       end subroutine B200_InterpWinds
+
+      ! useTopo: bind the terrain terms once, after Get_Topo and calc_s_mesh
+      ! (src/Ash3d.F90:233-240).  vh is then formed on the device after every
+      ! B200_SetWinds / B200_InterpWinds, in place of Calc_Vmod_Topo
+      ! (src/Ash3d.F90:398).  dhdx_comp and dhdy_comp are private to module
+      ! Topography (src/Topography.f90:181-182) and need the public attribute.
+      subroutine B200_SetTopo
+        use mesh,       only : s_cc_pd, Ztop
+        use Topography, only : dhdx_comp, dhdy_comp, DelDxonD_cc, DelDyonD_cc
+        call B200_Check(a3g_set_topo(b200_ctx, c_loc(dhdx_comp), c_loc(dhdy_comp), c_loc(DelDxonD_cc), &
+                        c_loc(DelDyonD_cc), c_loc(s_cc_pd), real(Ztop, c_double)), "a3g_set_topo")
+      end subroutine B200_SetTopo
 
       end module B200_Transport
 

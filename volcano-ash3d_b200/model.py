@@ -37,6 +37,7 @@ class Ash3dGPU:
         p.fast_subgrid = int(cfg.fast_subgrid)
         p.cfl = cfg.cfl
         p.magma_density = cfg.magma_density
+        p.zscaling_id = int(cfg.zscaling_id)
         self.ctx = C.c_void_p()
         check(lib.a3g_create(C.byref(g), C.byref(p), device, C.byref(self.ctx)))
         geo = geo if geo is not None else syn.geometry(cfg)
@@ -48,6 +49,8 @@ class Ash3dGPU:
         self._vf = syn.fall_velocity(cfg)
         check(lib.a3g_set_fall_velocity(self.ctx, dptr(self._vf)))
         self._dt = 0.0
+        if syn.use_topo(cfg):
+            self.set_topo(**syn.topo_fields(cfg))
 
     # --- lifetime ----------------------------------------------------------
     def close(self):
@@ -170,6 +173,14 @@ class Ash3dGPU:
     def set_winds(self, vx, vy, vz):
         a = [np.asfortranarray(v, dtype=np.float64) for v in (vx, vy, vz)]
         check(self.lib.a3g_set_winds(self.ctx, *[dptr(v) for v in a]))
+
+    def set_topo(self, dhdx, dhdy, deldx, deldy, s_cc, ztop):
+        """useTopo: dhdx_comp, dhdy_comp, DelDxonD_cc, DelDyonD_cc
+        (-1:nx+2,-1:ny+2), s_cc_pd (-1:nz+2), Ztop (km); vh is formed on
+        the device after every wind update (a3g_set_topo)."""
+        a = [np.asfortranarray(v, dtype=np.float64) for v in (dhdx, dhdy, deldx, deldy)]
+        sc = np.ascontiguousarray(s_cc, dtype=np.float64)
+        check(self.lib.a3g_set_topo(self.ctx, *[dptr(v) for v in a], dptr(sc), float(ztop)))
 
     def set_aloft(self, flags):
         f = np.asarray(flags, dtype=np.int32)

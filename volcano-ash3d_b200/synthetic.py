@@ -74,6 +74,9 @@ class Config:
     seed: int = 1
     fast_subgrid: bool = False
     magma_density: float = 2500.0
+    zscaling_id: int = 0     # ZScaling_ID: 0 s = z, 1 shifted by topography, 2 scaled (sigma-altitude)
+    topo_km: float = 0.0     # height of a Gaussian hill centred on the vent (0: no topography)
+    topo_width_km: float = 0.0   # its standard deviation (km); 0: three cell widths
 
     @property
     def cells(self) -> int:
@@ -188,7 +191,21 @@ def zgrid(cfg: Config):
 
 
 def geometry(cfg: Config) -> dict:
-    """kappa_pd, sigma_n{x,y,z}_pd (-1:nx+2,-1:ny+2,-1:nz+2) and dz_vec_pd (-1:nz+2)."""
+    """kappa_pd, sigma_n{x,y,z}_pd (-1:nx+2,-1:ny+2,-1:nz+2) and dz_vec_pd
+    (-1:nz+2) of calc_mesh_params, then calc_s_mesh's Jacobian scaling for
+    ZScaling_ID 2 (src/Calc_Mesh.f90:316-328)."""
+    g = _geometry_z(cfg)
+    if use_topo(cfg) and cfg.zscaling_id == 2:
+        jcc = jacobian(cfg)
+        for name in ("sig_nx", "sig_ny", "kappa"):
+            a = g[name]
+            for kk in range(a.shape[2]):
+                a[:, :, kk] = a[:, :, kk] * jcc
+    return g
+
+
+def _geometry_z(cfg: Config) -> dict:
+    """calc_mesh_params (src/Calc_Mesh.f90:23-220)."""
     NX, NY, NZ = cfg.nx + 4, cfg.ny + 4, cfg.nz + 4
     dz, zcc, zlb = zgrid(cfg)
     shp = (NX, NY, NZ)
@@ -225,6 +242,92 @@ def geometry(cfg: Config) -> dict:
                 snz[:, jj, kk] = rr_1 * del_lam * del_costheta
                 kap[:, jj, kk] = del_lam * drrr * del_costheta / 3.0
     return dict(kappa=kap, sig_nx=snx, sig_ny=sny, sig_nz=snz, dz_vec=dz, z_cc=zcc, z_lb=zlb)
+
+
+# ---------------------------------------------------------------------------
+# terrain (src/Topography.f90, src/Calc_Mesh.f90:237-329)
+# ---------------------------------------------------------------------------
+def use_topo(cfg: Config) -> bool:
+    return cfg.topo_km > 0.0 and cfg.zscaling_id in (1, 2)
+
+
+def ztop(cfg: Config) -> float:
+    """Ztop (km): the top of the computational grid, z_lb(nz+1)."""
+    return float(zgrid(cfg)[2][cfg.nz + 2])
+
+
+def topography(cfg: Config) -> np.ndarray:
+    """topo_comp(-1:nx+2,-1:ny+2) in km: a Gaussian hill of height topo_km
+    centred on the vent cell.  It stands in for the DEM that Get_Topo reads,
+    interpolates and smooths (src/Topography.f90:515-620), host
+    preprocessing outside the transport step."""
+    ic = np.arange(-1, cfg.nx + 3, dtype=np.float64)
+    jc = np.arange(-1, cfg.ny + 3, dtype=np.float64)
+    dx, dy = projected_dxdy(cfg)
+    X = (ic - cfg.ivent)[:, None] * dx
+    Y = (jc - cfg.jvent)[None, :] * dy
+    w = cfg.topo_width_km if cfg.topo_width_km > 0.0 else 3.0 * max(dx, dy)
+    return np.asfortranarray(cfg.topo_km * np.exp(-(X * X + Y * Y) / (2.0 * w * w)))
+
+
+def jacobian(cfg: Config) -> np.ndarray:
+    """j_cc_pd(-1:nx+2,-1:ny+2) of Get_Topo (src/Topography.f90:608-620)."""
+    if cfg.zscaling_id != 2 or not use_topo(cfg):
+        return np.ones((cfg.nx + 4, cfg.ny + 4), order="F")
+    zt = ztop(cfg)
+    return np.asfortranarray((zt - topography(cfg)) / zt)
+
+
+def topo_fields(cfg: Config) -> dict:
+    """Calc_FDGrad_Topo (src/Topography.f90:2471-2536) on the mesh of
+    calc_mesh_params (Get_Topo runs before calc_s_mesh scales it,
+    src/Ash3d.F90:232-240): dhdx_comp, dhdy_comp, DelDxonD_cc, DelDyonD_cc
+    (-1:nx+2,-1:ny+2), plus s_cc_pd (-1:nz+2; s = z for every ZScaling_ID,
+    src/Calc_Mesh.f90:271-289) and Ztop.  As in the reference, the interior
+    (two-sided) gradient divides the difference over two cells by
+    ds = 2*kappa/(sigma_i + sigma_i+1), one cell width, so it is twice the
+    slope; the one-sided edge values are the slope itself."""
+    g = _geometry_z(cfg)
+    kap, snx, sny = g["kappa"], g["sig_nx"], g["sig_ny"]
+    topo = topography(cfg)
+    zt = ztop(cfg)
+    NX, NY = cfg.nx + 4, cfg.ny + 4
+    dhdx, dhdy = np.zeros((NX, NY), order="F"), np.zeros((NX, NY), order="F")
+    ddx, ddy = np.zeros((NX, NY), order="F"), np.zeros((NX, NY), order="F")
+    k1 = 2  # k = 1
+    for a in range(NX):          # a = i + 1
+        for b in range(NY):      # b = j + 1
+            if a == 0:
+                ds = kap[a, b, k1] / snx[a, b, k1]
+                dhdx[a, b] = (topo[a + 1, b] - topo[a, b]) / ds
+                D1, D2, D3 = zt - topo[a, b], zt - topo[a + 1, b], zt - topo[a, b]
+                ddx[a, b] = (D2 - D1) / D3
+            elif a == NX - 1:
+                ds = kap[a, b, k1] / snx[a, b, k1]
+                dhdx[a, b] = (topo[a, b] - topo[a - 1, b]) / ds
+                D1, D2, D3 = zt - topo[a - 1, b], zt - topo[a, b], zt - topo[a, b]
+                ddx[a, b] = (D2 - D1) / D3
+            else:
+                ds = 2.0 * kap[a, b, k1] / (snx[a, b, k1] + snx[a + 1, b, k1])
+                dhdx[a, b] = (topo[a + 1, b] - topo[a - 1, b]) / ds
+                D1, D2, D3 = zt - topo[a - 1, b], zt - topo[a + 1, b], zt - topo[a, b]
+                ddx[a, b] = 0.5 * (D2 - D1) / D3
+            if b == 0:
+                ds = kap[a, b, k1] / sny[a, b, k1]
+                dhdy[a, b] = (topo[a, b + 1] - topo[a, b]) / ds
+                D1, D2, D3 = zt - topo[a, b], zt - topo[a, b + 1], zt - topo[a, b]
+                ddy[a, b] = (D2 - D1) / D3
+            elif b == NY - 1:
+                ds = kap[a, b, k1] / sny[a, b, k1]
+                dhdy[a, b] = (topo[a, b] - topo[a, b - 1]) / ds
+                D1, D2, D3 = zt - topo[a, b - 1], zt - topo[a, b], zt - topo[a, b]
+                ddy[a, b] = (D2 - D1) / D3
+            else:
+                ds = 2.0 * kap[a, b, k1] / (sny[a, b, k1] + sny[a, b + 1, k1])
+                dhdy[a, b] = (topo[a, b + 1] - topo[a, b - 1]) / ds
+                D1, D2, D3 = zt - topo[a, b - 1], zt - topo[a, b + 1], zt - topo[a, b]
+                ddy[a, b] = 0.5 * (D2 - D1) / D3
+    return dict(dhdx=dhdx, dhdy=dhdy, deldx=ddx, deldy=ddy, s_cc=zgrid(cfg)[1].copy(), ztop=zt)
 
 
 def projected_dxdy(cfg: Config):
@@ -325,16 +428,30 @@ class MetSource:
 # ---------------------------------------------------------------------------
 # source, src/Source.f90
 # ---------------------------------------------------------------------------
+def vent_s_coordinates(cfg: Config):
+    """(s_volcano, s_PlumeHeight) of Calc_Normalized_SourceCol
+    (src/Source.f90:324-340): the vent elevation and plume top in the
+    s-coordinate of ZScaling_ID, Zsurf(ivent,jvent) being the topography at
+    the vent."""
+    if not use_topo(cfg):
+        return cfg.z_volcano, cfg.plume_km
+    zs = float(topography(cfg)[cfg.ivent + 1, cfg.jvent + 1])
+    zv = max(cfg.z_volcano, zs)
+    if cfg.zscaling_id == 1:
+        return zv - zs, cfg.plume_km - zs
+    zt = ztop(cfg)
+    return zt * (zv - zs) / (zt - zs), zt * (cfg.plume_km - zs) / (zt - zs)
+
+
 def suzuki_column(cfg: Config) -> np.ndarray:
     """NormSourceColumn(1, 1:nz+1) for one eruption (Calc_Normalized_SourceCol,
-    ZScaling_ID 0: s = z)."""
+    src/Source.f90:287-490; the s-grid is the z-grid for every ZScaling_ID)."""
     nz = cfg.nz
     dz, zcc, zlb = zgrid(cfg)
     s_lb = lambda k: zlb[k + 1]
     s_cc = lambda k: zcc[k + 1]
     ds = lambda k: dz[k + 1]
-    s_volcano = cfg.z_volcano
-    H = cfg.plume_km
+    s_volcano, H = vent_s_coordinates(cfg)
     kground, ktop = 1, 0
     for k in range(1, nz + 1):
         if s_volcano >= s_lb(k) and s_volcano < s_lb(k + 1):
