@@ -46,7 +46,7 @@ def _variants(op):
     # advection: march / block-4 / block-8; diffusion: the CN x solve
     # warp-tiled / one thread per line and the y, z solves one / two grains
     # per thread
-    return (0, 1, 2, 3) if op in ADVECTION else (0, 1, 2)
+    return (0, 1, 2, 3, 4) if op in ADVECTION else (0, 1, 2)
 
 
 def _set_variant(gpu, op, variant):
@@ -115,7 +115,7 @@ def test_timestep_totals(name):
 
 
 @pytest.mark.parametrize("name", CONFIGS)
-@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
 def test_run_bitwise(name, variant):
     from volcano_ash3d_b200 import driver
     cfg, gpu, ref = pair(name)

@@ -50,7 +50,7 @@ def _same(gpu, ref):
 @pytest.mark.parametrize("name", CONFIGS)
 @pytest.mark.parametrize("z", [1, 2])
 @pytest.mark.parametrize("op", ["advect_x", "advect_y", "AdvectVert"])
-@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
 def test_topo_sweep_bitwise(name, z, op, variant):
     cfg, gpu, ref = _pair(name, z)
     for d in range(3):

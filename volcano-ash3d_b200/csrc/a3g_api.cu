@@ -192,9 +192,10 @@ int a3g_create(const a3g_grid_desc *grid, const a3g_params *params, int device, 
   ctx->h_aloft.assign(grid->ns, 1);
   ctx->n_gs_aloft = grid->ns;
   ctx->last_bc = 0;
-  // fastest measured advection variants on B200 (x: marching rows; y, z:
-  // 4-cell blocks); a3g_set_variant overrides them
-  ctx->tune_advect[0] = 0;
+  // fastest measured advection variants on B200 (x: warp-row chunks, C2
+  // 1.62 ms against 2.16 for marching rows; y, z: 4-cell blocks);
+  // a3g_set_variant overrides them
+  ctx->tune_advect[0] = 4;
   ctx->tune_advect[1] = 1;
   ctx->tune_advect[2] = 1;
   ctx->tune_cn_x = 0;
@@ -852,7 +853,7 @@ int a3g_kernel_times(a3g_ctx *ctx, double *ms, uint64_t *count) {
 
 int a3g_set_variant(a3g_ctx *ctx, int32_t dir, int32_t variant) {
   if (!ctx) return fail(A3G_ERR_ARG, "null context");
-  if (dir < 0 || dir > 4 || variant < 0 || variant > (dir == 0 ? 3 : dir == 3 ? 1 : 2))
+  if (dir < 0 || dir > 4 || variant < 0 || variant > (dir == 0 ? 4 : dir == 3 ? 1 : 2))
     return fail(A3G_ERR_ARG, "bad direction or variant");
   if (dir == 3) ctx->tune_cn_x = variant;
   else if (dir == 4) ctx->tune_cn_yz = variant;

@@ -815,6 +815,171 @@ static void launch_advect_xt(a3g_ctx *ctx) {
 }
 
 // ---------------------------------------------------------------------------
+// Warp-row x sweep.  A warp owns one x row (j, k) and a group of GC grains and
+// walks the row in chunks of 32 cells with the lanes along i, so every global
+// load and store is a coalesced row segment.  Lane l of the chunk starting at
+// cell b loads cell i = b + l, forms the flux area us(i), and computes the
+// fluxes of interface I = i - 1 (which needs q(I-2..I+1), us(I-1..I+1): the
+// cells behind it come from per-warp shared-memory rings of 64 entries); it
+// then updates cell c = I - 1 from interface I (its own) and interface c
+// (lane l-1's, through the same rings).  Each interface is computed once, in
+// the march's expressions (make_iface, iface_grain, cell_update), so the
+// results are the same bits.  Nothing is carried in registers between
+// chunks, which keeps the register count and the L1 traffic low.
+// ---------------------------------------------------------------------------
+constexpr int XW_WARPS = 4;
+
+template <int LIM, int GC, bool PER>
+__global__ void __launch_bounds__(32 * XW_WARPS, 6) k_advect_xw(Layout L, Box box, int nocycle, double eps,
+                                                          int ngroups, const double *__restrict__ cin,
+                                                          double *__restrict__ cout,
+                                                          const double *__restrict__ vel, Geo3 sig, Geo3 dtvt,
+                                                          const int32_t *__restrict__ aloft,
+                                                          double *__restrict__ out1, double *__restrict__ out2) {
+  __shared__ double s_q[XW_WARPS][GC][64];
+  __shared__ double s_fss[XW_WARPS][GC][64];
+  __shared__ double s_fsr[XW_WARPS][GC][64];
+  __shared__ double s_v[XW_WARPS][64];
+  __shared__ double s_u[XW_WARPS][64];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const long w = (long)blockIdx.x * XW_WARPS + wid;
+  if (w >= (long)L.ny * L.nz * ngroups) return;  // whole warps only; no block barrier below
+  const int j = (int)(w % L.ny) + 1;
+  const int k = (int)((w / L.ny) % L.nz) + 1;
+  const int g0 = (int)(w / ((long)L.ny * L.nz)) * GC;
+  const int n = L.nx;
+  const int rmin = box.imin, rmax = box.imax;
+  const bool row_active = j >= box.jmin && j <= box.jmax && k >= box.kmin && k <= box.kmax;
+  const long base = L.cell(1, j, k);
+  bool gval[GC], gal[GC];
+  const double *pq[GC];
+  double *po[GC];
+  bool any = false;
+#pragma unroll
+  for (int q = 0; q < GC; q++) {
+    const int g = g0 + q;
+    gval[q] = g < L.ns;
+    gal[q] = gval[q] && row_active && aloft[g] != 0;
+    pq[q] = cin + (long)(gval[q] ? g : 0) * L.PG + base;
+    po[q] = cout + (long)(gval[q] ? g : 0) * L.PG + base;
+    any = any || gal[q];
+  }
+  if (!any) {  // the reference leaves zeros
+#pragma unroll
+    for (int q = 0; q < GC; q++)
+      if (gval[q])
+        for (int c = 1 + lane; c <= n; c += 32) po[q][c - 1] = 0.0;
+    return;
+  }
+  const LineGeo gsig = line_of<0>(sig, j, k);
+  const LineGeo gdtv = line_of<0>(dtvt, j, k);
+  const double *pv = vel + base;
+  const bool out_lo = !PER && rmin == 1;
+  const bool out_hi = !PER && rmax == n;
+  const long oo = (long)(k - 1) * L.ny + (j - 1);
+  const long oslab = (long)L.ny * L.nz;
+  auto wrap = [&](int c) { return c < 1 ? c + n : (c > n ? c - n : c); };
+  auto fs_ok = [&](int I) { return I >= rmin - 1 && I <= rmax + 1; };
+  auto fss_ok = [&](int I) { return I >= rmin && I <= rmax + 1; };
+  // ring slots of the chunk before the first (cells -4..-2): zero
+#pragma unroll
+  for (int q = 0; q < GC; q++) {
+    s_q[wid][q][32 + lane] = 0.0;
+    s_fss[wid][q][32 + lane] = 0.0;
+    s_fsr[wid][q][32 + lane] = 0.0;
+  }
+  s_v[wid][32 + lane] = 0.0;
+  s_u[wid][32 + lane] = 0.0;
+  // chunk t covers loads i = 32t - 1 + lane and updates cells c = i - 2.  A
+  // chunk whose loads all lie in [max(rmin+2, 1), min(n, rmax+1)] needs no
+  // range check (its cells are inside the box, its interfaces and flux
+  // areas inside [rmin, rmax+1], no ghost or outflow cell); the others take
+  // the checked body.
+  const int ilo = max(rmin + 2, 1), ihi = min(n, rmax + 1);
+  auto chunk = [&](int t, auto checked) {
+    constexpr bool CK = decltype(checked)::value;
+    __syncwarp();
+    const int i = 32 * t - 1 + lane;
+    const int sl = (32 * t + lane) & 63;
+    const int sl1 = (sl + 63) & 63, sl2 = (sl + 62) & 63, sl3 = (sl + 61) & 63;
+    double qi[GC];
+#pragma unroll
+    for (int q = 0; q < GC; q++) {
+      double v = 0.0;
+      if (!CK) {
+        v = pq[q][i - 1];
+      } else if (i >= rmin - 2 && i <= rmax + 2) {  // ghost cells of Set_BC(1): zero, or wrapped
+        if (i >= 1 && i <= n) v = pq[q][i - 1];
+        else if (PER) v = pq[q][wrap(i) - 1];
+      }
+      qi[q] = v;
+      s_q[wid][q][sl] = v;
+    }
+    double vi = 0.0;  // vel(i) is read by us(i) and us(i+1) only
+    if (!CK) vi = pv[i - 1];
+    else if (i >= rmin - 2 && i <= rmax + 1) vi = pv[(PER ? wrap(i) : (i < 1 ? 1 : (i > n ? n : i))) - 1];
+    s_v[wid][sl] = vi;
+    __syncwarp();
+    const double usi = (!CK || fs_ok(i)) ? 0.5 * (s_v[wid][sl1] + vi) * gsig.at(i) : 0.0;
+    s_u[wid][sl] = usi;
+    __syncwarp();
+    const int I = i - 1;
+    const double dtvI = (!CK || (I >= -1 && I <= n + 2)) ? gdtv.at(I) : 0.0;
+    const Iface f = make_iface(s_u[wid][sl2], s_u[wid][sl1], usi, dtvI, !CK || fss_ok(I), !CK || fs_ok(I));
+    double qm[GC], fsl[GC], fss[GC];
+#pragma unroll
+    for (int q = 0; q < GC; q++) {
+      const double q3 = s_q[wid][q][sl3], q2 = s_q[wid][q][sl2], q1 = s_q[wid][q][sl1];
+      double fsr;
+      iface_grain<LIM>(f, q2 - q3, q1 - q2, qi[q] - q1, q2, q1, eps, nocycle, fss[q], fsr, fsl[q]);
+      qm[q] = q2;
+      s_fss[wid][q][sl] = fss[q];
+      s_fsr[wid][q][sl] = fsr;
+    }
+    __syncwarp();
+    const int c = I - 1;
+    if (!CK || (c >= 0 && c <= n + 1)) {
+      const double dtvc = gdtv.at(c);
+      const bool inbox = !CK || (c >= rmin && c <= rmax);
+#pragma unroll
+      for (int q = 0; q < GC; q++) {
+        const double upd = cell_update(dtvc, fsl[q], s_fsr[wid][q][sl1], fss[q], s_fss[wid][q][sl1]);
+        if (gval[q]) {
+          if (!CK || (c >= 1 && c <= n)) po[q][c - 1] = (gal[q] && inbox) ? qm[q] + upd : 0.0;
+          if (CK && gal[q]) {
+            if (out_lo && c == 0) out1[(long)(g0 + q) * oslab + oo] += upd;
+            if (out_hi && c == rmax + 1) out2[(long)(g0 + q) * oslab + oo] += upd;
+          }
+        }
+      }
+    }
+  };
+  for (int t = 0; 32 * t - 3 <= n + 1; t++) {
+    if (32 * t - 1 >= ilo && 32 * t + 30 <= ihi) chunk(t, FastT{});
+    else chunk(t, CkT{});
+  }
+}
+
+template <int LIM>
+static void launch_advect_xw(a3g_ctx *ctx) {
+  const Layout &L = ctx->L;
+  const int gc = (L.ns >= 2) ? 2 : 1;
+  const int ngroups = (L.ns + gc - 1) / gc;
+  const long nwarps = (long)L.ny * L.nz * ngroups;
+  const unsigned blocks = (unsigned)((nwarps + XW_WARPS - 1) / XW_WARPS);
+#define A3G_XW(GC_, PER_)                                                                                   \
+  k_advect_xw<LIM, GC_, PER_><<<blocks, 32 * XW_WARPS, 0, ctx->stream>>>(                                  \
+      L, ctx->box, ctx->prm.nocycle, ctx->prm.eps_thresh, ngroups, ctx->c0, ctx->c1, ctx->vx, ctx->snx,     \
+      ctx->dtv, ctx->aloft, ctx->out_yz1, ctx->out_yz2)
+  if (gc == 2) {
+    if (ctx->grid.periodic) A3G_XW(2, true); else A3G_XW(2, false);
+  } else {
+    if (ctx->grid.periodic) A3G_XW(1, true); else A3G_XW(1, false);
+  }
+#undef A3G_XW
+}
+
+// ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
 // the vertical wind of the z sweep: vz + vh once terrain is bound
@@ -882,9 +1047,15 @@ static void launch_dir_lim(a3g_ctx *ctx) {
       return;
     }
   }
-  if (DIR == 0 && variant == 3) {
-    launch_advect_xt<LIM>(ctx);
-    return;
+  if constexpr (DIR == 0) {
+    if (variant == 3) {
+      launch_advect_xt<LIM>(ctx);
+      return;
+    }
+    if (variant == 4) {
+      launch_advect_xw<LIM>(ctx);
+      return;
+    }
   }
   if (variant == 1) {
     if (per) launch_block_v<DIR, LIM, 4, true>(ctx);
