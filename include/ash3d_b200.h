@@ -124,6 +124,25 @@ int a3g_set_met_steps(a3g_ctx *ctx, const float *vx_last, const float *vy_last,
  * v = (dble(last) + dble(next-last)*frac)*3.6 */
 int a3g_interp_winds(a3g_ctx *ctx, double interval_frac);
 
+/* ---- umbrella source (SourceType 'umbrella' / 'umbrella_air'; lon/lat grids) ---- */
+/* Allocate_Source_Umbrella (src/Source_Umbrella.f90:85-153): the vent, the
+ * umbrella levels ibase..itop and AvgStenc_Umbrella (3,3,nz).  Allocates the
+ * per-step buffers once; the 3x3 patch must lie inside the grid. */
+int a3g_set_umbrella(a3g_ctx *ctx, int32_t ivent, int32_t jvent, int32_t ibase, int32_t itop,
+                     const double *avg_stencil);
+/* Adds umbrella_winds' radial winds (km/h; uvx, uvy over the box i0..i1 x
+ * j0..j1, i fastest) to vx, vy on levels ibase..itop, as MesoInterpolater
+ * does while the eruption lasts (src/MesoInterpolater.f90:233-248).  Call it
+ * after a3g_interp_winds / a3g_set_winds and before Adjust_DT; with terrain
+ * bound, vh is formed again from the updated winds. */
+int a3g_add_umbrella_winds(a3g_ctx *ctx, int32_t i0, int32_t i1, int32_t j0, int32_t j1,
+                           const double *uvx, const double *uvy);
+/* Umbrella source insertion (src/Ash3d.F90:435-458): on ibase..itop the 3x3
+ * patch is set to its AvgCon_Umbrella average, then every patch cell gains
+ * dt*SourceNodeFlux_Umbrella(3,3,nz+1,ns) (TephraSourceNodes_Umbrella,
+ * src/Source_Umbrella.f90:409-448). */
+int a3g_add_source_umbrella(a3g_ctx *ctx, const double *flux_umbrella, double dt);
+
 /* ---- terrain (useTopo; src/Topography.f90) ---- */
 /* Binds the topography terms of the step: dhdx_comp, dhdy_comp, DelDxonD_cc,
  * DelDyonD_cc (-1:nx+2,-1:ny+2, as Calc_FDGrad_Topo leaves them,

@@ -963,6 +963,41 @@ void orc_add_source(orc_state *s, int ivent, int jvent, const double *flux, doub
           s->concen[c5(s, ivent, jvent, k, n, 0)] + dt * flux[(size_t)(k - 1) + (size_t)(s->nz + 1) * (n - 1)];
 }
 
+void orc_add_umbrella_winds(orc_state *s, int ibase, int itop, int i0, int i1, int j0, int j1,
+                            const double *uvx, const double *uvy) {
+  const int ni = i1 - i0 + 1;
+  for (int k = ibase; k <= itop; k++)
+    for (int j = j0; j <= j1; j++)
+      for (int i = i0; i <= i1; i++) {
+        const size_t m = (size_t)(i - i0) + (size_t)ni * (j - j0);
+        s->vx[i3(s, i, j, k)] = s->vx[i3(s, i, j, k)] + uvx[m];
+        s->vy[i3(s, i, j, k)] = s->vy[i3(s, i, j, k)] + uvy[m];
+      }
+}
+
+void orc_add_source_umbrella(orc_state *s, int ivent, int jvent, int ibase, int itop,
+                             const double *stencil, const double *flux, double dt) {
+  const int nz = s->nz;
+  for (int k = ibase; k <= itop; k++)                              /* :448-453 */
+    for (int n = 1; n <= s->ns; n++) {
+      double avg = 0.0;                                            /* AvgCon_Umbrella */
+      for (int i = 1; i <= 3; i++)
+        for (int j = 1; j <= 3; j++)
+          avg = avg + s->concen[c5(s, ivent - 2 + i, jvent - 2 + j, k, n, 0)] *
+                          stencil[(i - 1) + 3 * (j - 1) + 9 * (k - 1)];
+      for (int i = 1; i <= 3; i++)
+        for (int j = 1; j <= 3; j++) s->concen[c5(s, ivent - 2 + i, jvent - 2 + j, k, n, 0)] = avg;
+    }
+  for (int n = 1; n <= s->ns; n++)                                 /* :455-458 */
+    for (int k = 1; k <= nz + 1; k++)
+      for (int j = 1; j <= 3; j++)
+        for (int i = 1; i <= 3; i++) {
+          const size_t a = c5(s, ivent - 2 + i, jvent - 2 + j, k, n, 0);
+          s->concen[a] = s->concen[a] +
+                         dt * flux[(i - 1) + 3 * (j - 1) + 9 * ((size_t)(k - 1) + (size_t)(nz + 1) * (n - 1))];
+        }
+}
+
 void orc_interp_winds(orc_state *s, const float *vx_last, const float *vx_next,
                       const float *vy_last, const float *vy_next,
                       const float *vz_last, const float *vz_next, double frac) {

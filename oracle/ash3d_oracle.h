@@ -141,6 +141,15 @@ void orc_add_source(orc_state *s, int ivent, int jvent, const double *flux,
 void orc_interp_winds(orc_state *s, const float *vx_last, const float *vx_next,
                       const float *vy_last, const float *vy_next,
                       const float *vz_last, const float *vz_next, double frac);
+/* Umbrella source: umbrella_winds' box (i0..i1 x j0..j1, i fastest) added to
+ * vx, vy on levels ibase..itop (src/MesoInterpolater.f90:237-241), and the
+ * 3x3 insertion of src/Ash3d.F90:446-458 (AvgCon_Umbrella smoothing on
+ * ibase..itop with stencil(3,3,nz), then concen += dt*flux(3,3,nz+1,ns) on
+ * levels 1..nz+1). */
+void orc_add_umbrella_winds(orc_state *s, int ibase, int itop, int i0, int i1, int j0, int j1,
+                            const double *uvx, const double *uvy);
+void orc_add_source_umbrella(orc_state *s, int ivent, int jvent, int ibase, int itop,
+                             const double *stencil, const double *flux, double dt);
 /* Prune_GS, src/Tephra.f90:782-812. */
 void orc_prune_gs(orc_state *s, double airborne_thresh);
 /* Restatement of LAPACK dgtsv for one right-hand side (reference LAPACK's

@@ -83,6 +83,8 @@ def load() -> C.CDLL:
             ("orc_add_source", None, [S, C.c_int, C.c_int, D, C.c_double]),
             ("orc_interp_winds", None, [S, F, F, F, F, F, F, C.c_double]),
             ("orc_prune_gs", None, [S, C.c_double]),
+            ("orc_add_umbrella_winds", None, [S, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, D, D]),
+            ("orc_add_source_umbrella", None, [S, C.c_int, C.c_int, C.c_int, C.c_int, D, D, C.c_double]),
             ("orc_dgtsv", C.c_int, [C.c_int, D, D, D, D]),
             ("orc_set_threads", None, [C.c_int]), ("orc_get_threads", C.c_int, []),
             ("orc_adj_advect_x", None, [S, D]), ("orc_adj_advect_y", None, [S, D]),
@@ -180,6 +182,7 @@ class OracleModel:
         self._topo = None
         if syn.use_topo(cfg):
             self.set_topo(**syn.topo_fields(cfg))
+        self.umbrella = syn.umbrella_setup(cfg, self.kappa) if syn.is_umbrella(cfg) else None
 
     # --- routines with the reference names ---------------------------------
     def Set_BC(self, code):
@@ -264,6 +267,19 @@ class OracleModel:
         self.vz[...] = vz
         if self.s.use_topo:
             self.lib.orc_calc_vmod_topo(self.ps)
+
+    def add_umbrella_winds(self, i0, i1, j0, j1, uvx, uvy):
+        u = self.umbrella
+        a, b = np.asfortranarray(uvx, dtype=np.float64), np.asfortranarray(uvy, dtype=np.float64)
+        self.lib.orc_add_umbrella_winds(self.ps, u.ibase, u.itop, i0, i1, j0, j1, _d(a), _d(b))
+        if self.s.use_topo:  # Calc_Vmod_Topo follows MesoInterpolater
+            self.lib.orc_calc_vmod_topo(self.ps)
+
+    def add_source_umbrella(self, flux_umbrella, dt):
+        u, c = self.umbrella, self.cfg
+        st = np.asfortranarray(u.stencil, dtype=np.float64)
+        f = np.asfortranarray(flux_umbrella, dtype=np.float64)
+        self.lib.orc_add_source_umbrella(self.ps, c.ivent, c.jvent, u.ibase, u.itop, _d(st), _d(f), dt)
 
     def set_topo(self, dhdx, dhdy, deldx, deldy, s_cc, ztop):
         """useTopo: dhdx_comp, dhdy_comp, DelDxonD_cc, DelDyonD_cc

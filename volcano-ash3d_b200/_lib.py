@@ -42,7 +42,8 @@ EXPORTED = [
     "a3g_adj_advect_vert", "a3g_adj_diffuse_horz", "a3g_adj_diffuse_vert", "a3g_adj_step",
     "a3g_adj_vent_column", "a3g_cloud_load", "a3g_adj_add_cloud_load", "a3g_snapshot_alloc",
     "a3g_snapshot_save", "a3g_snapshot_load", "a3g_set_output_params", "a3g_output_reset",
-    "a3g_output_vars", "a3g_set_topo",
+    "a3g_output_vars", "a3g_set_topo", "a3g_set_umbrella", "a3g_add_umbrella_winds",
+    "a3g_add_source_umbrella",
 ]
 KERNEL_CLASSES = ["advect_x", "advect_y", "advect_z", "diff_x", "diff_y", "diff_z", "cn_table",
                   "cn_solve_x", "cn_solve_y", "cn_solve_z", "cfl", "totals", "winds", "other",
@@ -103,6 +104,9 @@ def load(path: os.PathLike | str | None = None) -> C.CDLL:
         "a3g_set_met_steps": (C.c_int, [P, F, F, F, F, F, F]),
         "a3g_interp_winds": (C.c_int, [P, C.c_double]),
         "a3g_set_topo": (C.c_int, [P, D, D, D, D, D, C.c_double]),
+        "a3g_set_umbrella": (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, D]),
+        "a3g_add_umbrella_winds": (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, D, D]),
+        "a3g_add_source_umbrella": (C.c_int, [P, D, C.c_double]),
         "a3g_upload_concen": (C.c_int, [P, D]),
         "a3g_download_concen": (C.c_int, [P, D]),
         "a3g_upload_outflow": (C.c_int, [P, D, D, D, D, D, D]),

@@ -270,9 +270,11 @@ int a3g_destroy(a3g_ctx *ctx) {
   if (ctx->h_src) cudaFreeHost(ctx->h_src);
   if (ctx->h_tot) cudaFreeHost(ctx->h_tot);
   if (ctx->src_event) cudaEventDestroy(ctx->src_event);
+  if (ctx->umb_event) cudaEventDestroy(ctx->umb_event);
+  if (ctx->h_umb) cudaFreeHost(ctx->h_umb);
   for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
   double *aptrs[] = {ctx->lam0, ctx->lam1, ctx->lam_dep, ctx->stage1, ctx->stage2, ctx->adj_face,
-                     ctx->obs_buf, ctx->ov_buf, ctx->ov_zcc, ctx->topo_buf, ctx->vzh};
+                     ctx->obs_buf, ctx->ov_buf, ctx->ov_zcc, ctx->topo_buf, ctx->vzh, ctx->umb_buf};
   for (double *p : aptrs) if (p) cudaFree(p);
   for (double *p : ctx->snaps) if (p) cudaFree(p);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -592,6 +594,73 @@ int a3g_add_source_column(a3g_ctx *ctx, int32_t ivent, int32_t jvent, const doub
   A3G_CUDA(cudaMemcpyAsync(ctx->src_buf, ctx->h_src, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   A3G_CUDA(cudaEventRecord(ctx->src_event, ctx->stream));
   return launch_source(ctx, ivent, jvent, dt);
+}
+
+// ---- umbrella source (src/Source_Umbrella.f90) ----------------------------
+static size_t umb_flux_len(const a3g_ctx *ctx) { return (size_t)9 * (ctx->grid.nz + 1) * ctx->grid.ns; }
+static size_t umb_wind_len(const a3g_ctx *ctx) { return (size_t)2 * ctx->grid.nx * ctx->grid.ny; }
+
+int a3g_set_umbrella(a3g_ctx *ctx, int32_t ivent, int32_t jvent, int32_t ibase, int32_t itop,
+                     const double *avg_stencil) {
+  CTX_CHECK(ctx);
+  const int nx = ctx->grid.nx, ny = ctx->grid.ny, nz = ctx->grid.nz;
+  if (!avg_stencil) return fail(A3G_ERR_ARG, "null averaging stencil");
+  if (ivent < 2 || ivent > nx - 1 || jvent < 2 || jvent > ny - 1)
+    return fail(A3G_ERR_ARG, "the umbrella's 3x3 patch must lie inside the grid");
+  if (ibase < 1 || itop < ibase || itop > nz) return fail(A3G_ERR_ARG, "need 1 <= ibase <= itop <= nz");
+  const size_t nsten = (size_t)9 * nz;
+  const size_t total = nsten + umb_flux_len(ctx) + umb_wind_len(ctx);
+  if (!ctx->umb_buf) {
+    if (cudaMalloc((void **)&ctx->umb_buf, total * sizeof(double)) != cudaSuccess)
+      return fail(A3G_ERR_NOMEM, "umbrella buffer allocation failed");
+    ctx->bytes += total * sizeof(double);
+    A3G_CUDA(cudaMallocHost((void **)&ctx->h_umb, (umb_flux_len(ctx) + umb_wind_len(ctx)) * sizeof(double)));
+    A3G_CUDA(cudaEventCreateWithFlags(&ctx->umb_event, cudaEventDisableTiming));
+    A3G_CUDA(cudaEventRecord(ctx->umb_event, ctx->stream));
+  }
+  A3G_CUDA(cudaMemcpyAsync(ctx->umb_buf, avg_stencil, nsten * sizeof(double), cudaMemcpyHostToDevice,
+                           ctx->stream));
+  A3G_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->umb_ivent = ivent;
+  ctx->umb_jvent = jvent;
+  ctx->umb_ibase = ibase;
+  ctx->umb_itop = itop;
+  ctx->umb_on = true;
+  return A3G_OK;
+}
+
+int a3g_add_umbrella_winds(a3g_ctx *ctx, int32_t i0, int32_t i1, int32_t j0, int32_t j1, const double *uvx,
+                           const double *uvy) {
+  CTX_CHECK(ctx);
+  if (!ctx->umb_on) return fail(A3G_ERR_STATE, "a3g_set_umbrella has not been called");
+  if (!uvx || !uvy) return fail(A3G_ERR_ARG, "null umbrella winds");
+  if (i0 < 1 || i1 < i0 || i1 > ctx->grid.nx || j0 < 1 || j1 < j0 || j1 > ctx->grid.ny)
+    return fail(A3G_ERR_ARG, "umbrella wind box outside the grid");
+  const size_t m = (size_t)(i1 - i0 + 1) * (j1 - j0 + 1);
+  A3G_CUDA(cudaEventSynchronize(ctx->umb_event));  // previous staging copy done
+  double *h = ctx->h_umb + umb_flux_len(ctx);
+  std::memcpy(h, uvx, m * sizeof(double));
+  std::memcpy(h + m, uvy, m * sizeof(double));
+  double *d = ctx->umb_buf + (size_t)9 * ctx->grid.nz + umb_flux_len(ctx);
+  A3G_CUDA(cudaMemcpyAsync(d, h, 2 * m * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  A3G_CUDA(cudaEventRecord(ctx->umb_event, ctx->stream));
+  int rc = launch_umbrella_winds(ctx, i0, i1 - i0 + 1, j0, j1 - j0 + 1, d);
+  // vh is formed from the winds with the umbrella's added (Calc_Vmod_Topo
+  // runs after MesoInterpolater, src/Ash3d.F90:396-398)
+  if (!rc && ctx->topo_on) rc = launch_vmod_topo(ctx);
+  return rc;
+}
+
+int a3g_add_source_umbrella(a3g_ctx *ctx, const double *flux_umbrella, double dt) {
+  CTX_CHECK(ctx);
+  if (!ctx->umb_on) return fail(A3G_ERR_STATE, "a3g_set_umbrella has not been called");
+  if (!flux_umbrella) return fail(A3G_ERR_ARG, "null umbrella flux");
+  A3G_CUDA(cudaEventSynchronize(ctx->umb_event));
+  std::memcpy(ctx->h_umb, flux_umbrella, umb_flux_len(ctx) * sizeof(double));
+  A3G_CUDA(cudaMemcpyAsync(ctx->umb_buf + (size_t)9 * ctx->grid.nz, ctx->h_umb,
+                           umb_flux_len(ctx) * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  A3G_CUDA(cudaEventRecord(ctx->umb_event, ctx->stream));
+  return launch_source_umbrella(ctx, dt);
 }
 
 int a3g_set_bc(a3g_ctx *ctx, int32_t bc_code) {

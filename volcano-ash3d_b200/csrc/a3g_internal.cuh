@@ -149,6 +149,13 @@ struct a3g_ctx {
   bool topo_on;
   double *topo_buf;
   double *vzh;
+  // umbrella source (a3g_set_umbrella): stencil (9*nz), patch flux
+  // (9*(nz+1)*ns) and winds box (2*nx*ny) on the device, pinned staging
+  bool umb_on;
+  int umb_ivent, umb_jvent, umb_ibase, umb_itop;
+  double *umb_buf;
+  double *h_umb;
+  cudaEvent_t umb_event;
   // optional per-kernel timing (a3g_kernel_timing)
   bool timing;
   std::vector<cudaEvent_t> ev_pool;
@@ -193,6 +200,8 @@ int launch_totals(a3g_ctx *ctx, double *out4, double *mass_aloft);
 int launch_plane_flags(a3g_ctx *ctx);
 int launch_interp_winds(a3g_ctx *ctx, double frac);
 int launch_vmod_topo(a3g_ctx *ctx);
+int launch_umbrella_winds(a3g_ctx *ctx, int i0, int ni, int j0, int nj, const double *uv);
+int launch_source_umbrella(a3g_ctx *ctx, double dt);
 int launch_source(a3g_ctx *ctx, int ivent, int jvent, double dt);
 int launch_zero_state(a3g_ctx *ctx);
 int check_device_error(a3g_ctx *ctx);

@@ -487,6 +487,89 @@ int launch_vmod_topo(a3g_ctx *ctx) {
   return A3G_OK;
 }
 
+// umbrella_winds' radial winds added to the interpolated winds over the
+// cloud's bounding box and the levels ibase..itop
+// (src/MesoInterpolater.f90:237-241): vx += uvx, vy += uvy.
+__global__ void __launch_bounds__(256) k_umbrella_winds(Layout L, int i0, int ni, int j0, int nj, int kb,
+                                                        int nk, const double *__restrict__ uv,
+                                                        double *__restrict__ vx, double *__restrict__ vy) {
+  const long n = (long)ni * nj * nk;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    const int a = (int)(t % ni);
+    const long r = t / ni;
+    const int b = (int)(r % nj);
+    const int k = kb + (int)(r / nj);
+    const long c = L.cell(i0 + a, j0 + b, k);
+    const long m = a + (long)ni * b;
+    vx[c] = vx[c] + uv[m];
+    vy[c] = vy[c] + uv[(long)ni * nj + m];
+  }
+}
+
+int launch_umbrella_winds(a3g_ctx *ctx, int i0, int ni, int j0, int nj, const double *uv) {
+  const int nk = ctx->umb_itop - ctx->umb_ibase + 1;
+  const long n = (long)ni * nj * nk;
+  int blocks = (int)((n + 255) / 256);
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  tbegin(ctx, A3G_K_WINDS);
+  k_umbrella_winds<<<blocks, 256, 0, ctx->stream>>>(ctx->L, i0, ni, j0, nj, ctx->umb_ibase, nk, uv, ctx->vx,
+                                                    ctx->vy);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  return A3G_OK;
+}
+
+// Umbrella source insertion (src/Ash3d.F90:446-458): on ibase..itop the 3x3
+// patch around the vent is first set to its volume-weighted average
+// (AvgCon_Umbrella, src/Source_Umbrella.f90:539-560, i outer, j inner), then
+// every patch cell of levels 1..nz gains dt*SourceNodeFlux_Umbrella.  One
+// thread per (level, grain).
+__global__ void k_source_umbrella(Layout L, int ivent, int jvent, int ibase, int itop,
+                                  const double *__restrict__ sten, const double *__restrict__ flux, double dt,
+                                  double *__restrict__ c) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;  // (k-1) + nz*g
+  if (t >= L.nz * L.ns) return;
+  const int k = t % L.nz + 1, g = t / L.nz;
+  double v[3][3];
+  long a[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      a[i][j] = (long)g * L.PG + L.cell(ivent - 1 + i, jvent - 1 + j, k);
+      v[i][j] = c[a[i][j]];
+    }
+  if (k >= ibase && k <= itop) {
+    double avg = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+      for (int j = 0; j < 3; j++) avg = avg + v[i][j] * sten[i + 3 * j + 9 * (k - 1)];
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+      for (int j = 0; j < 3; j++) v[i][j] = avg;
+  }
+  const long f0 = 9 * ((long)(k - 1) + (long)(L.nz + 1) * g);
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) c[a[i][j]] = v[i][j] + dt * flux[f0 + i + 3 * j];
+}
+
+int launch_source_umbrella(a3g_ctx *ctx, double dt) {
+  const int n = ctx->L.nz * ctx->L.ns;
+  const double *sten = ctx->umb_buf;
+  const double *flux = ctx->umb_buf + 9 * (size_t)ctx->L.nz;
+  tbegin(ctx, A3G_K_OTHER);
+  k_source_umbrella<<<(n + 127) / 128, 128, 0, ctx->stream>>>(ctx->L, ctx->umb_ivent, ctx->umb_jvent,
+                                                              ctx->umb_ibase, ctx->umb_itop, sten, flux, dt,
+                                                              ctx->c0);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  return A3G_OK;
+}
+
 __global__ void k_source(Layout L, int ivent, int jvent, const double *__restrict__ flux, double dt,
                          double *__restrict__ c) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;  // (k-1) + nz*g

@@ -46,12 +46,15 @@ class RunState:
     kappa: np.ndarray = None
     met: syn.MetSource = None
     history: list = dataclasses.field(default_factory=list)
+    umbrella: syn.UmbrellaSetup = None
+    prev_dt: float = None    # time_data::dt when MesoInterpolater runs (the previous step's)
 
 
 def new_state(cfg: syn.Config, geo: dict | None = None) -> RunState:
     geo = geo if geo is not None else syn.geometry(cfg)
+    um = syn.umbrella_setup(cfg, geo["kappa"]) if syn.is_umbrella(cfg) else None
     return RunState(cfg=cfg, norm_col=syn.suzuki_column(cfg), kappa=geo["kappa"],
-                    met=syn.MetSource(cfg))
+                    met=syn.MetSource(cfg), umbrella=um)
 
 
 class Comm:
@@ -142,16 +145,32 @@ def step(model, st: RunState, simtime: float | None = None, totals: bool = True,
         model.set_met_steps(st.met.step(h), st.met.step(h + 1))
         st.hour = h
     model.interp_winds(st.time - h)
-    if comm is None:
-        dt = model.Adjust_DT(st.time, nwt, simtime)
-    else:
+
+    def adjust_dt():
+        if comm is None:
+            return model.Adjust_DT(st.time, nwt, simtime)
         vmax = comm.max(model.cfl_maxima())
-        dt = model.adjust_dt_from_maxima(vmax, n_gs_aloft_total, st.time, nwt, simtime)
+        return model.adjust_dt_from_maxima(vmax, n_gs_aloft_total, st.time, nwt, simtime)
+
+    if st.umbrella is not None and st.time < cfg.duration_h:  # src/MesoInterpolater.f90:233-248
+        if st.prev_dt is None:
+            # before the time loop Adjust_DT ran on the winds without the
+            # umbrella's (e_EndTime is still 0 then), src/Ash3d.F90:301,354
+            st.prev_dt = adjust_dt()
+        w = syn.umbrella_winds(cfg, st.time, st.prev_dt)
+        if w is not None:
+            model.add_umbrella_winds(*w)
+    dt = adjust_dt()
+    st.prev_dt = dt
     frac = syn.pulse_fraction(cfg, st.time, dt)
     if frac > 0.0:
         flux = syn.source_flux(cfg, st.norm_col, st.kappa, frac)
-        model.add_source(flux, dt)
-        st.source_cum = st.source_cum + syn.source_vol_inc(cfg, flux, st.kappa, dt)
+        if st.umbrella is not None:
+            model.add_source_umbrella(syn.umbrella_flux(cfg, flux, st.umbrella), dt)
+            st.source_cum = st.source_cum + syn.umbrella_vol_inc(cfg, flux, st.umbrella, st.kappa, dt)
+        else:
+            model.add_source(flux, dt)
+            st.source_cum = st.source_cum + syn.source_vol_inc(cfg, flux, st.kappa, dt)
     model.Set_BC(1)
     model.AdvectHorz(st.itime)
     model.AdvectVert()

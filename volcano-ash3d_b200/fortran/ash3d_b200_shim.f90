@@ -35,7 +35,8 @@
       private
       public B200_Init, B200_Finalize, B200_Upload, B200_Download, B200_Check, &
              B200_StepPrologue, B200_AddSource, B200_SetWinds, B200_SetMetSteps, &
-             B200_InterpWinds, B200_SetTopo, b200_ctx
+             B200_InterpWinds, B200_SetTopo, B200_SetUmbrella, B200_AddUmbrellaWinds, &
+             B200_AddSourceUmbrella, b200_ctx
 
       type, bind(C) :: a3g_grid_desc
         integer(c_int32_t) :: nx, ny, nz, ns
@@ -99,6 +100,22 @@
           import :: c_int, c_ptr, c_double
           type(c_ptr), value :: ctx
           real(c_double), value :: frac
+        end function
+        integer(c_int) function a3g_set_umbrella(ctx, iv, jv, ib, it, sten) bind(C, name="a3g_set_umbrella")
+          import :: c_int, c_ptr, c_int32_t
+          type(c_ptr), value :: ctx, sten
+          integer(c_int32_t), value :: iv, jv, ib, it
+        end function
+        integer(c_int) function a3g_add_umbrella_winds(ctx, i0, i1, j0, j1, ux, uy) &
+            bind(C, name="a3g_add_umbrella_winds")
+          import :: c_int, c_ptr, c_int32_t
+          type(c_ptr), value :: ctx, ux, uy
+          integer(c_int32_t), value :: i0, i1, j0, j1
+        end function
+        integer(c_int) function a3g_add_source_umbrella(ctx, flux, dt) bind(C, name="a3g_add_source_umbrella")
+          import :: c_int, c_ptr, c_double
+          type(c_ptr), value :: ctx, flux
+          real(c_double), value :: dt
         end function
         integer(c_int) function a3g_set_topo(ctx, dhdx, dhdy, ddx, ddy, scc, ztop) bind(C, name="a3g_set_topo")
           import :: c_int, c_ptr, c_double
@@ -310,6 +327,56 @@
         call B200_Check(a3g_set_topo(b200_ctx, c_loc(dhdx_comp), c_loc(dhdy_comp), c_loc(DelDxonD_cc), &
                         c_loc(DelDyonD_cc), c_loc(s_cc_pd), real(Ztop, c_double)), "a3g_set_topo")
       end subroutine B200_SetTopo
+
+      ! Umbrella source: once, after Allocate_Source_Umbrella (src/Ash3d.F90:242-244).
+      ! AvgStenc_Umbrella is private to module Source_Umbrella, so the stencil is
+      ! formed here from kappa_pd exactly as src/Source_Umbrella.f90:127-138 does.
+      subroutine B200_SetUmbrella
+        use mesh,            only : nzmax, kappa_pd, ivent, jvent
+        use Source_Umbrella, only : ibase, itop
+        real(kind=8), allocatable, target :: sten(:,:,:)
+        real(kind=8) :: tot_vol
+        integer :: i, j, k
+        allocate(sten(3,3,nzmax))
+        do k = 1, nzmax
+          tot_vol = 0.0d0
+          do i = 1, 3
+            do j = 1, 3
+              sten(i,j,k) = kappa_pd(ivent-2+i, jvent-2+j, k)
+              tot_vol = tot_vol + kappa_pd(ivent-2+i, jvent-2+j, k)
+            enddo
+          enddo
+          sten(:,:,k) = sten(:,:,k)/tot_vol
+        enddo
+        call B200_Check(a3g_set_umbrella(b200_ctx, int(ivent, c_int32_t), int(jvent, c_int32_t), &
+                        int(ibase, c_int32_t), int(itop, c_int32_t), c_loc(sten)), "a3g_set_umbrella")
+        deallocate(sten)
+      end subroutine B200_SetUmbrella
+
+      ! In place of the umbrella block of MesoInterpolater (src/MesoInterpolater.f90:
+      ! 233-248): after B200_SetWinds / B200_InterpWinds, while TimeNow < e_EndTime(1),
+      ! call umbrella_winds(first_time) on the host and pass its field (it is the
+      ! same on every level ibase..itop).
+      subroutine B200_AddUmbrellaWinds
+        use mesh,            only : nxmax, nymax
+        use Source_Umbrella, only : uvx_pd, uvy_pd, ibase
+        real(kind=8), allocatable, target :: ux(:,:), uy(:,:)
+        allocate(ux(nxmax,nymax), uy(nxmax,nymax))
+        ux = uvx_pd(1:nxmax,1:nymax,ibase)
+        uy = uvy_pd(1:nxmax,1:nymax,ibase)
+        call B200_Check(a3g_add_umbrella_winds(b200_ctx, 1_c_int32_t, int(nxmax, c_int32_t), 1_c_int32_t, &
+                        int(nymax, c_int32_t), c_loc(ux), c_loc(uy)), "a3g_add_umbrella_winds")
+        deallocate(ux, uy)
+      end subroutine B200_AddUmbrellaWinds
+
+      ! In place of the smoothing and 3x3 insertion of src/Ash3d.F90:446-458, after
+      ! TephraSourceNodes and TephraSourceNodes_Umbrella.
+      subroutine B200_AddSourceUmbrella
+        use Source_Umbrella, only : SourceNodeFlux_Umbrella
+        use time_data,       only : dt
+        call B200_Check(a3g_add_source_umbrella(b200_ctx, c_loc(SourceNodeFlux_Umbrella), real(dt, c_double)), &
+                        "a3g_add_source_umbrella")
+      end subroutine B200_AddSourceUmbrella
 
       end module B200_Transport
 

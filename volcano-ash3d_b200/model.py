@@ -51,6 +51,12 @@ class Ash3dGPU:
         self._dt = 0.0
         if syn.use_topo(cfg):
             self.set_topo(**syn.topo_fields(cfg))
+        self.umbrella = None
+        if syn.is_umbrella(cfg):
+            u = syn.umbrella_setup(cfg, geo["kappa"])
+            st = np.asfortranarray(u.stencil, dtype=np.float64)
+            check(lib.a3g_set_umbrella(self.ctx, cfg.ivent, cfg.jvent, u.ibase, u.itop, dptr(st)))
+            self.umbrella = u
 
     # --- lifetime ----------------------------------------------------------
     def close(self):
@@ -173,6 +179,14 @@ class Ash3dGPU:
     def set_winds(self, vx, vy, vz):
         a = [np.asfortranarray(v, dtype=np.float64) for v in (vx, vy, vz)]
         check(self.lib.a3g_set_winds(self.ctx, *[dptr(v) for v in a]))
+
+    def add_umbrella_winds(self, i0, i1, j0, j1, uvx, uvy):
+        a, b = np.asfortranarray(uvx, dtype=np.float64), np.asfortranarray(uvy, dtype=np.float64)
+        check(self.lib.a3g_add_umbrella_winds(self.ctx, i0, i1, j0, j1, dptr(a), dptr(b)))
+
+    def add_source_umbrella(self, flux_umbrella, dt):
+        f = np.asfortranarray(flux_umbrella, dtype=np.float64)
+        check(self.lib.a3g_add_source_umbrella(self.ctx, dptr(f), dt))
 
     def set_topo(self, dhdx, dhdy, deldx, deldy, s_cc, ztop):
         """useTopo: dhdx_comp, dhdy_comp, DelDxonD_cc, DelDyonD_cc

@@ -32,6 +32,16 @@ RAD_EARTH = 6371.229
 MPS_2_KMPHR = 3.6
 M2PS_2_KM2PHR = 3.6e-3
 KM3_2_M3 = 1.0e9
+DEG2KMLAT = 111.0
+DEG2KMLON = 111.321
+KM_2_M = 1.0e3
+HR_2_S = 3.6e3
+# umbrella-cloud parameters (src/Source_Umbrella.f90:47-52 defaults)
+UMB_VELMOD = 1
+UMB_K_ENTRAIN = 0.1
+UMB_LAMBDA = 0.2
+UMB_N_BV = 0.02
+UMB_SUZUKI_K = 12.0
 
 
 @dataclasses.dataclass
@@ -74,6 +84,7 @@ class Config:
     seed: int = 1
     fast_subgrid: bool = False
     magma_density: float = 2500.0
+    source_type: str = "suzuki"   # 'suzuki', 'umbrella', 'umbrella_air' (lon/lat grids; suzuki_a 12)
     zscaling_id: int = 0     # ZScaling_ID: 0 s = z, 1 shifted by topography, 2 scaled (sigma-altitude)
     topo_km: float = 0.0     # height of a Gaussian hill centred on the vent (0: no topography)
     topo_width_km: float = 0.0   # its standard deviation (km); 0: three cell widths
@@ -155,6 +166,11 @@ def make_config(name: str) -> Config:
                       ivent=37, jvent=5, fall_mps=(0.2, 1.2), bin_mass=(0.5, 0.5), plume_km=5.0,
                       volume_km3=1.0e-3, duration_h=1.0, use_cn=True, sim_hours=1.0,
                       winds="random", seed=18)
+    if name == "tiny_umbrella":  # umbrella source: 0.1 deg cells so that the cloud outgrows the 3x3 patch
+        return Config("tiny_umbrella", 40, 36, 18, 2, latlon=True, de=0.1, dn=0.1, lonLL=120.0,
+                      latLL=38.0, dz=1.0, ivent=20, jvent=18, fall_mps=(0.05, 1.0), bin_mass=(0.5, 0.5),
+                      plume_km=15.0, volume_km3=0.5, duration_h=2.0, suzuki_a=UMB_SUZUKI_K,
+                      use_cn=True, sim_hours=3.0, winds="random", seed=19, source_type="umbrella")
     raise KeyError(name)
 
 
@@ -505,6 +521,152 @@ def source_flux(cfg: Config, norm_col: np.ndarray, kappa: np.ndarray, frac: floa
         for g in range(ns):
             flux[k - 1, g] = cfg.bin_mass[g] * tfr[k - 1] / kap
     return flux
+
+
+# ---------------------------------------------------------------------------
+# umbrella cloud source (src/Source_Umbrella.f90, src/Ash3d.F90:435-463,
+# src/MesoInterpolater.f90:233-248).  Host-side, in the reference's
+# operations (the transcendental functions are the C library's, as
+# gfortran's are); the device adds the winds and inserts the patch.
+# ---------------------------------------------------------------------------
+def is_umbrella(cfg: Config) -> bool:
+    return cfg.source_type in ("umbrella", "umbrella_air")
+
+
+def lon_cc(cfg: Config, i: int) -> float:
+    return cfg.lonLL + cfg.de * float(i) - cfg.de * 0.5   # src/Calc_Mesh.f90:106
+
+
+def lat_cc(cfg: Config, j: int) -> float:
+    return cfg.latLL + cfg.dn * float(j) - cfg.dn * 0.5   # src/Calc_Mesh.f90:109
+
+
+def vent_lonlat(cfg: Config):
+    """(lon_volcano, lat_volcano): the centre of the vent cell."""
+    return lon_cc(cfg, cfg.ivent), lat_cc(cfg, cfg.jvent)
+
+
+@dataclasses.dataclass
+class UmbrellaSetup:
+    ibase: int
+    itop: int
+    stencil: np.ndarray    # AvgStenc_Umbrella(3,3,nz), Fortran order
+    scalefac: np.ndarray   # ScaleFac_Umbrella(1:nz)
+
+
+def umbrella_setup(cfg: Config, kappa: np.ndarray) -> UmbrellaSetup:
+    """Allocate_Source_Umbrella (src/Source_Umbrella.f90:85-153): the
+    volume-weighted 3x3 averaging stencil and the vent-to-patch scale factor
+    per level, and the levels ibase..itop of the umbrella."""
+    if not cfg.latlon:
+        raise ValueError("umbrella_winds is not set up for projected coordinates (Source_Umbrella.f90:252-259)")
+    nz = cfg.nz
+    kap = lambda i, j, k: kappa[i + 1, j + 1, k + 1]
+    sten = np.zeros((3, 3, nz), order="F")
+    fac = np.zeros(nz)
+    for k in range(1, nz + 1):
+        tot = 0.0
+        for i in range(1, 4):
+            ii = cfg.ivent - 2 + i
+            for j in range(1, 4):
+                jj = cfg.jvent - 2 + j
+                sten[i - 1, j - 1, k - 1] = kap(ii, jj, k)
+                tot = tot + kap(ii, jj, k)
+        fac[k - 1] = kap(cfg.ivent, cfg.jvent, k) / tot
+        sten[:, :, k - 1] = sten[:, :, k - 1] / tot
+    dz = zgrid(cfg)[0]
+    zvi = np.zeros(nz + 1)   # z_vec_init(0:nz), the level tops
+    for k in range(1, nz + 1):
+        zvi[k] = zvi[k - 1] + dz[k + 1] if cfg.dz_profile else cfg.dz * k
+    itop = ibase = 0
+    H = cfg.plume_km
+    for k in range(1, nz + 1):
+        if zvi[k] >= H and zvi[k - 1] < H:
+            itop = k
+        if zvi[k] >= 0.75 * H and zvi[k - 1] < 0.75 * H:
+            ibase = k
+    return UmbrellaSetup(ibase, itop, sten, fac)
+
+
+def umbrella_winds(cfg: Config, time: float, dt: float, first_time: bool = False):
+    """umbrella_winds (src/Source_Umbrella.f90:206-394): the radial winds
+    (km/h) of the spreading umbrella cloud, constant over ibase..itop.
+    Returns (i0, i1, j0, j1, uvx, uvy) with uvx, uvy over the bounding box
+    of the cloud (i fastest), or None while the cloud is within the source
+    nodes."""
+    lon_v, lat_v = vent_lonlat(cfg)
+    mfr = mass_flux_rate(cfg) / HR_2_S                 # kg/s
+    if cfg.source_type == "umbrella_air" and cfg.ns == 1:
+        mfr = 20.0 * mfr
+    c_costa = 0.43e3 if abs(lat_v) < 23.0 else 0.87e3
+    qnow = c_costa * math.sqrt(UMB_K_ENTRAIN) * mfr ** (3.0 / 4.0) / UMB_N_BV ** (5.0 / 4.0)
+    if not first_time:
+        etime_s = max(time, dt) * HR_2_S
+    else:
+        etime_s = min(cfg.sim_hours, cfg.duration_h) * HR_2_S
+    cloud_radius = (3.0 * UMB_LAMBDA * UMB_N_BV * qnow / (2.0 * PI)) ** (1.0 / 3.0) * \
+        etime_s ** (2.0 / 3.0) / KM_2_M
+    edge_speed = (2.0 / 3.0) * (3.0 * UMB_LAMBDA * UMB_N_BV * qnow / (2.0 * PI)) ** (1.0 / 3.0) * \
+        etime_s ** (-1.0 / 3.0)
+    de_km = cfg.de * math.cos(lat_v * DEG2RAD) * DEG2KMLON   # src/Calc_Mesh.f90:103-104
+    dn_km = cfg.dn * DEG2KMLAT
+    if cloud_radius <= max((3.0 / 2.0) * de_km, (3.0 / 2.0) * dn_km):
+        return None
+    ew_nodes = int(cloud_radius / de_km) + 1
+    ns_nodes = int(cloud_radius / dn_km) + 1
+    i0, i1 = max(1, cfg.ivent - ew_nodes), min(cfg.nx, cfg.ivent + ew_nodes)
+    j0, j1 = max(1, cfg.jvent - ns_nodes), min(cfg.ny, cfg.jvent + ns_nodes)
+    uvx = np.zeros((i1 - i0 + 1, j1 - j0 + 1), order="F")
+    uvy = np.zeros_like(uvx)
+    for ii in range(i0, i1 + 1):
+        for jj in range(j0, j1 + 1):
+            if ii == cfg.ivent and jj == cfg.jvent:
+                continue
+            avg_lat = (lat_cc(cfg, jj) + lat_v) / 2.0
+            ns_km = (lat_cc(cfg, jj) - lat_v) * DEG2KMLAT
+            ew_km = (lon_cc(cfg, ii) - lon_v) * math.cos(avg_lat * DEG2RAD) * DEG2KMLON
+            # x**2.0_ip is folded to x*x by gfortran
+            radnow = math.sqrt(ns_km * ns_km + ew_km * ew_km)
+            if radnow < cloud_radius:
+                if UMB_VELMOD == 1:
+                    rexp = 3.0
+                    w = edge_speed * MPS_2_KMPHR * (3.0 / 4.0) * (cloud_radius / radnow) * \
+                        (1.0 + (1.0 / 3.0) * (radnow / cloud_radius) ** rexp)
+                else:
+                    w = edge_speed * MPS_2_KMPHR * (cloud_radius / radnow) ** 0.5
+                theta = math.atan2(ns_km, ew_km)
+                uvx[ii - i0, jj - j0] = w * math.cos(theta)
+                uvy[ii - i0, jj - j0] = w * math.sin(theta)
+    return i0, i1, j0, j1, uvx, uvy
+
+
+def umbrella_flux(cfg: Config, flux: np.ndarray, um: UmbrellaSetup) -> np.ndarray:
+    """TephraSourceNodes_Umbrella (src/Source_Umbrella.f90:409-448):
+    SourceNodeFlux_Umbrella(3,3,nz+1,ns) from the vent column's flux."""
+    nz = cfg.nz
+    f = np.zeros((3, 3, nz + 1, cfg.ns), order="F")
+    for k in range(1, nz + 2):
+        if k < um.ibase:
+            f[1, 1, k - 1, :] = flux[k - 1, :]
+        elif k <= um.itop:
+            f[:, :, k - 1, :] = flux[k - 1, :][None, None, :] * um.scalefac[k - 1]
+    return f
+
+
+def umbrella_vol_inc(cfg: Config, flux: np.ndarray, um: UmbrellaSetup, kappa: np.ndarray, dt: float) -> float:
+    """SourceVolInc_Umbrella (src/Source_Umbrella.f90:464-522), km^3 DRE."""
+    tmp = 0.0
+    iv, jv = cfg.ivent, cfg.jvent
+    for g in range(cfg.ns):
+        for k in range(1, um.ibase):
+            tmp = tmp + dt * flux[k - 1, g] * kappa[iv + 1, jv + 1, k + 1] / cfg.magma_density / KM3_2_M3
+    for i in range(3):
+        for j in range(3):
+            for k in range(um.ibase, um.itop + 1):
+                for g in range(cfg.ns):
+                    tmp = tmp + dt * flux[k - 1, g] * um.stencil[i, j, k - 1] * \
+                        kappa[iv + 1, jv + 1, k + 1] / cfg.magma_density / KM3_2_M3
+    return tmp
 
 
 def source_vol_inc(cfg: Config, flux: np.ndarray, kappa: np.ndarray, dt: float) -> float:
