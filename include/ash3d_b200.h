@@ -298,6 +298,14 @@ int a3g_output_reset(a3g_ctx *ctx);
 int a3g_output_vars(a3g_ctx *ctx, double time, double *cloud_load, double *max_height,
                     double *min_height, double *max_conc, int32_t *mask_cloud, double *dep_thick,
                     int32_t *mask_dep, double *cloud_arrival, double *dep_arrival, double *areas);
+/* Calc_vprofile (src/Output_Vars.f90:1308-1360): for each of npts points
+ * (i_pts, j_pts, 1-based) whose column total of the current state is at
+ * least CLOUDCON_THRESH (a3g_set_output_params), pr_ash(1:nz, point) = the
+ * sum over the grains, in mg/m3, and written[point] = 1; the profiles of the
+ * other points are left as they are and written[point] = 0.  The reference
+ * reads the scratch level ts1, equal to the state after a step. */
+int a3g_vprofiles(a3g_ctx *ctx, int32_t npts, const int32_t *i_pts, const int32_t *j_pts, double *pr_ash,
+                  int32_t *written);
 
 /* ---- discrete adjoint (no counterpart in the reference) ----
  * Reverse mode of the transport step for source inversion.  Every sweep is

@@ -963,6 +963,23 @@ void orc_add_source(orc_state *s, int ivent, int jvent, const double *flux, doub
           s->concen[c5(s, ivent, jvent, k, n, 0)] + dt * flux[(size_t)(k - 1) + (size_t)(s->nz + 1) * (n - 1)];
 }
 
+void orc_vprofiles(orc_state *s, int npts, const int32_t *i_pts, const int32_t *j_pts, double thresh,
+                   double *out, int32_t *written) {
+  for (int p = 0; p < npts; p++) {
+    const int i = i_pts[p], j = j_pts[p];
+    double total = 0.0;                       /* sum(concen(i,j,1:nz,1:ns,ts1)), k fastest */
+    for (int n = 1; n <= s->ns; n++)
+      for (int k = 1; k <= s->nz; k++) total = total + s->concen[c5(s, i, j, k, n, 1)];
+    written[p] = !(total < thresh);
+    if (!written[p]) continue;                /* :1350 */
+    for (int k = 1; k <= s->nz; k++) {
+      double sum = 0.0;
+      for (int n = 1; n <= s->ns; n++) sum = sum + s->concen[c5(s, i, j, k, n, 1)];
+      out[(size_t)(k - 1) + (size_t)s->nz * p] = sum * 1.0e6 / 1.0e9;
+    }
+  }
+}
+
 void orc_add_umbrella_winds(orc_state *s, int ibase, int itop, int i0, int i1, int j0, int j1,
                             const double *uvx, const double *uvy) {
   const int ni = i1 - i0 + 1;

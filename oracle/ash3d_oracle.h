@@ -178,6 +178,11 @@ void orc_output_vars(orc_state *s, const double *z_cc, double cloudcon_thresh,
                      double time, double *cloud_load, double *max_height, double *min_height,
                      double *max_conc, int32_t *mask_cloud, double *dep_thick, int32_t *mask_dep,
                      double *cloud_arrival, double *dep_arrival, double *areas);
+/* Calc_vprofile (src/Output_Vars.f90:1308-1360) on concen(:,:,:,:,ts1):
+ * out (nz x npts, k fastest) is filled for the points whose column total is
+ * at least thresh (written = 1), left as it is for the others. */
+void orc_vprofiles(orc_state *s, int npts, const int32_t *i_pts, const int32_t *j_pts, double thresh,
+                   double *out, int32_t *written);
 /* OpenMP thread count for the advection rows (<=0: runtime default). */
 void orc_set_threads(int n);
 int  orc_get_threads(void);

@@ -83,6 +83,8 @@ def load() -> C.CDLL:
             ("orc_add_source", None, [S, C.c_int, C.c_int, D, C.c_double]),
             ("orc_interp_winds", None, [S, F, F, F, F, F, F, C.c_double]),
             ("orc_prune_gs", None, [S, C.c_double]),
+            ("orc_vprofiles", None, [S, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_double, D,
+                                     C.POINTER(C.c_int32)]),
             ("orc_add_umbrella_winds", None, [S, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, D, D]),
             ("orc_add_source_umbrella", None, [S, C.c_int, C.c_int, C.c_int, C.c_int, D, D, C.c_double]),
             ("orc_dgtsv", C.c_int, [C.c_int, D, D, D, D]),
@@ -267,6 +269,17 @@ class OracleModel:
         self.vz[...] = vz
         if self.s.use_topo:
             self.lib.orc_calc_vmod_topo(self.ps)
+
+    def vprofiles(self, points, pr_ash=None, thresh=1.0e-3):
+        """Calc_vprofile: (pr_ash (nz, npts) in mg/m3, written flags)."""
+        ip = np.ascontiguousarray([p[0] for p in points], dtype=np.int32)
+        jp = np.ascontiguousarray([p[1] for p in points], dtype=np.int32)
+        out = np.zeros((self.cfg.nz, len(points)), order="F") if pr_ash is None else pr_ash
+        w = np.zeros(len(points), dtype=np.int32)
+        I = C.POINTER(C.c_int32)
+        self.lib.orc_vprofiles(self.ps, len(points), ip.ctypes.data_as(I), jp.ctypes.data_as(I), thresh,
+                               _d(out), w.ctypes.data_as(I))
+        return out, w
 
     def add_umbrella_winds(self, i0, i1, j0, j1, uvx, uvy):
         u = self.umbrella

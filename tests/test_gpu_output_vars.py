@@ -32,3 +32,25 @@ def test_output_vars_match_oracle(name):
         assert og["cloud_area"] == orf["cloud_area"] and og["dep_area"] == orf["dep_area"]
     assert og["mask_cloud"].any() and og["mask_dep"].any()
     gpu.close()
+
+
+@pytest.mark.parametrize("name", ["tiny_proj", "tiny_latlon", "tiny_umbrella"])
+def test_vprofiles_match_oracle(name):
+    """Calc_vprofile at the vent, near it, and at a corner far from the cloud
+    (below CLOUDCON_THRESH: its profile keeps the previous values)."""
+    from volcano_ash3d_b200 import driver
+    cfg, gpu, ref = pair(name)
+    pts = [(cfg.ivent, cfg.jvent), (cfg.ivent + 1, cfg.jvent - 1), (1, cfg.ny)]
+    sg, sr = driver.new_state(cfg), driver.new_state(cfg)
+    pg = np.full((cfg.nz, len(pts)), -7.0, order="F")
+    pr = pg.copy(order="F")
+    gpu.set_output_params(cloudcon_thresh=1.0e-3)
+    for _ in range(6):
+        driver.step(gpu, sg)
+        driver.step(ref, sr)
+        pg, wg = gpu.vprofiles(pts, pg)
+        pr, wr = ref.vprofiles(pts, pr, thresh=1.0e-3)
+        assert np.array_equal(wg, wr)
+        assert np.array_equal(pg, pr)
+    assert wg[0] == 1 and pg[:, 0].max() > 0.0
+    gpu.close()

@@ -274,7 +274,8 @@ int a3g_destroy(a3g_ctx *ctx) {
   if (ctx->h_umb) cudaFreeHost(ctx->h_umb);
   for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
   double *aptrs[] = {ctx->lam0, ctx->lam1, ctx->lam_dep, ctx->stage1, ctx->stage2, ctx->adj_face,
-                     ctx->obs_buf, ctx->ov_buf, ctx->ov_zcc, ctx->topo_buf, ctx->vzh, ctx->umb_buf};
+                     ctx->obs_buf, ctx->ov_buf, ctx->ov_zcc, ctx->topo_buf, ctx->vzh, ctx->umb_buf,
+                     ctx->vp_buf};
   for (double *p : aptrs) if (p) cudaFree(p);
   for (double *p : ctx->snaps) if (p) cudaFree(p);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1228,6 +1229,42 @@ int a3g_output_reset(a3g_ctx *ctx) {
                            ctx->stream));
   A3G_CUDA(cudaStreamSynchronize(ctx->stream));
   return A3G_OK;
+}
+
+int a3g_vprofiles(a3g_ctx *ctx, int32_t npts, const int32_t *i_pts, const int32_t *j_pts, double *pr_ash,
+                  int32_t *written) {
+  CTX_CHECK(ctx);
+  if (npts < 0 || (npts > 0 && (!i_pts || !j_pts || !pr_ash || !written)))
+    return fail(A3G_ERR_ARG, "bad profile point arrays");
+  if (npts == 0) return A3G_OK;
+  const int nz = ctx->grid.nz;
+  for (int p = 0; p < npts; p++)
+    if (i_pts[p] < 1 || i_pts[p] > ctx->grid.nx || j_pts[p] < 1 || j_pts[p] > ctx->grid.ny)
+      return fail(A3G_ERR_ARG, "profile point outside the grid");
+  // doubles: results (nz*npts), then points and flags as int32 pairs
+  const size_t need = (size_t)nz * npts + (size_t)npts * 2;
+  if (need > ctx->vp_cap) {
+    if (ctx->vp_buf) cudaFree(ctx->vp_buf);
+    ctx->vp_buf = nullptr;
+    if (cudaMalloc((void **)&ctx->vp_buf, need * sizeof(double)) != cudaSuccess)
+      return fail(A3G_ERR_NOMEM, "profile buffer allocation failed");
+    ctx->vp_cap = need;
+  }
+  double *out = ctx->vp_buf;
+  int32_t *pts = reinterpret_cast<int32_t *>(ctx->vp_buf + (size_t)nz * npts);
+  int32_t *flags = pts + 2 * (size_t)npts;
+  std::vector<int32_t> hp(2 * (size_t)npts);
+  for (int p = 0; p < npts; p++) { hp[2 * p] = i_pts[p]; hp[2 * p + 1] = j_pts[p]; }
+  A3G_CUDA(cudaMemcpyAsync(pts, hp.data(), hp.size() * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
+  int rc = launch_vprofiles(ctx, npts, pts, out, flags);
+  if (rc) return rc;
+  std::vector<double> ho((size_t)nz * npts);
+  A3G_CUDA(cudaMemcpyAsync(ho.data(), out, ho.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  A3G_CUDA(cudaMemcpyAsync(written, flags, npts * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  A3G_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (int p = 0; p < npts; p++)  // points below the threshold keep their previous profile
+    if (written[p]) std::memcpy(pr_ash + (size_t)nz * p, ho.data() + (size_t)nz * p, nz * sizeof(double));
+  return check_device_error(ctx);
 }
 
 int a3g_output_vars(a3g_ctx *ctx, double time, double *cloud_load, double *max_height, double *min_height,

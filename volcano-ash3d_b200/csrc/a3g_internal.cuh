@@ -143,6 +143,9 @@ struct a3g_ctx {
   double *ov_zcc;
   double ov_cloudcon, ov_cloudload, ov_depo, ov_density;
   std::vector<double> h_area;  // sigma_nz_pd(1:nx,1:ny,1)
+  // vertical profiles (a3g_vprofiles): points and results, grown on demand
+  double *vp_buf;
+  size_t vp_cap;
   // terrain (a3g_set_topo): dhdx, dhdy, DelDxonD, DelDyonD ((nx+4)*(ny+4) each,
   // ghosted, i fastest) and the per-level factor of vh (nz); vzh = vz + vh on
   // the interior, the vertical wind of the z sweep
@@ -200,6 +203,7 @@ int launch_totals(a3g_ctx *ctx, double *out4, double *mass_aloft);
 int launch_plane_flags(a3g_ctx *ctx);
 int launch_interp_winds(a3g_ctx *ctx, double frac);
 int launch_vmod_topo(a3g_ctx *ctx);
+int launch_vprofiles(a3g_ctx *ctx, int npts, const int32_t *pts, double *out, int32_t *written);
 int launch_umbrella_winds(a3g_ctx *ctx, int i0, int ni, int j0, int nj, const double *uv);
 int launch_source_umbrella(a3g_ctx *ctx, double dt);
 int launch_source(a3g_ctx *ctx, int ivent, int jvent, double dt);

@@ -713,6 +713,36 @@ __global__ void k_output_vars(Layout L, Box box, const double *__restrict__ c, c
   if (mc && carr[o] < 0.0) carr[o] = time;
 }
 
+// Calc_vprofile (src/Output_Vars.f90:1308-1360): per profile point the
+// column total (Fortran SUM order: k fastest, then the grains) against
+// CLOUDCON_THRESH, and per level the sum over the grains in mg/m3.  One block
+// per point; thread 0 forms the total.
+__global__ void k_vprofiles(Layout L, const int32_t *__restrict__ pts, double thresh,
+                            const double *__restrict__ c, double *__restrict__ out,
+                            int32_t *__restrict__ written) {
+  const int p = blockIdx.x;
+  const int i = pts[2 * p], j = pts[2 * p + 1];
+  if (threadIdx.x == 0) {
+    double total = 0.0;
+    for (int g = 0; g < L.ns; g++)
+      for (int k = 1; k <= L.nz; k++) total = total + c[(long)g * L.PG + L.cell(i, j, k)];
+    written[p] = !(total < thresh);
+  }
+  for (int k = 1 + threadIdx.x; k <= L.nz; k += blockDim.x) {
+    double sum = 0.0;
+    for (int g = 0; g < L.ns; g++) sum = sum + c[(long)g * L.PG + L.cell(i, j, k)];
+    out[(long)(k - 1) + (long)L.nz * p] = sum * 1.0e6 / 1.0e9;  // KG_2_MG / KM3_2_M3
+  }
+}
+
+int launch_vprofiles(a3g_ctx *ctx, int npts, const int32_t *pts, double *out, int32_t *written) {
+  tbegin(ctx, A3G_K_OTHER);
+  k_vprofiles<<<npts, 64, 0, ctx->stream>>>(ctx->L, pts, ctx->ov_cloudcon, ctx->c0, out, written);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  return A3G_OK;
+}
+
 int launch_output_vars(a3g_ctx *ctx, double time, double *load, double *maxh, double *minh, double *maxc,
                        int32_t *mcl, double *dthick, int32_t *mdep, double *carr, double *darr) {
   const Layout &L = ctx->L;

@@ -180,6 +180,16 @@ class Ash3dGPU:
         a = [np.asfortranarray(v, dtype=np.float64) for v in (vx, vy, vz)]
         check(self.lib.a3g_set_winds(self.ctx, *[dptr(v) for v in a]))
 
+    def vprofiles(self, points, pr_ash=None):
+        """Calc_vprofile: (pr_ash (nz, npts) in mg/m3, written flags).  Points
+        whose column is below CLOUDCON_THRESH keep pr_ash's previous column."""
+        ip = np.ascontiguousarray([p[0] for p in points], dtype=np.int32)
+        jp = np.ascontiguousarray([p[1] for p in points], dtype=np.int32)
+        out = np.zeros((self.cfg.nz, len(points)), order="F") if pr_ash is None else pr_ash
+        w = np.zeros(len(points), dtype=np.int32)
+        check(self.lib.a3g_vprofiles(self.ctx, len(points), iptr(ip), iptr(jp), dptr(out), iptr(w)))
+        return out, w
+
     def add_umbrella_winds(self, i0, i1, j0, j1, uvx, uvy):
         a, b = np.asfortranarray(uvx, dtype=np.float64), np.asfortranarray(uvy, dtype=np.float64)
         check(self.lib.a3g_add_umbrella_winds(self.ctx, i0, i1, j0, j1, dptr(a), dptr(b)))
