@@ -124,6 +124,32 @@ int a3g_set_met_steps(a3g_ctx *ctx, const float *vx_last, const float *vy_last,
  * v = (dble(last) + dble(next-last)*frac)*3.6 */
 int a3g_interp_winds(a3g_ctx *ctx, double interval_frac);
 
+/* ---- lag-one host loop (no counterpart in the reference) ----
+ * The reference's host reads dt back every step; these let a host queue a
+ * whole step without waiting for the GPU, and read dt and the totals back
+ * later, while the GPU works on the step's sweeps.
+ * a3g_adjust_dt_async: Adjust_DT as a3g_adjust_dt, with dt left on the device
+ * (the sweeps and the scheduled source read it there) and copied to a pinned
+ * ring behind an event.  a3g_wait_dt: dt of the latest a3g_adjust_dt_async,
+ * waiting only for that copy (and reporting a device error word).
+ * a3g_timestep_totals_async / a3g_totals_get: TimeStepTotals with the
+ * partial sums copied behind an event; a ticket stays valid for the next 4
+ * calls. */
+int a3g_adjust_dt_async(a3g_ctx *ctx, double time, double next_write_time, double simtime);
+int a3g_wait_dt(a3g_ctx *ctx, double *dt);
+int a3g_timestep_totals_async(a3g_ctx *ctx, int64_t *ticket);
+int a3g_totals_get(a3g_ctx *ctx, int64_t ticket, double *out4, double *mass_aloft);
+/* The eruption schedule for a3g_add_source_scheduled: per pulse the start and
+ * end times (h) and MassFluxRate (kg/h), NormSourceColumn(npulses, nz+1)
+ * (Fortran layout), Tephra_bin_mass(1:ns) (src/Source.f90:508-592,287-490). */
+int a3g_set_source_pulses(a3g_ctx *ctx, int32_t ivent, int32_t jvent, int32_t npulses, const double *start_h,
+                          const double *end_h, const double *mass_flux_rate, const double *norm_col,
+                          const double *bin_mass);
+/* CheckEruptivePulses + TephraSourceNodes + the vent-column insertion
+ * (src/Source.f90:613-783, src/Ash3d.F90:416-431) on the device, with the dt
+ * of the last Adjust_DT; ieruption/jeruption are kept on the device. */
+int a3g_add_source_scheduled(a3g_ctx *ctx, double time);
+
 /* ---- umbrella source (SourceType 'umbrella' / 'umbrella_air'; lon/lat grids) ---- */
 /* Allocate_Source_Umbrella (src/Source_Umbrella.f90:85-153): the vent, the
  * umbrella levels ibase..itop and AvgStenc_Umbrella (3,3,nz).  Allocates the

@@ -43,7 +43,8 @@ EXPORTED = [
     "a3g_adj_vent_column", "a3g_cloud_load", "a3g_adj_add_cloud_load", "a3g_snapshot_alloc",
     "a3g_snapshot_save", "a3g_snapshot_load", "a3g_set_output_params", "a3g_output_reset",
     "a3g_output_vars", "a3g_set_topo", "a3g_set_umbrella", "a3g_add_umbrella_winds",
-    "a3g_add_source_umbrella", "a3g_vprofiles",
+    "a3g_add_source_umbrella", "a3g_vprofiles", "a3g_adjust_dt_async", "a3g_wait_dt",
+    "a3g_timestep_totals_async", "a3g_totals_get", "a3g_set_source_pulses", "a3g_add_source_scheduled",
 ]
 KERNEL_CLASSES = ["advect_x", "advect_y", "advect_z", "diff_x", "diff_y", "diff_z", "cn_table",
                   "cn_solve_x", "cn_solve_y", "cn_solve_z", "cfl", "totals", "winds", "other",
@@ -108,6 +109,12 @@ def load(path: os.PathLike | str | None = None) -> C.CDLL:
         "a3g_add_umbrella_winds": (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, D, D]),
         "a3g_add_source_umbrella": (C.c_int, [P, D, C.c_double]),
         "a3g_vprofiles": (C.c_int, [P, C.c_int32, I, I, D, I]),
+        "a3g_adjust_dt_async": (C.c_int, [P, C.c_double, C.c_double, C.c_double]),
+        "a3g_wait_dt": (C.c_int, [P, D]),
+        "a3g_timestep_totals_async": (C.c_int, [P, C.POINTER(C.c_int64)]),
+        "a3g_totals_get": (C.c_int, [P, C.c_int64, D, D]),
+        "a3g_set_source_pulses": (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, D, D, D, D, D]),
+        "a3g_add_source_scheduled": (C.c_int, [P, C.c_double]),
         "a3g_upload_concen": (C.c_int, [P, D]),
         "a3g_download_concen": (C.c_int, [P, D]),
         "a3g_upload_outflow": (C.c_int, [P, D, D, D, D, D, D]),

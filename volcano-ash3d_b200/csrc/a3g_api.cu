@@ -235,6 +235,12 @@ int a3g_create(const a3g_grid_desc *grid, const a3g_params *params, int device, 
   if (e == cudaSuccess) e = cudaMallocHost((void **)&ctx->h_src, sizeof(double) * (L.nz + 1) * ns);
   if (e == cudaSuccess) e = cudaMallocHost((void **)&ctx->h_tot, sizeof(double) * 7 * ns);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->src_event, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaMallocHost((void **)&ctx->h_sc_ring, 4 * sizeof(DevScalars));
+  if (e == cudaSuccess) e = cudaMallocHost((void **)&ctx->h_tot_ring, sizeof(double) * 4 * 7 * ns);
+  for (int q = 0; q < 4 && e == cudaSuccess; q++) {
+    e = cudaEventCreateWithFlags(&ctx->sc_ev[q], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->tot_ev[q], cudaEventDisableTiming);
+  }
   if (e == cudaSuccess) {
     std::memset(ctx->h_sc, 0, sizeof(DevScalars));
     std::vector<int32_t> ones(ns, 1);
@@ -271,6 +277,14 @@ int a3g_destroy(a3g_ctx *ctx) {
   if (ctx->h_tot) cudaFreeHost(ctx->h_tot);
   if (ctx->src_event) cudaEventDestroy(ctx->src_event);
   if (ctx->umb_event) cudaEventDestroy(ctx->umb_event);
+  for (int q = 0; q < 4; q++) {
+    if (ctx->sc_ev[q]) cudaEventDestroy(ctx->sc_ev[q]);
+    if (ctx->tot_ev[q]) cudaEventDestroy(ctx->tot_ev[q]);
+  }
+  if (ctx->h_sc_ring) cudaFreeHost(ctx->h_sc_ring);
+  if (ctx->h_tot_ring) cudaFreeHost(ctx->h_tot_ring);
+  if (ctx->src_sched) cudaFree(ctx->src_sched);
+  if (ctx->src_state) cudaFree(ctx->src_state);
   if (ctx->h_umb) cudaFreeHost(ctx->h_umb);
   for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
   double *aptrs[] = {ctx->lam0, ctx->lam1, ctx->lam_dep, ctx->stage1, ctx->stage2, ctx->adj_face,
@@ -831,6 +845,101 @@ int a3g_adjust_dt(a3g_ctx *ctx, double time, double next_write_time, double simt
   ctx->host_dt = ctx->h_sc->dt;
   if (dt_out) *dt_out = ctx->h_sc->dt;
   return A3G_OK;
+}
+
+// ---- lag-one host loop ------------------------------------------------------
+int a3g_adjust_dt_async(a3g_ctx *ctx, double time, double next_write_time, double simtime) {
+  CTX_CHECK(ctx);
+  if (!ctx->have_geometry || !ctx->have_vf || !ctx->have_winds)
+    return fail(A3G_ERR_STATE, "geometry, fall velocities and winds must be set");
+  if (ctx->prm.use_diffusion && !ctx->have_diffusivity) return fail(A3G_ERR_STATE, "diffusivity not set");
+  int rc = launch_cfl(ctx, time, next_write_time, simtime);
+  if (rc) return rc;
+  ctx->dt_stamp++;
+  const int slot = (int)(ctx->dt_seq % 4);
+  A3G_CUDA(cudaMemcpyAsync(ctx->h_sc_ring + slot, ctx->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+  A3G_CUDA(cudaEventRecord(ctx->sc_ev[slot], ctx->stream));
+  ctx->dt_seq++;
+  return A3G_OK;
+}
+
+int a3g_wait_dt(a3g_ctx *ctx, double *dt_out) {
+  CTX_CHECK(ctx);
+  if (!dt_out) return fail(A3G_ERR_ARG, "null dt");
+  if (ctx->dt_seq == 0) return fail(A3G_ERR_STATE, "a3g_adjust_dt_async has not been called");
+  const int slot = (int)((ctx->dt_seq - 1) % 4);
+  A3G_CUDA(cudaEventSynchronize(ctx->sc_ev[slot]));
+  *ctx->h_sc = ctx->h_sc_ring[slot];
+  ctx->host_dt = ctx->h_sc->dt;
+  *dt_out = ctx->h_sc->dt;
+  return check_device_error(ctx);
+}
+
+int a3g_timestep_totals_async(a3g_ctx *ctx, int64_t *ticket) {
+  CTX_CHECK(ctx);
+  if (!ticket) return fail(A3G_ERR_ARG, "null ticket");
+  if (!ctx->have_geometry) return fail(A3G_ERR_STATE, "geometry not set");
+  const int slot = (int)(ctx->tot_seq % 4);
+  // the slot's previous copy must have been consumed: at most 4 in flight
+  A3G_CUDA(cudaEventSynchronize(ctx->tot_ev[slot]));
+  int rc = launch_totals_partials(ctx, ctx->h_tot_ring + (size_t)slot * 7 * ctx->grid.ns);
+  if (rc) return rc;
+  A3G_CUDA(cudaEventRecord(ctx->tot_ev[slot], ctx->stream));
+  *ticket = (int64_t)ctx->tot_seq++;
+  return A3G_OK;
+}
+
+int a3g_totals_get(a3g_ctx *ctx, int64_t ticket, double *out4, double *mass_aloft) {
+  CTX_CHECK(ctx);
+  if (!out4) return fail(A3G_ERR_ARG, "null out4");
+  if (ticket < 0 || (uint64_t)ticket >= ctx->tot_seq || (uint64_t)ticket + 4 < ctx->tot_seq)
+    return fail(A3G_ERR_ARG, "totals ticket unknown or overwritten (at most 4 in flight)");
+  const int slot = (int)(ticket % 4);
+  A3G_CUDA(cudaEventSynchronize(ctx->tot_ev[slot]));
+  totals_volumes(ctx, ctx->h_tot_ring + (size_t)slot * 7 * ctx->grid.ns, out4, mass_aloft);
+  for (int q = 0; q < 4; q++)
+    if (!std::isfinite(out4[q])) return fail(A3G_ERR_NONFINITE, "non-finite mass total (NaN/Inf in the state)");
+  return A3G_OK;
+}
+
+int a3g_set_source_pulses(a3g_ctx *ctx, int32_t ivent, int32_t jvent, int32_t npulses, const double *start_h,
+                          const double *end_h, const double *mass_flux_rate, const double *norm_col,
+                          const double *bin_mass) {
+  CTX_CHECK(ctx);
+  const int nz = ctx->grid.nz, ns = ctx->grid.ns;
+  if (npulses < 1 || npulses > 64) return fail(A3G_ERR_ARG, "need 1 <= npulses <= 64");
+  if (!start_h || !end_h || !mass_flux_rate || !norm_col || !bin_mass) return fail(A3G_ERR_ARG, "null source array");
+  if (ivent < 1 || ivent > ctx->grid.nx || jvent < 1 || jvent > ctx->grid.ny)
+    return fail(A3G_ERR_ARG, "vent outside the grid");
+  const size_t n = (size_t)3 * npulses + (size_t)npulses * (nz + 1) + ns;
+  std::vector<double> h(n);
+  std::memcpy(h.data(), start_h, sizeof(double) * npulses);
+  std::memcpy(h.data() + npulses, end_h, sizeof(double) * npulses);
+  std::memcpy(h.data() + 2 * npulses, mass_flux_rate, sizeof(double) * npulses);
+  std::memcpy(h.data() + 3 * npulses, norm_col, sizeof(double) * npulses * (nz + 1));
+  std::memcpy(h.data() + 3 * npulses + (size_t)npulses * (nz + 1), bin_mass, sizeof(double) * ns);
+  if (ctx->src_sched) cudaFree(ctx->src_sched);
+  ctx->src_sched = nullptr;
+  if (cudaMalloc((void **)&ctx->src_sched, n * sizeof(double)) != cudaSuccess)
+    return fail(A3G_ERR_NOMEM, "source schedule allocation failed");
+  if (!ctx->src_state && cudaMalloc((void **)&ctx->src_state, 2 * sizeof(int32_t)) != cudaSuccess)
+    return fail(A3G_ERR_NOMEM, "source state allocation failed");
+  const int32_t st[2] = {1, 1};  // ieruption = jeruption = 1, src/Source.f90:173-174
+  A3G_CUDA(cudaMemcpyAsync(ctx->src_sched, h.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  A3G_CUDA(cudaMemcpyAsync(ctx->src_state, st, sizeof(st), cudaMemcpyHostToDevice, ctx->stream));
+  A3G_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->src_np = npulses;
+  ctx->src_iv = ivent;
+  ctx->src_jv = jvent;
+  return A3G_OK;
+}
+
+int a3g_add_source_scheduled(a3g_ctx *ctx, double time) {
+  CTX_CHECK(ctx);
+  if (!ctx->src_sched) return fail(A3G_ERR_STATE, "a3g_set_source_pulses has not been called");
+  if (!ctx->have_geometry) return fail(A3G_ERR_STATE, "geometry not set");
+  return launch_source_sched(ctx, time);
 }
 
 int a3g_cfl_maxima(a3g_ctx *ctx, double *vmax3) {

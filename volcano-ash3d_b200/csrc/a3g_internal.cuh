@@ -143,6 +143,20 @@ struct a3g_ctx {
   double *ov_zcc;
   double ov_cloudcon, ov_cloudload, ov_depo, ov_density;
   std::vector<double> h_area;  // sigma_nz_pd(1:nx,1:ny,1)
+  // lag-one host loop: pinned rings of the device scalars (a3g_adjust_dt_async
+  // / a3g_wait_dt) and of the totals partials (a3g_timestep_totals_async /
+  // a3g_totals_get), each slot guarded by an event
+  a3g::DevScalars *h_sc_ring;
+  cudaEvent_t sc_ev[4];
+  uint64_t dt_seq;
+  double *h_tot_ring;
+  cudaEvent_t tot_ev[4];
+  uint64_t tot_seq;
+  // scheduled source (a3g_set_source_pulses): start, end, rate, NormSourceColumn,
+  // bin mass on the device; ieruption/jeruption live on the device
+  double *src_sched;
+  int32_t *src_state;
+  int src_np, src_iv, src_jv;
   // vertical profiles (a3g_vprofiles): points and results, grown on demand
   double *vp_buf;
   size_t vp_cap;
@@ -203,6 +217,9 @@ int launch_totals(a3g_ctx *ctx, double *out4, double *mass_aloft);
 int launch_plane_flags(a3g_ctx *ctx);
 int launch_interp_winds(a3g_ctx *ctx, double frac);
 int launch_vmod_topo(a3g_ctx *ctx);
+int launch_totals_partials(a3g_ctx *ctx, double *h_dst);
+void totals_volumes(a3g_ctx *ctx, const double *h_src, double *out4, double *mass_aloft);
+int launch_source_sched(a3g_ctx *ctx, double time);
 int launch_vprofiles(a3g_ctx *ctx, int npts, const int32_t *pts, double *out, int32_t *written);
 int launch_umbrella_winds(a3g_ctx *ctx, int i0, int ni, int j0, int nj, const double *uv);
 int launch_source_umbrella(a3g_ctx *ctx, double dt);

@@ -339,6 +339,48 @@ __global__ void k_totals_final(int ns, int nblk, const double *__restrict__ part
   out[t] = s.hi + s.lo;  // out[g*NJOBS + job]
 }
 
+// the partial sums of the totals, copied (asynchronously) to h_dst
+// (ns*NJOBS doubles of pinned memory)
+int launch_totals_partials(a3g_ctx *ctx, double *h_dst) {
+  const Layout &L = ctx->L;
+  const int ns = L.ns;
+  dim3 grid(TOT_BLOCKS, NJOBS, ns);
+  tbegin(ctx, A3G_K_TOTALS);
+  k_totals<<<grid, 256, 0, ctx->stream>>>(L, ctx->c0, ctx->kappa, ctx->out_yz1, ctx->out_yz2,
+                                          ctx->out_xz1, ctx->out_xz2, ctx->out_xy1, ctx->out_xy2,
+                                          ctx->red_buf);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  double *fin = ctx->red_buf + (size_t)2 * TOT_BLOCKS * NJOBS * ns;
+  tbegin(ctx, A3G_K_TOTALS);
+  k_totals_final<<<(ns * NJOBS + 127) / 128, 128, 0, ctx->stream>>>(ns, TOT_BLOCKS, ctx->red_buf, fin);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  A3G_CUDA(cudaMemcpyAsync(h_dst, fin, sizeof(double) * ns * NJOBS, cudaMemcpyDeviceToHost, ctx->stream));
+  return A3G_OK;
+}
+
+// volumes in the reference's order, src/Output_Vars.f90:1285-1290,1395-1401,1440-1456
+void totals_volumes(a3g_ctx *ctx, const double *h_src, double *out4, double *mass_aloft) {
+  const int ns = ctx->L.ns;
+  const double rho = ctx->prm.magma_density, km3 = 1.0e9;
+  double aloft = 0.0, depv = 0.0, outv = 0.0;
+  for (int g = 0; g < ns; g++) {
+    const double *r = h_src + (size_t)g * NJOBS;
+    if (mass_aloft) mass_aloft[g] = r[0];
+    aloft = aloft + r[0] / rho / km3;
+  }
+  for (int g = 0; g < ns; g++) depv = depv + h_src[(size_t)g * NJOBS + 1] / rho / km3;
+  for (int g = 0; g < ns; g++) {
+    const double *r = h_src + (size_t)g * NJOBS;
+    outv = outv + (r[2] + r[3] + r[4] + r[5] + r[6]) / rho / km3;
+  }
+  out4[0] = aloft;
+  out4[1] = depv;
+  out4[2] = outv;
+  out4[3] = aloft + depv + outv;
+}
+
 int launch_totals(a3g_ctx *ctx, double *out4, double *mass_aloft) {
   const Layout &L = ctx->L;
   const int ns = L.ns;
@@ -565,6 +607,78 @@ int launch_source_umbrella(a3g_ctx *ctx, double dt) {
   k_source_umbrella<<<(n + 127) / 128, 128, 0, ctx->stream>>>(ctx->L, ctx->umb_ivent, ctx->umb_jvent,
                                                               ctx->umb_ibase, ctx->umb_itop, sten, flux, dt,
                                                               ctx->c0);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  return A3G_OK;
+}
+
+// Scheduled source on the device: CheckEruptivePulses (src/Source.f90:613-685)
+// and TephraSourceNodes (:708-783) with the step's dt from the device
+// scalars, then the vent-column insertion of src/Ash3d.F90:428-431.  One
+// block; thread 0 runs the pulse bookkeeping (ieruption/jeruption persist in
+// state), the block inserts the (level, grain) fluxes.
+constexpr int SRC_MAX_PULSES = 64;
+
+__global__ void k_source_sched(Layout L, int ivent, int jvent, int np, const double *__restrict__ sched,
+                               int32_t *__restrict__ state, const DevScalars *__restrict__ sc, Geo3 kap,
+                               double time, double *__restrict__ c) {
+  __shared__ double frac[SRC_MAX_PULSES + 1];
+  __shared__ int ie_s, je_s, in_s;
+  const double *t0 = sched, *t1 = sched + np, *mfr = sched + 2 * np, *col = sched + 3 * np;
+  const double *bin = col + (size_t)np * (L.nz + 1);
+  const double dt = sc->dt;
+  if (threadIdx.x == 0) {
+    const double tstart = time, tend = time + dt;
+    const int ie = state[0];
+    int je = state[1];
+    int in = 0;
+    for (int i = 1; i <= np; i++) frac[i] = 0.0;
+    for (int i = ie; i <= np; i++) {
+      bool pc = false;
+      if (tstart >= t0[i - 1] && tstart < t1[i - 1]) {
+        pc = true;
+        je = i;
+      } else if (tend > t0[i - 1] && tend <= t1[i - 1]) {
+        je = i;  // :646-651: the loop exits before this pulse's fraction is formed
+        break;
+      } else if (tstart < t0[i - 1] && tend > t1[i - 1]) {
+        pc = true;
+        je = i;
+      }
+      if (pc) {
+        in = 1;
+        frac[i] = (fmin(tend, t1[i - 1]) - fmax(tstart, t0[i - 1])) / dt;
+      }
+    }
+    ie_s = ie;
+    je_s = je;
+    in_s = in;
+  }
+  __syncthreads();
+  const int ie = ie_s, je = je_s;
+  if (in_s) {
+    for (int t = threadIdx.x; t < L.nz * L.ns; t += blockDim.x) {
+      const int k = t % L.nz + 1, g = t / L.nz;
+      double tfr = 0.0;
+      for (int i = ie; i <= je; i++)
+        tfr = tfr + mfr[i - 1] * frac[i] * col[(ie - 1) + (size_t)np * (k - 1)];
+      const double kv = kap.p[(long)(ivent + 1) * kap.si + (long)(jvent + 1) * kap.sj + (long)(k + 1) * kap.sk];
+      const double flux = bin[g] * tfr / kv;
+      const long a = (long)g * L.PG + L.cell(ivent, jvent, k);
+      c[a] = c[a] + dt * flux;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    state[1] = je;
+    if (in_s) state[0] = je;  // :776, only when TephraSourceNodes ran
+  }
+}
+
+int launch_source_sched(a3g_ctx *ctx, double time) {
+  tbegin(ctx, A3G_K_OTHER);
+  k_source_sched<<<1, 256, 0, ctx->stream>>>(ctx->L, ctx->src_iv, ctx->src_jv, ctx->src_np, ctx->src_sched,
+                                             ctx->src_state, ctx->sc, ctx->kappa, time, ctx->c0);
   tend(ctx);
   A3G_LAUNCH_CHECK(ctx);
   return A3G_OK;

@@ -190,6 +190,83 @@ def step(model, st: RunState, simtime: float | None = None, totals: bool = True,
     return rec
 
 
+class Pipeline:
+    """Lag-one host loop for the GPU model: the same operator sequence as
+    step(), but no call waits for the GPU while a step is being queued.  dt
+    stays on the device (Adjust_DT, the scheduled source and the sweeps read
+    it there); the host reads it back after queuing the whole step, waiting
+    only for the early Adjust_DT copy while the GPU runs the step's sweeps,
+    and needs it for the next step's time.  The totals of a step are
+    collected after the next step is queued.  The host mirrors the source
+    arithmetic for SourceCumulativeVol once it knows dt.  Single rank, vent-
+    column sources, FAST_SUBGRID off (the subgrid box needs the state on the
+    host every step)."""
+
+    def __init__(self, model, cfg: syn.Config, geo: dict | None = None):
+        if cfg.fast_subgrid or syn.is_umbrella(cfg):
+            raise ValueError("the pipelined loop needs FAST_SUBGRID off and a vent-column source")
+        self.model, self.cfg = model, cfg
+        self.st = new_state(cfg, geo)
+        self.pulses = syn.eruption_pulses(cfg)
+        model.set_source_pulses(cfg.ivent, cfg.jvent, self.pulses, self.st.norm_col)
+        self.state = [1, 1]      # ieruption, jeruption (host mirror of the device's)
+        self.pending = None      # (record, totals ticket) of the previous step
+
+    def step(self, simtime: float | None = None, totals: bool = True, write_times=None) -> StepRecord:
+        m, cfg, st = self.model, self.cfg, self.st
+        simtime = cfg.sim_hours if simtime is None else simtime
+        nwt = next_write_time(write_times, st.time) if write_times is not None else simtime
+        st.itime += 1
+        m.step_prologue()
+        h = int(math.floor(st.time))
+        if h != st.hour:
+            m.set_met_steps(st.met.step(h), st.met.step(h + 1))
+            st.hour = h
+        m.interp_winds(st.time - h)
+        m.adjust_dt_async(st.time, nwt, simtime)
+        m.add_source_scheduled(st.time)
+        m.Set_BC(1)
+        m.AdvectHorz(st.itime)
+        m.AdvectVert()
+        if cfg.use_diffusion:
+            m.Set_BC(2)
+            m.DiffuseHorz(st.itime)
+            m.DiffuseVert()
+        ticket = m.totals_async() if totals else None
+        self._collect()
+        dt = m.wait_dt()
+        flux = syn.scheduled_source_flux(cfg, self.pulses, st.norm_col, st.kappa, self.state, st.time, dt)
+        if flux is not None:
+            st.source_cum = st.source_cum + syn.source_vol_inc(cfg, flux, st.kappa, dt)
+        st.time = st.time + dt
+        rec = StepRecord(st.itime, st.time, dt, 0.0, 0.0, 0.0, 0.0, st.source_cum)
+        st.history.append(rec)
+        self.pending = (rec, ticket) if totals else None
+        return rec
+
+    def _collect(self):
+        if self.pending is not None:
+            rec, ticket = self.pending
+            vols, _ = self.model.totals_get(ticket)
+            rec.aloft, rec.dep, rec.outflow, rec.tot = (float(v) for v in vols)
+            self.pending = None
+
+    def flush(self) -> RunState:
+        """Fills the last step's totals; returns the run state."""
+        self._collect()
+        return self.st
+
+
+def run_pipelined(model, cfg: syn.Config, max_steps: int | None = None, sim_hours: float | None = None,
+                  geo: dict | None = None, totals: bool = True) -> RunState:
+    """run() through the lag-one loop (Pipeline)."""
+    p = Pipeline(model, cfg, geo)
+    simtime = cfg.sim_hours if sim_hours is None else sim_hours
+    while p.st.time < simtime and (max_steps is None or p.st.itime < max_steps):
+        p.step(simtime, totals)
+    return p.flush()
+
+
 def run(model, cfg: syn.Config, max_steps: int | None = None, sim_hours: float | None = None,
         geo: dict | None = None, totals: bool = True, comm: Comm | None = None,
         n_gs_aloft_total: int | None = None) -> RunState:

@@ -180,6 +180,41 @@ class Ash3dGPU:
         a = [np.asfortranarray(v, dtype=np.float64) for v in (vx, vy, vz)]
         check(self.lib.a3g_set_winds(self.ctx, *[dptr(v) for v in a]))
 
+    # --- lag-one host loop (driver.Pipeline) -----------------------------------
+    def adjust_dt_async(self, time, next_write_time, simtime):
+        check(self.lib.a3g_adjust_dt_async(self.ctx, time, next_write_time, simtime))
+
+    def wait_dt(self) -> float:
+        d = C.c_double()
+        check(self.lib.a3g_wait_dt(self.ctx, C.byref(d)))
+        self._dt = d.value
+        return d.value
+
+    def totals_async(self) -> int:
+        t = C.c_int64()
+        check(self.lib.a3g_timestep_totals_async(self.ctx, C.byref(t)))
+        return t.value
+
+    def totals_get(self, ticket: int):
+        out = np.zeros(4)
+        ma = np.zeros(self.cfg.ns)
+        check(self.lib.a3g_totals_get(self.ctx, ticket, dptr(out), dptr(ma)))
+        return out, ma
+
+    def set_source_pulses(self, ivent, jvent, pulses, norm_col):
+        t0 = np.ascontiguousarray([p[0] for p in pulses], dtype=np.float64)
+        t1 = np.ascontiguousarray([p[1] for p in pulses], dtype=np.float64)
+        mfr = np.ascontiguousarray([p[2] for p in pulses], dtype=np.float64)
+        # NormSourceColumn(npulses, nz+1); one column given for one pulse
+        c = np.asarray(norm_col, dtype=np.float64)
+        col = np.asfortranarray(c.reshape(len(pulses), self.cfg.nz + 1))
+        bm = np.ascontiguousarray(self.cfg.bin_mass, dtype=np.float64)
+        check(self.lib.a3g_set_source_pulses(self.ctx, ivent, jvent, len(pulses), dptr(t0), dptr(t1), dptr(mfr),
+                                             dptr(col), dptr(bm)))
+
+    def add_source_scheduled(self, time):
+        check(self.lib.a3g_add_source_scheduled(self.ctx, time))
+
     def vprofiles(self, points, pr_ash=None):
         """Calc_vprofile: (pr_ash (nz, npts) in mg/m3, written flags).  Points
         whose column is below CLOUDCON_THRESH keep pr_ash's previous column."""

@@ -508,6 +508,52 @@ def pulse_fraction(cfg: Config, time: float, dt: float) -> float:
     return (min(tend, t1) - max(tstart, t0)) / dt
 
 
+def eruption_pulses(cfg: Config):
+    """(start_h, end_h, MassFluxRate kg/h) per eruptive pulse: one pulse from t = 0."""
+    return [(0.0, 0.0 + cfg.duration_h, mass_flux_rate(cfg))]
+
+
+def scheduled_source_flux(cfg: Config, pulses, norm_col: np.ndarray, kappa: np.ndarray, state: list,
+                          time: float, dt: float):
+    """CheckEruptivePulses + TephraSourceNodes (src/Source.f90:613-783) for
+    the pulses, with state = [ieruption, jeruption] (1-based, updated): the
+    SourceNodeFlux (nz+1) x ns of this step, or None when no pulse is active.
+    The same operations as the device's a3g_add_source_scheduled."""
+    tstart, tend = time, time + dt
+    ie, je = state
+    frac = [0.0] * (len(pulses) + 1)
+    active = False
+    for i in range(ie, len(pulses) + 1):
+        t0, t1, _ = pulses[i - 1]
+        pc = False
+        if tstart >= t0 and tstart < t1:
+            pc, je = True, i
+        elif tend > t0 and tend <= t1:
+            je = i   # the reference exits here before forming this pulse's fraction
+            break
+        elif tstart < t0 and tend > t1:
+            pc, je = True, i
+        if pc:
+            active = True
+            frac[i] = (min(tend, t1) - max(tstart, t0)) / dt
+    state[1] = je
+    if not active:
+        return None
+    nz, ns = cfg.nz, cfg.ns
+    cols = np.asarray(norm_col, dtype=np.float64).reshape(len(pulses), nz + 1)
+    tfr = np.zeros(nz)
+    for i in range(ie, je + 1):
+        tfr = tfr + pulses[i - 1][2] * frac[i] * cols[ie - 1, :nz]
+    flux = np.zeros((nz + 1, ns), order="F")
+    iv, jv = cfg.ivent, cfg.jvent
+    for k in range(1, nz + 1):
+        kap = kappa[iv + 1, jv + 1, k + 1]
+        for g in range(ns):
+            flux[k - 1, g] = cfg.bin_mass[g] * tfr[k - 1] / kap
+    state[0] = je
+    return flux
+
+
 def source_flux(cfg: Config, norm_col: np.ndarray, kappa: np.ndarray, frac: float) -> np.ndarray:
     """SourceNodeFlux(1:nz+1, 1:ns) (k fastest) of TephraSourceNodes, kg/km^3/h."""
     nz, ns = cfg.nz, cfg.ns
