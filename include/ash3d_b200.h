@@ -120,6 +120,17 @@ int a3g_set_winds(a3g_ctx *ctx, const double *vx_pd, const double *vy_pd, const 
 int a3g_set_met_steps(a3g_ctx *ctx, const float *vx_last, const float *vy_last,
                       const float *vz_last, const float *vx_next, const float *vy_next,
                       const float *vz_next);
+/* Read_NextMesoStep's toggle (src/MesoInterpolater.f90:168-199) without a
+ * stall: a3g_prefetch_met_step copies the met step after next (FP32 nx*ny*nz,
+ * m/s) into a spare slot on a copy stream (asynchronous for pinned host
+ * memory); at the met-step boundary a3g_advance_met_step makes the old next
+ * step the last one and the prefetched step the next one (the compute stream
+ * waits for the copy).  a3g_met_prefetch_fence makes the compute stream wait
+ * for a prefetch in flight.  Pinned host arrays given to a prefetch must stay
+ * unchanged until then. */
+int a3g_prefetch_met_step(a3g_ctx *ctx, const float *vx, const float *vy, const float *vz);
+int a3g_advance_met_step(a3g_ctx *ctx);
+int a3g_met_prefetch_fence(a3g_ctx *ctx);
 /* Device form of src/MesoInterpolater.f90:207-223:
  * v = (dble(last) + dble(next-last)*frac)*3.6 */
 int a3g_interp_winds(a3g_ctx *ctx, double interval_frac);

@@ -257,6 +257,13 @@ class OracleModel:
     def set_met_steps(self, last, nxt):
         self._met = [np.asfortranarray(a, dtype=np.float32) for a in (*last, *nxt)]
 
+    def prefetch_met_step(self, step):
+        self._met_ahead = [np.asfortranarray(a, dtype=np.float32) for a in step]
+
+    def advance_met_step(self):
+        self._met = [*self._met[3:], *self._met_ahead]
+        self._met_ahead = None
+
     def interp_winds(self, frac):
         m = self._met
         self.lib.orc_interp_winds(self.ps, _f(m[0]), _f(m[3]), _f(m[1]), _f(m[4]), _f(m[2]), _f(m[5]), frac)

@@ -235,6 +235,9 @@ int a3g_create(const a3g_grid_desc *grid, const a3g_params *params, int device, 
   if (e == cudaSuccess) e = cudaMallocHost((void **)&ctx->h_src, sizeof(double) * (L.nz + 1) * ns);
   if (e == cudaSuccess) e = cudaMallocHost((void **)&ctx->h_tot, sizeof(double) * 7 * ns);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->src_event, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->met_copy_ev, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->met_free_ev, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMallocHost((void **)&ctx->h_sc_ring, 4 * sizeof(DevScalars));
   if (e == cudaSuccess) e = cudaMallocHost((void **)&ctx->h_tot_ring, sizeof(double) * 4 * 7 * ns);
   for (int q = 0; q < 4 && e == cudaSuccess; q++) {
@@ -262,6 +265,7 @@ int a3g_destroy(a3g_ctx *ctx) {
   if (!ctx) return A3G_OK;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
   double *dptrs[] = {ctx->c0, ctx->c1, ctx->vx, ctx->vy, ctx->vz, ctx->out_yz1, ctx->out_yz2,
                      ctx->out_xz1, ctx->out_xz2, ctx->out_xy1, ctx->out_xy2, ctx->red_buf,
                      ctx->src_buf, ctx->cn_buf, ctx->dz_vec, ctx->dtv_buf};
@@ -292,6 +296,9 @@ int a3g_destroy(a3g_ctx *ctx) {
                      ctx->vp_buf};
   for (double *p : aptrs) if (p) cudaFree(p);
   for (double *p : ctx->snaps) if (p) cudaFree(p);
+  if (ctx->met_copy_ev) cudaEventDestroy(ctx->met_copy_ev);
+  if (ctx->met_free_ev) cudaEventDestroy(ctx->met_free_ev);
+  if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return A3G_OK;
@@ -441,21 +448,72 @@ int a3g_set_winds(a3g_ctx *ctx, const double *vx_pd, const double *vy_pd, const 
   return A3G_OK;
 }
 
+static int ensure_met(a3g_ctx *ctx) {
+  if (ctx->met) return A3G_OK;
+  const long n = (long)ctx->grid.nx * ctx->grid.ny * ctx->grid.nz;
+  if (cudaMalloc((void **)&ctx->met, sizeof(float) * 9 * n) != cudaSuccess)
+    return fail(A3G_ERR_NOMEM, "met-step allocation failed");
+  ctx->bytes += sizeof(float) * 9 * n;
+  ctx->met_n = n;
+  ctx->met_last = 0;
+  ctx->met_next = 1;
+  ctx->met_spare = 2;
+  ctx->met_prefetched = false;
+  return A3G_OK;
+}
+
 int a3g_set_met_steps(a3g_ctx *ctx, const float *vx_last, const float *vy_last, const float *vz_last,
                       const float *vx_next, const float *vy_next, const float *vz_next) {
   CTX_CHECK(ctx);
   const float *src[6] = {vx_last, vy_last, vz_last, vx_next, vy_next, vz_next};
   for (int c = 0; c < 6; c++)
     if (!src[c]) return fail(A3G_ERR_ARG, "null met-step array");
-  const long n = (long)ctx->grid.nx * ctx->grid.ny * ctx->grid.nz;
-  if (!ctx->met) {
-    A3G_CUDA(cudaMalloc((void **)&ctx->met, sizeof(float) * 6 * n));
-    ctx->bytes += sizeof(float) * 6 * n;
-    ctx->met_n = n;
+  int rc = ensure_met(ctx);
+  if (rc) return rc;
+  const long n = ctx->met_n;
+  for (int c = 0; c < 6; c++) {
+    float *dst = ctx->met + (size_t)3 * n * (c < 3 ? ctx->met_last : ctx->met_next) + (size_t)(c % 3) * n;
+    A3G_CUDA(cudaMemcpyAsync(dst, src[c], sizeof(float) * n, cudaMemcpyHostToDevice, ctx->stream));
   }
-  for (int c = 0; c < 6; c++)
-    A3G_CUDA(cudaMemcpyAsync(ctx->met + c * n, src[c], sizeof(float) * n, cudaMemcpyHostToDevice,
-                             ctx->stream));
+  return A3G_OK;
+}
+
+// Read_NextMesoStep's toggle (src/MesoInterpolater.f90:168-199): the next met
+// step is copied into the spare slot on the copy stream, ahead of need;
+// a3g_advance_met_step makes it the next step and the old next the last one.
+int a3g_prefetch_met_step(a3g_ctx *ctx, const float *vx, const float *vy, const float *vz) {
+  CTX_CHECK(ctx);
+  if (!vx || !vy || !vz) return fail(A3G_ERR_ARG, "null met-step array");
+  int rc = ensure_met(ctx);
+  if (rc) return rc;
+  const long n = ctx->met_n;
+  // the spare slot was last read by work queued before the latest advance
+  A3G_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ctx->met_free_ev, 0));
+  const float *src[3] = {vx, vy, vz};
+  for (int c = 0; c < 3; c++)
+    A3G_CUDA(cudaMemcpyAsync(ctx->met + (size_t)3 * n * ctx->met_spare + (size_t)c * n, src[c],
+                             sizeof(float) * n, cudaMemcpyHostToDevice, ctx->copy_stream));
+  A3G_CUDA(cudaEventRecord(ctx->met_copy_ev, ctx->copy_stream));
+  ctx->met_prefetched = true;
+  return A3G_OK;
+}
+
+int a3g_advance_met_step(a3g_ctx *ctx) {
+  CTX_CHECK(ctx);
+  if (!ctx->met || !ctx->met_prefetched) return fail(A3G_ERR_STATE, "no met step prefetched");
+  A3G_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->met_copy_ev, 0));
+  A3G_CUDA(cudaEventRecord(ctx->met_free_ev, ctx->stream));  // the old last slot's readers end here
+  const int old_last = ctx->met_last;
+  ctx->met_last = ctx->met_next;
+  ctx->met_next = ctx->met_spare;
+  ctx->met_spare = old_last;
+  ctx->met_prefetched = false;
+  return A3G_OK;
+}
+
+int a3g_met_prefetch_fence(a3g_ctx *ctx) {
+  CTX_CHECK(ctx);
+  A3G_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->met_copy_ev, 0));
   return A3G_OK;
 }
 

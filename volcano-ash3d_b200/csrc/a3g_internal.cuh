@@ -89,8 +89,13 @@ struct a3g_ctx {
 
   double *c0, *c1;          // concentration levels (state = c0)
   double *vx, *vy, *vz;     // winds (km/h)
-  float *met;               // 6 FP32 met arrays: vx_last,vy_last,vz_last,vx_next,vy_next,vz_next
+  float *met;               // 3 met slots of 3 FP32 arrays (vx, vy, vz): last, next, spare
   long met_n;               // nx*ny*nz
+  int met_last, met_next, met_spare;  // slot indices
+  bool met_prefetched;      // the spare slot holds a prefetched step
+  cudaStream_t copy_stream; // met-step prefetches
+  cudaEvent_t met_copy_ev;  // end of the last prefetch copy
+  cudaEvent_t met_free_ev;  // the spare slot's last reader is done
   double *geo_ptrs[8];      // compressed kappa,snx,sny,snz,kx,ky,kz,vf
   a3g::Geo3 kappa, snx, sny, snz, kx, ky, kz;
   a3g::Geo3 dtv;            // dt/kappa of the current step (kappa's layout)

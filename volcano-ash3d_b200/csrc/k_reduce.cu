@@ -463,9 +463,9 @@ int launch_plane_flags(a3g_ctx *ctx) {
 // ---------------------------------------------------------------------------
 // winds and source
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_interp_winds(Layout L, const float *__restrict__ met,
-                                                      long n, double frac, double *__restrict__ vx,
-                                                      double *__restrict__ vy,
+__global__ void __launch_bounds__(256) k_interp_winds(Layout L, const float *__restrict__ last,
+                                                      const float *__restrict__ next, long n, double frac,
+                                                      double *__restrict__ vx, double *__restrict__ vy,
                                                       double *__restrict__ vz) {
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
     const int i = (int)(t % L.nx) + 1;
@@ -473,12 +473,12 @@ __global__ void __launch_bounds__(256) k_interp_winds(Layout L, const float *__r
     const int j = (int)(r % L.ny) + 1;
     const int k = (int)(r / L.ny) + 1;
     const long c = L.cell(i, j, k);
-    const float dx = met[3 * n + t] - met[t];
-    const float dy = met[4 * n + t] - met[n + t];
-    const float dz = met[5 * n + t] - met[2 * n + t];
-    vx[c] = ((double)met[t] + (double)dx * frac) * 3.6;
-    vy[c] = ((double)met[n + t] + (double)dy * frac) * 3.6;
-    vz[c] = ((double)met[2 * n + t] + (double)dz * frac) * 3.6;
+    const float dx = next[t] - last[t];
+    const float dy = next[n + t] - last[n + t];
+    const float dz = next[2 * n + t] - last[2 * n + t];
+    vx[c] = ((double)last[t] + (double)dx * frac) * 3.6;
+    vy[c] = ((double)last[n + t] + (double)dy * frac) * 3.6;
+    vz[c] = ((double)last[2 * n + t] + (double)dz * frac) * 3.6;
   }
 }
 
@@ -487,7 +487,9 @@ int launch_interp_winds(a3g_ctx *ctx, double frac) {
   int blocks = (int)((n + 255) / 256);
   if (blocks > 148 * 16) blocks = 148 * 16;
   tbegin(ctx, A3G_K_WINDS);
-  k_interp_winds<<<blocks, 256, 0, ctx->stream>>>(ctx->L, ctx->met, n, frac, ctx->vx, ctx->vy, ctx->vz);
+  k_interp_winds<<<blocks, 256, 0, ctx->stream>>>(ctx->L, ctx->met + (size_t)3 * n * ctx->met_last,
+                                                  ctx->met + (size_t)3 * n * ctx->met_next, n, frac, ctx->vx,
+                                                  ctx->vy, ctx->vz);
   tend(ctx);
   A3G_LAUNCH_CHECK(ctx);
   return A3G_OK;

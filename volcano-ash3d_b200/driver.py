@@ -48,6 +48,7 @@ class RunState:
     history: list = dataclasses.field(default_factory=list)
     umbrella: syn.UmbrellaSetup = None
     prev_dt: float = None    # time_data::dt when MesoInterpolater runs (the previous step's)
+    met_ahead: int = -1      # the hour whose met step was prefetched into the spare slot
 
 
 def new_state(cfg: syn.Config, geo: dict | None = None) -> RunState:
@@ -129,6 +130,22 @@ def next_write_time(write_times, time: float) -> float:
     return 1.0 / 1.0e-6
 
 
+def update_met(model, st: RunState, h: int):
+    """The met pair for hour h.  Crossing into the next hour advances onto the
+    step prefetched an hour earlier (Read_NextMesoStep's toggle,
+    src/MesoInterpolater.f90:168-199); any other jump uploads the pair.  The
+    step after next is then prefetched on the copy stream."""
+    if h == st.hour:
+        return
+    if st.hour >= 0 and h == st.hour + 1 and st.met_ahead == h + 1:
+        model.advance_met_step()
+    else:
+        model.set_met_steps(st.met.step(h), st.met.step(h + 1))
+    st.hour = h
+    model.prefetch_met_step(st.met.step(h + 2))
+    st.met_ahead = h + 2
+
+
 def step(model, st: RunState, simtime: float | None = None, totals: bool = True,
          comm: Comm | None = None, n_gs_aloft_total: int | None = None,
          write_times=None) -> StepRecord:
@@ -141,9 +158,7 @@ def step(model, st: RunState, simtime: float | None = None, totals: bool = True,
     st.itime += 1
     model.step_prologue()
     h = int(math.floor(st.time))
-    if h != st.hour:
-        model.set_met_steps(st.met.step(h), st.met.step(h + 1))
-        st.hour = h
+    update_met(model, st, h)
     model.interp_winds(st.time - h)
 
     def adjust_dt():
@@ -219,9 +234,7 @@ class Pipeline:
         st.itime += 1
         m.step_prologue()
         h = int(math.floor(st.time))
-        if h != st.hour:
-            m.set_met_steps(st.met.step(h), st.met.step(h + 1))
-            st.hour = h
+        update_met(m, st, h)
         m.interp_winds(st.time - h)
         m.adjust_dt_async(st.time, nwt, simtime)
         m.add_source_scheduled(st.time)

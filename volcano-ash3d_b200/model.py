@@ -173,6 +173,18 @@ class Ash3dGPU:
         check(self.lib.a3g_set_met_steps(self.ctx, *[fptr(a) for a in arrs]))
         self._met_keep = arrs  # the copies are asynchronous
 
+    def prefetch_met_step(self, step):
+        """Copies one met step (vx, vy, vz) into the spare slot on the copy stream."""
+        arrs = [np.asfortranarray(a, dtype=np.float32) for a in step]
+        check(self.lib.a3g_prefetch_met_step(self.ctx, *[fptr(a) for a in arrs]))
+        self._prefetch_keep = arrs  # the copy may still be reading them
+
+    def advance_met_step(self):
+        check(self.lib.a3g_advance_met_step(self.ctx))
+
+    def met_prefetch_fence(self):
+        check(self.lib.a3g_met_prefetch_fence(self.ctx))
+
     def interp_winds(self, frac: float):
         check(self.lib.a3g_interp_winds(self.ctx, frac))
 
