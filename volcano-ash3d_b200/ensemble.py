@@ -3,8 +3,9 @@
 No counterpart in the reference (one Ash3d process runs one eruption).  An
 ensemble (different grids, grain sets, plumes and durations) runs its members
 concurrently: every member owns a context, and so its own CUDA stream, and a
-host thread drives the member's time loop (the reference loop of
-driver.run).  The C-ABI releases the interpreter lock on every call, so one
+host thread drives the member's time loop (driver.run_pipelined, which
+queues each step without waiting for the GPU; driver.run where a member needs
+the host every step).  The C-ABI releases the interpreter lock on every call, so one
 member's host work and small launches overlap the other members' kernels.
 Each member's results are the bits its run gives alone, because members
 share no device data.
@@ -106,7 +107,11 @@ class Ensemble:
             m.set_variant(d, v)
         m.set_interior(np.zeros((cfg.nx, cfg.ny, cfg.nz, cfg.ns), order="F"))
         t0 = time.perf_counter()
-        st = driver.run(m, cfg, sim_hours=hours)
+        # the lag-one loop when the member allows it (same bits as driver.run)
+        if cfg.fast_subgrid or syn.is_umbrella(cfg):
+            st = driver.run(m, cfg, sim_hours=hours)
+        else:
+            st = driver.run_pipelined(m, cfg, sim_hours=hours)
         m.sync()
         el = time.perf_counter() - t0
         res = MemberResult(cfg.name, st.itime, float(cfg.cell_grains) * st.itime, el,
