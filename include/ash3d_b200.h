@@ -161,6 +161,10 @@ int a3g_set_source_pulses(a3g_ctx *ctx, int32_t ivent, int32_t jvent, int32_t np
  * of the last Adjust_DT; ieruption/jeruption are kept on the device. */
 int a3g_add_source_scheduled(a3g_ctx *ctx, double time);
 
+/* The vent-column insertion of a3g_add_source_column with the dt that the
+ * last Adjust_DT left on the device (for a host that reads dt late). */
+int a3g_add_source_column_devdt(a3g_ctx *ctx, int32_t ivent, int32_t jvent, const double *flux);
+
 /* ---- umbrella source (SourceType 'umbrella' / 'umbrella_air'; lon/lat grids) ---- */
 /* Allocate_Source_Umbrella (src/Source_Umbrella.f90:85-153): the vent, the
  * umbrella levels ibase..itop and AvgStenc_Umbrella (3,3,nz).  Allocates the
@@ -381,6 +385,14 @@ int a3g_adj_step(a3g_ctx *ctx, int32_t itime);
 /* lam at the vent column, (nz+1) x ns with k fastest (the layout of the
  * source flux): the adjoint of the source insertion before dt/kappa. */
 int a3g_adj_vent_column(a3g_ctx *ctx, int32_t ivent, int32_t jvent, double *out);
+/* The source gradient gathered on the device: a3g_adj_grad_reset zeroes
+ * nbins x ns x nz bins; each reverse step a3g_adj_vent_accumulate adds
+ * dt*lam(ivent,jvent,k,g)/kappa(ivent,jvent,k) (k = 1..nz) to bin `bin`, in
+ * the order of the calls; a3g_adj_grad_get copies the bins back (bin-major,
+ * then grain, k fastest). */
+int a3g_adj_grad_reset(a3g_ctx *ctx, int32_t nbins);
+int a3g_adj_vent_accumulate(a3g_ctx *ctx, int32_t ivent, int32_t jvent, int32_t bin, double dt);
+int a3g_adj_grad_get(a3g_ctx *ctx, double *out);
 /* Unmasked column load (CloudLoad of src/Output_Vars.f90:1061-1069,
  * tonnes/km^2) of the current state, (nx,ny); and lam += H^T w for a
  * weight w (nx,ny), H that column load. */

@@ -257,6 +257,29 @@ class OracleModel:
     def set_met_steps(self, last, nxt):
         self._met = [np.asfortranarray(a, dtype=np.float32) for a in (*last, *nxt)]
 
+    # --- the device loop's entry points, restated on the host --------------
+    def adjust_dt_async(self, time, next_write_time, simtime):
+        self._dt_pending = self.Adjust_DT(time, next_write_time, simtime)
+
+    def wait_dt(self):
+        return self._dt_pending
+
+    def add_source_devdt(self, flux):
+        self.add_source(flux, self.s.dt)
+
+    def adj_grad_reset(self, nbins):
+        c = self.cfg
+        self._grad = np.zeros((c.nz, nbins, c.ns))
+        kap = self.kappa
+        self._kap_col = np.array([kap[c.ivent + 1, c.jvent + 1, k + 1] for k in range(1, c.nz + 1)])
+
+    def adj_vent_accumulate(self, bin_, dt):
+        col = self.adj_vent_column()
+        self._grad[:, bin_, :] += dt * col[:self.cfg.nz, :] / self._kap_col[:, None]
+
+    def adj_grad_get(self):
+        return self._grad.copy()
+
     def prefetch_met_step(self, step):
         self._met_ahead = [np.asfortranarray(a, dtype=np.float32) for a in step]
 

@@ -46,6 +46,7 @@ EXPORTED = [
     "a3g_add_source_umbrella", "a3g_vprofiles", "a3g_adjust_dt_async", "a3g_wait_dt",
     "a3g_timestep_totals_async", "a3g_totals_get", "a3g_set_source_pulses", "a3g_add_source_scheduled",
     "a3g_prefetch_met_step", "a3g_advance_met_step", "a3g_met_prefetch_fence",
+    "a3g_add_source_column_devdt", "a3g_adj_grad_reset", "a3g_adj_vent_accumulate", "a3g_adj_grad_get",
 ]
 KERNEL_CLASSES = ["advect_x", "advect_y", "advect_z", "diff_x", "diff_y", "diff_z", "cn_table",
                   "cn_solve_x", "cn_solve_y", "cn_solve_z", "cfl", "totals", "winds", "other",
@@ -119,6 +120,10 @@ def load(path: os.PathLike | str | None = None) -> C.CDLL:
         "a3g_prefetch_met_step": (C.c_int, [P, F, F, F]),
         "a3g_advance_met_step": (C.c_int, [P]),
         "a3g_met_prefetch_fence": (C.c_int, [P]),
+        "a3g_add_source_column_devdt": (C.c_int, [P, C.c_int32, C.c_int32, D]),
+        "a3g_adj_grad_reset": (C.c_int, [P, C.c_int32]),
+        "a3g_adj_vent_accumulate": (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, C.c_double]),
+        "a3g_adj_grad_get": (C.c_int, [P, D]),
         "a3g_upload_concen": (C.c_int, [P, D]),
         "a3g_download_concen": (C.c_int, [P, D]),
         "a3g_upload_outflow": (C.c_int, [P, D, D, D, D, D, D]),

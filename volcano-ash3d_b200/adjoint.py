@@ -116,15 +116,18 @@ class SourceInversion:
             model.step_prologue()
             self._winds(model, time)
             next_obs = math.floor(time + 1e-12) + 1.0
-            dt = model.Adjust_DT(time, next_obs, simtime)
+            # dt stays on the device while the step is queued; the host reads
+            # it once the step's sweeps are on the stream (lag-one loop)
+            model.adjust_dt_async(time, next_obs, simtime)
             hour = int(math.floor(time + 1e-12))
             if K:
                 n = itime - 1
                 if n % K == 0:
                     model.snapshot_alloc(K + n // K + 1)
                     model.snapshot_save(K + n // K)
-            model.add_source(self.flux(p, hour), dt)
+            model.add_source_devdt(self.flux(p, hour))
             self._step_ops(model, itime)
+            dt = model.wait_dt()
             time = time + dt
             ob = -1
             if abs(time - round(time)) < 1e-9 and round(time) >= 1:
@@ -147,7 +150,7 @@ class SourceInversion:
         nseg = (N + K - 1) // K
         model.adj_enable()
         model.adj_zero()
-        grad = np.zeros(self.shape)
+        model.adj_grad_reset(self.hours)  # gathered on the device, read back once
         for seg in range(nseg - 1, -1, -1):
             n0, n1 = seg * K, min(N, seg * K + K)
             # recompute the segment, keeping each step's post-source state
@@ -172,6 +175,6 @@ class SourceInversion:
                 model.set_dt(lg.dt)
                 model.adj_step(lg.itime)
                 if 0 <= lg.hour < self.hours:
-                    col = model.adj_vent_column()
-                    grad[:, lg.hour, :] += lg.dt * col[:cfg.nz, :] / self.kappa_col[:, None]
-        return J, grad
+                    # grad[:, hour, :] += dt * lam_vent / kappa, in step order
+                    model.adj_vent_accumulate(lg.hour, lg.dt)
+        return J, model.adj_grad_get()

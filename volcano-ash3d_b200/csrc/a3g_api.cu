@@ -293,7 +293,7 @@ int a3g_destroy(a3g_ctx *ctx) {
   for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
   double *aptrs[] = {ctx->lam0, ctx->lam1, ctx->lam_dep, ctx->stage1, ctx->stage2, ctx->adj_face,
                      ctx->obs_buf, ctx->ov_buf, ctx->ov_zcc, ctx->topo_buf, ctx->vzh, ctx->umb_buf,
-                     ctx->vp_buf};
+                     ctx->vp_buf, ctx->adj_grad};
   for (double *p : aptrs) if (p) cudaFree(p);
   for (double *p : ctx->snaps) if (p) cudaFree(p);
   if (ctx->met_copy_ev) cudaEventDestroy(ctx->met_copy_ev);
@@ -734,6 +734,19 @@ int a3g_add_source_umbrella(a3g_ctx *ctx, const double *flux_umbrella, double dt
                            umb_flux_len(ctx) * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   A3G_CUDA(cudaEventRecord(ctx->umb_event, ctx->stream));
   return launch_source_umbrella(ctx, dt);
+}
+
+int a3g_add_source_column_devdt(a3g_ctx *ctx, int32_t ivent, int32_t jvent, const double *flux) {
+  CTX_CHECK(ctx);
+  if (!flux) return fail(A3G_ERR_ARG, "null flux");
+  if (ivent < 1 || ivent > ctx->grid.nx || jvent < 1 || jvent > ctx->grid.ny)
+    return fail(A3G_ERR_ARG, "vent outside the grid");
+  A3G_CUDA(cudaEventSynchronize(ctx->src_event));  // previous staging copy done
+  const size_t n = (size_t)(ctx->grid.nz + 1) * ctx->grid.ns;
+  std::memcpy(ctx->h_src, flux, n * sizeof(double));
+  A3G_CUDA(cudaMemcpyAsync(ctx->src_buf, ctx->h_src, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  A3G_CUDA(cudaEventRecord(ctx->src_event, ctx->stream));
+  return launch_source_devdt(ctx, ivent, jvent);
 }
 
 int a3g_set_bc(a3g_ctx *ctx, int32_t bc_code) {
@@ -1289,6 +1302,41 @@ int a3g_adj_step(a3g_ctx *ctx, int32_t itime) {
   if ((rc = adj_advect_dir(ctx, 2, ctx->stage2))) return rc;         // AdvectVert^T at state c
   if ((rc = adj_advect_dir(ctx, 1 - first, ctx->stage1))) return rc; // second horizontal sweep at b
   return adj_advect_dir(ctx, first, ctx->c0);                        // first horizontal sweep at a
+}
+
+int a3g_adj_grad_reset(a3g_ctx *ctx, int32_t nbins) {
+  CTX_CHECK(ctx);
+  if (nbins < 1) return fail(A3G_ERR_ARG, "need nbins >= 1");
+  const size_t n = (size_t)nbins * ctx->grid.nz * ctx->grid.ns;
+  if (nbins != ctx->adj_grad_bins) {
+    if (ctx->adj_grad) cudaFree(ctx->adj_grad);
+    ctx->adj_grad = nullptr;
+    if (cudaMalloc((void **)&ctx->adj_grad, n * sizeof(double)) != cudaSuccess)
+      return fail(A3G_ERR_NOMEM, "gradient buffer allocation failed");
+    ctx->adj_grad_bins = nbins;
+  }
+  A3G_CUDA(cudaMemsetAsync(ctx->adj_grad, 0, n * sizeof(double), ctx->stream));
+  return A3G_OK;
+}
+
+int a3g_adj_vent_accumulate(a3g_ctx *ctx, int32_t ivent, int32_t jvent, int32_t bin, double dt) {
+  CTX_CHECK(ctx);
+  if (!ctx->lam0) return fail(A3G_ERR_STATE, "a3g_adj_enable has not been called");
+  if (!ctx->adj_grad) return fail(A3G_ERR_STATE, "a3g_adj_grad_reset has not been called");
+  if (bin < 0 || bin >= ctx->adj_grad_bins) return fail(A3G_ERR_ARG, "gradient bin out of range");
+  if (ivent < 1 || ivent > ctx->grid.nx || jvent < 1 || jvent > ctx->grid.ny)
+    return fail(A3G_ERR_ARG, "vent outside the grid");
+  return launch_vent_accumulate(ctx, ivent, jvent, dt,
+                                ctx->adj_grad + (size_t)bin * ctx->grid.nz * ctx->grid.ns);
+}
+
+int a3g_adj_grad_get(a3g_ctx *ctx, double *out) {
+  CTX_CHECK(ctx);
+  if (!out) return fail(A3G_ERR_ARG, "null out");
+  if (!ctx->adj_grad) return fail(A3G_ERR_STATE, "a3g_adj_grad_reset has not been called");
+  const size_t n = (size_t)ctx->adj_grad_bins * ctx->grid.nz * ctx->grid.ns;
+  A3G_CUDA(cudaMemcpyAsync(out, ctx->adj_grad, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  return sync_scalars(ctx);
 }
 
 int a3g_adj_vent_column(a3g_ctx *ctx, int32_t ivent, int32_t jvent, double *out) {

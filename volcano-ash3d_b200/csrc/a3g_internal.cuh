@@ -162,6 +162,9 @@ struct a3g_ctx {
   double *src_sched;
   int32_t *src_state;
   int src_np, src_iv, src_jv;
+  // device-accumulated source gradient (a3g_adj_grad_reset): nbins x ns x nz
+  double *adj_grad;
+  int adj_grad_bins;
   // vertical profiles (a3g_vprofiles): points and results, grown on demand
   double *vp_buf;
   size_t vp_cap;
@@ -229,6 +232,8 @@ int launch_vprofiles(a3g_ctx *ctx, int npts, const int32_t *pts, double *out, in
 int launch_umbrella_winds(a3g_ctx *ctx, int i0, int ni, int j0, int nj, const double *uv);
 int launch_source_umbrella(a3g_ctx *ctx, double dt);
 int launch_source(a3g_ctx *ctx, int ivent, int jvent, double dt);
+int launch_source_devdt(a3g_ctx *ctx, int ivent, int jvent);
+int launch_vent_accumulate(a3g_ctx *ctx, int ivent, int jvent, double dt, double *dst);
 int launch_zero_state(a3g_ctx *ctx);
 int check_device_error(a3g_ctx *ctx);
 int launch_adj_advect(a3g_ctx *ctx, int dir, const double *cq, const double *lin, double *lout,

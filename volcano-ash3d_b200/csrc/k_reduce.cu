@@ -695,6 +695,25 @@ __global__ void k_source(Layout L, int ivent, int jvent, const double *__restric
   c[a] = c[a] + dt * flux[(long)(k - 1) + (long)(L.nz + 1) * g];
 }
 
+// the vent-column insertion with the step's dt read from the device scalars
+__global__ void k_source_devdt(Layout L, int ivent, int jvent, const double *__restrict__ flux,
+                               const DevScalars *__restrict__ sc, double *__restrict__ c) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;  // (k-1) + nz*g
+  if (t >= L.nz * L.ns) return;
+  const int k = t % L.nz + 1, g = t / L.nz;
+  const long a = (long)g * L.PG + L.cell(ivent, jvent, k);
+  c[a] = c[a] + sc->dt * flux[(long)(k - 1) + (long)(L.nz + 1) * g];
+}
+
+int launch_source_devdt(a3g_ctx *ctx, int ivent, int jvent) {
+  const int n = ctx->L.nz * ctx->L.ns;
+  tbegin(ctx, A3G_K_OTHER);
+  k_source_devdt<<<(n + 127) / 128, 128, 0, ctx->stream>>>(ctx->L, ivent, jvent, ctx->src_buf, ctx->sc, ctx->c0);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  return A3G_OK;
+}
+
 int launch_source(a3g_ctx *ctx, int ivent, int jvent, double dt) {
   const int n = ctx->L.nz * ctx->L.ns;
   tbegin(ctx, A3G_K_OTHER);
@@ -760,6 +779,28 @@ int launch_adj_cloud_load(a3g_ctx *ctx, const double *w, double *lam) {
   tbegin(ctx, A3G_K_ADJOINT);
   k_adj_cloud_load<<<dim3((L.nx + 127) / 128, L.ny, L.nz * L.ns), 128, 0, ctx->stream>>>(L, w, ctx->dz_vec,
                                                                                         lam);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  return A3G_OK;
+}
+
+// grad(k, g) += dt * lam(ivent, jvent, k, g) / kappa(ivent, jvent, k) for
+// k = 1..nz: the source-gradient gather of one reverse step, on the device
+// (the same operations as the host's dt*col/kappa added to grad).
+__global__ void k_vent_accumulate(Layout L, int ivent, int jvent, const double *__restrict__ lam, Geo3 kap,
+                                  double dt, double *__restrict__ dst) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;  // (k-1) + nz*g
+  if (t >= L.nz * L.ns) return;
+  const int k = t % L.nz + 1, g = t / L.nz;
+  const double kv = kap.p[(long)(ivent + 1) * kap.si + (long)(jvent + 1) * kap.sj + (long)(k + 1) * kap.sk];
+  dst[t] = dst[t] + dt * lam[(long)g * L.PG + L.cell(ivent, jvent, k)] / kv;
+}
+
+int launch_vent_accumulate(a3g_ctx *ctx, int ivent, int jvent, double dt, double *dst) {
+  const int n = ctx->L.nz * ctx->L.ns;
+  tbegin(ctx, A3G_K_ADJOINT);
+  k_vent_accumulate<<<(n + 127) / 128, 128, 0, ctx->stream>>>(ctx->L, ivent, jvent, ctx->lam0, ctx->kappa, dt,
+                                                              dst);
   tend(ctx);
   A3G_LAUNCH_CHECK(ctx);
   return A3G_OK;

@@ -320,6 +320,24 @@ class Ash3dGPU:
     def adj_step(self, itime: int):
         check(self.lib.a3g_adj_step(self.ctx, itime))
 
+    def adj_grad_reset(self, nbins: int):
+        check(self.lib.a3g_adj_grad_reset(self.ctx, nbins))
+        self._grad_bins = nbins
+
+    def adj_vent_accumulate(self, bin_: int, dt: float):
+        check(self.lib.a3g_adj_vent_accumulate(self.ctx, self.cfg.ivent, self.cfg.jvent, bin_, dt))
+
+    def adj_grad_get(self) -> np.ndarray:
+        """The accumulated gradient, (nz, nbins, ns)."""
+        c = self.cfg
+        out = np.zeros(self._grad_bins * c.ns * c.nz)
+        check(self.lib.a3g_adj_grad_get(self.ctx, dptr(out)))
+        return np.ascontiguousarray(out.reshape(self._grad_bins, c.ns, c.nz).transpose(2, 0, 1))
+
+    def add_source_devdt(self, flux: np.ndarray):
+        f = np.asfortranarray(flux, dtype=np.float64)
+        check(self.lib.a3g_add_source_column_devdt(self.ctx, self.cfg.ivent, self.cfg.jvent, dptr(f)))
+
     def adj_vent_column(self) -> np.ndarray:
         c = self.cfg
         out = np.zeros((c.nz + 1, c.ns), order="F")
