@@ -173,3 +173,23 @@ def test_exact_division_matches_ieee():
     bad = C.c_uint64(99)
     _lib.check(lib.a3g_selftest_div(0, 1 << 26, 12345, C.byref(bad)))
     assert bad.value == 0
+
+
+@pytest.mark.parametrize("name", ["tiny_cn", "tiny_latlon", "tiny_subgrid"])
+def test_cn_tables_follow_dt_and_box(name):
+    """The CN factor tables are kept between steps while dt, the box, the
+    geometry and the diffusivity stay the same; changing dt back and forth,
+    and the box, must rebuild them (bitwise against the oracle)."""
+    cfg, gpu, ref = pair(name)
+    dt0 = prime(cfg, gpu, ref, seed=31)
+    boxes = [(1, cfg.nx, 1, cfg.ny, 1, cfg.nz), (3, cfg.nx - 2, 2, cfg.ny - 3, 2, cfg.nz - 1)]
+    for n, (dt, box) in enumerate([(dt0, 0), (dt0, 0), (0.5 * dt0, 0), (dt0, 0), (dt0, 1), (dt0, 1), (dt0, 0)]):
+        for m in (gpu, ref):
+            m.set_dt(dt)
+            m.set_subgrid(boxes[box])
+            m.Set_BC(2)
+            m.DiffuseHorz(n)
+            m.DiffuseVert()
+        bad = np.argwhere(gpu.interior() != ref.interior())
+        assert bad.size == 0, (n, f"{len(bad)} cells differ, first {bad[:3].tolist()}")
+    gpu.close()

@@ -293,7 +293,7 @@ int a3g_destroy(a3g_ctx *ctx) {
   for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
   double *aptrs[] = {ctx->lam0, ctx->lam1, ctx->lam_dep, ctx->stage1, ctx->stage2, ctx->adj_face,
                      ctx->obs_buf, ctx->ov_buf, ctx->ov_zcc, ctx->topo_buf, ctx->vzh, ctx->umb_buf,
-                     ctx->vp_buf, ctx->adj_grad};
+                     ctx->vp_buf, ctx->adj_grad, ctx->cn_state};
   for (double *p : aptrs) if (p) cudaFree(p);
   for (double *p : ctx->snaps) if (p) cudaFree(p);
   if (ctx->met_copy_ev) cudaEventDestroy(ctx->met_copy_ev);
@@ -331,18 +331,30 @@ static int set_geo3(a3g_ctx *ctx, const double *src, long n0, long n1, long n2, 
 }
 
 static int ensure_cn_buf(a3g_ctx *ctx) {
+  for (int d = 0; d < 3; d++) ctx->cn_valid[d] = false;  // geometry or diffusivity changed
   if (!ctx->have_geometry || !ctx->have_diffusivity) return A3G_OK;
-  size_t need = 0;
+  size_t len[3], need = 0;
   for (int d = 0; d < 3; d++) {
-    size_t n = cn_table_doubles(ctx, d);
-    if (n > need) need = n;
+    len[d] = (cn_table_doubles(ctx, d) + 31) / 32 * 32;  // 256-byte aligned regions
+    need += len[d];
   }
-  if (need <= ctx->cn_len) return A3G_OK;
-  if (ctx->cn_buf) { cudaFree(ctx->cn_buf); ctx->bytes -= ctx->cn_len * sizeof(double); ctx->cn_buf = nullptr; }
-  cudaError_t e = cudaMalloc((void **)&ctx->cn_buf, need * sizeof(double));
-  if (e != cudaSuccess) { ctx->cn_len = 0; return fail(A3G_ERR_NOMEM, "CN table allocation failed"); }
-  ctx->cn_len = need;
-  ctx->bytes += need * sizeof(double);
+  if (!ctx->cn_state) {
+    if (cudaMalloc((void **)&ctx->cn_state, 6 * sizeof(double)) != cudaSuccess)
+      return fail(A3G_ERR_NOMEM, "CN table state allocation failed");
+    A3G_CUDA(cudaMemsetAsync(ctx->cn_state, 0, 6 * sizeof(double), ctx->stream));
+  }
+  if (need > ctx->cn_len) {
+    if (ctx->cn_buf) { cudaFree(ctx->cn_buf); ctx->bytes -= ctx->cn_len * sizeof(double); ctx->cn_buf = nullptr; }
+    cudaError_t e = cudaMalloc((void **)&ctx->cn_buf, need * sizeof(double));
+    if (e != cudaSuccess) { ctx->cn_len = 0; return fail(A3G_ERR_NOMEM, "CN table allocation failed"); }
+    ctx->cn_len = need;
+    ctx->bytes += need * sizeof(double);
+  }
+  size_t off = 0;
+  for (int d = 0; d < 3; d++) {
+    ctx->cn_tab[d] = ctx->cn_buf + off;
+    off += len[d];
+  }
   return A3G_OK;
 }
 

@@ -121,9 +121,15 @@ struct a3g_ctx {
   double *h_src;            // pinned staging
   cudaEvent_t src_event;    // guards reuse of h_src
   double *h_tot;            // pinned totals staging
-  // CN line coefficient scratch
+  // CN factor tables, one region per direction (cn_tab[d] inside cn_buf),
+  // reused while dt, the box, the geometry and the diffusivity stay the same:
+  // cn_state = {dt of each table (3), skip flags (3)} on the device
   double *cn_buf;
   size_t cn_len;
+  double *cn_tab[3];
+  bool cn_valid[3];
+  a3g::Box cn_box[3];
+  double *cn_state;
 
   a3g::Box box;
   int last_bc;

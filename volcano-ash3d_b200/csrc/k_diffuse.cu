@@ -137,10 +137,11 @@ __device__ __forceinline__ bool same_bits(double a, double b) {
 // read every row.
 template <int DIR>
 __global__ void k_cn_table(Layout L, Box box, double imp, LineMap map, Geo3 sig, Geo3 kap, Geo3 kk,
-                           DevScalars *sc, double *__restrict__ tab) {
+                           DevScalars *sc, const double *__restrict__ cstate, double *__restrict__ tab) {
   constexpr bool COMPRESS = (DIR == 0);
   const int u = blockIdx.x * blockDim.x + threadIdx.x;
   if (u >= map.U) return;
+  if (cstate[3 + DIR] != 0.0) return;  // the table already holds this dt's factors
   // representative fixed indices of this distinct line
   const int amin = (DIR == 0) ? box.jmin : box.imin;
   const int bmin = (DIR == 2) ? box.jmin : box.kmin;
@@ -478,16 +479,14 @@ __global__ void __launch_bounds__(128, 12) k_cn_solve_gc_y(Layout L, Box box, Li
 }
 
 template <int DIR, int GC>
-static void launch_cn_solve_gc(a3g_ctx *ctx, const LineMap &map) {
+static void launch_cn_solve_gc(a3g_ctx *ctx, const LineMap &map, const double *tab) {
   const Layout &L = ctx->L;
   const long n = (long)map.na * map.nb * ((L.ns + GC - 1) / GC);
   const unsigned grid = (unsigned)((n + 127) / 128);
   if constexpr (DIR == 1)
-    k_cn_solve_gc_y<GC><<<grid, 128, 0, ctx->stream>>>(L, ctx->box, map, ctx->c0, ctx->c1, ctx->cn_buf,
-                                                       ctx->aloft);
+    k_cn_solve_gc_y<GC><<<grid, 128, 0, ctx->stream>>>(L, ctx->box, map, ctx->c0, ctx->c1, tab, ctx->aloft);
   else
-    k_cn_solve_gc<DIR, GC><<<grid, 128, 0, ctx->stream>>>(L, ctx->box, map, ctx->c0, ctx->c1, ctx->cn_buf,
-                                                          ctx->aloft);
+    k_cn_solve_gc<DIR, GC><<<grid, 128, 0, ctx->stream>>>(L, ctx->box, map, ctx->c0, ctx->c1, tab, ctx->aloft);
 }
 
 // Solve kernel: one thread per line (a, b, grain), lines enumerated with a
@@ -730,6 +729,37 @@ size_t cn_table_doubles(const a3g_ctx *ctx, int dir) {
   return (size_t)CN_NF * n * U + 2 * U;
 }
 
+// Decides on the device whether direction dir's table can be kept: the host
+// allows it (same box, geometry and diffusivity as when it was built) and
+// the step's dt equals the table's.
+__global__ void k_cn_check(const DevScalars *__restrict__ sc, double *__restrict__ st, int dir, int may) {
+  const double dt = sc->dt;
+  const bool keep = may && st[dir] == dt;
+  st[3 + dir] = keep ? 1.0 : 0.0;
+  st[dir] = dt;
+}
+
+static inline bool same_box(const Box &a, const Box &b) {
+  return a.imin == b.imin && a.imax == b.imax && a.jmin == b.jmin && a.jmax == b.jmax && a.kmin == b.kmin &&
+         a.kmax == b.kmax;
+}
+
+// The factor table of direction DIR for the step's dt: built by k_cn_table,
+// or kept from the previous build when nothing it depends on has changed.
+template <int DIR>
+static int cn_table(a3g_ctx *ctx, const LineMap &map, const Geo3 &sig, const Geo3 &kk) {
+  const bool may = ctx->cn_valid[DIR] && same_box(ctx->cn_box[DIR], ctx->box);
+  k_cn_check<<<1, 1, 0, ctx->stream>>>(ctx->sc, ctx->cn_state, DIR, may ? 1 : 0);
+  A3G_LAUNCH_CHECK(ctx);
+  k_cn_table<DIR><<<(map.U + 127) / 128, 128, 0, ctx->stream>>>(ctx->L, ctx->box, ctx->prm.imp_fac, map, sig,
+                                                                ctx->kappa, kk, ctx->sc, ctx->cn_state,
+                                                                ctx->cn_tab[DIR]);
+  A3G_LAUNCH_CHECK(ctx);
+  ctx->cn_valid[DIR] = true;
+  ctx->cn_box[DIR] = ctx->box;
+  return A3G_OK;
+}
+
 template <int DIR>
 static int launch_cn_dir(a3g_ctx *ctx) {
   const Layout &L = ctx->L;
@@ -751,23 +781,23 @@ static int launch_cn_dir(a3g_ctx *ctx) {
   map.db = varies(ctx->kappa, ib) || varies(sig, ib) || varies(kk, ib);
   map.U = (map.da ? map.na : 1) * (map.db ? map.nb : 1);
   tbegin(ctx, A3G_K_CN_TABLE);
-  k_cn_table<DIR><<<(map.U + 127) / 128, 128, 0, ctx->stream>>>(L, box, ctx->prm.imp_fac, map, sig,
-                                                                ctx->kappa, kk, ctx->sc, ctx->cn_buf);
+  int rc = cn_table<DIR>(ctx, map, sig, kk);
   tend(ctx);
-  A3G_LAUNCH_CHECK(ctx);
+  if (rc) return rc;
+  const double *tab = ctx->cn_tab[DIR];
   const long nlines = (long)map.na * map.nb * L.ns;
   tbegin(ctx, A3G_K_CN_SOLVE_X + DIR);
   if (DIR == 0 && ctx->tune_cn_x == 0) {
     const long nwarps = (nlines + 31) / 32;
     k_cn_solve_xt<<<(unsigned)((nwarps + XT_WARPS - 1) / XT_WARPS), 32 * XT_WARPS, 0, ctx->stream>>>(
-        L, box, map, ctx->c0, ctx->c1, ctx->cn_buf, ctx->aloft);
+        L, box, map, ctx->c0, ctx->c1, tab, ctx->aloft);
   } else if (DIR != 0 && ctx->tune_cn_yz == 1 && L.ns >= 2) {
-    launch_cn_solve_gc<DIR == 0 ? 1 : DIR, 2>(ctx, map);
+    launch_cn_solve_gc<DIR == 0 ? 1 : DIR, 2>(ctx, map, tab);
   } else if (DIR != 0 && ctx->tune_cn_yz == 2 && L.ns >= 2) {
-    launch_cn_solve_gc<DIR == 0 ? 1 : DIR, 4>(ctx, map);
+    launch_cn_solve_gc<DIR == 0 ? 1 : DIR, 4>(ctx, map, tab);
   } else {
     k_cn_solve<DIR><<<(unsigned)((nlines + 127) / 128), 128, 0, ctx->stream>>>(
-        L, box, map, ctx->c0, ctx->c1, ctx->cn_buf, ctx->aloft);
+        L, box, map, ctx->c0, ctx->c1, tab, ctx->aloft);
   }
   tend(ctx);
   A3G_LAUNCH_CHECK(ctx);
@@ -932,11 +962,10 @@ static int launch_adj_cn_dir(a3g_ctx *ctx, const double *lin, double *lout) {
   map.db = varies(ctx->kappa, ib) || varies(sig, ib) || varies(kk, ib);
   map.U = (map.da ? map.na : 1) * (map.db ? map.nb : 1);
   tbegin(ctx, A3G_K_ADJOINT);
-  k_cn_table<DIR><<<(map.U + 127) / 128, 128, 0, ctx->stream>>>(L, ctx->box, ctx->prm.imp_fac, map, sig,
-                                                                ctx->kappa, kk, ctx->sc, ctx->cn_buf);
-  A3G_LAUNCH_CHECK(ctx);
+  int rc = cn_table<DIR>(ctx, map, sig, kk);
+  if (rc) return rc;
   const long nlines = (long)map.na * map.nb * L.ns;
-  k_adj_cn<DIR><<<(unsigned)((nlines + 127) / 128), 128, 0, ctx->stream>>>(L, map, lin, lout, ctx->cn_buf,
+  k_adj_cn<DIR><<<(unsigned)((nlines + 127) / 128), 128, 0, ctx->stream>>>(L, map, lin, lout, ctx->cn_tab[DIR],
                                                                            ctx->aloft);
   tend(ctx);
   A3G_LAUNCH_CHECK(ctx);
