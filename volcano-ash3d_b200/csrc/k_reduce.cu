@@ -277,7 +277,9 @@ __global__ void __launch_bounds__(256) k_totals(Layout L, const double *__restri
                                                 const double *__restrict__ xy1,
                                                 const double *__restrict__ xy2,
                                                 double *__restrict__ part) {
-  const int job = blockIdx.y, g = blockIdx.z;
+  // job is the slowest grid index: the airborne-mass blocks of every grain
+  // are resident together (more loads in flight) before the small face sums
+  const int job = blockIdx.z, g = blockIdx.y;
   __shared__ double sh[2][8];
   DD acc = {0.0, 0.0};
   long n;
@@ -344,7 +346,7 @@ __global__ void k_totals_final(int ns, int nblk, const double *__restrict__ part
 int launch_totals_partials(a3g_ctx *ctx, double *h_dst) {
   const Layout &L = ctx->L;
   const int ns = L.ns;
-  dim3 grid(TOT_BLOCKS, NJOBS, ns);
+  dim3 grid(TOT_BLOCKS, ns, NJOBS);
   tbegin(ctx, A3G_K_TOTALS);
   k_totals<<<grid, 256, 0, ctx->stream>>>(L, ctx->c0, ctx->kappa, ctx->out_yz1, ctx->out_yz2,
                                           ctx->out_xz1, ctx->out_xz2, ctx->out_xy1, ctx->out_xy2,
@@ -384,7 +386,7 @@ void totals_volumes(a3g_ctx *ctx, const double *h_src, double *out4, double *mas
 int launch_totals(a3g_ctx *ctx, double *out4, double *mass_aloft) {
   const Layout &L = ctx->L;
   const int ns = L.ns;
-  dim3 grid(TOT_BLOCKS, NJOBS, ns);
+  dim3 grid(TOT_BLOCKS, ns, NJOBS);
   tbegin(ctx, A3G_K_TOTALS);
   k_totals<<<grid, 256, 0, ctx->stream>>>(L, ctx->c0, ctx->kappa, ctx->out_yz1, ctx->out_yz2,
                                           ctx->out_xz1, ctx->out_xz2, ctx->out_xy1, ctx->out_xy2,
