@@ -193,3 +193,33 @@ def test_cn_tables_follow_dt_and_box(name):
         bad = np.argwhere(gpu.interior() != ref.interior())
         assert bad.size == 0, (n, f"{len(bad)} cells differ, first {bad[:3].tolist()}")
     gpu.close()
+
+
+def test_totals_follow_the_state():
+    """TimeStepTotals after a CN z solve, after a new state and after a
+    source insertion each describe the state of that moment (totals
+    against the oracle at 1e-13)."""
+    cfg, gpu, ref = pair("tiny_cn")
+    prime(cfg, gpu, ref, seed=41)
+    for m in (gpu, ref):
+        m.Set_BC(2)
+        m.DiffuseHorz(1)
+        m.DiffuseVert()
+
+    def same_totals():
+        vg, mg = gpu.TimeStepTotals()
+        vr, mr = ref.TimeStepTotals()
+        np.testing.assert_allclose(vg, vr, rtol=1e-13, atol=0)
+        np.testing.assert_allclose(mg, mr, rtol=1e-13, atol=0)
+
+    same_totals()
+    q = random_state(cfg, 77)
+    for m in (gpu, ref):
+        m.set_interior(q)
+    same_totals()
+    for m in (gpu, ref):
+        m.Set_BC(2)
+        m.DiffuseVert()
+        m.add_source(np.full((cfg.nz + 1, cfg.ns), 3.0e4, order="F"), 0.1)
+    same_totals()
+    gpu.close()
