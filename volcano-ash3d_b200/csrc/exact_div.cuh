@@ -22,6 +22,11 @@
 
 namespace a3g {
 
+// The IEEE division operator for the rare operands the fast path does not
+// certify, kept out of line so that its code is not repeated at every call
+// site (the sweeps inline many divisions).
+static __device__ __noinline__ double ieee_div(double a, double b) { return a / b; }
+
 __device__ __forceinline__ double rcp_approx(double b) {
   double y;
   asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
@@ -46,8 +51,8 @@ __device__ __forceinline__ bool certified(double a, double b, double q) {
 
 // RN(a/b).
 __device__ __forceinline__ double div_rn(double a, double b) {
-  if (!(in_fast_range(b, false) && in_fast_range(a, true))) return a / b;
-  if (a == 0.0) return a / b;
+  if (!(in_fast_range(b, false) && in_fast_range(a, true))) return ieee_div(a, b);
+  if (a == 0.0) return ieee_div(a, b);
   double y = rcp_approx(b);
   double e = fma(-b, y, 1.0);
   y = fma(y, e, y);
@@ -57,19 +62,19 @@ __device__ __forceinline__ double div_rn(double a, double b) {
   const double r = fma(-b, q, a);
   q = fma(r, y, q);
   if (certified(a, b, q)) return q;
-  return a / b;
+  return ieee_div(a, b);
 }
 
 // RN(a/b) given y = RN(1/b) (precomputed once for a divisor shared by many
 // quotients, e.g. a tridiagonal pivot).
 __device__ __forceinline__ double div_rn_rcp(double a, double b, double y) {
-  if (!(in_fast_range(b, false) && in_fast_range(a, true))) return a / b;
-  if (a == 0.0) return a / b;
+  if (!(in_fast_range(b, false) && in_fast_range(a, true))) return ieee_div(a, b);
+  if (a == 0.0) return ieee_div(a, b);
   double q = a * y;
   const double r = fma(-b, q, a);
   q = fma(r, y, q);
   if (certified(a, b, q)) return q;
-  return a / b;
+  return ieee_div(a, b);
 }
 
 }  // namespace a3g
