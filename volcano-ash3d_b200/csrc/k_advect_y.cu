@@ -1,5 +1,8 @@
 // k_advect_y.cu -- the y sweep's instantiations (advect_y).  One
-// translation unit per direction lets the three compile in parallel.
+// translation unit per direction lets the three compile in parallel.  The y
+// block kernel measured faster on B200 with the division fallback inlined
+// (C2: 1.43 against 1.51 ms), unlike x and z.
+#define A3G_DIV_FALLBACK_INLINE
 #include "k_advect.cuh"
 
 namespace a3g {
