@@ -214,6 +214,28 @@ int a3g_upload_outflow(a3g_ctx *ctx, const double *yz1, const double *yz2, const
 int a3g_download_outflow(a3g_ctx *ctx, double *yz1, double *yz2, double *xz1, double *xz2,
                          double *xy1, double *xy2, double *deposit);
 
+/* ---- NetCDF output arrays and restart (src/write_NETCDF.f90) ---- */
+/* The 3-D and 4-D arrays the NetCDF writer puts, formed on the device from
+ * the current state (src/write_NETCDF.f90:3287-3300, 3307-3330):
+ *   ashcon(1:nx,1:ny,1:nz,1:ns) = real(concen_pd(1:nx,1:ny,1:nz,1:ns,ts1), kind=op)
+ *   depocon(1:nx,1:ny,1:ns)     = real(DepositGranularity*dz_vec_pd(0)/KM2_2_M2, kind=op),
+ *                                 then 0 where depocon <= EPS_SMALL (1e-6; the FP32
+ *                                 value compared in FP64, as Fortran promotes it)
+ * op = 4 (src/Ash3d_VariableModules.f90:31): FP32, x fastest, nx*ny*nz*ns and
+ * nx*ny*ns floats.  Either pointer may be NULL.  Each may be host or device
+ * memory: device memory of the context's device (or managed memory) is
+ * written by the kernel directly, anything else through one FP32 copy, half
+ * the bytes of a3g_download_concen.  Synchronous. */
+int a3g_output_ashcon(a3g_ctx *ctx, float *ashcon, float *depocon);
+/* NC_RestartFile_LoadConcen (src/write_NETCDF.f90:3646-3716):
+ * concen_pd(1:nx,1:ny,1:nz,:,ts1) = real(ashcon, ip), then concen(ts0) =
+ * concen(ts1); outflow_xy1_pd(1:nx,1:ny,:) = DepositGranularity =
+ * real(depocon, ip).  As in the reference, depocon is loaded as the file
+ * holds it (kg/m^2, the writer's dz_vec_pd(0)/KM2_2_M2 scaling is not undone)
+ * and the other outflow accumulators are left as they are.  Layouts, NULL and
+ * pointer rules as a3g_output_ashcon.  Synchronous. */
+int a3g_restart_load(a3g_ctx *ctx, const float *ashcon, const float *depocon);
+
 /* ---- the per-step path (callers: src/Ash3d.F90:372-642) ---- */
 /* Step prologue, src/Ash3d.F90:376-378 (ts0 <- ts1; ts1 <- 0). */
 int a3g_step_prologue(a3g_ctx *ctx);

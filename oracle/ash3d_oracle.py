@@ -532,6 +532,31 @@ class OracleModel:
             xy1=self.out_xy1[2:c.nx + 2, 2:c.ny + 2, :].copy(), xy2=self.out_xy2[2:c.nx + 2, 2:c.ny + 2, :].copy(),
             deposit=self.deposit.copy())
 
+    # --- NetCDF output arrays and restart (src/write_NETCDF.f90) -------------
+    def output_ashcon(self):
+        """ashcon = real(concen_pd(1:nx,1:ny,1:nz,1:ns,ts1), op) (:3296-3298);
+        depocon = real(DepositGranularity*dz_vec_pd(0)/KM2_2_M2, op), then
+        0.0 where depocon <= EPS_SMALL (:3320-3330).  op = 4 (FP32,
+        src/Ash3d_VariableModules.f90:31); Fortran compares the FP32 value
+        with the FP64 EPS_SMALL after promoting it."""
+        c = self.cfg
+        ash = np.asfortranarray(self.concen[2:c.nx + 2, 2:c.ny + 2, 2:c.nz + 2, :, 1].astype(np.float32))
+        dz0 = self.dz_vec[1]  # dz_vec_pd(0) (index = Fortran k + 1)
+        dep = np.asfortranarray((self.deposit * dz0 / 1.0e6).astype(np.float32))
+        dep[dep.astype(np.float64) <= 1.0e-6] = np.float32(0.0)
+        return ash, dep
+
+    def restart_load(self, ashcon, depocon):
+        """NC_RestartFile_LoadConcen (src/write_NETCDF.f90:3701-3709):
+        concen_pd(1:nx,1:ny,1:nz,i,ts1) = real(ashcon(:,:,:,i), ip),
+        outflow_xy1_pd = DepositGranularity = real(depocon, ip), then
+        concen(:,:,:,:,ts0) = concen(:,:,:,:,ts1)."""
+        c = self.cfg
+        self.concen[2:c.nx + 2, 2:c.ny + 2, 2:c.nz + 2, :, 1] = np.asarray(ashcon, np.float32).astype(np.float64)
+        self.out_xy1[2:c.nx + 2, 2:c.ny + 2, :] = np.asarray(depocon, np.float32).astype(np.float64)
+        self.deposit[...] = self.out_xy1[2:c.nx + 2, 2:c.ny + 2, :]
+        self.concen[..., 0] = self.concen[..., 1]
+
     @property
     def dt(self):
         return self.s.dt

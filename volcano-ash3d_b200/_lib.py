@@ -30,7 +30,8 @@ EXPORTED = [
     "a3g_sync", "a3g_device_bytes", "a3g_set_geometry", "a3g_set_diffusivity",
     "a3g_set_fall_velocity", "a3g_set_aloft", "a3g_set_winds", "a3g_set_met_steps",
     "a3g_interp_winds", "a3g_upload_concen", "a3g_download_concen", "a3g_upload_outflow",
-    "a3g_download_outflow", "a3g_step_prologue", "a3g_set_dt", "a3g_add_source_column",
+    "a3g_download_outflow", "a3g_output_ashcon", "a3g_restart_load", "a3g_step_prologue",
+    "a3g_set_dt", "a3g_add_source_column",
     "a3g_set_bc", "a3g_advect_horz", "a3g_advect_x", "a3g_advect_y", "a3g_advect_vert",
     "a3g_diffuse_horz", "a3g_diffuse_vert", "a3g_adjust_dt", "a3g_timestep_totals",
     "a3g_get_minmax_index", "a3g_set_subgrid", "a3g_get_subgrid", "a3g_step",
@@ -128,6 +129,9 @@ def load(path: os.PathLike | str | None = None) -> C.CDLL:
         "a3g_download_concen": (C.c_int, [P, D]),
         "a3g_upload_outflow": (C.c_int, [P, D, D, D, D, D, D]),
         "a3g_download_outflow": (C.c_int, [P, D, D, D, D, D, D, D]),
+        # FP32 arrays as addresses: host (numpy) or device (a tensor's data_ptr)
+        "a3g_output_ashcon": (C.c_int, [P, P, P]),
+        "a3g_restart_load": (C.c_int, [P, P, P]),
         "a3g_step_prologue": (C.c_int, [P]),
         "a3g_set_dt": (C.c_int, [P, C.c_double]),
         "a3g_add_source_column": (C.c_int, [P, C.c_int32, C.c_int32, D, C.c_double]),

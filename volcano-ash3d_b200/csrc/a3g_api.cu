@@ -295,6 +295,7 @@ int a3g_destroy(a3g_ctx *ctx) {
                      ctx->obs_buf, ctx->ov_buf, ctx->ov_zcc, ctx->topo_buf, ctx->vzh, ctx->umb_buf,
                      ctx->vp_buf, ctx->adj_grad, ctx->cn_state};
   for (double *p : aptrs) if (p) cudaFree(p);
+  if (ctx->nc_buf) cudaFree(ctx->nc_buf);
   for (double *p : ctx->snaps) if (p) cudaFree(p);
   if (ctx->met_copy_ev) cudaEventDestroy(ctx->met_copy_ev);
   if (ctx->met_free_ev) cudaEventDestroy(ctx->met_free_ev);
@@ -649,6 +650,81 @@ int a3g_download_outflow(a3g_ctx *ctx, double *yz1, double *yz2, double *xz1, do
     A3G_CUDA(cudaMemcpyAsync(deposit, ctx->out_xy1, sizeof(double) * nx * ny * ctx->grid.ns,
                              cudaMemcpyDeviceToHost, ctx->stream));
   return sync_scalars(ctx);
+}
+
+// ---- NetCDF output arrays and restart ---------------------------------------
+// A caller's pointer that the kernels can address: device memory of this
+// context's device, or managed memory.  Anything else goes through staging.
+static bool device_addressable(a3g_ctx *ctx, const void *p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return (a.type == cudaMemoryTypeDevice && a.device == ctx->device) || a.type == cudaMemoryTypeManaged;
+}
+
+static int ensure_nc_buf(a3g_ctx *ctx, size_t n) {
+  if (n <= ctx->nc_cap) return A3G_OK;
+  if (ctx->nc_buf) cudaFree(ctx->nc_buf);
+  ctx->nc_buf = nullptr;
+  ctx->nc_cap = 0;
+  if (cudaMalloc((void **)&ctx->nc_buf, n * sizeof(float)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(A3G_ERR_NOMEM, "NetCDF staging buffer allocation failed");
+  }
+  ctx->nc_cap = n;
+  return A3G_OK;
+}
+
+// Device addresses of ashcon and depocon for the kernels: the caller's own
+// when addressable, else slices of the staging buffer.
+static int nc_targets(a3g_ctx *ctx, const float *ashcon, const float *depocon, float **da, float **dd) {
+  const Layout &L = ctx->L;
+  const size_t na = (size_t)L.nx * L.ny * L.nz * L.ns, nd = (size_t)L.nx * L.ny * L.ns;
+  const bool a_dev = ashcon && device_addressable(ctx, ashcon);
+  const bool d_dev = depocon && device_addressable(ctx, depocon);
+  const size_t sa = (ashcon && !a_dev) ? na : 0, sd = (depocon && !d_dev) ? nd : 0;
+  int rc = ensure_nc_buf(ctx, sa + sd);
+  if (rc) return rc;
+  *da = !ashcon ? nullptr : a_dev ? const_cast<float *>(ashcon) : ctx->nc_buf;
+  *dd = !depocon ? nullptr : d_dev ? const_cast<float *>(depocon) : ctx->nc_buf + sa;
+  return A3G_OK;
+}
+
+int a3g_output_ashcon(a3g_ctx *ctx, float *ashcon, float *depocon) {
+  CTX_CHECK(ctx);
+  const Layout &L = ctx->L;
+  const size_t na = (size_t)L.nx * L.ny * L.nz * L.ns, nd = (size_t)L.nx * L.ny * L.ns;
+  float *da, *dd;
+  int rc = nc_targets(ctx, ashcon, depocon, &da, &dd);
+  if (rc) return rc;
+  rc = launch_netcdf_pack(ctx, da, dd);
+  if (rc) return rc;
+  if (ashcon && da != ashcon)
+    A3G_CUDA(cudaMemcpyAsync(ashcon, da, na * sizeof(float), cudaMemcpyDefault, ctx->stream));
+  if (depocon && dd != depocon)
+    A3G_CUDA(cudaMemcpyAsync(depocon, dd, nd * sizeof(float), cudaMemcpyDefault, ctx->stream));
+  A3G_CUDA(cudaStreamSynchronize(ctx->stream));
+  return check_device_error(ctx);
+}
+
+int a3g_restart_load(a3g_ctx *ctx, const float *ashcon, const float *depocon) {
+  CTX_CHECK(ctx);
+  const Layout &L = ctx->L;
+  const size_t na = (size_t)L.nx * L.ny * L.nz * L.ns, nd = (size_t)L.nx * L.ny * L.ns;
+  float *da, *dd;
+  int rc = nc_targets(ctx, ashcon, depocon, &da, &dd);
+  if (rc) return rc;
+  if (ashcon && da != ashcon)
+    A3G_CUDA(cudaMemcpyAsync(da, ashcon, na * sizeof(float), cudaMemcpyDefault, ctx->stream));
+  if (depocon && dd != depocon)
+    A3G_CUDA(cudaMemcpyAsync(dd, depocon, nd * sizeof(float), cudaMemcpyDefault, ctx->stream));
+  rc = launch_netcdf_unpack(ctx, da, dd);
+  if (rc) return rc;
+  A3G_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (ashcon) ctx->ts1_zeroed = false;
+  return check_device_error(ctx);
 }
 
 int a3g_step_prologue(a3g_ctx *ctx) {

@@ -174,6 +174,9 @@ struct a3g_ctx {
   // vertical profiles (a3g_vprofiles): points and results, grown on demand
   double *vp_buf;
   size_t vp_cap;
+  // NetCDF output / restart staging for host pointers (FP32), grown on demand
+  float *nc_buf;
+  size_t nc_cap;
   // terrain (a3g_set_topo): dhdx, dhdy, DelDxonD, DelDyonD ((nx+4)*(ny+4) each,
   // ghosted, i fastest) and the per-level factor of vh (nz); vzh = vz + vh on
   // the interior, the vertical wind of the z sweep
@@ -235,6 +238,8 @@ int launch_totals_partials(a3g_ctx *ctx, double *h_dst);
 void totals_volumes(a3g_ctx *ctx, const double *h_src, double *out4, double *mass_aloft);
 int launch_source_sched(a3g_ctx *ctx, double time);
 int launch_vprofiles(a3g_ctx *ctx, int npts, const int32_t *pts, double *out, int32_t *written);
+int launch_netcdf_pack(a3g_ctx *ctx, float *ashcon, float *depocon);
+int launch_netcdf_unpack(a3g_ctx *ctx, const float *ashcon, const float *depocon);
 int launch_umbrella_winds(a3g_ctx *ctx, int i0, int ni, int j0, int nj, const double *uv);
 int launch_source_umbrella(a3g_ctx *ctx, double dt);
 int launch_source(a3g_ctx *ctx, int ivent, int jvent, double dt);

@@ -915,6 +915,86 @@ int launch_output_vars(a3g_ctx *ctx, double time, double *load, double *maxh, do
 }
 
 // ---------------------------------------------------------------------------
+// NetCDF output arrays and restart (src/write_NETCDF.f90): FP32 (op = 4,
+// src/Ash3d_VariableModules.f90:31) arrays with x fastest, the layout the
+// writer passes to nf90_put_var.  One thread per cell of a row; blockIdx.y =
+// j, blockIdx.z strides over the (k, g) planes.
+// ---------------------------------------------------------------------------
+// ashcon(i,j,k,g) = real(concen_pd(i,j,k,g,ts1), kind=op) (:3296-3298)
+__global__ void k_pack_ashcon(Layout L, const double *__restrict__ c, float *__restrict__ ashcon) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (i >= L.nx) return;
+  for (int kg = blockIdx.z; kg < L.nz * L.ns; kg += gridDim.z) {
+    const int k = kg % L.nz, g = kg / L.nz;
+    ashcon[((long)kg * L.ny + j) * L.nx + i] = __double2float_rn(c[(long)g * L.PG + L.cell(i + 1, j + 1, k + 1)]);
+  }
+}
+
+// depocon(i,j,g) = real(DepositGranularity*dz_vec_pd(0)/KM2_2_M2, kind=op),
+// then 0 where depocon <= EPS_SMALL, the FP32 value compared in FP64
+// (:3320-3330).  DepositGranularity is outflow_xy1 ([g][j][i]).
+__global__ void k_pack_depocon(Layout L, const double *__restrict__ xy1, const double *__restrict__ dz_vec,
+                               float *__restrict__ depocon) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (i >= L.nx) return;
+  for (int g = blockIdx.z; g < L.ns; g += gridDim.z) {
+    const long a = ((long)g * L.ny + j) * L.nx + i;
+    float d = __double2float_rn(xy1[a] * dz_vec[1] / 1.0e6);  // dz_vec[1] = dz_vec_pd(0)
+    if ((double)d <= 1.0e-6) d = 0.0f;
+    depocon[a] = d;
+  }
+}
+
+// NC_RestartFile_LoadConcen (:3701-3707): concen_pd(i,j,k,g) = real(ashcon, ip)
+__global__ void k_unpack_ashcon(Layout L, const float *__restrict__ ashcon, double *__restrict__ c) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (i >= L.nx) return;
+  for (int kg = blockIdx.z; kg < L.nz * L.ns; kg += gridDim.z) {
+    const int k = kg % L.nz, g = kg / L.nz;
+    c[(long)g * L.PG + L.cell(i + 1, j + 1, k + 1)] = (double)ashcon[((long)kg * L.ny + j) * L.nx + i];
+  }
+}
+
+// outflow_xy1_pd(i,j,g) = DepositGranularity(i,j,g) = real(depocon(i,j,g), ip)
+__global__ void k_unpack_depocon(Layout L, const float *__restrict__ depocon, double *__restrict__ xy1) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (i >= L.nx) return;
+  for (int g = blockIdx.z; g < L.ns; g += gridDim.z) {
+    const long a = ((long)g * L.ny + j) * L.nx + i;
+    xy1[a] = (double)depocon[a];
+  }
+}
+
+static dim3 netcdf_grid(const Layout &L, int planes) {
+  return dim3((L.nx + 255) / 256, L.ny, planes < 65535 ? planes : 65535);
+}
+
+int launch_netcdf_pack(a3g_ctx *ctx, float *ashcon, float *depocon) {
+  const Layout &L = ctx->L;
+  tbegin(ctx, A3G_K_OTHER);
+  if (ashcon) k_pack_ashcon<<<netcdf_grid(L, L.nz * L.ns), 256, 0, ctx->stream>>>(L, ctx->c0, ashcon);
+  if (depocon)
+    k_pack_depocon<<<netcdf_grid(L, L.ns), 256, 0, ctx->stream>>>(L, ctx->out_xy1, ctx->dz_vec, depocon);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  return A3G_OK;
+}
+
+int launch_netcdf_unpack(a3g_ctx *ctx, const float *ashcon, const float *depocon) {
+  const Layout &L = ctx->L;
+  tbegin(ctx, A3G_K_OTHER);
+  if (ashcon) k_unpack_ashcon<<<netcdf_grid(L, L.nz * L.ns), 256, 0, ctx->stream>>>(L, ashcon, ctx->c0);
+  if (depocon) k_unpack_depocon<<<netcdf_grid(L, L.ns), 256, 0, ctx->stream>>>(L, depocon, ctx->out_xy1);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  return A3G_OK;
+}
+
+// ---------------------------------------------------------------------------
 // self-test of exact_div.cuh against the IEEE division operator
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint64_t mix64(uint64_t x) {  // splitmix64 finaliser

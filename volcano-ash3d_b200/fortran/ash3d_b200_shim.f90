@@ -36,7 +36,7 @@
       public B200_Init, B200_Finalize, B200_Upload, B200_Download, B200_Check, &
              B200_StepPrologue, B200_AddSource, B200_SetWinds, B200_SetMetSteps, &
              B200_InterpWinds, B200_SetTopo, B200_SetUmbrella, B200_AddUmbrellaWinds, &
-             B200_AddSourceUmbrella, b200_ctx
+             B200_AddSourceUmbrella, B200_OutputAshcon, B200_RestartLoad, b200_ctx
 
       type, bind(C) :: a3g_grid_desc
         integer(c_int32_t) :: nx, ny, nz, ns
@@ -138,6 +138,14 @@
             bind(C, name="a3g_download_outflow")
           import :: c_int, c_ptr
           type(c_ptr), value :: ctx, a, b, c, d, e, f, dep
+        end function
+        integer(c_int) function a3g_output_ashcon(ctx, ash, dep) bind(C, name="a3g_output_ashcon")
+          import :: c_int, c_ptr
+          type(c_ptr), value :: ctx, ash, dep
+        end function
+        integer(c_int) function a3g_restart_load(ctx, ash, dep) bind(C, name="a3g_restart_load")
+          import :: c_int, c_ptr
+          type(c_ptr), value :: ctx, ash, dep
         end function
         integer(c_int) function a3g_step_prologue(ctx) bind(C, name="a3g_step_prologue")
           import :: c_int, c_ptr
@@ -377,6 +385,22 @@
         call B200_Check(a3g_add_source_umbrella(b200_ctx, c_loc(SourceNodeFlux_Umbrella), real(dt, c_double)), &
                         "a3g_add_source_umbrella")
       end subroutine B200_AddSourceUmbrella
+
+      ! In place of the conversions of src/write_NETCDF.f90:3296-3298 (ashcon) and
+      ! 3320-3330 (depocon, scaled and thresholded), before their nf90_put_var:
+      ! the writer's own real(kind=op) buffers, op = 4, are filled on the device.
+      subroutine B200_OutputAshcon(ashcon, depocon)
+        real(c_float), intent(out), target, contiguous :: ashcon(:,:,:,:), depocon(:,:,:)
+        call B200_Check(a3g_output_ashcon(b200_ctx, c_loc(ashcon), c_loc(depocon)), "a3g_output_ashcon")
+      end subroutine B200_OutputAshcon
+
+      ! NC_RestartFile_LoadConcen (src/write_NETCDF.f90:3701-3709), after its
+      ! nf90_get_var calls: concen_pd(ts1) = ashcon, concen(ts0) = concen(ts1),
+      ! outflow_xy1_pd = DepositGranularity = depocon, on the device.
+      subroutine B200_RestartLoad(ashcon, depocon)
+        real(c_float), intent(in), target, contiguous :: ashcon(:,:,:,:), depocon(:,:,:)
+        call B200_Check(a3g_restart_load(b200_ctx, c_loc(ashcon), c_loc(depocon)), "a3g_restart_load")
+      end subroutine B200_RestartLoad
 
       end module B200_Transport
 

@@ -434,6 +434,27 @@ class Ash3dGPU:
                     xz1=xz1[2:c.nx + 2, 2:c.nz + 2, :], xz2=xz2[2:c.nx + 2, 2:c.nz + 2, :],
                     xy1=xy1[2:c.nx + 2, 2:c.ny + 2, :], xy2=xy2[2:c.nx + 2, 2:c.ny + 2, :], deposit=dep)
 
+    # --- NetCDF output arrays and restart (src/write_NETCDF.f90) --------------
+    def output_ashcon(self) -> tuple[np.ndarray, np.ndarray]:
+        """(ashcon, depocon) as the NetCDF writer forms them: FP32,
+        (nx, ny, nz, ns) and (nx, ny, ns), Fortran order
+        (src/write_NETCDF.f90:3296-3298, 3320-3330)."""
+        c = self.cfg
+        ash = np.empty((c.nx, c.ny, c.nz, c.ns), np.float32, order="F")
+        dep = np.empty((c.nx, c.ny, c.ns), np.float32, order="F")
+        check(self.lib.a3g_output_ashcon(self.ctx, ash.ctypes.data, dep.ctypes.data))
+        return ash, dep
+
+    def restart_load(self, ashcon: np.ndarray, depocon: np.ndarray):
+        """NC_RestartFile_LoadConcen (src/write_NETCDF.f90:3646-3716): the
+        state from ashcon, outflow_xy1 and DepositGranularity from depocon."""
+        c = self.cfg
+        ash = np.asfortranarray(ashcon, dtype=np.float32)
+        dep = np.asfortranarray(depocon, dtype=np.float32)
+        if ash.shape != (c.nx, c.ny, c.nz, c.ns) or dep.shape != (c.nx, c.ny, c.ns):
+            raise ValueError(f"ashcon {ash.shape} / depocon {dep.shape} do not match the grid")
+        check(self.lib.a3g_restart_load(self.ctx, ash.ctypes.data, dep.ctypes.data))
+
     @property
     def dt(self):
         return self._dt
