@@ -1,7 +1,7 @@
 // k_advect_y.cu -- the y sweep's instantiations (advect_y).  One
 // translation unit per direction lets the three compile in parallel.  The y
 // block kernel measured faster on B200 with the division fallback inlined
-// (C2: 1.43 against 1.51 ms), unlike x and z.
+// (C2: 1.42 against 1.50 ms), unlike x and z.
 #define A3G_DIV_FALLBACK_INLINE
 #include "k_advect.cuh"
 
