@@ -26,16 +26,30 @@ namespace a3g {
 // certify, kept out of line so that its code is not repeated at every call
 // site (the sweeps inline many divisions).  A translation unit that measured
 // faster with it inlined defines A3G_DIV_FALLBACK_INLINE first.
-#ifdef A3G_DIV_FALLBACK_INLINE
+#if defined(A3G_HOST_TEST)
+// A host build of this header (the CPU test of the certification) supplies
+// its own reciprocal estimates, including deliberately poor ones, and counts
+// the quotients that were not certified.
+double host_rcp_estimate(double b);
+long &host_fallback_count();
+static inline double ieee_div(double a, double b) {
+  ++host_fallback_count();
+  return a / b;
+}
+#elif defined(A3G_DIV_FALLBACK_INLINE)
 static __device__ __forceinline__ double ieee_div(double a, double b) { return a / b; }
 #else
 static __device__ __noinline__ double ieee_div(double a, double b) { return a / b; }
 #endif
 
 __device__ __forceinline__ double rcp_approx(double b) {
+#ifdef A3G_HOST_TEST
+  return host_rcp_estimate(b);
+#else
   double y;
   asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
   return y;
+#endif
 }
 
 // True when |x| is zero or its binary exponent lies in [-200, 200].
