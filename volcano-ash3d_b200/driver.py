@@ -78,6 +78,56 @@ class Comm:
     def sum(self, a):
         return self._reduce(a, self.dist.ReduceOp.SUM)
 
+    # --- per-rank grain blocks (the last axis of ashcon / depocon) -----------
+    def _world(self):
+        return self.dist.get_rank(self.group), self.dist.get_world_size(self.group)
+
+    def _peer(self, r: int) -> int:
+        return r if self.group is None else self.dist.get_global_rank(self.group, r)
+
+    def _empty(self, n: int, dtype):
+        tdt = self.torch.from_numpy(np.empty(0, dtype=dtype)).dtype
+        return self.torch.empty(n, dtype=tdt, device=self.device)
+
+    def gather_grains(self, arr: np.ndarray, ns_total: int, root: int = 0):
+        """The full array on ``root`` from every rank's block of grain bins
+        (the last axis, blocks in rank order as split_grains deals them),
+        Fortran order; None on the other ranks.  Point-to-point sends, one
+        per non-root rank."""
+        rank, world = self._world()
+        shape = arr.shape[:-1]
+        if rank != root:
+            t = self.torch.from_numpy(np.ascontiguousarray(arr.ravel(order="F"))).to(self.device)
+            self.dist.send(t, dst=self._peer(root), group=self.group)
+            return None
+        out = np.empty(shape + (ns_total,), dtype=arr.dtype, order="F")
+        for r in range(world):
+            lo, hi = grain_range(ns_total, r, world)
+            if r == root:
+                out[..., lo:hi] = arr
+                continue
+            t = self._empty(int(np.prod(shape)) * (hi - lo), arr.dtype)
+            self.dist.recv(t, src=self._peer(r), group=self.group)
+            out[..., lo:hi] = t.cpu().numpy().reshape(shape + (hi - lo,), order="F")
+        return out
+
+    def scatter_grains(self, full, shape: tuple, dtype, ns_total: int, root: int = 0) -> np.ndarray:
+        """This rank's block of grain bins of ``full`` (given on ``root``;
+        ``shape`` is its shape without the grain axis on every rank)."""
+        rank, world = self._world()
+        lo, hi = grain_range(ns_total, rank, world)
+        if rank == root:
+            for r in range(world):
+                if r != root:
+                    a, b = grain_range(ns_total, r, world)
+                    blk = np.asarray(full, dtype=dtype)[..., a:b].ravel(order="F")
+                    self.dist.send(self.torch.from_numpy(np.ascontiguousarray(blk)).to(self.device),
+                                   dst=self._peer(r), group=self.group)
+            return np.asfortranarray(np.asarray(full, dtype=dtype)[..., lo:hi])
+        t = self._empty(int(np.prod(shape)) * (hi - lo), dtype)
+        self.dist.recv(t, src=self._peer(root), group=self.group)
+        return np.asfortranarray(t.cpu().numpy().reshape(tuple(shape) + (hi - lo,), order="F"))
+
 
 def shard_config(cfg: syn.Config, rank: int, world: int) -> syn.Config:
     """Grain sharding: the global run has ns*world grain bins (fall speeds
@@ -119,6 +169,23 @@ def grain_range(ns: int, rank: int, world: int) -> tuple[int, int]:
     base, extra = divmod(ns, world)
     lo = rank * base + min(rank, extra)
     return lo, lo + base + (1 if rank < extra else 0)
+
+
+def gather_netcdf(model, comm: Comm, ns_total: int, root: int = 0):
+    """(ashcon, depocon) of the whole grain-sharded run on ``root`` (None
+    elsewhere): each rank forms its bins' arrays on its device
+    (a3g_output_ashcon) and root places them at the rank's bin offset."""
+    ash, dep = model.output_ashcon()
+    return comm.gather_grains(ash, ns_total, root), comm.gather_grains(dep, ns_total, root)
+
+
+def scatter_restart(model, comm: Comm, cfg: syn.Config, ns_total: int, ashcon=None, depocon=None,
+                    root: int = 0):
+    """NC_RestartFile_LoadConcen for a grain-sharded run: ``root`` holds the
+    file's arrays; every rank loads its own bins (a3g_restart_load)."""
+    a = comm.scatter_grains(ashcon, (cfg.nx, cfg.ny, cfg.nz), np.float32, ns_total, root)
+    d = comm.scatter_grains(depocon, (cfg.nx, cfg.ny), np.float32, ns_total, root)
+    model.restart_load(a, d)
 
 
 def next_write_time(write_times, time: float) -> float:
