@@ -67,3 +67,51 @@ def test_no_cpu_fallback_without_gpu(pkg):
     ctx = C.c_void_p()
     rc = lib.a3g_create(C.byref(g), C.byref(p), 0, C.byref(ctx))
     assert rc != 0 and not ctx
+
+
+def _header_kinds():
+    """Parameter kinds of every a3g_ prototype: 'int32', 'int64', 'uint64',
+    'double', or 'p:<element>' for pointers."""
+    txt = (ROOT / "include" / "ash3d_b200.h").read_text()
+    txt = re.sub(r"/\*.*?\*/", " ", txt, flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(a3g_\w+)\s*\(([^)]*)\)\s*;", txt):
+        kinds = []
+        for p in (q.strip() for q in m.group(2).split(",")):
+            if not p or p == "void":
+                continue
+            base = ("double" if re.search(r"\bdouble\b", p) else "float" if re.search(r"\bfloat\b", p)
+                    else "int32" if re.search(r"\bint32_t\b|\bint\b", p) else "int64" if "int64_t" in p
+                    and "uint" not in p else "uint64" if re.search(r"\buint64_t\b|\bsize_t\b", p)
+                    else "other")
+            stars = p.count("*")
+            kinds.append("p:p" if stars >= 2 else "p:" + base if stars else base)
+        out[m.group(1)] = kinds
+    return out
+
+
+def _ctypes_kind(t):
+    if t is C.c_void_p:
+        return "p:void"
+    if hasattr(t, "_type_") and isinstance(t, type) and issubclass(t, C._Pointer):
+        inner = _ctypes_kind(t._type_)
+        if inner.startswith("p:"):
+            return "p:p"
+        return "p:" + (inner if not inner.startswith("?") else "other")
+    return {C.c_int32: "int32", C.c_int64: "int64", C.c_uint64: "uint64", C.c_double: "double",
+            C.c_float: "float"}.get(t, "?" + getattr(t, "__name__", str(t)))
+
+
+def test_ctypes_signatures_match_header(pkg):
+    """Every argtypes list the binding sets has the prototype's arity, scalar
+    types and pointer element types (c_void_p stands for any pointer)."""
+    from volcano_ash3d_b200 import _lib
+    lib = _lib.load()
+    hdr = _header_kinds()
+    for name in _lib.EXPORTED:
+        got = [_ctypes_kind(t) for t in (getattr(lib, name).argtypes or [])]
+        want = hdr[name]
+        assert len(got) == len(want), f"{name}: {got} against {want}"
+        for g, w in zip(got, want):
+            assert g == w or (g == "p:void" and w.startswith("p:")) or (g == "p:other" and w == "p:other"), \
+                f"{name}: {got} against {want}"
