@@ -2,7 +2,8 @@
  * ash3d_b200.h -- C-ABI of the B200 (sm_100a) transport path for Ash3d.
  *
  * The Fortran host (Ash3d.F90's main loop) reaches the GPU through these
- * functions, bound with ISO_C_BINDING (see INTEGRATION.md for the shim).
+ * functions, bound with ISO_C_BINDING (the shim module
+ * volcano-ash3d_b200/fortran/ash3d_b200_shim.f90 holds the interfaces).
  * Every function returns an int status (A3G_OK = 0); a nonzero status is
  * what the reference turns into "write(errlog) ... ; stop 1".
  *
@@ -427,24 +428,28 @@ int a3g_snapshot_save(a3g_ctx *ctx, int32_t slot);
 int a3g_snapshot_load(a3g_ctx *ctx, int32_t slot);
 
 /* ---- allocation-free entry point (no counterpart in the reference) ---- */
-/* Per-grain airborne mass sum(c*kappa) (the mass_aloft of Calc_AshVol_Aloft,
- * src/Output_Vars.f90:1255-1293) for callers that cannot allocate device
- * memory at the time of the call: hosts that reserve all GPU memory at
- * start-up, hosts that pass buffers from their own memory manager, or code
- * running where allocation calls are not allowed (such as a host function
- * enqueued on a stream).  It calls no allocation routine: its partial sums
- * live in a fixed device array of the library (64 grains x 296 blocks x 2
- * doubles, about 296 KiB per device, held until the process exits).
+/* Per-grain airborne mass, sum(c*kappa) over the interior cells, for callers
+ * that cannot allocate device memory at the time of the call: hosts that
+ * reserve all GPU memory at start-up and forbid allocation afterwards, or
+ * hosts that hand the library buffers from their own memory manager.  It
+ * calls no allocation routine: its partial sums live in a fixed device array
+ * of the library (64 grains x 296 blocks x 2 doubles, about 296 KiB per
+ * device, held until the process exits).  It launches two kernels, so call
+ * it from ordinary host code, not from a stream callback or host function.
  *   conc:  device array [ns][nz][ny][row_pitch] (i fastest, interior cells)
  *   kappa: device array [nz][ny][nx] (interior cell volumes)
  *   mass_out: device array [ns] (written)
  *   stream: a cudaStream_t, or NULL for the default stream; the call is
  *           asynchronous on it.
- * ns above 64 is rejected with A3G_ERR_ARG.  The first call on a device looks
- * up the array's device address with that device current; make that first
- * call before any stream capture.  All calls share the array and it keeps
- * the last call's contents (nothing in it needs to start at zero); calls
- * whose kernels overlap on the same device race on it. */
+ * ns above 64 is rejected with A3G_ERR_ARG.  The launches run with `device`
+ * current; the caller's current device is restored before the call returns.
+ * The first call on a device looks up the array's device address with that
+ * device current and caches it for the life of the process: make that first
+ * call before any stream capture, and do not call again on a device after a
+ * cudaDeviceReset of it (the cached address would be stale).  All calls
+ * share the array and it keeps the last call's contents (nothing in it needs
+ * to start at zero); calls whose kernels overlap on the same device race on
+ * it. */
 int a3g_mass_aloft_noalloc(int device, const double *conc, const double *kappa, int32_t nx,
                            int32_t ny, int32_t nz, int32_t ns, int64_t row_pitch,
                            double *mass_out, void *stream);

@@ -81,4 +81,6 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_ref_cloudload.py <path of the Ash3d source tree>")
+    main(sys.argv[1])

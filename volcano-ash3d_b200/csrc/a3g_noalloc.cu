@@ -3,15 +3,15 @@
 // Some callers cannot allocate device memory when they need this sum: an
 // operational forecast host that reserves all GPU memory at start-up and
 // forbids allocation afterwards (so a long run cannot fail part-way with an
-// out-of-memory error), a host that hands the library device buffers from
-// its own memory manager, or code running where CUDA allocation calls are
-// not allowed (for example inside a host function enqueued on a stream).
+// out-of-memory error), or a host that hands the library device buffers from
+// its own memory manager and keeps allocation to itself.
 // a3g_mass_aloft_noalloc serves them: it computes the per-grain airborne
-// mass sum(c*kappa) of Calc_AshVol_Aloft (src/Output_Vars.f90:1255-1293),
-// with the same blocking and double-double accumulation as the context path
-// (a3g_timestep_totals), but keeps its per-block partial sums in the
-// file-scope device array below instead of a buffer obtained from
-// cudaMalloc.
+// mass sum(c*kappa) over the interior cells, with the same blocking and
+// double-double accumulation as the context path (a3g_timestep_totals), but
+// keeps its per-block partial sums in the file-scope device array below
+// instead of a buffer obtained from cudaMalloc.  It launches kernels, so it
+// is called from ordinary host code (CUDA forbids CUDA calls inside a stream
+// callback or host function).
 //
 // Limits and sharing: the array holds A3G_NOALLOC_MAX_GRAINS grains x
 // NOALLOC_BLOCKS blocks x 2 doubles (about 296 KiB) on every device that
@@ -19,6 +19,11 @@
 // overwrites its own slot before the final pass reads it, so nothing in the
 // array has to start at zero; the array keeps the last call's contents, and
 // two calls whose kernels overlap on the same device race on it.
+//
+// The array's device address is looked up once per device and cached for the
+// life of the process.  A cudaDeviceReset (or any other reset of the primary
+// context) unloads the module and leaves that cached address stale, so a
+// process that resets a device must not call this entry point on it again.
 #include <mutex>
 
 #include "a3g_internal.cuh"
@@ -132,17 +137,33 @@ extern "C" int a3g_mass_aloft_noalloc(int device, const double *conc, const doub
     a3g::set_error("a3g_mass_aloft_noalloc: device ordinal out of range");
     return A3G_ERR_ARG;
   }
-  cudaError_t e = cudaSetDevice(device);
-  if (e != cudaSuccess) return a3g::cuda_fail(e, "cudaSetDevice");
+  // the launches need `device` current; the caller's current device is put
+  // back before returning, on every path
+  int prev = -1;
+  cudaError_t e = cudaGetDevice(&prev);
+  if (e != cudaSuccess) return a3g::cuda_fail(e, "cudaGetDevice");
+  if (prev != device) {
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) return a3g::cuda_fail(e, "cudaSetDevice");
+  }
+  int rc = A3G_OK;
   double *part = nullptr;
-  int rc = scratch_for(device, &part);
-  if (rc) return rc;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  k_mass_partial<<<dim3(NOALLOC_BLOCKS, ns), 256, 0, s>>>(conc, kappa, nx, ny, nz, (long)row_pitch, part);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return a3g::cuda_fail(e, "k_mass_partial launch");
-  k_mass_final<<<(ns + 63) / 64, 64, 0, s>>>(ns, NOALLOC_BLOCKS, part, mass_out);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return a3g::cuda_fail(e, "k_mass_final launch");
-  return A3G_OK;
+  rc = scratch_for(device, &part);
+  if (rc == A3G_OK) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    k_mass_partial<<<dim3(NOALLOC_BLOCKS, ns), 256, 0, s>>>(conc, kappa, nx, ny, nz, (long)row_pitch, part);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) rc = a3g::cuda_fail(e, "k_mass_partial launch");
+  }
+  if (rc == A3G_OK) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    k_mass_final<<<(ns + 63) / 64, 64, 0, s>>>(ns, NOALLOC_BLOCKS, part, mass_out);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) rc = a3g::cuda_fail(e, "k_mass_final launch");
+  }
+  if (prev != device) {
+    e = cudaSetDevice(prev);
+    if (e != cudaSuccess && rc == A3G_OK) rc = a3g::cuda_fail(e, "cudaSetDevice (restoring the caller's device)");
+  }
+  return rc;
 }
