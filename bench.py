@@ -24,9 +24,14 @@ N > 1: grains are sharded across GPUs (weak scaling: 10 grains per GPU of a
 10*N-grain run); the only exchange is an all-reduce MAX of three CFL maxima
 and an all-reduce SUM of the totals per step (NCCL).
 
+Build choices: FAST_DT on (dt from the met steps, interpolated every step:
+the reference's default makefile, src/makefile:91) unless --no-fast-dt;
+FAST_SUBGRID off (the filled domain's box is the whole grid).
+
 --impl reference times the CPU restatement of the reference (the oracle,
-OpenMP in the advection rows as the reference) on the host cores, on a
-bounded y-slab of the same workload.
+OpenMP in the advection rows as the reference) on the host cores, on the
+same full grid, state and build choices: at most 4 timed steps after one
+warm-up step (a full-grid CPU step takes ~15 s).
 """
 from __future__ import annotations
 
@@ -186,15 +191,25 @@ def ncu_traffic(config: str, kclass: str):
 # ---------------------------------------------------------------------------
 # CPU arm: the oracle on a bounded slab of the workload
 # ---------------------------------------------------------------------------
-def cpu_sample(config: str, steps: int, warmup: int, ny_sample: int | None = None):
+def bench_config(args):
+    """The workload of both arms: the named configuration with the bench's
+    build choices (FAST_DT on unless --no-fast-dt: the reference's default
+    build, src/makefile:91) and an optional y-slab for profiling."""
+    cfg = syn.make_config(args.config)
+    if args.ny:
+        cfg.ny = args.ny
+        cfg.jvent = max(1, args.ny // 2)
+    cfg.limiter = args.limiter
+    cfg.fast_dt = not args.no_fast_dt
+    return cfg
+
+
+def cpu_sample(cfg, steps: int, warmup: int):
+    """The oracle (the CPU restatement of the reference step, OpenMP on the
+    advection rows as the reference has it) on the same grid, state and
+    build choices as the GPU arm: `warmup` untimed steps, then `steps` timed
+    ones."""
     orc = _load_oracle()
-    cfg = syn.make_config(config)
-    full_cells = cfg.cells
-    if ny_sample is None:
-        # about 1-3 s of CPU work per step: keep ~0.8M cells per sample step
-        ny_sample = max(4, min(cfg.ny, int(8.0e5 // (cfg.nx * cfg.nz))))
-    cfg.ny = ny_sample
-    cfg.jvent = max(1, ny_sample // 2)
     m = orc.OracleModel(cfg)
     m.set_interior(filled_state(cfg))
     st = driver.new_state(cfg)
@@ -206,24 +221,39 @@ def cpu_sample(config: str, steps: int, warmup: int, ny_sample: int | None = Non
     el = time.perf_counter() - t0
     value = cfg.cell_grains * steps / el
     threads = orc.load().orc_get_threads()
-    sample = (f"oracle port of the reference step on a y-slab {cfg.nx}x{ny_sample}x{cfg.nz}x{cfg.ns} "
-              f"({cfg.cells / full_cells:.3f} of the grid), {steps} steps after {warmup} warm-up")
+    sample = (f"oracle port of the reference step on the full grid {cfg.nx}x{cfg.ny}x{cfg.nz}x{cfg.ns}, "
+              f"{steps} steps after {warmup} warm-up, {threads} OpenMP threads on the advection rows "
+              "(diffusion, Adjust_DT and the sums serial, as in the reference)")
     return value, el, threads, sample
+
+
+def host_cpu():
+    try:
+        for ln in pathlib.Path("/proc/cpuinfo").read_text().splitlines():
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
 
 
 def run_reference(args, rank: int, world: int):
     if rank != 0:
         return
-    steps, warmup = args.steps, args.warmup
-    value, el, threads, sample = cpu_sample(args.config, steps, warmup)
-    cfg = syn.make_config(args.config)
+    cfg = bench_config(args)
+    # full-grid CPU steps take ~15 s each: the arm times at most 4 of them after
+    # one warm-up step so that the run ends within a few minutes
+    steps, warmup = min(args.steps, 4), 1
+    value, el, threads, sample = cpu_sample(cfg, steps, warmup)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-        "steps": steps, "warmup": warmup, "ms_per_step": 1e3 * el / steps, "higher_is_better": True,
+        "steps": steps, "warmup": warmup, "requested_steps": args.steps, "requested_warmup": args.warmup,
+        "ms_per_step": 1e3 * el / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"{args.config}: {WORKLOAD[args.config]}", "grid": [cfg.nx, cfg.ny, cfg.nz],
-                   "grains": cfg.ns, "sample": sample},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+                   "grains": cfg.ns, "fast_dt": cfg.fast_dt, "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+                         "cpu_model": host_cpu(), "same_config": True},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -281,11 +311,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         dist.init_process_group("nccl", timeout=timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
         comm = driver.Comm(device=torch.device("cuda", local_rank))
-    cfg_g = syn.make_config(args.config)
-    if args.ny:
-        cfg_g.ny = args.ny
-        cfg_g.jvent = max(1, args.ny // 2)
-    cfg_g.limiter = args.limiter
+    cfg_g = bench_config(args)
     cfg = driver.shard_config(cfg_g, rank, world)
     geo = syn.geometry(cfg)
     gpu = Ash3dGPU(cfg, device=local_rank, geo=geo)
@@ -356,7 +382,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     # copy stream, overlapping the steps.  Crossing an hour in the window adds
     # the loop's own advance and prefetch.  The compute stream waits for the
     # copies before the window closes, so they are inside the timed region.
-    h0 = int(math.floor(st.time))
+    h0 = max(st.hour, 0)
     pinned = PinnedMet(st.met, range(h0, h0 + 3 + int(args.steps * 0.2)), torch)
     st.met = pinned
     step_bytes_met = 3 * cfg.cells * 4  # one FP32 met step (vx, vy, vz)
@@ -410,15 +436,17 @@ def run_ours(args, rank: int, world: int, local_rank: int):
               for k, v in ktimes.items() if v[1] > 0}
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            cv, cel, thr, sample = cpu_sample(args.config, steps=2, warmup=1)
-            cpu = {"value": cv, "unit": UNIT, "cores": thr, "kind": "port", "sample": sample}
+            # one full-grid step (~15 s of CPU work) after one warm-up step
+            cv, cel, thr, sample = cpu_sample(cfg_g, steps=1, warmup=1)
+            cpu = {"value": cv, "unit": UNIT, "cores": thr, "kind": "port", "sample": sample,
+                   "cpu_model": host_cpu(), "same_config": True}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded filled concentration, analytic winds with seeded noise)",
             "config": {"workload": f"{args.config}: {WORKLOAD[args.config]}",
-                       "grid": [cfg.nx, cfg.ny, cfg.nz], "grains_per_gpu": cfg.ns,
+                       "grid": [cfg.nx, cfg.ny, cfg.nz], "grains_per_gpu": cfg.ns, "fast_dt": cfg.fast_dt,
                        "grains_total": n_total, "parallelism": f"grain-sharded x{world}",
                        "l2": "inputs larger than L2 (one concentration level is "
                              f"{cfg.cell_grains * 8 / 1e9:.2f} GB)"},
@@ -536,6 +564,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="C2", choices=sorted(WORKLOAD))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fast-dt", action="store_true",
+                    help="Adjust_DT every step instead of FAST_DT (the reference's default build)")
     ap.add_argument("--limiter", default="superbee",
                     choices=["none", "laxwen", "bw", "fromm", "minmod", "superbee", "mc"],
                     help="the reference's LIM_* build choice (default superbee)")

@@ -277,6 +277,44 @@ int a3g_cfl_maxima(a3g_ctx *ctx, double *vmax3);
 int a3g_adjust_dt_from_maxima(a3g_ctx *ctx, const double *vmax3, int32_t n_gs_aloft_total,
                               double time, double next_write_time, double simtime,
                               double *dt_out);
+/* ---- FAST_DT: the time step of the reference's default build
+ *      (FASTFPPFLAG = -DFAST_DT, src/makefile:91) ----
+ * With FAST_DT the CFL maxima are taken only when a met step is loaded, on the
+ * FP32 met step itself (Adjust_DT(mesostep=.true.), src/Adjust_dt.f90:96-135),
+ * and every step's dt is interpolated between the dt of the last and of the
+ * next met step (src/MesoInterpolater.f90:250-258).
+ * a3g_set_fall_velocity_meso: vf_meso_next_step_sp (m/s, FP32), which
+ * Read_NextMesoStep fills: per_grain=0, the whole (nx,ny,nz,ns) array in
+ * Fortran order (fall models evaluated per cell); per_grain=1, ns values, the
+ * real(Tephra_v_s(isize), sp) that Read_NextMesoStep puts in every cell when
+ * the fall velocities come from the input file (src/MesoInterpolater.f90:
+ * 567-574).  Only max_g |vf| per cell is kept.
+ * a3g_cfl_maxima_meso: the three maxima of src/Adjust_dt.f90:96-135 over the
+ * FP32 met step in device slot `slot` (0: last, 1: next, as a3g_set_met_steps
+ * and a3g_advance_met_step leave them): real(max|vx|)*3.6 (projected; divided
+ * by dx later) or real(|vx|)*3.6*minsig/kappa (lon/lat), and
+ * real(|vz| + max_g|vf|)*3.6/dz_k with the sum in FP32.
+ * a3g_adjust_dt_meso: Adjust_DT(mesostep=.true.) on that slot: dt formed from
+ * those maxima as in :176-332 (snapped to DT_MIN, clipped to the next write
+ * time and the end) becomes time_data::dt and dt_meso_next, both kept on the
+ * device.  shift=1 first copies dt_meso_next to dt_meso_last, the toggle of
+ * src/MesoInterpolater.f90:187.  dt_out may be NULL (nothing waits then).
+ * The first met-step load of a run is a3g_adjust_dt_meso(slot 0, shift 0)
+ * then (slot 1, shift 1) (src/MesoInterpolater.f90:142-150,187-195); every
+ * later load, after a3g_advance_met_step, is (slot 1, shift 1).
+ * a3g_adjust_dt_meso_from_maxima: the same from maxima all-reduced over the
+ * ranks of a grain-sharded run (a3g_cfl_maxima_meso on each).
+ * a3g_fast_dt_async: the step's dt = dt_meso_last + (dt_meso_next -
+ * dt_meso_last)*interval_frac, clipped to the next write time and the end,
+ * on the device (the sweeps read it there) and copied back behind an event
+ * like a3g_adjust_dt_async; a3g_wait_dt returns it. */
+int a3g_set_fall_velocity_meso(a3g_ctx *ctx, const float *vf_meso_sp, int32_t per_grain);
+int a3g_cfl_maxima_meso(a3g_ctx *ctx, int32_t slot, double *vmax3);
+int a3g_adjust_dt_meso(a3g_ctx *ctx, int32_t slot, int32_t shift, double time, double next_write_time,
+                       double simtime, double *dt_out);
+int a3g_adjust_dt_meso_from_maxima(a3g_ctx *ctx, const double *vmax3, int32_t n_gs_aloft_total, int32_t shift,
+                                   double time, double next_write_time, double simtime, double *dt_out);
+int a3g_fast_dt_async(a3g_ctx *ctx, double interval_frac, double time, double next_write_time, double simtime);
 /* TimeStepTotals sums, src/TimeStepTotals.f90:57-66 with Calc_AshVol_Aloft/
  * Deposit/Outflow (src/Output_Vars.f90:1255-1459).  out4 = {aloft_vol,
  * dep_vol, outflow_vol, tot_vol} (km^3 DRE); mass_aloft (ns, kg) may be NULL.

@@ -854,6 +854,65 @@ void orc_cfl_maxima(orc_state *s, double out3[3]) {
   out3[0] = vxmax_dx; out3[1] = vymax_dy; out3[2] = vzmax_dz;
 }
 
+/* Adjust_DT(mesostep=.true.), the FAST_DT branch of src/Adjust_dt.f90:96-135:
+ * the maxima over the FP32 met step (vx_sp, vy_sp, vz_sp: (nx,ny,nz), m/s)
+ * and vf_meso_next_step_sp (per_grain: ns values, the real(Tephra_v_s,sp)
+ * that Read_NextMesoStep puts in every cell; else (nx,ny,nz,ns)).  Projected
+ * grids: real(maxval(abs(vx_sp)))*MPS_2_KMPHR, divided by dx in
+ * orc_dt_from_maxima as the non-meso branch is. */
+void orc_cfl_maxima_meso(orc_state *s, const float *vx_sp, const float *vy_sp, const float *vz_sp,
+                         const float *vf_sp, int per_grain, double out3[3]) {
+  const int nx = s->nx, ny = s->ny, nz = s->nz, ns = s->ns;
+  const size_t n3 = (size_t)nx * ny * nz;
+  double vxmax_dx = 0.0, vymax_dy = 0.0, vzmax_dz = 0.0;
+  if (!s->latlon) {                                                           /* :99-108 */
+    float ax = 0.0f, ay = 0.0f;  /* maxval over (1:nx,1:ny,1:nz), column-major */
+    for (size_t m = 0; m < n3; m++) {
+      if (m == 0 || fabsf(vx_sp[m]) > ax) ax = fabsf(vx_sp[m]);
+      if (m == 0 || fabsf(vy_sp[m]) > ay) ay = fabsf(vy_sp[m]);
+    }
+    double vxmax = (double)ax;
+    vxmax = vxmax * 3.6;
+    double vymax = (double)ay;
+    vymax = vymax * 3.6;
+    vxmax_dx = vxmax;   /* divided by dx, dy in orc_dt_from_maxima */
+    vymax_dy = vymax;
+  }
+  for (int i = 1; i <= nx; i++)                                               /* :112-134 */
+    for (int j = 1; j <= ny; j++)
+      for (int k = 1; k <= nz; k++) {
+        const size_t m = (size_t)(i - 1) + (size_t)nx * ((size_t)(j - 1) + (size_t)ny * (k - 1));
+        if (s->latlon) {
+          double minsig = fmn(s->sig_nx[i3(s, i, j, k)], s->sig_nx[i3(s, i + 1, j, k)]);
+          double tmp1 = (double)fabsf(vx_sp[m]) * 3.6 * minsig / s->kappa[i3(s, i, j, k)];
+          if (tmp1 > vxmax_dx) vxmax_dx = tmp1;
+          minsig = fmn(s->sig_ny[i3(s, i, j, k)], s->sig_ny[i3(s, i, j + 1, k)]);
+          double tmp2 = (double)fabsf(vy_sp[m]) * 3.6 * minsig / s->kappa[i3(s, i, j, k)];
+          if (tmp2 > vymax_dy) vymax_dy = tmp2;
+        }
+        float vfmax = 0.0f;
+        for (int n = 1; n <= ns; n++) {
+          const float a = fabsf(per_grain ? vf_sp[n - 1] : vf_sp[m + n3 * (size_t)(n - 1)]);
+          if (n == 1 || a > vfmax) vfmax = a;
+        }
+        const float sum = fabsf(vz_sp[m]) + vfmax;   /* FP32 sum before widening */
+        double tmp3 = (double)sum * 3.6 / s->dz_vec[k + 1];
+        if (tmp3 > vzmax_dz) vzmax_dz = tmp3;
+      }
+  out3[0] = vxmax_dx; out3[1] = vymax_dy; out3[2] = vzmax_dz;
+}
+
+/* The FAST_DT step dt, src/MesoInterpolater.f90:250-258. */
+double orc_fast_dt(orc_state *s, double dt_meso_last, double dt_meso_next, double interval_frac,
+                   double time, double next_write_time, double simtime) {
+  double dt = dt_meso_last + (dt_meso_next - dt_meso_last) * interval_frac;
+  if (((next_write_time - time) > s->eps_small) && (next_write_time - time < dt))
+    dt = next_write_time - time;
+  if (time + dt > simtime) dt = simtime - time;
+  s->dt = dt;
+  return dt;
+}
+
 /* src/Adjust_dt.f90:137-146 (division by dx, dy) and :176-332. */
 void orc_dt_from_maxima(orc_state *s, const double v3[3], int n_gs_aloft, double time,
                         double next_write_time, double simtime, double *dt_out) {

@@ -121,6 +121,13 @@ void orc_adjust_dt(orc_state *s, double time, double next_write_time,
  * across ranks in between): maxima {vx, vy, vz+vf terms}; projected grids
  * return max|vx|, max|vy| undivided. */
 void orc_cfl_maxima(orc_state *s, double out3[3]);
+/* Adjust_DT(mesostep=.true.) maxima on an FP32 met step (FAST_DT,
+ * src/Adjust_dt.f90:96-135), and the FAST_DT step dt
+ * (src/MesoInterpolater.f90:250-258). */
+void orc_cfl_maxima_meso(orc_state *s, const float *vx_sp, const float *vy_sp, const float *vz_sp,
+                         const float *vf_sp, int per_grain, double out3[3]);
+double orc_fast_dt(orc_state *s, double dt_meso_last, double dt_meso_next, double interval_frac,
+                   double time, double next_write_time, double simtime);
 void orc_dt_from_maxima(orc_state *s, const double v3[3], int n_gs_aloft, double time,
                         double next_write_time, double simtime, double *dt_out);
 /* Calc_AshVol_{Aloft,Deposit,Outflow} + TimeStepTotals sums,

@@ -77,6 +77,9 @@ def load() -> C.CDLL:
             ("orc_adjust_dt", None, [S, C.c_double, C.c_double, C.c_double, D]),
             ("orc_cfl_maxima", None, [S, D]),
             ("orc_dt_from_maxima", None, [S, D, C.c_int, C.c_double, C.c_double, C.c_double, D]),
+            ("orc_cfl_maxima_meso", None, [S, F, F, F, F, C.c_int, D]),
+            ("orc_fast_dt", C.c_double, [S, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                                         C.c_double]),
             ("orc_timestep_totals", None, [S, D]),
             ("orc_get_minmax_index", C.c_int, [S, C.c_int, C.c_int, C.c_int]),
             ("orc_step_prologue", None, [S]),
@@ -185,6 +188,8 @@ class OracleModel:
         if syn.use_topo(cfg):
             self.set_topo(**syn.topo_fields(cfg))
         self.umbrella = syn.umbrella_setup(cfg, self.kappa) if syn.is_umbrella(cfg) else None
+        self.dt_meso_last = self.dt_meso_next = 0.0
+        self.set_fall_velocity_meso(syn.fall_velocity_meso(cfg), per_grain=True)
 
     # --- routines with the reference names ---------------------------------
     def Set_BC(self, code):
@@ -230,6 +235,40 @@ class OracleModel:
 
     def set_dt(self, dt):
         self.s.dt = dt
+
+    # --- FAST_DT (src/Adjust_dt.f90:96-135, src/MesoInterpolater.f90:142-150,
+    #     187-195, 250-258) ---------------------------------------------------
+    def set_fall_velocity_meso(self, vf_sp, per_grain=True):
+        self._vf_meso = (np.asfortranarray(vf_sp, dtype=np.float32), int(bool(per_grain)))
+
+    def _met_slot(self, slot):
+        return self._met[0:3] if slot == 0 else self._met[3:6]
+
+    def cfl_maxima_meso(self, slot):
+        vx, vy, vz = self._met_slot(slot)
+        vf, pg = self._vf_meso
+        v = np.zeros(3)
+        self.lib.orc_cfl_maxima_meso(self.ps, _f(vx), _f(vy), _f(vz), _f(vf), pg, _d(v))
+        return v
+
+    def adjust_dt_meso_from_maxima(self, vmax3, n_gs_aloft_total, shift, time, next_write_time, simtime):
+        if shift:
+            self.dt_meso_last = self.dt_meso_next
+        dt = self.adjust_dt_from_maxima(vmax3, n_gs_aloft_total, time, next_write_time, simtime)
+        self.dt_meso_next = dt
+        return dt
+
+    def adjust_dt_meso(self, slot, shift, time, next_write_time, simtime, wait=True):
+        return self.adjust_dt_meso_from_maxima(self.cfl_maxima_meso(slot), self.s.n_gs_aloft, shift, time,
+                                               next_write_time, simtime)
+
+    def fast_dt_async(self, frac, time, next_write_time, simtime):
+        self._dt_pending = self.lib.orc_fast_dt(self.ps, self.dt_meso_last, self.dt_meso_next, frac, time,
+                                                next_write_time, simtime)
+
+    def fast_dt(self, frac, time, next_write_time, simtime):
+        self.fast_dt_async(frac, time, next_write_time, simtime)
+        return self._dt_pending
 
     def TimeStepTotals(self):
         out = np.zeros(4)

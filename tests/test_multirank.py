@@ -25,7 +25,7 @@ def _free_port() -> int:
         return s.getsockname()[1]
 
 
-def _rank_main(rank: int, world: int, port: int, cfg_name: str, steps: int, out_dir: str):
+def _rank_main(rank: int, world: int, port: int, cfg_name: str, steps: int, out_dir: str, fast: bool = False):
     sys.path.insert(0, str(ROOT / "tests"))
     sys.path.insert(0, str(ROOT / "oracle"))
     import torch.distributed as dist
@@ -38,22 +38,32 @@ def _rank_main(rank: int, world: int, port: int, cfg_name: str, steps: int, out_
         import ash3d_oracle as orc
         mod = conftest._load_pkg()
         pkg, syn = mod.driver, mod.synthetic
-        gcfg = syn.make_config(cfg_name)
+        import dataclasses
+        gcfg = dataclasses.replace(syn.make_config(cfg_name), fast_dt=fast)
         cfg = pkg.split_grains(gcfg, rank, world)
         model = orc.OracleModel(cfg, threads=1)
-        st = pkg.run(model, cfg, max_steps=steps, comm=pkg.Comm(), n_gs_aloft_total=gcfg.ns)
+
+        class CountingComm(pkg.Comm):
+            max_calls = 0
+
+            def max(self, a):
+                CountingComm.max_calls += 1
+                return super().max(a)
+
+        comm = CountingComm()
+        st = pkg.run(model, cfg, max_steps=steps, comm=comm, n_gs_aloft_total=gcfg.ns)
         hist = np.array([[r.time, r.dt, r.aloft, r.dep, r.outflow, r.tot] for r in st.history])
         np.savez(os.path.join(out_dir, f"rank{rank}.npz"), hist=hist, conc=model.interior(),
-                 dep=model.outflows()["deposit"])
+                 dep=model.outflows()["deposit"], max_calls=CountingComm.max_calls, hour=st.hour)
     finally:
         dist.destroy_process_group()
 
 
-def _sharded(cfg_name: str, world: int, steps: int, tmp_path):
+def _sharded(cfg_name: str, world: int, steps: int, tmp_path, fast: bool = False):
     import torch.multiprocessing as mp
     port = _free_port()
     ctx = mp.get_context("spawn")
-    procs = [ctx.Process(target=_rank_main, args=(r, world, port, cfg_name, steps, str(tmp_path)))
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, cfg_name, steps, str(tmp_path), fast))
              for r in range(world)]
     for p in procs:
         p.start()
@@ -67,12 +77,16 @@ def _sharded(cfg_name: str, world: int, steps: int, tmp_path):
     return [np.load(tmp_path / f"rank{r}.npz") for r in range(world)]
 
 
-@pytest.mark.parametrize("cfg_name,steps", [("tiny_proj", 12), ("tiny_latlon", 8)])
-def test_grain_sharded_matches_single(pkg, oracle_mod, cfg_name, steps, tmp_path):
+@pytest.mark.parametrize("cfg_name,steps,fast", [("tiny_proj", 12, False), ("tiny_latlon", 8, False),
+                                                 ("tiny_proj", None, True), ("tiny_latlon", None, True)])
+def test_grain_sharded_matches_single(pkg, oracle_mod, cfg_name, steps, fast, tmp_path):
+    """With FAST_DT the ranks exchange the CFL maxima only at the met-step
+    loads (the first pair: two, then one per later load), not every step."""
+    import dataclasses
     syn, drv = pkg.synthetic, pkg.driver
-    gcfg = syn.make_config(cfg_name)
+    gcfg = dataclasses.replace(syn.make_config(cfg_name), fast_dt=fast)
     world = 2
-    ranks = _sharded(cfg_name, world, steps, tmp_path)
+    ranks = _sharded(cfg_name, world, steps, tmp_path, fast)
 
     ref = oracle_mod.OracleModel(gcfg, threads=1)
     st = drv.run(ref, gcfg, max_steps=steps)
@@ -90,6 +104,11 @@ def test_grain_sharded_matches_single(pkg, oracle_mod, cfg_name, steps, tmp_path
         assert np.array_equal(ranks[r]["dep"], ref_dep[..., lo:hi])
         # totals are all-reduced: every rank holds the global sums
         np.testing.assert_allclose(h[:, 2:], ref_hist[:, 2:], rtol=1e-13, atol=1e-300)
+        if fast:
+            assert int(ranks[r]["hour"]) >= 1
+            assert int(ranks[r]["max_calls"]) == 2 + int(ranks[r]["hour"])
+        else:
+            assert int(ranks[r]["max_calls"]) == len(h)
 
 
 def test_split_grains_partition(pkg):

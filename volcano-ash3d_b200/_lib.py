@@ -48,6 +48,8 @@ EXPORTED = [
     "a3g_timestep_totals_async", "a3g_totals_get", "a3g_set_source_pulses", "a3g_add_source_scheduled",
     "a3g_prefetch_met_step", "a3g_advance_met_step", "a3g_met_prefetch_fence",
     "a3g_add_source_column_devdt", "a3g_adj_grad_reset", "a3g_adj_vent_accumulate", "a3g_adj_grad_get",
+    "a3g_set_fall_velocity_meso", "a3g_cfl_maxima_meso", "a3g_adjust_dt_meso",
+    "a3g_adjust_dt_meso_from_maxima", "a3g_fast_dt_async",
 ]
 KERNEL_CLASSES = ["advect_x", "advect_y", "advect_z", "diff_x", "diff_y", "diff_z", "cn_table",
                   "cn_solve_x", "cn_solve_y", "cn_solve_z", "cfl", "totals", "winds", "other",
@@ -151,6 +153,12 @@ def load(path: os.PathLike | str | None = None) -> C.CDLL:
                                              C.c_int64, D, C.c_void_p]),
         "a3g_selftest_div": (C.c_int, [C.c_int, C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)]),
         "a3g_adjust_dt_from_maxima": (C.c_int, [P, D, C.c_int32, C.c_double, C.c_double, C.c_double, D]),
+        "a3g_set_fall_velocity_meso": (C.c_int, [P, F, C.c_int32]),
+        "a3g_cfl_maxima_meso": (C.c_int, [P, C.c_int32, D]),
+        "a3g_adjust_dt_meso": (C.c_int, [P, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, D]),
+        "a3g_adjust_dt_meso_from_maxima": (C.c_int, [P, D, C.c_int32, C.c_int32, C.c_double, C.c_double,
+                                                     C.c_double, D]),
+        "a3g_fast_dt_async": (C.c_int, [P, C.c_double, C.c_double, C.c_double, C.c_double]),
         "a3g_get_minmax_index": (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, I]),
         "a3g_set_subgrid": (C.c_int, [P, I]),
         "a3g_get_subgrid": (C.c_int, [P, I]),

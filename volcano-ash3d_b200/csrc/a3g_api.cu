@@ -296,6 +296,7 @@ int a3g_destroy(a3g_ctx *ctx) {
                      ctx->vp_buf, ctx->adj_grad, ctx->cn_state};
   for (double *p : aptrs) if (p) cudaFree(p);
   if (ctx->nc_buf) cudaFree(ctx->nc_buf);
+  if (ctx->vfm_sp) cudaFree(ctx->vfm_sp);
   for (double *p : ctx->snaps) if (p) cudaFree(p);
   if (ctx->met_copy_ev) cudaEventDestroy(ctx->met_copy_ev);
   if (ctx->met_free_ev) cudaEventDestroy(ctx->met_free_ev);
@@ -1126,6 +1127,115 @@ int a3g_adjust_dt_from_maxima(a3g_ctx *ctx, const double *vmax3, int32_t n_gs_al
   if ((rc = sync_scalars(ctx))) return rc;
   ctx->host_dt = ctx->h_sc->dt;
   if (dt_out) *dt_out = ctx->h_sc->dt;
+  return A3G_OK;
+}
+
+// ---- FAST_DT (src/makefile:91; src/Adjust_dt.f90:96-135, src/MesoInterpolater.f90:
+// 142-150, 187-195, 250-258) ------------------------------------------------
+int a3g_set_fall_velocity_meso(a3g_ctx *ctx, const float *vf_meso_sp, int32_t per_grain) {
+  CTX_CHECK(ctx);
+  if (!vf_meso_sp) return fail(A3G_ERR_ARG, "null vf_meso_next_step_sp");
+  const int ns = ctx->grid.ns;
+  if (ctx->vfm_sp) cudaFree(ctx->vfm_sp);
+  ctx->vfm_sp = nullptr;
+  ctx->have_vf_meso = false;
+  if (per_grain) {
+    // real(Tephra_v_s(isize), sp) in every cell (src/MesoInterpolater.f90:567-574)
+    float v = 0.0f;
+    for (int g = 0; g < ns; g++) {
+      const float a = std::fabs(vf_meso_sp[g]);
+      if (g == 0 || a > v) v = a;
+    }
+    ctx->vfm_sp_const = v;
+    ctx->have_vf_meso = true;
+    return A3G_OK;
+  }
+  const long n = (long)ctx->grid.nx * ctx->grid.ny * ctx->grid.nz;
+  // maxval(abs(vf_meso_next_step_sp(i,j,k,1:nsmax))) per cell
+  std::vector<float> m((size_t)n);
+  bool uniform = true;
+  for (long c = 0; c < n; c++) {
+    float v = 0.0f;
+    for (int g = 0; g < ns; g++) {
+      const float a = std::fabs(vf_meso_sp[(size_t)g * n + c]);
+      if (g == 0 || a > v) v = a;
+    }
+    m[(size_t)c] = v;
+    if (std::memcmp(&m[(size_t)c], &m[0], sizeof(float)) != 0) uniform = false;
+  }
+  ctx->vfm_sp_const = m[0];
+  if (!uniform) {
+    if (cudaMalloc((void **)&ctx->vfm_sp, sizeof(float) * n) != cudaSuccess)
+      return fail(A3G_ERR_NOMEM, "fall-velocity maxima allocation failed");
+    A3G_CUDA(cudaMemcpyAsync(ctx->vfm_sp, m.data(), sizeof(float) * n, cudaMemcpyHostToDevice, ctx->stream));
+    A3G_CUDA(cudaStreamSynchronize(ctx->stream));
+  }
+  ctx->have_vf_meso = true;
+  return A3G_OK;
+}
+
+static int meso_ready(a3g_ctx *ctx, int slot) {
+  if (slot != 0 && slot != 1) return fail(A3G_ERR_ARG, "met slot must be 0 (last) or 1 (next)");
+  if (!ctx->met) return fail(A3G_ERR_STATE, "a3g_set_met_steps has not been called");
+  if (!ctx->have_geometry) return fail(A3G_ERR_STATE, "geometry not set");
+  if (!ctx->have_vf_meso) return fail(A3G_ERR_STATE, "a3g_set_fall_velocity_meso has not been called");
+  if (ctx->prm.use_diffusion && !ctx->have_diffusivity) return fail(A3G_ERR_STATE, "diffusivity not set");
+  return A3G_OK;
+}
+
+int a3g_cfl_maxima_meso(a3g_ctx *ctx, int32_t slot, double *vmax3) {
+  CTX_CHECK(ctx);
+  if (!vmax3) return fail(A3G_ERR_ARG, "null vmax3");
+  int rc = meso_ready(ctx, slot);
+  if (rc) return rc;
+  if ((rc = launch_cfl_maxima_meso(ctx, slot))) return rc;
+  if ((rc = sync_scalars(ctx))) return rc;
+  for (int q = 0; q < 3; q++) vmax3[q] = ctx->h_sc->vmax[q];
+  return A3G_OK;
+}
+
+int a3g_adjust_dt_meso(a3g_ctx *ctx, int32_t slot, int32_t shift, double time, double next_write_time,
+                       double simtime, double *dt_out) {
+  CTX_CHECK(ctx);
+  int rc = meso_ready(ctx, slot);
+  if (rc) return rc;
+  if ((rc = launch_cfl_maxima_meso(ctx, slot))) return rc;
+  if ((rc = launch_dt_from_maxima(ctx, ctx->n_gs_aloft, time, next_write_time, simtime, shift ? 3 : 1)))
+    return rc;
+  ctx->dt_stamp++;
+  if (!dt_out) return A3G_OK;
+  if ((rc = sync_scalars(ctx))) return rc;
+  ctx->host_dt = ctx->h_sc->dt;
+  *dt_out = ctx->h_sc->dt;
+  return A3G_OK;
+}
+
+int a3g_adjust_dt_meso_from_maxima(a3g_ctx *ctx, const double *vmax3, int32_t n_gs_aloft_total, int32_t shift,
+                                   double time, double next_write_time, double simtime, double *dt_out) {
+  CTX_CHECK(ctx);
+  if (!vmax3) return fail(A3G_ERR_ARG, "null vmax3");
+  if (ctx->prm.use_diffusion && !ctx->have_diffusivity) return fail(A3G_ERR_STATE, "diffusivity not set");
+  double v[4] = {vmax3[0], vmax3[1], vmax3[2], 0.0};
+  A3G_CUDA(cudaMemcpyAsync(ctx->sc->vmax, v, sizeof(v), cudaMemcpyHostToDevice, ctx->stream));
+  int rc = launch_dt_from_maxima(ctx, n_gs_aloft_total, time, next_write_time, simtime, shift ? 3 : 1);
+  if (rc) return rc;
+  ctx->dt_stamp++;
+  if ((rc = sync_scalars(ctx))) return rc;
+  ctx->host_dt = ctx->h_sc->dt;
+  if (dt_out) *dt_out = ctx->h_sc->dt;
+  return A3G_OK;
+}
+
+int a3g_fast_dt_async(a3g_ctx *ctx, double interval_frac, double time, double next_write_time, double simtime) {
+  CTX_CHECK(ctx);
+  int rc = launch_fast_dt(ctx, interval_frac, time, next_write_time, simtime);
+  if (rc) return rc;
+  ctx->dt_stamp++;
+  const int slot = (int)(ctx->dt_seq % 4);
+  A3G_CUDA(cudaMemcpyAsync(ctx->h_sc_ring + slot, ctx->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+  A3G_CUDA(cudaEventRecord(ctx->sc_ev[slot], ctx->stream));
+  ctx->dt_seq++;
   return A3G_OK;
 }
 

@@ -72,6 +72,8 @@ struct DevScalars {
   double dt;              // time_data::dt
   double vmax[4];         // CFL maxima as bit patterns (atomicMax on uint64)
   double time_diffuse;    // cached diffusion limit
+  double dt_meso_last;    // FAST_DT: dt of the last met step (time_data::dt_meso_last)
+  double dt_meso_next;    // FAST_DT: dt of the next met step (time_data::dt_meso_next)
   int32_t have_diffuse;   // time_diffuse valid
   int32_t err;            // device error word (A3G_ERR_*), first error wins
   int32_t err_info;       // where it happened
@@ -104,6 +106,11 @@ struct a3g_ctx {
   bool dtv_valid;
   uint64_t dt_stamp, dtv_stamp;  // dt_stamp changes whenever dt may have changed
   a3g::Geo4 vf;
+  // FAST_DT: max over grains of |vf_meso_next_step_sp| (m/s, FP32), one value
+  // when it is the same in every cell, else per cell (nx*ny*nz, i fastest)
+  float vfm_sp_const;
+  float *vfm_sp;
+  bool have_vf_meso;
   double *dz_vec;           // (-1:nz+2) on device
   std::vector<double> h_dz; // host copy
   // outflow accumulators, interior only: yz (ns,nz,ny), xz (ns,nz,nx), xy (ns,ny,nx)
@@ -229,7 +236,9 @@ int launch_diffcn_z(a3g_ctx *ctx);
 int launch_cfl(a3g_ctx *ctx, double time, double next_write_time, double simtime);
 int launch_cfl_maxima(a3g_ctx *ctx);
 int launch_dt_from_maxima(a3g_ctx *ctx, int n_gs_aloft, double time, double next_write_time,
-                          double simtime);
+                          double simtime, int meso = 0);
+int launch_cfl_maxima_meso(a3g_ctx *ctx, int slot);
+int launch_fast_dt(a3g_ctx *ctx, double frac, double time, double next_write_time, double simtime);
 int launch_totals(a3g_ctx *ctx, double *out4, double *mass_aloft);
 int launch_plane_flags(a3g_ctx *ctx);
 int launch_interp_winds(a3g_ctx *ctx, double frac);

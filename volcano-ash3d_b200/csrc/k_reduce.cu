@@ -122,10 +122,14 @@ __global__ void __launch_bounds__(256) k_diff_limit(Layout L, Geo3 snx, Geo3 sny
 }
 
 // dt arithmetic, src/Adjust_dt.f90:176-179 and :288-332.
+// meso (FAST_DT, Adjust_DT(mesostep=.true.)): bit 1 first copies
+// dt_meso_next to dt_meso_last (the toggle of src/MesoInterpolater.f90:187),
+// bit 0 stores the dt formed here as dt_meso_next (src/Adjust_dt.f90:335-337).
 __global__ void k_dt_finalize(int latlon, int use_diffusion, int use_cn, int n_gs_aloft, double dx,
                               double dy, double cfl, double dt_min, double dt_max, double imp_dt_fac,
                               double eps_small, double time, double next_write_time,
-                              double simtime, int diff_fresh, DevScalars *sc) {
+                              double simtime, int diff_fresh, int meso, DevScalars *sc) {
+  if (meso & 2) sc->dt_meso_last = sc->dt_meso_next;
   double vx_dx = sc->vmax[0], vy_dy = sc->vmax[1], vz_dz = sc->vmax[2];
   if (!latlon) {
     vx_dx = vx_dx / dx;
@@ -156,6 +160,92 @@ __global__ void k_dt_finalize(int latlon, int use_diffusion, int use_cn, int n_g
   if ((next_write_time - time) > eps_small && (next_write_time - time) < dt) dt = next_write_time - time;
   if (time + dt > simtime) dt = simtime - time;
   sc->dt = dt;
+  if (meso & 1) sc->dt_meso_next = dt;
+}
+
+// Adjust_DT(mesostep=.true.), the FAST_DT branch of src/Adjust_dt.f90:96-135:
+// the maxima over the FP32 met step `vx,vy,vz` (m/s, [k][j][i] without
+// padding), widened and scaled as the reference writes them:
+//   projected: real(max|vx_sp|)*3.6 (divided by dx in k_dt_finalize);
+//   lon/lat:   real(|vx_sp|)*3.6*minsig/kappa per cell;
+//   vertical:  real(|vz_sp| + max_g|vf_sp|)*3.6/dz_k, the sum in FP32.
+// real(.)*3.6 is monotone, so the projected maximum of the scaled cells is the
+// scaled maximum.  vfm: max_g |vf_meso_next_step_sp| per cell, or null for
+// the single value vfm0.
+__global__ void __launch_bounds__(256) k_cfl_meso(Layout L, int latlon, const float *__restrict__ vx,
+                                                  const float *__restrict__ vy, const float *__restrict__ vz,
+                                                  const float *__restrict__ vfm, float vfm0, Geo3 snx, Geo3 sny,
+                                                  Geo3 kap, const double *__restrict__ dz_vec, DevScalars *sc) {
+  const int nrow = L.ny * L.nz;
+  double m0 = 0.0, m1 = 0.0, m2 = 0.0;
+  for (int r = blockIdx.x; r < nrow; r += gridDim.x) {
+    const int j = r % L.ny + 1, k = r / L.ny + 1;
+    const double rdz = dz_vec[k + 1];
+    const long rb = (long)r * L.nx;
+    for (int i = threadIdx.x + 1; i <= L.nx; i += blockDim.x) {
+      const long c = rb + (i - 1);
+      const double ax = (double)fabsf(vx[c]) * 3.6, ay = (double)fabsf(vy[c]) * 3.6;
+      double t1, t2;
+      if (latlon) {
+        const double kp = kap.at(i, j, k);
+        t1 = ax * fmn(snx.at(i, j, k), snx.at(i + 1, j, k)) / kp;
+        t2 = ay * fmn(sny.at(i, j, k), sny.at(i, j + 1, k)) / kp;
+      } else {
+        t1 = ax;
+        t2 = ay;
+      }
+      const float s = __fadd_rn(fabsf(vz[c]), vfm ? vfm[c] : vfm0);
+      const double t3 = (double)s * 3.6 / rdz;
+      if (t1 > m0) m0 = t1;
+      if (t2 > m1) m1 = t2;
+      if (t3 > m2) m2 = t3;
+    }
+  }
+  m0 = warp_max(m0);
+  m1 = warp_max(m1);
+  m2 = warp_max(m2);
+  if ((threadIdx.x & 31) == 0) {
+    atomic_max_pos(&sc->vmax[0], m0);
+    atomic_max_pos(&sc->vmax[1], m1);
+    atomic_max_pos(&sc->vmax[2], m2);
+  }
+}
+
+// The FAST_DT step dt of src/MesoInterpolater.f90:250-258: interpolated
+// between the met steps' dt (no DT_MIN rounding), then clipped to the next
+// write time and the end of the simulation.
+__global__ void k_fast_dt(double frac, double eps_small, double time, double next_write_time, double simtime,
+                          DevScalars *sc) {
+  const double last = sc->dt_meso_last, next = sc->dt_meso_next;
+  double dt = last + (next - last) * frac;
+  if ((next_write_time - time) > eps_small && (next_write_time - time) < dt) dt = next_write_time - time;
+  if (time + dt > simtime) dt = simtime - time;
+  sc->dt = dt;
+}
+
+int launch_cfl_maxima_meso(a3g_ctx *ctx, int slot) {
+  const Layout &L = ctx->L;
+  A3G_CUDA(cudaMemsetAsync(ctx->sc->vmax, 0, sizeof(ctx->sc->vmax), ctx->stream));
+  const long n = ctx->met_n;
+  const float *m = ctx->met + (size_t)3 * n * (slot == 0 ? ctx->met_last : ctx->met_next);
+  const long ncell = (long)L.nx * L.ny * L.nz;
+  int blocks = (int)((ncell + 255) / 256);
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  tbegin(ctx, A3G_K_CFL);
+  k_cfl_meso<<<blocks, 256, 0, ctx->stream>>>(L, ctx->grid.latlon, m, m + n, m + 2 * n, ctx->vfm_sp,
+                                              ctx->vfm_sp_const, ctx->snx, ctx->sny, ctx->kappa, ctx->dz_vec,
+                                              ctx->sc);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  return A3G_OK;
+}
+
+int launch_fast_dt(a3g_ctx *ctx, double frac, double time, double next_write_time, double simtime) {
+  tbegin(ctx, A3G_K_OTHER);
+  k_fast_dt<<<1, 1, 0, ctx->stream>>>(frac, ctx->prm.eps_small, time, next_write_time, simtime, ctx->sc);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  return A3G_OK;
 }
 
 int launch_cfl_maxima(a3g_ctx *ctx) {
@@ -174,7 +264,7 @@ int launch_cfl_maxima(a3g_ctx *ctx) {
 
 // dt from maxima already in sc->vmax (local, or set from an all-reduce).
 int launch_dt_from_maxima(a3g_ctx *ctx, int n_gs_aloft, double time, double next_write_time,
-                          double simtime) {
+                          double simtime, int meso) {
   const Layout &L = ctx->L;
   const long ncell = (long)L.nx * L.ny * L.nz;
   int blocks = (int)((ncell + 255) / 256);
@@ -196,7 +286,7 @@ int launch_dt_from_maxima(a3g_ctx *ctx, int n_gs_aloft, double time, double next
   k_dt_finalize<<<1, 1, 0, ctx->stream>>>(
       ctx->grid.latlon, ctx->prm.use_diffusion, ctx->prm.use_cn, n_gs_aloft, ctx->grid.dx,
       ctx->grid.dy, ctx->prm.cfl, ctx->prm.dt_min, ctx->prm.dt_max, ctx->prm.imp_dt_fac,
-      ctx->prm.eps_small, time, next_write_time, simtime, fresh, ctx->sc);
+      ctx->prm.eps_small, time, next_write_time, simtime, fresh, meso, ctx->sc);
   tend(ctx);
   A3G_LAUNCH_CHECK(ctx);
   return A3G_OK;
@@ -230,7 +320,7 @@ int launch_cfl(a3g_ctx *ctx, double time, double next_write_time, double simtime
   k_dt_finalize<<<1, 1, 0, ctx->stream>>>(
       ctx->grid.latlon, ctx->prm.use_diffusion, ctx->prm.use_cn, ctx->n_gs_aloft, ctx->grid.dx,
       ctx->grid.dy, ctx->prm.cfl, ctx->prm.dt_min, ctx->prm.dt_max, ctx->prm.imp_dt_fac,
-      ctx->prm.eps_small, time, next_write_time, simtime, fresh, ctx->sc);
+      ctx->prm.eps_small, time, next_write_time, simtime, fresh, 0, ctx->sc);
   tend(ctx);
   A3G_LAUNCH_CHECK(ctx);
   return A3G_OK;

@@ -197,20 +197,53 @@ def next_write_time(write_times, time: float) -> float:
     return 1.0 / 1.0e-6
 
 
+def met_hour(st: RunState) -> int:
+    """MR_iMetStep_Now for the current time (hourly met steps): the interval
+    holding the time at the first call (H(i) <= t < H(i+1),
+    src/MesoInterpolater.f90:122-129), then one interval ahead whenever the
+    time has moved strictly past the interval's end (t > H(now+1), :135-145),
+    so a time landing exactly on an hour still interpolates the old pair at
+    Interval_Frac = 1."""
+    if st.hour < 0:
+        return int(math.floor(st.time))
+    return st.hour + 1 if st.time > st.hour + 1 else st.hour
+
+
 def update_met(model, st: RunState, h: int):
     """The met pair for hour h.  Crossing into the next hour advances onto the
     step prefetched an hour earlier (Read_NextMesoStep's toggle,
     src/MesoInterpolater.f90:168-199); any other jump uploads the pair.  The
-    step after next is then prefetched on the copy stream."""
+    step after next is then prefetched on the copy stream.  Returns "advance",
+    "pair" or None (no load)."""
     if h == st.hour:
-        return
+        return None
     if st.hour >= 0 and h == st.hour + 1 and st.met_ahead == h + 1:
         model.advance_met_step()
+        loaded = "advance"
     else:
         model.set_met_steps(st.met.step(h), st.met.step(h + 1))
+        loaded = "pair"
     st.hour = h
     model.prefetch_met_step(st.met.step(h + 2))
     st.met_ahead = h + 2
+    return loaded
+
+
+def meso_dt(model, st: RunState, loaded: str, next_write_time: float, simtime: float,
+            comm: Comm | None = None, n_gs_aloft_total: int | None = None, wait: bool = True):
+    """FAST_DT's Adjust_DT(mesostep=.true.) calls at a met-step load
+    (src/MesoInterpolater.f90:142-150 on the first load: the last step, then
+    dt_meso_last = dt_meso_next and the next step; :187-195 at every later
+    load: dt_meso_last = dt_meso_next, then the next step).  A grain-sharded
+    run takes the maxima's MAX over the ranks once per load; the per-step dt
+    then needs no exchange."""
+    loads = ((0, False), (1, True)) if loaded == "pair" else ((1, True),)
+    for slot, shift in loads:
+        if comm is None:
+            model.adjust_dt_meso(slot, shift, st.time, next_write_time, simtime, wait=wait)
+        else:
+            vmax = comm.max(model.cfl_maxima_meso(slot))
+            model.adjust_dt_meso_from_maxima(vmax, n_gs_aloft_total, shift, st.time, next_write_time, simtime)
 
 
 def step(model, st: RunState, simtime: float | None = None, totals: bool = True,
@@ -224,9 +257,12 @@ def step(model, st: RunState, simtime: float | None = None, totals: bool = True,
     nwt = next_write_time(write_times, st.time) if write_times is not None else simtime
     st.itime += 1
     model.step_prologue()
-    h = int(math.floor(st.time))
-    update_met(model, st, h)
-    model.interp_winds(st.time - h)
+    h = met_hour(st)
+    loaded = update_met(model, st, h)
+    if cfg.fast_dt and loaded:
+        meso_dt(model, st, loaded, nwt, simtime, comm, n_gs_aloft_total)
+    frac = st.time - h  # Interval_Frac (hourly met steps)
+    model.interp_winds(frac)
 
     def adjust_dt():
         if comm is None:
@@ -234,15 +270,21 @@ def step(model, st: RunState, simtime: float | None = None, totals: bool = True,
         vmax = comm.max(model.cfl_maxima())
         return model.adjust_dt_from_maxima(vmax, n_gs_aloft_total, st.time, nwt, simtime)
 
-    if st.umbrella is not None and st.time < cfg.duration_h:  # src/MesoInterpolater.f90:233-248
+    def fast_dt():
+        return model.fast_dt(frac, st.time, nwt, simtime)
+
+    # FastDt_suppress while the umbrella spreads (src/MesoInterpolater.f90:233-248)
+    suppress = st.umbrella is not None and st.time < cfg.duration_h
+    if suppress:
         if st.prev_dt is None:
-            # before the time loop Adjust_DT ran on the winds without the
-            # umbrella's (e_EndTime is still 0 then), src/Ash3d.F90:301,354
-            st.prev_dt = adjust_dt()
+            # before the time loop MesoInterpolater ran on the winds without
+            # the umbrella's (e_EndTime is still 0 then, src/Ash3d.F90:301,354),
+            # so its dt is the FAST_DT one when FAST_DT is on
+            st.prev_dt = fast_dt() if cfg.fast_dt else adjust_dt()
         w = syn.umbrella_winds(cfg, st.time, st.prev_dt)
         if w is not None:
             model.add_umbrella_winds(*w)
-    dt = adjust_dt()
+    dt = fast_dt() if (cfg.fast_dt and not suppress) else adjust_dt()
     st.prev_dt = dt
     frac = syn.pulse_fraction(cfg, st.time, dt)
     if frac > 0.0:
@@ -300,10 +342,16 @@ class Pipeline:
         nwt = next_write_time(write_times, st.time) if write_times is not None else simtime
         st.itime += 1
         m.step_prologue()
-        h = int(math.floor(st.time))
-        update_met(m, st, h)
-        m.interp_winds(st.time - h)
-        m.adjust_dt_async(st.time, nwt, simtime)
+        h = met_hour(st)
+        loaded = update_met(m, st, h)
+        if cfg.fast_dt and loaded:
+            meso_dt(m, st, loaded, nwt, simtime, wait=False)
+        frac = st.time - h
+        m.interp_winds(frac)
+        if cfg.fast_dt:
+            m.fast_dt_async(frac, st.time, nwt, simtime)
+        else:
+            m.adjust_dt_async(st.time, nwt, simtime)
         m.add_source_scheduled(st.time)
         m.Set_BC(1)
         m.AdvectHorz(st.itime)

@@ -191,6 +191,20 @@
           real(c_double), value :: time, nwt, simtime
           real(c_double), intent(out) :: dt
         end function
+        integer(c_int) function a3g_set_fall_velocity_meso(ctx, vf, per_grain) &
+            bind(C, name="a3g_set_fall_velocity_meso")
+          import :: c_int, c_ptr, c_int32_t
+          type(c_ptr), value :: ctx, vf
+          integer(c_int32_t), value :: per_grain
+        end function
+        integer(c_int) function a3g_adjust_dt_meso(ctx, slot, shift, time, nwt, simtime, dt) &
+            bind(C, name="a3g_adjust_dt_meso")
+          import :: c_int, c_ptr, c_int32_t, c_double
+          type(c_ptr), value :: ctx
+          integer(c_int32_t), value :: slot, shift
+          real(c_double), value :: time, nwt, simtime
+          real(c_double), intent(out) :: dt
+        end function
         integer(c_int) function a3g_timestep_totals(ctx, out4, mass) bind(C, name="a3g_timestep_totals")
           import :: c_int, c_ptr
           type(c_ptr), value :: ctx, out4, mass
@@ -309,13 +323,35 @@
         call B200_Check(a3g_set_winds(b200_ctx, c_loc(vx_pd), c_loc(vy_pd), c_loc(vz_pd)), "a3g_set_winds")
       end subroutine B200_SetWinds
 
-      ! device interpolation: upload the bracketing FP32 met steps once per met step ...
+      ! device interpolation: upload the bracketing FP32 met steps once per met
+      ! step, right after each call of Read_NextMesoStep in MesoInterpolater
+      ! (src/MesoInterpolater.f90:142 and :189), so that FAST_DT's
+      ! Adjust_DT(.true.) that follows it reads them on the device.  The met
+      ! steps' fall velocities go with them: per cell when a fall model fills
+      ! vf_meso_next_step_sp (useCalcFallVel), else the input file's
+      ! real(Tephra_v_s, sp), which Read_NextMesoStep puts in every cell
+      ! (:567-574).
       subroutine B200_SetMetSteps
+        use global_param, only : useCalcFallVel
+        use mesh,      only : nsmax
+        use Tephra,    only : Tephra_v_s
         use wind_grid, only : vx_meso_last_step_sp, vy_meso_last_step_sp, vz_meso_last_step_sp, &
-                              vx_meso_next_step_sp, vy_meso_next_step_sp, vz_meso_next_step_sp
+                              vx_meso_next_step_sp, vy_meso_next_step_sp, vz_meso_next_step_sp, &
+                              vf_meso_next_step_sp
+        real(c_float), allocatable, target :: vs(:)
         call B200_Check(a3g_set_met_steps(b200_ctx, c_loc(vx_meso_last_step_sp), c_loc(vy_meso_last_step_sp), &
                         c_loc(vz_meso_last_step_sp), c_loc(vx_meso_next_step_sp), &
                         c_loc(vy_meso_next_step_sp), c_loc(vz_meso_next_step_sp)), "a3g_set_met_steps")
+        if (useCalcFallVel) then
+          call B200_Check(a3g_set_fall_velocity_meso(b200_ctx, c_loc(vf_meso_next_step_sp), 0_c_int32_t), &
+                          "a3g_set_fall_velocity_meso")
+        else
+          allocate(vs(nsmax))
+          vs = real(Tephra_v_s(1:nsmax), c_float)
+          call B200_Check(a3g_set_fall_velocity_meso(b200_ctx, c_loc(vs), 1_c_int32_t), &
+                          "a3g_set_fall_velocity_meso")
+          deallocate(vs)
+        endif
       end subroutine B200_SetMetSteps
 
       ! ... and interpolate on the device every step (src/MesoInterpolater.f90:207-223)
@@ -480,22 +516,55 @@
         use time_data, only : time, dt, dt_ip, dt_meso_next, Simtime_in_hours
         logical, intent(in), optional :: mesostep
         real(c_double) :: dtn
-        ! FAST_DT's met-step estimate (mesostep=.true.) uses the same device maxima
-        call B200_Check(a3g_adjust_dt(b200_ctx, real(time, c_double), real(NextWriteTime, c_double), &
-                        real(Simtime_in_hours, c_double), dtn), "Adjust_DT")
-        dt = dtn
-        dt_ip = dtn
-        if (present(mesostep)) then
-          if (mesostep) dt_meso_next = dt
+        logical :: meso
+        meso = .false.
+        if (present(mesostep)) meso = mesostep
+        if (meso) then
+          ! FAST_DT (src/Adjust_dt.f90:96-135): the maxima of the FP32 next met
+          ! step, uploaded by B200_SetMetSteps right after Read_NextMesoStep;
+          ! MesoInterpolater keeps dt_meso_last and does the per-step
+          ! interpolation (src/MesoInterpolater.f90:250-258) itself
+          call B200_Check(a3g_adjust_dt_meso(b200_ctx, 1_c_int32_t, 0_c_int32_t, real(time, c_double), &
+                          real(NextWriteTime, c_double), real(Simtime_in_hours, c_double), dtn), "Adjust_DT")
+          dt = dtn
+          dt_ip = dtn
+          dt_meso_next = dt
+        else
+          call B200_Check(a3g_adjust_dt(b200_ctx, real(time, c_double), real(NextWriteTime, c_double), &
+                          real(Simtime_in_hours, c_double), dtn), "Adjust_DT")
+          dt = dtn
+          dt_ip = dtn
         endif
       end subroutine Adjust_DT
 
       subroutine TimeStepTotals(itime)
         use iso_c_binding
         use B200_Transport
-        use solution, only : aloft_vol, dep_vol, outflow_vol, tot_vol, mass_aloft
+        use io_units
+        use io_data,     only : OutputStep_Marker
+        use solution,    only : aloft_vol, dep_vol, outflow_vol, tot_vol, mass_aloft, SourceCumulativeVol
+        use time_data,   only : time, SimStartHour, Simtime_in_hours, BaseYear, useLeap
+        use Output_Vars, only : CloudArea
         integer, intent(in) :: itime
         real(c_double), target :: out4(4)
+        character(len=13) :: DateTime
+        interface
+          character (len=13) function HS_yyyymmddhhmm_since(HoursSince,byear,useLeaps)
+            real(kind=8) :: HoursSince
+            integer      :: byear
+            logical      :: useLeaps
+          end function HS_yyyymmddhhmm_since
+        end interface
         call B200_Check(a3g_timestep_totals(b200_ctx, c_loc(out4), c_loc(mass_aloft)), "TimeStepTotals")
         aloft_vol = out4(1); dep_vol = out4(2); outflow_vol = out4(3); tot_vol = out4(4)
+        ! the per-log-step line and progress.txt of src/TimeStepTotals.f90:69-82
+        DateTime = HS_yyyymmddhhmm_since(time+SimStartHour, BaseYear, useLeap)
+        do io=1,2;if(VB(io).le.verbosity_info)then
+          write(outlog(io),'(6x,i6,a1,f11.3,3x,a,5f12.5,f13.1)') itime, OutputStep_Marker, time, DateTime, &
+                SourceCumulativeVol, dep_vol, aloft_vol, outflow_vol, tot_vol, CloudArea
+        endif;enddo
+        open(unit=fid_progress, file='progress.txt', status='replace', action='write')
+        write(fid_progress,*) real(time/Simtime_in_hours, kind=4)
+        close(fid_progress)
+        OutputStep_Marker = ' '
       end subroutine TimeStepTotals

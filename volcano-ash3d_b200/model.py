@@ -48,6 +48,7 @@ class Ash3dGPU:
         check(lib.a3g_set_diffusivity(self.ctx, dptr(kx), dptr(ky), dptr(kz)))
         self._vf = syn.fall_velocity(cfg)
         check(lib.a3g_set_fall_velocity(self.ctx, dptr(self._vf)))
+        self.set_fall_velocity_meso(syn.fall_velocity_meso(cfg), per_grain=True)
         self._dt = 0.0
         if syn.use_topo(cfg):
             self.set_topo(**syn.topo_fields(cfg))
@@ -144,6 +145,47 @@ class Ash3dGPU:
     def set_dt(self, dt: float):
         self._dt = dt
         check(self.lib.a3g_set_dt(self.ctx, dt))
+
+    # --- FAST_DT: Adjust_DT(mesostep=.true.) at met-step loads, the
+    #     interpolated dt every step (src/MesoInterpolater.f90:142-150,187-195,
+    #     250-258) ----------------------------------------------------------
+    def set_fall_velocity_meso(self, vf_sp, per_grain: bool = True):
+        a = np.asfortranarray(vf_sp, dtype=np.float32)
+        check(self.lib.a3g_set_fall_velocity_meso(self.ctx, fptr(a), 1 if per_grain else 0))
+
+    def cfl_maxima_meso(self, slot: int) -> np.ndarray:
+        v = np.zeros(3)
+        check(self.lib.a3g_cfl_maxima_meso(self.ctx, slot, dptr(v)))
+        return v
+
+    def adjust_dt_meso(self, slot: int, shift: bool, time: float, next_write_time: float, simtime: float,
+                       wait: bool = True):
+        """Adjust_DT(mesostep=.true.) on met slot 0 (last) or 1 (next); the
+        result is dt_meso_next on the device.  With wait=False nothing is
+        read back (returns None)."""
+        if not wait:
+            check(self.lib.a3g_adjust_dt_meso(self.ctx, slot, 1 if shift else 0, time, next_write_time,
+                                              simtime, None))
+            return None
+        out = C.c_double()
+        check(self.lib.a3g_adjust_dt_meso(self.ctx, slot, 1 if shift else 0, time, next_write_time, simtime,
+                                          C.byref(out)))
+        return out.value
+
+    def adjust_dt_meso_from_maxima(self, vmax3, n_gs_aloft_total: int, shift: bool, time: float,
+                                   next_write_time: float, simtime: float) -> float:
+        v = np.ascontiguousarray(vmax3, dtype=np.float64)
+        out = C.c_double()
+        check(self.lib.a3g_adjust_dt_meso_from_maxima(self.ctx, dptr(v), n_gs_aloft_total, 1 if shift else 0,
+                                                      time, next_write_time, simtime, C.byref(out)))
+        return out.value
+
+    def fast_dt_async(self, frac: float, time: float, next_write_time: float, simtime: float):
+        check(self.lib.a3g_fast_dt_async(self.ctx, frac, time, next_write_time, simtime))
+
+    def fast_dt(self, frac: float, time: float, next_write_time: float, simtime: float) -> float:
+        self.fast_dt_async(frac, time, next_write_time, simtime)
+        return self.wait_dt()
 
     def TimeStepTotals(self):
         out = np.zeros(4)

@@ -83,6 +83,7 @@ class Config:
     sounding: tuple = ()     # 'sounding': ((z_m, u_mps, v_mps), ...) of a 1-D wind profile
     seed: int = 1
     fast_subgrid: bool = False
+    fast_dt: bool = False    # FAST_DT: dt from the met steps, interpolated every step
     magma_density: float = 2500.0
     source_type: str = "suzuki"   # 'suzuki', 'umbrella', 'umbrella_air' (lon/lat grids; suzuki_a 12)
     zscaling_id: int = 0     # ZScaling_ID: 0 s = z, 1 shifted by topography, 2 scaled (sigma-altitude)
@@ -370,6 +371,14 @@ def fall_velocity(cfg: Config) -> np.ndarray:
     for g in range(cfg.ns):
         vf[:, :, :, g] = (-1.0 * cfg.fall_mps[g]) * MPS_2_KMPHR
     return vf
+
+
+def fall_velocity_meso(cfg: Config) -> np.ndarray:
+    """vf_meso_next_step_sp per grain: real(Tephra_v_s(isize), sp) with
+    Tephra_v_s = -v_s (m/s), which Read_NextMesoStep puts in every cell when
+    the fall velocities come from the input file (MesoInterpolater.f90:
+    567-574)."""
+    return np.array([-1.0 * v for v in cfg.fall_mps], dtype=np.float32)
 
 
 # ---------------------------------------------------------------------------
