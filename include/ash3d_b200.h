@@ -465,6 +465,66 @@ int a3g_snapshot_alloc(a3g_ctx *ctx, int32_t nslots);
 int a3g_snapshot_save(a3g_ctx *ctx, int32_t slot);
 int a3g_snapshot_load(a3g_ctx *ctx, int32_t slot);
 
+/* ---- source inversion over a whole run: forward/adjoint pair (no counterpart
+ *      in the reference, which runs forward only) ----
+ * The control p is the erupted mass rate (kg/h) per model level, hourly bin
+ * and grain bin, Fortran order (nz, nbins, ns), inserted at the vent column
+ * as src/Ash3d.F90:428-431 inserts SourceNodeFlux: concen(ivent,jvent,k,g)
+ * += dt*p(k,bin,g)/kappa(ivent,jvent,k), bin = the hour the step starts in.
+ * Observations: the unmasked column load (CloudLoad, src/Output_Vars.f90:
+ * 1061-1069, tonnes/km^2) at the end of every hour, (nx,ny) per hour, and the
+ * deposit thickness (AshThicknessCalculator, src/Output_Vars.f90:880-884, mm,
+ * unmasked) accumulated after hour dep_from, (nx,ny).  Misfit:
+ *   J = 1/2 sum_{hours h >= load_from} |load_h - y_h|^2 + 1/2 |dep - y_dep|^2
+ * (either term as `misfit` selects).  The run starts from a clean atmosphere
+ * at time 0; dt is clipped to the next hour so that observations fall on step
+ * ends; FAST_SUBGRID must be off and no terrain or umbrella source bound. */
+#define A3G_MISFIT_LOAD    1
+#define A3G_MISFIT_DEPOSIT 2
+typedef struct a3g_inv_desc {
+  int32_t ivent, jvent;      /* vent column (1-based) */
+  int32_t nbins;             /* hourly source bins of the control */
+  int32_t misfit;            /* A3G_MISFIT_LOAD | A3G_MISFIT_DEPOSIT */
+  int32_t fast_dt;           /* 1: FAST_DT (met-step dt interpolated), 0: Adjust_DT every step */
+  int32_t load_from;         /* first observed hour of the column loads (0-based) */
+  int32_t dep_from;          /* the deposit misfit counts the deposit laid down after this hour */
+  int32_t pad;
+  double sim_hours;          /* run length, whole hours */
+  double snapshot_bytes;     /* device memory for checkpoints; <= 0: the free memory less 2 GiB */
+} a3g_inv_desc;
+/* Met-step provider: sets three pointers to the FP32 met step of `hour`
+ * (vx, vy, vz; nx*ny*nz, m/s, i fastest) in host memory, valid until the next
+ * call; returns 0, nonzero on failure. */
+typedef int (*a3g_met_provider)(void *user, int32_t hour, const float **vx, const float **vy, const float **vz);
+/* Binds the problem: observations (obs_load: nhours*nx*ny, hour-major;
+ * obs_dep: nx*ny; either may be NULL when its misfit term is off), the met
+ * steps (all copied to the device when they take at most a quarter of the
+ * free memory, else fetched per hour), and the dt of every step, formed here
+ * from the winds alone.  Allocates the adjoint buffers. */
+int a3g_inv_setup(a3g_ctx *ctx, const a3g_inv_desc *desc, a3g_met_provider met, void *user,
+                  const double *obs_load, const double *obs_dep);
+/* The forward run for control p: every step in the reference's order, the
+ * observations, J (J_out may be NULL) and the step count.  Keeps the
+ * checkpoints the reversal starts from: binomial placement under the budget
+ * (with room for every state, every state). */
+int a3g_forward_checkpointed(a3g_ctx *ctx, const double *p, double *J_out, int32_t *nsteps);
+/* The reverse run after a3g_forward_checkpointed: grad (nz, nbins, ns) =
+ * J_obs^T w, the vector-Jacobian product with weights w_load (nhours*nx*ny)
+ * and w_dep (nx*ny) on every observation (both given); NULL weights take the
+ * residuals of the misfit's terms, so that grad = dJ/dp.  Steps between checkpoints are recomputed
+ * on the device; the forward run's checkpoints are spent. */
+int a3g_adjoint(a3g_ctx *ctx, const double *w_load, const double *w_dep, double *grad);
+/* The tangent-linear run: the observations' perturbation for a control
+ * perturbation dp at control p (limiter branches of the run at p). */
+int a3g_tangent_linear(a3g_ctx *ctx, const double *p, const double *dp, double *dloads, double *ddep);
+/* The last run's observations (loads: nhours*nx*ny, dep: nx*ny; either may
+ * be NULL) and stats = {steps, checkpoint slots, forward steps the last
+ * reversal recomputed}. */
+int a3g_inv_observations(a3g_ctx *ctx, double *loads, double *dep, int64_t *stats);
+/* Forward steps the binomial reversal of nsteps steps repeats with nslots
+ * free checkpoint slots, and its first split (host arithmetic only). */
+int a3g_checkpoint_cost(int32_t nsteps, int32_t nslots, int64_t *recomputed, int32_t *first_split);
+
 /* ---- allocation-free entry point (no counterpart in the reference) ---- */
 /* Per-grain airborne mass, sum(c*kappa) over the interior cells, for callers
  * that cannot allocate device memory at the time of the call: hosts that

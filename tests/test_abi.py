@@ -85,12 +85,17 @@ def _header_kinds():
                     and "uint" not in p else "uint64" if re.search(r"\buint64_t\b|\bsize_t\b", p)
                     else "other")
             stars = p.count("*")
+            if re.search(r"\ba3g_met_provider\b", p):  # the met-step callback (a function pointer)
+                kinds.append("fn")
+                continue
             kinds.append("p:p" if stars >= 2 else "p:" + base if stars else base)
         out[m.group(1)] = kinds
     return out
 
 
 def _ctypes_kind(t):
+    if isinstance(t, type) and issubclass(t, C._CFuncPtr):
+        return "fn"
     if t is C.c_void_p:
         return "p:void"
     if hasattr(t, "_type_") and isinstance(t, type) and issubclass(t, C._Pointer):

@@ -191,3 +191,34 @@ def test_source_gradient_matches_finite_differences():
         pm[i] -= h
         fd = (inv.forward(m, pp, obs)[0] - inv.forward(m, pm, obs)[0]) / (2 * h)
         assert abs(g[i] - fd) <= 1e-4 * abs(fd), (i, g[i], fd)
+
+
+@pytest.mark.parametrize("fast_dt", [False, True])
+def test_deposit_misfit_gradient_matches_finite_differences(fast_dt):
+    """dJ/dp with the deposit term (the thickness of the deposit laid down
+    after hour 1, AshThicknessCalculator unmasked) and the column loads of
+    hour 1 on, with FAST_DT off and on, against central differences of J."""
+    from volcano_ash3d_b200 import adjoint as adj
+    cfg = syn.make_config("tiny_proj")
+    inv = adj.SourceInversion(cfg, hours=2)
+    m = orc.OracleModel(cfg, threads=1)
+    zero_dep = np.zeros((cfg.nx, cfg.ny))
+    _, loads, _, _ = inv.forward(m, inv.prior(seed=2, lognormal_sigma=0.5), fast_dt=fast_dt, obs_dep=zero_dep,
+                                 dep_from=1)
+    rng = np.random.default_rng(9)
+    obs = {h: loads[h] * (1 + 0.05 * rng.standard_normal(loads[h].shape)) for h in loads if h != "dep"}
+    obs_dep = loads["dep"] * (1 + 0.05 * rng.standard_normal(loads["dep"].shape))
+    assert np.abs(loads["dep"]).max() > 0.0
+    p = inv.prior()
+    kw = dict(fast_dt=fast_dt, obs_dep=obs_dep, dep_from=1, load_from=1)
+    J, g = inv.gradient(m, p, obs, K=5, **kw)
+    assert J > 0 and np.all(np.isfinite(g))
+    active = np.argwhere(p > 0)
+    for _ in range(6):
+        i = tuple(int(v) for v in active[rng.integers(0, len(active))])
+        h = 1e-4 * p[i]
+        pp, pm = p.copy(), p.copy()
+        pp[i] += h
+        pm[i] -= h
+        fd = (inv.forward(m, pp, obs, **kw)[0] - inv.forward(m, pm, obs, **kw)[0]) / (2 * h)
+        assert abs(g[i] - fd) <= 1e-4 * abs(fd), (i, g[i], fd)

@@ -43,16 +43,24 @@ ADVECTION = ("advect_x", "advect_y", "AdvectVert")
 
 
 def _variants(op):
-    # advection: march / block-4 / block-8; diffusion: the CN x solve
-    # warp-tiled / one thread per line and the y, z solves one / two grains
-    # per thread
-    return (0, 1, 2, 3, 4) if op in ADVECTION else (0, 1, 2)
+    # advection: march / block-4 / block-8 / x warp-tiled / x warp-row / y, z
+    # column march; diffusion: the CN x solve warp-tiled / one thread per line
+    # and the y, z solves one / two grains per thread
+    return (0, 1, 2, 3, 4, 5) if op in ADVECTION else (0, 1, 2)
+
+
+def _adv_variant(d, variant):
+    """The variant a direction takes for a parametrised advection variant:
+    3 and 4 exist for x only, 5 (the column march) for y and z only."""
+    if d == 0:
+        return 4 if variant == 5 else variant
+    return 5 if variant == 5 else min(variant, 2)
 
 
 def _set_variant(gpu, op, variant):
-    if op in ADVECTION:  # variant 3 (warp-tiled) exists for x only
+    if op in ADVECTION:
         for d in range(3):
-            gpu.set_variant(d, variant if d == 0 else min(variant, 2))
+            gpu.set_variant(d, _adv_variant(d, variant))
     else:
         gpu.set_variant(3, variant % 2)
         gpu.set_variant(4, variant)
@@ -115,12 +123,12 @@ def test_timestep_totals(name):
 
 
 @pytest.mark.parametrize("name", CONFIGS)
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
 def test_run_bitwise(name, variant):
     from volcano_ash3d_b200 import driver
     cfg, gpu, ref = pair(name)
     for d in range(3):
-        gpu.set_variant(d, variant if d == 0 else min(variant, 2))
+        gpu.set_variant(d, _adv_variant(d, variant))
     gpu.set_variant(3, variant % 2)
     gpu.set_variant(4, min(variant, 2))
     sg = driver.run(gpu, cfg, max_steps=16)

@@ -20,7 +20,7 @@ def _run(cfg, variant, steps=20):
     geo = syn.geometry(cfg)
     gpu, ref = Ash3dGPU(cfg, geo=geo), orc.OracleModel(cfg, geo=geo)
     for d in range(3):
-        gpu.set_variant(d, variant if d == 0 else min(variant, 2))
+        gpu.set_variant(d, (4 if variant == 5 else variant) if d == 0 else (5 if variant == 5 else min(variant, 2)))
     sg = driver.run(gpu, cfg, max_steps=steps, geo=geo)
     sr = driver.run(ref, cfg, max_steps=steps, geo=geo)
     assert [h.dt for h in sg.history] == [h.dt for h in sr.history]
@@ -35,7 +35,7 @@ def _run(cfg, variant, steps=20):
     return sg
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
 def test_umbrella_run_bitwise(variant):
     sg = _run(syn.make_config("tiny_umbrella"), variant)
     h = sg.history[-1]

@@ -50,6 +50,8 @@ EXPORTED = [
     "a3g_add_source_column_devdt", "a3g_adj_grad_reset", "a3g_adj_vent_accumulate", "a3g_adj_grad_get",
     "a3g_set_fall_velocity_meso", "a3g_cfl_maxima_meso", "a3g_adjust_dt_meso",
     "a3g_adjust_dt_meso_from_maxima", "a3g_fast_dt_async",
+    "a3g_inv_setup", "a3g_forward_checkpointed", "a3g_adjoint", "a3g_tangent_linear",
+    "a3g_inv_observations", "a3g_checkpoint_cost",
 ]
 KERNEL_CLASSES = ["advect_x", "advect_y", "advect_z", "diff_x", "diff_y", "diff_z", "cn_table",
                   "cn_solve_x", "cn_solve_y", "cn_solve_z", "cfl", "totals", "winds", "other",
@@ -65,6 +67,17 @@ class A3GError(RuntimeError):
 class GridDesc(C.Structure):
     _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("ns", C.c_int32),
                 ("periodic", C.c_int32), ("latlon", C.c_int32), ("dx", C.c_double), ("dy", C.c_double)]
+
+
+class InvDesc(C.Structure):
+    _fields_ = [("ivent", C.c_int32), ("jvent", C.c_int32), ("nbins", C.c_int32), ("misfit", C.c_int32),
+                ("fast_dt", C.c_int32), ("load_from", C.c_int32), ("dep_from", C.c_int32), ("pad", C.c_int32),
+                ("sim_hours", C.c_double), ("snapshot_bytes", C.c_double)]
+
+
+MISFIT_LOAD, MISFIT_DEPOSIT = 1, 2
+FP = C.POINTER(C.c_float)
+MET_PROVIDER = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.POINTER(FP), C.POINTER(FP), C.POINTER(FP))
 
 
 class Params(C.Structure):
@@ -159,6 +172,12 @@ def load(path: os.PathLike | str | None = None) -> C.CDLL:
         "a3g_adjust_dt_meso_from_maxima": (C.c_int, [P, D, C.c_int32, C.c_int32, C.c_double, C.c_double,
                                                      C.c_double, D]),
         "a3g_fast_dt_async": (C.c_int, [P, C.c_double, C.c_double, C.c_double, C.c_double]),
+        "a3g_inv_setup": (C.c_int, [P, C.POINTER(InvDesc), MET_PROVIDER, C.c_void_p, D, D]),
+        "a3g_forward_checkpointed": (C.c_int, [P, D, D, C.POINTER(C.c_int32)]),
+        "a3g_adjoint": (C.c_int, [P, D, D, D]),
+        "a3g_tangent_linear": (C.c_int, [P, D, D, D, D]),
+        "a3g_inv_observations": (C.c_int, [P, D, D, C.POINTER(C.c_int64)]),
+        "a3g_checkpoint_cost": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
         "a3g_get_minmax_index": (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, I]),
         "a3g_set_subgrid": (C.c_int, [P, I]),
         "a3g_get_subgrid": (C.c_int, [P, I]),

@@ -17,7 +17,7 @@ import sys
 
 HERE = pathlib.Path(__file__).resolve().parent
 SRCS = ["k_advect_x.cu", "k_advect_y.cu", "k_advect_z.cu", "k_advect.cu", "k_diffuse.cu", "k_reduce.cu",
-        "a3g_api.cu", "a3g_noalloc.cu"]
+        "a3g_api.cu", "a3g_inverse.cu", "a3g_noalloc.cu"]
 OUT = HERE / "libash3d_b200.so"
 OBJ_DIR = HERE / "_build"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -265,6 +265,7 @@ int a3g_destroy(a3g_ctx *ctx) {
   if (!ctx) return A3G_OK;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  inv_free(ctx);
   if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
   double *dptrs[] = {ctx->c0, ctx->c1, ctx->vx, ctx->vy, ctx->vz, ctx->out_yz1, ctx->out_yz2,
                      ctx->out_xz1, ctx->out_xz2, ctx->out_xy1, ctx->out_xy2, ctx->red_buf,
@@ -1301,7 +1302,8 @@ int a3g_kernel_times(a3g_ctx *ctx, double *ms, uint64_t *count) {
 
 int a3g_set_variant(a3g_ctx *ctx, int32_t dir, int32_t variant) {
   if (!ctx) return fail(A3G_ERR_ARG, "null context");
-  if (dir < 0 || dir > 4 || variant < 0 || variant > (dir == 0 ? 4 : dir == 3 ? 1 : 2))
+  const bool col = (dir == 1 || dir == 2) && variant == 5;  // the column march (y, z)
+  if (dir < 0 || dir > 4 || variant < 0 || (!col && variant > (dir == 0 ? 4 : dir == 3 ? 1 : 2)))
     return fail(A3G_ERR_ARG, "bad direction or variant");
   if (dir == 3) ctx->tune_cn_x = variant;
   else if (dir == 4) ctx->tune_cn_yz = variant;

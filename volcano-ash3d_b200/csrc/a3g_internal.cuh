@@ -82,6 +82,8 @@ struct DevScalars {
 
 }  // namespace a3g
 
+struct a3g_inv;  // source inversion state (a3g_inverse.cu)
+
 struct a3g_ctx {
   a3g_grid_desc grid;
   a3g_params prm;
@@ -197,6 +199,8 @@ struct a3g_ctx {
   double *umb_buf;
   double *h_umb;
   cudaEvent_t umb_event;
+  // source inversion (a3g_inv_setup)
+  a3g_inv *inv;
   // optional per-kernel timing (a3g_kernel_timing)
   bool timing;
   std::vector<cudaEvent_t> ev_pool;
@@ -238,6 +242,8 @@ int launch_cfl_maxima(a3g_ctx *ctx);
 int launch_dt_from_maxima(a3g_ctx *ctx, int n_gs_aloft, double time, double next_write_time,
                           double simtime, int meso = 0);
 int launch_cfl_maxima_meso(a3g_ctx *ctx, int slot);
+int launch_cfl_maxima_meso_ptr(a3g_ctx *ctx, const float *met_step);
+void inv_free(a3g_ctx *ctx);
 int launch_fast_dt(a3g_ctx *ctx, double frac, double time, double next_write_time, double simtime);
 int launch_totals(a3g_ctx *ctx, double *out4, double *mass_aloft);
 int launch_plane_flags(a3g_ctx *ctx);
@@ -259,6 +265,7 @@ int check_device_error(a3g_ctx *ctx);
 int launch_adj_advect(a3g_ctx *ctx, int dir, const double *cq, const double *lin, double *lout,
                       const double *lam_lo);
 int launch_adj_diffuse(a3g_ctx *ctx, int dir, const double *lin, double *lout);
+int launch_tl_advect(a3g_ctx *ctx, int dir, const double *cq, const double *din, double *dout, double *dep);
 int launch_cloud_load(a3g_ctx *ctx, const double *c, double *out);
 int launch_adj_cloud_load(a3g_ctx *ctx, const double *w, double *lam);
 int launch_vent_column(a3g_ctx *ctx, int ivent, int jvent, const double *lam, double *out);

@@ -245,4 +245,143 @@ int launch_adj_advect(a3g_ctx *ctx, int dir, const double *cq, const double *lin
   return A3G_OK;
 }
 
+// ===========================================================================
+// Tangent-linear of one advection sweep (no counterpart in the reference).
+//
+// The same linear map k_adj_advect transposes: with the limiter branches
+// fixed by the sweep's input state q (lim_coef: ldq = a*dq + b*dqu), a
+// perturbation d of the input goes to
+//   d_fss(I) = cf(I)*(a(I)*dd(I) + b(I)*dd_u(I))   (active fss interfaces)
+//   d_fsr(I) = max(0,us)*dd(I) + d(I)*divu_m(I),  d_fsl(I) = min(0,us)*dd(I) + d(I-1)*divu_p(I)
+//   d_out(m) = d(m) - dt/kappa(m)*(d_fsl(m+1) + d_fsr(m) + d_fss(m+1) - d_fss(m))
+// with dd = the perturbation's slopes and Set_BC(1) ghosts (zero, x-periodic
+// wrap).  The z sweep adds the perturbation of the bottom outflow (the
+// deposit) to dep.  One thread per cell-grain, full box.
+// ===========================================================================
+template <int DIR, int LIM, bool PER>
+__global__ void __launch_bounds__(256) k_tl_advect(Layout L, int nocycle, double eps,
+                                                   const double *__restrict__ cq,
+                                                   const double *__restrict__ din,
+                                                   double *__restrict__ dout,
+                                                   const double *__restrict__ vel, Geo4 vf, Geo3 sig,
+                                                   Geo3 dtvt, const int32_t *__restrict__ aloft,
+                                                   double *__restrict__ dep) {
+  const int i = blockIdx.x * 32 + threadIdx.x + 1;
+  const int j = blockIdx.y * 8 + threadIdx.y + 1;
+  const int k = (int)(blockIdx.z % L.nz) + 1;
+  const int g = (int)(blockIdx.z / L.nz);
+  if (i > L.nx || j > L.ny) return;
+  const long cell = L.cell(i, j, k);
+  const long gb = (long)g * L.PG;
+  if (!aloft[g]) {
+    dout[gb + cell] = 0.0;
+    return;
+  }
+  const int n = (DIR == 0) ? L.nx : (DIR == 1) ? L.ny : L.nz;
+  const int m = (DIR == 0) ? i : (DIR == 1) ? j : k;
+  const long st = (DIR == 0) ? 1 : (DIR == 1) ? L.P : L.PY;
+  const long lb = cell - (long)(m - 1) * st;
+  const int la = (DIR == 0) ? j : i, lo_ = (DIR == 2) ? j : k;
+  const LineGeo gsig = line_of<DIR>(sig, la, lo_);
+  const LineGeo gdtv = line_of<DIR>(dtvt, la, lo_);
+  const double *pq = cq + gb + lb;
+  const double *pd = din + gb + lb;
+  const double *pv = vel + lb;
+  const double *pvf = vf.p + (long)(i + 1) * vf.si + (long)(j + 1) * vf.sj + (long)g * vf.sg;
+  auto wrap = [&](int c) { return c < 1 ? c + n : (c > n ? c - n : c); };
+  auto ghosted = [&](const double *p, int c) -> double {
+    if (c < -1 || c > n + 2) return 0.0;
+    if (c >= 1 && c <= n) return p[(long)(c - 1) * st];
+    return PER ? p[(long)(wrap(c) - 1) * st] : 0.0;
+  };
+  auto V = [&](int c) -> double {
+    const int cl = PER ? wrap(c) : (c < 1 ? 1 : (c > n ? n : c));
+    double v = pv[(long)(cl - 1) * st];
+    if (DIR == 2) v = v + pvf[(long)(cl + 1) * vf.sk];
+    return v;
+  };
+  auto US = [&](int I) -> double {  // usig(I), zero outside [0, n+1]
+    if (I < 0 || I > n + 1) return 0.0;
+    return 0.5 * (V(I - 1) + V(I)) * gsig.at(I);
+  };
+  // d_fss, d_fsr, d_fsl of interface I
+  auto iface = [&](int I, double &dfss, double &dfsr, double &dfsl) {
+    const double us = US(I), usm = US(I - 1), usp = US(I + 1);
+    dfss = 0.0;
+    dfsr = 0.0;
+    dfsl = 0.0;
+    if (I < 0 || I > n + 1) return;
+    const double qm2 = ghosted(pq, I - 2), qm1 = ghosted(pq, I - 1), q0 = ghosted(pq, I), qp1 = ghosted(pq, I + 1);
+    const double dm2 = ghosted(pd, I - 2), dm1 = ghosted(pd, I - 1), d0 = ghosted(pd, I), dp1 = ghosted(pd, I + 1);
+    const double dq = q0 - qm1, ddq = d0 - dm1;
+    const bool up = us > 0.0;
+    if (LIM != A3G_LIM_NONE && I >= 1 && (nocycle || !(fabs(dq) <= eps))) {
+      const double dqu = up ? qm1 - qm2 : qp1 - q0;
+      const double ddqu = up ? dm1 - dm2 : dp1 - d0;
+      double a, b;
+      lim_coef<LIM>(dq, dqu, eps, a, b);
+      const double aus = fabs(us);
+      const double cf = 0.5 * aus * (1.0 - gdtv.at(I) * aus);
+      dfss = cf * (a * ddq + b * ddqu);
+    }
+    const double divm = fmn(0.0, usp) - fmn(0.0, us);
+    const double divp = fmx(0.0, us) - fmx(0.0, usm);
+    dfsr = fmx(0.0, us) * ddq + d0 * divm;
+    dfsl = fmn(0.0, us) * ddq + dm1 * divp;
+  };
+  double fssL, fsrL, fslL, fssR, fsrR, fslR;
+  iface(m, fssL, fsrL, fslL);
+  iface(m + 1, fssR, fsrR, fslR);
+  const double dupd = -(gdtv.at(m) * (fslR + fsrL + fssR - fssL));
+  dout[gb + cell] = pd[(long)(m - 1) * st] + dupd;
+  if (DIR == 2 && dep && m == 1) {  // cell 0 (the bottom outflow): interfaces 0 and 1, fss(0) = 0
+    double fss0, fsr0, fsl0;
+    iface(0, fss0, fsr0, fsl0);
+    const double d0upd = -(gdtv.at(0) * (fslL + fsr0 + fssL - 0.0));
+    dep[(long)g * L.nx * L.ny + (long)(j - 1) * L.nx + (i - 1)] += d0upd;
+  }
+}
+
+template <int DIR, int LIM>
+static void launch_tl_dir_lim(a3g_ctx *ctx, const double *cq, const double *din, double *dout, double *dep) {
+  const Layout &L = ctx->L;
+  dim3 grid((L.nx + 31) / 32, (L.ny + 7) / 8, L.nz * L.ns);
+  const bool per = (DIR == 0) && ctx->grid.periodic;
+  const double *vel = (DIR == 0) ? ctx->vx : (DIR == 1) ? ctx->vy : ctx->vz;
+  const Geo3 &sig = (DIR == 0) ? ctx->snx : (DIR == 1) ? ctx->sny : ctx->snz;
+  if (per)
+    k_tl_advect<DIR, LIM, true><<<grid, dim3(32, 8), 0, ctx->stream>>>(
+        L, ctx->prm.nocycle, ctx->prm.eps_thresh, cq, din, dout, vel, ctx->vf, sig, ctx->dtv, ctx->aloft, dep);
+  else
+    k_tl_advect<DIR, LIM, false><<<grid, dim3(32, 8), 0, ctx->stream>>>(
+        L, ctx->prm.nocycle, ctx->prm.eps_thresh, cq, din, dout, vel, ctx->vf, sig, ctx->dtv, ctx->aloft, dep);
+}
+
+template <int DIR>
+static void launch_tl_dir(a3g_ctx *ctx, const double *cq, const double *din, double *dout, double *dep) {
+  switch (ctx->prm.limiter) {
+    case A3G_LIM_NONE: launch_tl_dir_lim<DIR, A3G_LIM_NONE>(ctx, cq, din, dout, dep); break;
+    case A3G_LIM_LAXWEN: launch_tl_dir_lim<DIR, A3G_LIM_LAXWEN>(ctx, cq, din, dout, dep); break;
+    case A3G_LIM_BW: launch_tl_dir_lim<DIR, A3G_LIM_BW>(ctx, cq, din, dout, dep); break;
+    case A3G_LIM_FROMM: launch_tl_dir_lim<DIR, A3G_LIM_FROMM>(ctx, cq, din, dout, dep); break;
+    case A3G_LIM_MINMOD: launch_tl_dir_lim<DIR, A3G_LIM_MINMOD>(ctx, cq, din, dout, dep); break;
+    case A3G_LIM_MC: launch_tl_dir_lim<DIR, A3G_LIM_MC>(ctx, cq, din, dout, dep); break;
+    default: launch_tl_dir_lim<DIR, A3G_LIM_SUPERBEE>(ctx, cq, din, dout, dep); break;
+  }
+}
+
+// dout <- J(cq) din for the advection sweep along dir; dep (z only, may be
+// null) gains the perturbation of the bottom outflow.
+int launch_tl_advect(a3g_ctx *ctx, int dir, const double *cq, const double *din, double *dout, double *dep) {
+  int rc = refresh_dtv(ctx);
+  if (rc) return rc;
+  tbegin(ctx, A3G_K_ADJOINT);
+  if (dir == 0) launch_tl_dir<0>(ctx, cq, din, dout, nullptr);
+  else if (dir == 1) launch_tl_dir<1>(ctx, cq, din, dout, nullptr);
+  else launch_tl_dir<2>(ctx, cq, din, dout, dep);
+  tend(ctx);
+  A3G_LAUNCH_CHECK(ctx);
+  return A3G_OK;
+}
+
 }  // namespace a3g

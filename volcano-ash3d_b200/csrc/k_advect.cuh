@@ -979,9 +979,6 @@ static void launch_advect_xw(a3g_ctx *ctx) {
 #undef A3G_XW
 }
 
-// ---------------------------------------------------------------------------
-// launchers
-// ---------------------------------------------------------------------------
 // the vertical wind of the z sweep: vz + vh once terrain is bound
 static inline const double *dir_vel(a3g_ctx *ctx, int dir) {
   return (dir == 0) ? ctx->vx : (dir == 1) ? ctx->vy : (ctx->topo_on ? ctx->vzh : ctx->vz);
@@ -990,6 +987,175 @@ static inline const double *dir_vghost(a3g_ctx *ctx, int dir) {
   return (dir == 0) ? ctx->vx : (dir == 1) ? ctx->vy : ctx->vz;
 }
 
+// ---------------------------------------------------------------------------
+// Column march for the y and z sweeps (DIR 1, 2): one thread per line and
+// grain, lanes along i (every load and store a coalesced 256-byte row
+// segment), marching the whole line with a rolling window so that each
+// interface is formed once (the block kernel forms V+1 interfaces for V
+// cells and loads a V+4 window).  Offsets along the line are 32-bit strides
+// from per-line base pointers, the grain's fall speed is loaded once when it
+// is the same in every cell (VFC), and the interior of the line runs without
+// range checks.  The arithmetic of every interface and cell is block_body's
+// (make_iface, fss_select, the fs_r/fs_l order, cell_update), so the results
+// are the same bits.  Not periodic (only x can be), no ZScaling_ID 2 terms.
+// ---------------------------------------------------------------------------
+template <int DIR, int LIM, bool VFC>
+__global__ void __launch_bounds__(128, 5) k_advect_col(Layout L, Box box, int nocycle, double eps,
+                                                    const double *__restrict__ cin,
+                                                    double *__restrict__ cout,
+                                                    const double *__restrict__ vel,
+                                                    const double *__restrict__ vghost, Geo4 vf, Geo3 sig,
+                                                    Geo3 dtvt, const int32_t *__restrict__ aloft,
+                                                    DevScalars *sc, double *__restrict__ out1,
+                                                    double *__restrict__ out2) {
+  static_assert(DIR == 1 || DIR == 2, "lanes along i: y and z sweeps only");
+  const int a = blockIdx.x * 32 + threadIdx.x + 1;  // i
+  const int o = blockIdx.y * 4 + threadIdx.y + 1;   // k (y sweep) or j (z sweep)
+  const int g = blockIdx.z;
+  const int nother = (DIR == 1) ? L.nz : L.ny;
+  if (a > L.nx || o > nother) return;  // no barriers below
+  const int n = (DIR == 1) ? L.ny : L.nz;
+  const int rmin = (DIR == 1) ? box.jmin : box.kmin;
+  const int rmax = (DIR == 1) ? box.jmax : box.kmax;
+  const int ncells = rmax - rmin + 1;
+  const int st = (DIR == 1) ? (int)L.P : (int)L.PY;
+  const long base = (DIR == 1) ? L.cell(a, 1, o) : L.cell(a, o, 1);
+  const bool lane_active = (DIR == 1) ? (a >= box.imin && a <= box.imax && o >= box.kmin && o <= box.kmax)
+                                      : (a >= box.imin && a <= box.imax && o >= box.jmin && o <= box.jmax);
+  const bool al = lane_active && aloft[g] != 0;
+  double *po = cout + (long)g * L.PG + base;
+  if (!al) {  // the reference leaves zeros
+    for (int c = 1; c <= n; c++) po[(c - 1) * st] = 0.0;
+    return;
+  }
+  const double *pq = cin + (long)g * L.PG + base;
+  const double *pv = vel + base;
+  const double *pvg = vghost + base;
+  const LineGeo gsig = line_of<DIR>(sig, a, o);
+  const LineGeo gdtv = line_of<DIR>(dtvt, a, o);
+  // fall speed of this grain along the line (z only): vf(c) at pvf[(c+1)*vfs]
+  const double *pvf = vf.p + (long)(a + 1) * vf.si + (long)(((DIR == 2) ? o : 0) + 1) * vf.sj + (long)g * vf.sg;
+  const long vfs = vf.sk;
+  const double vf0 = (DIR == 2 && VFC) ? pvf[0] : 0.0;
+  const bool out_lo = rmin == 1;
+  const bool out_hi = rmax == n;
+  const int ctop = (DIR == 2) ? ncells + 1 : rmax + 1;  // update_cc(ncells+1) for z (:309-311)
+  if (DIR == 2 && out_hi && ctop < rmin - 1) raise_error(sc, A3G_ERR_UNSUPPORTED, 311);
+  const long na = L.nx;
+  const long oo = (long)g * na * nother + (long)(o - 1) * na + (a - 1);
+  auto fs_ok = [&](int I) { return I >= rmin - 1 && I <= rmax + 1; };
+  auto fss_ok = [&](int I) { return I >= rmin && I <= rmax + 1; };
+  // ghost-aware loads (Set_BC(1): zero concentration, edge winds; the z
+  // ghost levels read the plain vertical wind)
+  auto qload = [&](int c) -> double {
+    return (c >= rmin - 2 && c <= rmax + 2 && c >= 1 && c <= n) ? pq[(c - 1) * st] : 0.0;
+  };
+  auto vload = [&](int c) -> double {
+    const int cl = c < 1 ? 1 : (c > n ? n : c);
+    double v = ((DIR == 2 && (c < 1 || c > n)) ? pvg : pv)[(cl - 1) * st];
+    if (DIR == 2) v = v + (VFC ? vf0 : pvf[(long)(cl + 1) * vfs]);
+    return v;
+  };
+  const int cs = out_lo ? 0 : 1;
+  const int ce = out_hi ? n + 1 : n;
+  // ---- interface cs and the window at cs ----------------------------------
+  double q0 = qload(cs), q1 = qload(cs + 1);
+  double d0 = q0 - qload(cs - 1), d1 = q1 - q0;
+  double usA, usB, vB, dtv0 = gdtv.at(cs), fss0, fsr0;
+  {
+    const double vm2 = vload(cs - 2), vm1 = vload(cs - 1), v0 = vload(cs);
+    vB = vload(cs + 1);
+    const double usm1 = fs_ok(cs - 1) ? 0.5 * (vm2 + vm1) * gsig.at(cs - 1) : 0.0;
+    usA = fs_ok(cs) ? 0.5 * (vm1 + v0) * gsig.at(cs) : 0.0;
+    usB = fs_ok(cs + 1) ? 0.5 * (v0 + vB) * gsig.at(cs + 1) : 0.0;
+    const double qm1 = qload(cs - 1);
+    const double dm = qm1 - qload(cs - 2);
+    const Iface f = make_iface(usm1, usA, usB, dtv0, fss_ok(cs), fs_ok(cs));
+    fss0 = fss_select<LIM>(dm, d0, d1, f.up, f.cf, f.fss_ok, eps, nocycle);
+    fsr0 = f.fs_ok ? (f.usp * d0) + q0 * f.divm : 0.0;
+  }
+  // ---- one step: interface c+1 and the update of cell c --------------------
+  auto step = [&](int c, auto checked, double q2, double vn, double s2, double dtv1) {
+    constexpr bool CK = decltype(checked)::value;
+    const int I = c + 1;
+    const bool fsok2 = !CK || fs_ok(c + 2);
+    const double usC = fsok2 ? 0.5 * (vB + vn) * s2 : 0.0;
+    vB = vn;
+    const Iface f = make_iface(usA, usB, usC, dtv1, !CK || fss_ok(I), !CK || fs_ok(I));
+    usA = usB;
+    usB = usC;
+    const double d2 = q2 - q1;
+    const double fss1 = fss_select<LIM>(d0, d1, d2, f.up, f.cf, f.fss_ok, eps, nocycle);
+    double fsr1 = 0.0, fsl1 = 0.0;
+    if (f.fs_ok) {
+      fsr1 = f.usp * d1;
+      fsl1 = f.usm * d1;
+      fsr1 = fsr1 + q1 * f.divm;
+      fsl1 = fsl1 + q0 * f.divp;
+    }
+    const double upd = cell_update(dtv0, fsl1, fsr0, fss1, fss0);
+    if (!CK || (c >= 1 && c <= n)) {
+      const bool inbox = !CK || (c >= rmin && c <= rmax);
+      po[(c - 1) * st] = inbox ? q0 + upd : 0.0;
+    }
+    if (CK && out_lo && c == 0) out1[oo] += upd;
+    if (out_hi && c == ctop) out2[oo] += upd;
+    fss0 = fss1;
+    fsr0 = fsr1;
+    q0 = q1;
+    q1 = q2;
+    d0 = d1;
+    d1 = d2;
+    dtv0 = dtv1;
+  };
+  auto checked_step = [&](int c) {
+    step(c, CkT{}, qload(c + 2), vload(c + 2), fs_ok(c + 2) ? gsig.at(c + 2) : 0.0, gdtv.at(c + 1));
+  };
+  // steps without range checks: c >= rmin, c+2 <= min(n, rmax+1)
+  int fa = max(cs, rmin), fb = min(n - 2, rmax - 1);
+  if (fb < fa) { fa = ce + 1; fb = ce; }
+  int c = cs;
+  for (; c < fa; c++) checked_step(c);
+  if (fa <= fb) {
+    const double *qn = pq + (fa + 1) * st;   // q(c+2)
+    const double *vn = pv + (fa + 1) * st;   // vel(c+2)
+    const double *sn = gsig.p + (long)(fa + 3) * gsig.s;   // sigma(c+2)
+    const double *dn = gdtv.p + (long)(fa + 2) * gdtv.s;   // dt/kappa(c+1)
+    const double *fn = pvf + (long)(fa + 3) * vfs;         // vf(c+2)
+    const int ss = (int)gsig.s, ds = (int)gdtv.s, fs = (int)vfs;
+#pragma unroll 4
+    for (; c <= fb; c++) {
+      double v = *vn;
+      if (DIR == 2) v = v + (VFC ? vf0 : *fn);
+      step(c, FastT{}, *qn, v, *sn, *dn);
+      qn += st;
+      vn += st;
+      sn += ss;
+      dn += ds;
+      if (DIR == 2 && !VFC) fn += fs;
+    }
+  }
+  for (; c <= ce; c++) checked_step(c);
+}
+
+template <int DIR, int LIM>
+static void launch_col(a3g_ctx *ctx) {
+  const Layout &L = ctx->L;
+  const int nother = (DIR == 1) ? L.nz : L.ny;
+  dim3 grid((L.nx + 31) / 32, (nother + 3) / 4, L.ns);
+  const bool vfc = ctx->vf.si == 0 && ctx->vf.sj == 0 && ctx->vf.sk == 0;
+#define A3G_COL(VFC_)                                                                                     \
+  k_advect_col<DIR, LIM, VFC_><<<grid, dim3(32, 4), 0, ctx->stream>>>(                                  \
+      L, ctx->box, ctx->prm.nocycle, ctx->prm.eps_thresh, ctx->c0, ctx->c1, dir_vel(ctx, DIR),           \
+      dir_vghost(ctx, DIR), ctx->vf, (DIR == 1) ? ctx->sny : ctx->snz, ctx->dtv, ctx->aloft, ctx->sc,    \
+      (DIR == 1) ? ctx->out_xz1 : ctx->out_xy1, (DIR == 1) ? ctx->out_xz2 : ctx->out_xy2)
+  if (DIR == 2 && !vfc) A3G_COL(false); else A3G_COL(true);
+#undef A3G_COL
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
 template <int DIR, int LIM, int GC, bool PER, bool TOPO = false>
 static void launch_march_gc(a3g_ctx *ctx) {
   const Layout &L = ctx->L;
@@ -1054,6 +1220,12 @@ static void launch_dir_lim(a3g_ctx *ctx) {
     }
     if (variant == 4) {
       launch_advect_xw<LIM>(ctx);
+      return;
+    }
+  }
+  if constexpr (DIR != 0) {
+    if (variant == 5) {
+      launch_col<DIR, LIM>(ctx);
       return;
     }
   }

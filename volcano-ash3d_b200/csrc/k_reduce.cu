@@ -224,10 +224,15 @@ __global__ void k_fast_dt(double frac, double eps_small, double time, double nex
 }
 
 int launch_cfl_maxima_meso(a3g_ctx *ctx, int slot) {
+  const long n = ctx->met_n;
+  return launch_cfl_maxima_meso_ptr(ctx, ctx->met + (size_t)3 * n * (slot == 0 ? ctx->met_last : ctx->met_next));
+}
+
+// the maxima over a met step (vx, vy, vz of nx*ny*nz FP32 each) at m
+int launch_cfl_maxima_meso_ptr(a3g_ctx *ctx, const float *m) {
   const Layout &L = ctx->L;
   A3G_CUDA(cudaMemsetAsync(ctx->sc->vmax, 0, sizeof(ctx->sc->vmax), ctx->stream));
-  const long n = ctx->met_n;
-  const float *m = ctx->met + (size_t)3 * n * (slot == 0 ? ctx->met_last : ctx->met_next);
+  const long n = (long)L.nx * L.ny * L.nz;
   const long ncell = (long)L.nx * L.ny * L.nz;
   int blocks = (int)((ncell + 255) / 256);
   if (blocks > 148 * 8) blocks = 148 * 8;

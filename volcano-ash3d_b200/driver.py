@@ -197,16 +197,21 @@ def next_write_time(write_times, time: float) -> float:
     return 1.0 / 1.0e-6
 
 
+def met_interval(time: float, hour: int) -> int:
+    """MR_iMetStep_Now at `time` after interval `hour` (-1 before the first
+    call), hourly met steps: the interval holding the time at the first call
+    (H(i) <= t < H(i+1), src/MesoInterpolater.f90:122-129), then one interval
+    ahead whenever the time has moved strictly past the interval's end
+    (t > H(now+1), :135-145), so a time landing exactly on an hour still
+    interpolates the old pair at Interval_Frac = 1."""
+    if hour < 0:
+        return int(math.floor(time))
+    return hour + 1 if time > hour + 1 else hour
+
+
 def met_hour(st: RunState) -> int:
-    """MR_iMetStep_Now for the current time (hourly met steps): the interval
-    holding the time at the first call (H(i) <= t < H(i+1),
-    src/MesoInterpolater.f90:122-129), then one interval ahead whenever the
-    time has moved strictly past the interval's end (t > H(now+1), :135-145),
-    so a time landing exactly on an hour still interpolates the old pair at
-    Interval_Frac = 1."""
-    if st.hour < 0:
-        return int(math.floor(st.time))
-    return st.hour + 1 if st.time > st.hour + 1 else st.hour
+    """met_interval for a run's state."""
+    return met_interval(st.time, st.hour)
 
 
 def update_met(model, st: RunState, h: int):

@@ -464,6 +464,14 @@ class Ash3dGPU:
         lv[2:c.nx + 2, 2:c.ny + 2, 2:c.nz + 2, :] = q
         self.upload_level(lv)
 
+    def zero_outflows(self):
+        """The outflow accumulators and the deposit back to zero."""
+        c = self.cfg
+        NX, NY, NZ, ns = c.nx + 4, c.ny + 4, c.nz + 4, c.ns
+        z = lambda *s: np.zeros(s, order="F")
+        check(self.lib.a3g_upload_outflow(self.ctx, dptr(z(NY, NZ, ns)), dptr(z(NY, NZ, ns)), dptr(z(NX, NZ, ns)),
+                                          dptr(z(NX, NZ, ns)), dptr(z(NX, NY, ns)), dptr(z(NX, NY, ns))))
+
     def outflows(self) -> dict:
         c = self.cfg
         NX, NY, NZ, ns = c.nx + 4, c.ny + 4, c.nz + 4, c.ns
