@@ -178,6 +178,24 @@ def measured_peak():
     return 6650.0, "fallback 6.65 TB/s"
 
 
+def compute_floors(config: str, cell_grains: float):
+    """The step's FP64-pipe and instruction-issue floors (ms) on 148 SMs at
+    1965 MHz from the committed per-cell-grain instruction counts, or None."""
+    p = ROOT / "profiles" / "instruction_mix.json"
+    if not p.exists():
+        return None
+    d = json.loads(p.read_text()).get(config)
+    if not d:
+        return None
+    inst = sum(v["thread_inst_per_cg"] for v in d.values())
+    fp64 = sum(v["fp64_inst_per_cg"] for v in d.values())
+    sms, hz = 148, 1965e6
+    return {"fp64_floor_ms": cell_grains * fp64 / (sms * 64 * hz) * 1e3,
+            "issue_floor_ms": cell_grains * inst / 32 / (sms * 4 * hz) * 1e3,
+            "thread_inst_per_cell_grain": inst, "fp64_inst_per_cell_grain": fp64,
+            "source": "profiles/instruction_mix.json (ncu counters of the C2 slab)"}
+
+
 def ncu_traffic(config: str, kclass: str):
     """dram read+write bytes per launch from the committed ncu summary."""
     p = ROOT / "profiles" / "ncu_traffic.json"
@@ -432,6 +450,11 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                 "step_frac": None}
         step_bytes = (48 + 24 / cfg.ns) * cfg.cell_grains if cfg.use_cn else (16 + 24 / cfg.ns) * cfg.cell_grains
         roof["step_frac"] = (step_bytes * args.steps / (ms / 1e3) / 1e9) / peak
+        fl = compute_floors(args.config, cfg.cell_grains) if not args.ny else None
+        if fl:
+            fl["step_ms"] = ms / args.steps
+            fl["issue_frac"] = fl["issue_floor_ms"] / fl["step_ms"]
+            roof["compute"] = fl
         kt = {k: {"ms": round(v[0] / max(v[1], 1), 4), "launches_per_step": v[1] / nk}
               for k, v in ktimes.items() if v[1] > 0}
         cpu = None
@@ -468,58 +491,87 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 
 def run_adjoint(args):
     """Source inversion on C4 (projected 200x200x50, 6 grains, 24 h, explicit
-    diffusion): control = mass rate per (level, hour, grain) = 7200
-    parameters; observations = hourly column loads of a seeded truth (the
-    prior times a lognormal sigma=0.5 perturbation) with 5% noise.  Times one
-    forward run and one checkpointed gradient (K=32) through the public API,
-    host loop included, and checks the gradient against central differences
-    on --fd seeded active parameters."""
+    diffusion) through the library's forward/adjoint pair
+    (a3g_forward_checkpointed, a3g_adjoint): control = mass rate per (level,
+    hour, grain) = 7200 parameters; observations = hourly column loads of a
+    seeded truth (the prior times a lognormal sigma=0.5 perturbation) with 5%
+    noise.  Times a plain forward run (one checkpoint slot, so nothing is
+    stored), the gradient with every state kept (the budget holds them all)
+    and the gradient under a 16-slot budget (binomial recomputation), and
+    checks the gradient against central differences on --fd seeded active
+    parameters over a sweep of relative steps."""
     import torch
     from volcano_ash3d_b200 import adjoint as adj
     from volcano_ash3d_b200.model import Ash3dGPU
     cfg = syn.make_config("C4")
-    inv = adj.SourceInversion(cfg, hours=int(cfg.sim_hours))
+    hours = int(cfg.sim_hours)
+    inv = adj.SourceInversion(cfg, hours=hours)
     gpu = Ash3dGPU(cfg)
-    p_true = inv.prior(seed=4, lognormal_sigma=0.5, active_hours=inv.hours)
-    _, loads, logs, _ = inv.forward(gpu, p_true)
+    p_true = inv.prior(seed=4, lognormal_sigma=0.5, active_hours=hours)
+    level = 8.0 * (-(-cfg.nx // 8) * 8) * cfg.ny * cfg.nz * cfg.ns  # one device level (bytes)
+    truth = adj.InversionGPU(gpu, cfg, hours, obs={h: np.zeros((cfg.nx, cfg.ny)) for h in range(hours)},
+                             snapshot_bytes=1.5 * level)
+    _, loads, _ = truth.forward(p_true)
     obs = {h: loads[h] * (1 + 0.05 * np.random.default_rng(100 + h).standard_normal(loads[h].shape))
-           for h in loads}
-    p = inv.prior(active_hours=inv.hours)
-    inv.forward(gpu, p, obs)  # warm-up
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    J, _, logs, _ = inv.forward(gpu, p, obs)
-    gpu.sync()
-    t_fwd = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    J2, grad = inv.gradient(gpu, p, obs, K=32)
-    gpu.sync()
-    t_grad = time.perf_counter() - t0
-    steps = len(logs)
+           for h in range(hours)}
+    p = inv.prior(active_hours=hours)
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        gpu.sync()
+        t0 = time.perf_counter()
+        out = fn()
+        gpu.sync()
+        return out, time.perf_counter() - t0
+
+    plain = adj.InversionGPU(gpu, cfg, hours, obs=obs, snapshot_bytes=1.5 * level)
+    plain.forward(p)  # warm-up
+    (J, _, _), t_fwd = timed(lambda: plain.forward(p))
+    full = adj.InversionGPU(gpu, cfg, hours, obs=obs)
+    full.forward(p)
+    full.adjoint()  # warm-up (allocates every checkpoint slot)
+    (_, t_fwd_ck) = timed(lambda: full.forward(p))
+    g, t_adj = timed(lambda: full.adjoint())
+    st_full = dict(full.stats)
+    tight = adj.InversionGPU(gpu, cfg, hours, obs=obs, snapshot_bytes=16.5 * level)
+    tight.forward(p)
+    (_, t_fwd16) = timed(lambda: tight.forward(p))
+    g16, t_adj16 = timed(lambda: tight.adjoint())
+    st16 = dict(tight.stats)
     fd = None
     if args.fd:
         rng = np.random.default_rng(7)
         active = np.argwhere(p > 0)
-        errs = []
-        for _ in range(args.fd):
-            i = tuple(int(v) for v in active[rng.integers(0, len(active))])
-            h = 1e-4 * p[i]
-            pp, pm = p.copy(), p.copy()
-            pp[i] += h
-            pm[i] -= h
-            d = (inv.forward(gpu, pp, obs)[0] - inv.forward(gpu, pm, obs)[0]) / (2 * h)
-            errs.append(abs(grad[i] - d) / max(abs(d), 1e-300))
-        fd = {"params": args.fd, "step": "1e-4 of the component", "max_rel_err": float(max(errs)),
-              "median_rel_err": float(np.median(errs))}
+        picks = [tuple(int(v) for v in active[rng.integers(0, len(active))]) for _ in range(args.fd)]
+        sweep = {}
+        for rel in (1e-3, 1e-4, 1e-5, 1e-6, 1e-7):
+            errs = []
+            for i in picks:
+                h = rel * p[i]
+                pp, pm = p.copy(), p.copy()
+                pp[i] += h
+                pm[i] -= h
+                d = (plain.forward(pp)[0] - plain.forward(pm)[0]) / (2 * h)
+                errs.append(abs(g[i] - d) / max(abs(d), 1e-300))
+            sweep[f"{rel:g}"] = {"max_rel_err": float(max(errs)), "median_rel_err": float(np.median(errs))}
+        best = min(sweep, key=lambda k: sweep[k]["max_rel_err"])
+        fd = {"params": args.fd, "steps_relative": sweep, "chosen_step": best,
+              "max_rel_err": sweep[best]["max_rel_err"], "median_rel_err": sweep[best]["median_rel_err"]}
+    steps = st_full["steps"]
     line = {
-        "metric": "C4 source-inversion gradient wall time", "value": t_grad, "unit": "s",
+        "metric": "C4 source-inversion gradient wall time", "value": t_fwd_ck + t_adj, "unit": "s",
         "higher_is_better": False, "n_gpus": 1, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "C4: " + WORKLOAD["C4"] + ", 24 h, 7200 controls, hourly column loads",
                    "grid": [cfg.nx, cfg.ny, cfg.nz], "grains": cfg.ns, "steps": steps,
-                   "checkpoint_every": 32},
-        "forward_s": t_fwd, "adjoint_forward_ratio": t_grad / t_fwd, "J": J2,
-        "forward_cell_grain_steps_per_s": cfg.cell_grains * steps / t_fwd,
-        "gradient_norm": float(np.linalg.norm(grad)), "fd_check": fd,
+                   "path": "C-ABI a3g_forward_checkpointed + a3g_adjoint (whole run in the library)"},
+        "forward_s": t_fwd, "adjoint_forward_ratio": (t_fwd_ck + t_adj) / t_fwd,
+        "checkpointed_forward_s": t_fwd_ck, "reverse_s": t_adj, "checkpoint_slots": st_full["slots"],
+        "recomputed_steps": st_full["recomputed"],
+        "budget_16_slots": {"gradient_s": t_fwd16 + t_adj16, "ratio": (t_fwd16 + t_adj16) / t_fwd,
+                            "recomputed_steps": st16["recomputed"],
+                            "same_gradient_bits": bool(np.array_equal(g, g16))},
+        "J": J, "forward_cell_grain_steps_per_s": cfg.cell_grains * steps / t_fwd,
+        "gradient_norm": float(np.linalg.norm(g)), "fd_check": fd,
         "gpu_launches": int(gpu.kernel_launches()),
     }
     print(json.dumps(line), flush=True)

@@ -375,7 +375,10 @@ int a3g_kernel_times(a3g_ctx *ctx, double *ms, uint64_t *count);
  * (defaults: x 4, y 1, z 1).
  * dir 3: the Crank-Nicolson x solve, variant 0 warp-tiled (default), 1 one
  * thread per line.  dir 4: the Crank-Nicolson y and z solves, variant 0 one
- * grain per thread, 1 two grains of a line per thread (default), 2 four.  All variants
+ * grain per thread, 1 two grains of a line per thread (default), 2 four.
+ * dir 1, 2 variant 5: the column march (one thread per line and grain, lanes
+ * along i, each interface formed once).  dir 5: the adjoint advection sweeps,
+ * variant 0 four-cell blocks (default), 1 one cell per thread.  All variants
  * produce identical results; only their speed differs. */
 int a3g_set_variant(a3g_ctx *ctx, int32_t dir, int32_t variant);
 int a3g_get_variant(a3g_ctx *ctx, int32_t dir, int32_t *variant);
@@ -488,7 +491,9 @@ typedef struct a3g_inv_desc {
   int32_t fast_dt;           /* 1: FAST_DT (met-step dt interpolated), 0: Adjust_DT every step */
   int32_t load_from;         /* first observed hour of the column loads (0-based) */
   int32_t dep_from;          /* the deposit misfit counts the deposit laid down after this hour */
-  int32_t pad;
+  int32_t adj_from;          /* the reverse run covers the steps from this hour on (0: the whole run);
+                              * the gradient then holds the bins of those steps, and lam
+                              * (a3g_adj_get_lambda) is the misfit's adjoint at that hour */
   double sim_hours;          /* run length, whole hours */
   double snapshot_bytes;     /* device memory for checkpoints; <= 0: the free memory less 2 GiB */
 } a3g_inv_desc;

@@ -44,14 +44,14 @@ def test_every_quotient_is_ieee(results):
 
 
 def test_fast_path_takes_in_range_quotients(results):
-    # limiter-like ratios: only exact zeros and power-of-two quotients fall back
+    # limiter-like ratios: only power-of-two quotients fall back (a zero dividend is a*b)
     for rel in (0.0, 1.2e-7, 6.0e-5):
         r = results[("div_rn", "limiter", rel)]
         assert r["fallbacks"] < 0.002 * r["n"], (rel, r)
 
 
 def test_poor_estimates_fall_back(results):
-    # a 20 % estimate defeats two Newton steps: the IEEE operator answers, still exactly
+    # a 20 % estimate defeats the iteration: the IEEE operator answers, still exactly
     for fam in ("wide", "near_exact", "limiter", "special"):
         r = results[("div_rn", fam, 0.2)]
         assert r["fallbacks"] > 0.9 * r["n"], (fam, r)

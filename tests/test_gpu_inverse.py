@@ -175,3 +175,22 @@ def test_autograd_function():
     assert abs(float(loss.detach()) - J) <= 1e-12 * J
     np.testing.assert_allclose(pt.grad.numpy(), g, rtol=0, atol=1e-12 * np.abs(g).max())
     gpu.close()
+
+
+def test_reversal_window():
+    """adj_from = 1: the reverse run covers the steps of the second hour only;
+    the bins of those steps equal the whole run's bit for bit (their adjoint
+    does not depend on earlier steps) and the first hour's bins stay zero."""
+    cfg, inv, ref, obs, obs_dep = _problem()
+    p = inv.prior(active_hours=HOURS)
+    gpu, ig = _gpu(cfg, inv, obs=obs, obs_dep=obs_dep, dep_from=1)
+    ig.forward(p)
+    g_full = ig.adjoint()
+    iw = adj.InversionGPU(gpu, cfg, HOURS, obs=obs, obs_dep=obs_dep, dep_from=1, adj_from=1)
+    iw.forward(p)
+    g_win = iw.adjoint()
+    assert np.any(g_full[:, 1, :] != 0.0)
+    assert np.array_equal(g_win[:, 1, :], g_full[:, 1, :])
+    assert not np.any(g_win[:, 0, :])
+    assert iw.stats["slots"] < ig.stats["slots"]
+    gpu.close()

@@ -71,7 +71,7 @@ class GridDesc(C.Structure):
 
 class InvDesc(C.Structure):
     _fields_ = [("ivent", C.c_int32), ("jvent", C.c_int32), ("nbins", C.c_int32), ("misfit", C.c_int32),
-                ("fast_dt", C.c_int32), ("load_from", C.c_int32), ("dep_from", C.c_int32), ("pad", C.c_int32),
+                ("fast_dt", C.c_int32), ("load_from", C.c_int32), ("dep_from", C.c_int32), ("adj_from", C.c_int32),
                 ("sim_hours", C.c_double), ("snapshot_bytes", C.c_double)]
 
 

@@ -258,7 +258,7 @@ class InversionGPU:
 
     def __init__(self, model, cfg: syn.Config, hours: int, obs: dict | None = None,
                  obs_dep: np.ndarray | None = None, nbins: int | None = None, load_from: int = 0,
-                 dep_from: int = 0, fast_dt: bool = False, snapshot_bytes: float = 0.0):
+                 dep_from: int = 0, fast_dt: bool = False, snapshot_bytes: float = 0.0, adj_from: int = 0):
         import ctypes as C
         from . import _lib
         self.model, self.cfg, self.hours = model, cfg, hours
@@ -285,7 +285,7 @@ class InversionGPU:
         d.misfit = (_lib.MISFIT_LOAD if obs is not None else 0) | (_lib.MISFIT_DEPOSIT if obs_dep is not None else 0)
         if d.misfit == 0:
             d.misfit = _lib.MISFIT_LOAD
-        d.fast_dt, d.load_from, d.dep_from = int(fast_dt), load_from, dep_from
+        d.fast_dt, d.load_from, d.dep_from, d.adj_from = int(fast_dt), load_from, dep_from, adj_from
         d.sim_hours, d.snapshot_bytes = float(hours), float(snapshot_bytes)
         nxy = (cfg.nx, cfg.ny)
         ol = np.zeros((hours, cfg.ny, cfg.nx))

@@ -1303,17 +1303,22 @@ int a3g_kernel_times(a3g_ctx *ctx, double *ms, uint64_t *count) {
 int a3g_set_variant(a3g_ctx *ctx, int32_t dir, int32_t variant) {
   if (!ctx) return fail(A3G_ERR_ARG, "null context");
   const bool col = (dir == 1 || dir == 2) && variant == 5;  // the column march (y, z)
-  if (dir < 0 || dir > 4 || variant < 0 || (!col && variant > (dir == 0 ? 4 : dir == 3 ? 1 : 2)))
+  if (dir < 0 || dir > 5 || variant < 0 ||
+      (!col && variant > (dir == 0 ? 4 : dir == 3 ? 1 : dir == 5 ? 1 : 2)))
     return fail(A3G_ERR_ARG, "bad direction or variant");
   if (dir == 3) ctx->tune_cn_x = variant;
   else if (dir == 4) ctx->tune_cn_yz = variant;
+  else if (dir == 5) ctx->adj_gather = variant == 1;
   else ctx->tune_advect[dir] = variant;
   return A3G_OK;
 }
 
 int a3g_get_variant(a3g_ctx *ctx, int32_t dir, int32_t *variant) {
-  if (!ctx || !variant || dir < 0 || dir > 4) return fail(A3G_ERR_ARG, "bad argument");
-  *variant = (dir == 3) ? ctx->tune_cn_x : (dir == 4) ? ctx->tune_cn_yz : ctx->tune_advect[dir];
+  if (!ctx || !variant || dir < 0 || dir > 5) return fail(A3G_ERR_ARG, "bad argument");
+  *variant = (dir == 3)   ? ctx->tune_cn_x
+             : (dir == 4) ? ctx->tune_cn_yz
+             : (dir == 5) ? (ctx->adj_gather ? 1 : 0)
+                          : ctx->tune_advect[dir];
   return A3G_OK;
 }
 

@@ -151,6 +151,7 @@ struct a3g_ctx {
   int tune_advect[3];
   int tune_cn_x;            // CN x solve: 0 warp-tiled, 1 one thread per line
   int tune_cn_yz;           // CN y/z solves: 0 one grain per thread, 1 two grains per thread
+  bool adj_gather;          // adjoint advection: cell-per-thread gather (true) or 4-cell blocks (false)
   // discrete adjoint (a3g_adj_*)
   double *lam0, *lam1;      // lam and its scratch level
   double *lam_dep;          // adjoint of DepositGranularity (ns,ny,nx)

@@ -390,6 +390,13 @@ bool obs_used(const a3g_inv *v, int ob) {
   return v->w_all || ((v->d.misfit & A3G_MISFIT_LOAD) && ob >= v->d.load_from);
 }
 
+// the first step of the reversal window (the first step starting at or after adj_from)
+int first_reversed(const a3g_inv *v) {
+  int n = 0;
+  while (n < (int)v->steps.size() && v->steps[n].time + 1.0e-9 < (double)v->d.adj_from) n++;
+  return n;
+}
+
 bool dep_used(const a3g_inv *v) { return v->w_all || (v->d.misfit & A3G_MISFIT_DEPOSIT) != 0; }
 
 // the step ends inside the deposit window (after hour dep_from)
@@ -431,8 +438,9 @@ extern "C" int a3g_inv_setup(a3g_ctx *ctx, const a3g_inv_desc *d, a3g_met_provid
   if ((d->misfit & ~3) || !d->misfit) return ifail(A3G_ERR_ARG, "misfit must be A3G_MISFIT_LOAD and/or A3G_MISFIT_DEPOSIT");
   if ((d->misfit & A3G_MISFIT_LOAD) && !obs_load) return ifail(A3G_ERR_ARG, "column-load misfit without observations");
   if ((d->misfit & A3G_MISFIT_DEPOSIT) && !obs_dep) return ifail(A3G_ERR_ARG, "deposit misfit without an observation");
-  if (d->dep_from < 0 || d->dep_from >= (int)d->sim_hours || d->load_from < 0)
-    return ifail(A3G_ERR_ARG, "observation windows outside the run");
+  if (d->dep_from < 0 || d->dep_from >= (int)d->sim_hours || d->load_from < 0 || d->adj_from < 0 ||
+      d->adj_from >= (int)d->sim_hours)
+    return ifail(A3G_ERR_ARG, "observation or reversal windows outside the run");
   int rc;
   if (ctx->prm.fast_subgrid) return ifail(A3G_ERR_UNSUPPORTED, "the inversion needs fast_subgrid off");
   if (ctx->topo_on) return ifail(A3G_ERR_UNSUPPORTED, "the inversion does not cover the terrain terms");
@@ -534,7 +542,7 @@ extern "C" int a3g_inv_setup(a3g_ctx *ctx, const a3g_inv_desc *d, a3g_met_provid
   const double lb = (double)level_bytes(ctx);
   long slots = (long)std::floor(budget / lb);
   if (slots < 1) return ifail(A3G_ERR_NOMEM, "the snapshot budget holds no checkpoint");
-  v->max_slots = (size_t)std::min<long>(slots, (long)v->steps.size());
+  v->max_slots = (size_t)std::min<long>(slots, (long)v->steps.size() - first_reversed(v));
   return sync_check(ctx);
 }
 
@@ -718,10 +726,11 @@ extern "C" int a3g_forward_checkpointed(a3g_ctx *ctx, const double *p, double *J
   const size_t ctl = (size_t)ctx->grid.nz * v->d.nbins * ctx->grid.ns;
   A3G_CUDA(cudaMemcpyAsync(v->p, p, sizeof(double) * ctl, cudaMemcpyHostToDevice, ctx->stream));
   ctx->box = Box{1, ctx->grid.nx, 1, ctx->grid.ny, 1, ctx->grid.nz};
-  const int N = (int)v->steps.size();
+  const int N = (int)v->steps.size(), n0 = first_reversed(v);
   Schedule sc;
-  sc.build(N, (int)v->max_slots - 1);
-  const std::vector<int> keep = spine(sc, N, (int)v->max_slots - 1);
+  sc.build(N - n0, (int)v->max_slots - 1);
+  std::vector<int> keep = spine(sc, N - n0, (int)v->max_slots - 1);
+  for (int &k : keep) k += n0;
   if ((rc = forward_run(ctx, v, keep))) return rc;
   if ((rc = sync_check(ctx))) return rc;
   v->J = host_misfit(ctx, v, &rc);
@@ -758,14 +767,15 @@ extern "C" int a3g_adjoint(a3g_ctx *ctx, const double *w_load, const double *w_d
   const size_t ctl = (size_t)ctx->grid.nz * v->d.nbins * ctx->grid.ns;
   A3G_CUDA(cudaMemsetAsync(v->grad, 0, sizeof(double) * ctl, ctx->stream));
   ctx->box = Box{1, ctx->grid.nx, 1, ctx->grid.ny, 1, ctx->grid.nz};
-  const int N = (int)v->steps.size();
+  const int N = (int)v->steps.size(), n0 = first_reversed(v);
   Reverser R;
   R.ctx = ctx;
   R.v = v;
-  R.sc.build(N, (int)v->max_slots - 1);
-  const std::vector<int> keep = spine(R.sc, N, (int)v->max_slots - 1);
+  R.sc.build(N - n0, (int)v->max_slots - 1);
+  std::vector<int> keep = spine(R.sc, N - n0, (int)v->max_slots - 1);
+  for (int &k : keep) k += n0;
   R.slot_step.assign(keep.begin(), keep.end());
-  rc = R.reverse(0, N, (int)v->max_slots - 1);
+  rc = R.reverse(n0, N, (int)v->max_slots - 1);
   if (rc) return rc;
   v->recomputed = R.recomputed;
   A3G_CUDA(cudaMemcpyAsync(grad, v->grad, sizeof(double) * ctl, cudaMemcpyDeviceToHost, ctx->stream));

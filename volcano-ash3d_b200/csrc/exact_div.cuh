@@ -3,13 +3,19 @@
 //
 // The transport path needs quotients that are bit-identical to IEEE division
 // (the limiter's theta = dqu/dq, src/AdvectionHorz_DCU.f90:204, and the back
-// substitution of the tridiagonal solve).  Method (Markstein, "Computation of
-// elementary functions on the IBM RISC System/6000 processor", IBM J. R&D
-// 1990; also Muller et al., Handbook of Floating-Point Arithmetic, ch. 5):
+// substitution of the tridiagonal solve).  Method: Goldschmidt's iteration
+// (R. E. Goldschmidt, "Applications of division by convergence", MIT thesis
+// 1964) for the quotient, then Markstein's correction step (Markstein,
+// "Computation of elementary functions on the IBM RISC System/6000
+// processor", IBM J. R&D 1990; Muller et al., Handbook of Floating-Point
+// Arithmetic, ch. 5):
 //   y  ~ 1/b from the hardware reciprocal approximation (PTX
-//        rcp.approx.ftz.f64), refined by two Newton-Raphson steps
-//        e = 1 - b*y, y = y + y*e (each one fused multiply-add);
-//   q  = a*y;  r = a - b*q (exact with an FMA);  q = q + r*y.
+//        rcp.approx.ftz.f64), e = 1 - b*y (exact with an FMA);
+//   q  = a*y*(1 + e)*(1 + e^2): relative error e^4, the two products and
+//        y' = y*(1 + e) formed side by side, so the dependent chain after
+//        the estimate is five operations instead of the seven of two
+//        sequential Newton-Raphson steps on y;
+//   r  = a - b*q (exact with an FMA);  q = q + r*y'.
 // The result is then certified exactly: r = a - b*q is computed again with an
 // FMA (exact for a q within an ulp or two of a/b and operands far from the
 // underflow range), and q is accepted only if |r| < |b| * ulp(q)/2, i.e. the
@@ -17,7 +23,9 @@
 // a power of two (whose rounding interval is asymmetric).  Everything else --
 // operands outside [2^-200, 2^200], a zero divisor, non-finite values, a
 // residual on or beyond the half-ulp bound -- falls back to the IEEE division
-// operator.  Both paths therefore return RN(a/b) exactly.
+// operator.  A zero dividend over an in-range divisor returns a*b, the zero
+// whose sign IEEE division gives (the signs' exclusive or).  Every path
+// therefore returns RN(a/b) exactly.
 #pragma once
 
 namespace a3g {
@@ -71,13 +79,14 @@ __device__ __forceinline__ bool certified(double a, double b, double q) {
 // RN(a/b).
 __device__ __forceinline__ double div_rn(double a, double b) {
   if (!(in_fast_range(b, false) && in_fast_range(a, true))) return ieee_div(a, b);
-  if (a == 0.0) return ieee_div(a, b);
+  if (a == 0.0) return a * b;  // +-0 with the quotient's sign (b finite, nonzero)
   double y = rcp_approx(b);
-  double e = fma(-b, y, 1.0);
-  y = fma(y, e, y);
-  e = fma(-b, y, 1.0);
-  y = fma(y, e, y);
+  const double e = fma(-b, y, 1.0);
   double q = a * y;
+  const double e2 = e * e;
+  q = fma(q, e, q);
+  y = fma(y, e, y);
+  q = fma(q, e2, q);
   const double r = fma(-b, q, a);
   q = fma(r, y, q);
   if (certified(a, b, q)) return q;
@@ -88,7 +97,7 @@ __device__ __forceinline__ double div_rn(double a, double b) {
 // quotients, e.g. a tridiagonal pivot).
 __device__ __forceinline__ double div_rn_rcp(double a, double b, double y) {
   if (!(in_fast_range(b, false) && in_fast_range(a, true))) return ieee_div(a, b);
-  if (a == 0.0) return ieee_div(a, b);
+  if (a == 0.0) return a * b;  // +-0 with the quotient's sign (b finite, nonzero)
   double q = a * y;
   const double r = fma(-b, q, a);
   q = fma(r, y, q);

@@ -199,6 +199,153 @@ __global__ void __launch_bounds__(256) k_adj_advect(Layout L, int nocycle, doubl
   lout[gb + cell] = lam;
 }
 
+// Block form of k_adj_advect: a thread takes V consecutive cells of a line
+// and forms each of the V+3 interfaces they read (c0-1 .. c0+V+1) once,
+// instead of the four a cell-per-thread gather forms for every cell; the
+// expressions and their order are lam_at's, so the results are the same
+// bits.  Not x-periodic (the wrapped ghosts stay with the gather kernel).
+// DIR 0: lanes are consecutive blocks along i; DIR 1, 2: lanes along i.
+template <int DIR, int LIM, int V, bool CK>
+__device__ __forceinline__ void adj_block_body(const Layout &L, int nocycle, double eps, int n, int c0, long st,
+                                               const double *__restrict__ pq, const double *__restrict__ pl,
+                                               double *__restrict__ po, const double *__restrict__ pv,
+                                               const double *__restrict__ pvf, long vfs, const LineGeo &gsig,
+                                               const LineGeo &gdtv, double lam_lo0) {
+  auto Q = [&](int c) -> double {
+    if (CK && (c < 1 || c > n)) return 0.0;
+    return pq[(long)(c - 1) * st];
+  };
+  auto VV = [&](int c) -> double {
+    const int cl = CK ? (c < 1 ? 1 : (c > n ? n : c)) : c;
+    double v = pv[(long)(cl - 1) * st];
+    if (DIR == 2) v = v + pvf[(long)(cl + 1) * vfs];
+    return v;
+  };
+  auto T = [&](int c) -> double {  // t(c) = -dtv(c)*lam_u(c)
+    if (CK && (c < 0 || c > n + 1)) return 0.0;
+    double lu = 0.0;
+    if (!CK || (c >= 1 && c <= n)) lu = pl[(long)(c - 1) * st];
+    else if (c == 0 && DIR == 2) lu = lam_lo0;
+    return -(gdtv.at(c) * lu);
+  };
+  // window: q(c0-3 .. c0+V+2), vel(c0-3 .. c0+V+2), t(c0-2 .. c0+V+1)
+  double q[V + 6], vv[V + 6], tt[V + 4];
+#pragma unroll
+  for (int m = 0; m < V + 6; m++) {
+    q[m] = Q(c0 - 3 + m);
+    vv[m] = VV(c0 - 3 + m);
+  }
+#pragma unroll
+  for (int m = 0; m < V + 4; m++) tt[m] = T(c0 - 2 + m);
+  // dq(c0-2 .. c0+V+2): dq(I) = q(I) - q(I-1), zero outside [0, n+2]
+  double dq[V + 5];
+#pragma unroll
+  for (int m = 0; m < V + 5; m++) {
+    const int I = c0 - 2 + m;
+    dq[m] = (CK && (I < 0 || I > n + 2)) ? 0.0 : q[m + 1] - q[m];
+  }
+  // interfaces J = c0-1+r, r = 0 .. V+2: usig, upwind side, a*e, b*e
+  double us[V + 3], ea[V + 3], eb[V + 3];
+  bool up[V + 3];
+#pragma unroll
+  for (int r = 0; r < V + 3; r++) {
+    const int J = c0 - 1 + r;
+    const double u = (CK && (J < 0 || J > n + 1)) ? 0.0 : 0.5 * (vv[r + 1] + vv[r + 2]) * gsig.at(J);
+    us[r] = u;
+    up[r] = u > 0.0;
+    ea[r] = 0.0;
+    eb[r] = 0.0;
+    if (LIM != A3G_LIM_NONE && (!CK || (J >= 1 && J <= n + 1))) {
+      const double dqJ = dq[r + 1];
+      if (nocycle || !(fabs(dqJ) <= eps)) {
+        const double aus = fabs(u);
+        const double w = 0.5 * aus * (1.0 - gdtv.at(J) * aus);
+        const double e = w * (tt[r] - tt[r + 1]);  // t(J-1) - t(J)
+        double a, b;
+        lim_coef<LIM>(dqJ, up[r] ? dq[r] : dq[r + 2], eps, a, b);
+        ea[r] = a * e;
+        eb[r] = b * e;
+      }
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < V; v++) {
+    const int c = c0 + v;
+    if (CK && c > n) break;
+    double ldq[2];
+#pragma unroll
+    for (int s2 = 0; s2 < 2; s2++) {
+      const int I = c + s2, r = v + 1 + s2;
+      double val = 0.0;
+      if (!CK || (I >= 0 && I <= n + 2)) {
+        const double u = us[r];
+        const double lfsr = tt[v + 2 + s2];                              // t(I)
+        const double lfsl = (!CK || I <= n + 1) ? tt[v + 1 + s2] : 0.0;  // t(I-1)
+        val = dmx(0.0, u) * lfsr + dmn(0.0, u) * lfsl + ea[r];
+        if (up[r + 1]) val = val + eb[r + 1];
+        if (!up[r - 1]) val = val + eb[r - 1];
+      }
+      ldq[s2] = val;
+    }
+    double lam = pl[(long)(c - 1) * st];
+    const double divm = dmn(0.0, us[v + 2]) - dmn(0.0, us[v + 1]);
+    lam = lam + divm * tt[v + 2];
+    const double divp = dmx(0.0, us[v + 2]) - dmx(0.0, us[v + 1]);
+    lam = lam + divp * tt[v + 2];
+    po[(long)(c - 1) * st] = lam + ldq[0] - ldq[1];
+  }
+}
+
+template <int DIR, int LIM, int V>
+__global__ void __launch_bounds__(128) k_adj_advect_blk(Layout L, int nocycle, double eps, int nblk,
+                                                        const double *__restrict__ cq,
+                                                        const double *__restrict__ lin,
+                                                        double *__restrict__ lout,
+                                                        const double *__restrict__ vel, Geo4 vf, Geo3 sig,
+                                                        Geo3 dtvt, const int32_t *__restrict__ aloft,
+                                                        const double *__restrict__ lam_lo) {
+  const int n = (DIR == 0) ? L.nx : (DIR == 1) ? L.ny : L.nz;
+  int a, o, blk, g;  // lane index (i or j), other index, block, grain (k_advect_block's mapping)
+  if (DIR == 0) {
+    blk = blockIdx.x * 32 + threadIdx.x;
+    a = blockIdx.y * 4 + threadIdx.y + 1;  // j
+    o = (int)(blockIdx.z % L.nz) + 1;      // k
+    g = (int)(blockIdx.z / L.nz);
+    if (blk >= nblk || a > L.ny) return;
+  } else {
+    a = blockIdx.x * 32 + threadIdx.x + 1;  // i
+    const int w = blockIdx.y * 4 + threadIdx.y;
+    blk = w % nblk;
+    o = w / nblk + 1;
+    g = blockIdx.z;
+    const int nother = (DIR == 1) ? L.nz : L.ny;
+    if (a > L.nx || o > nother) return;
+  }
+  const int c0 = 1 + blk * V;
+  const long base = (DIR == 0) ? L.cell(1, a, o) : (DIR == 1) ? L.cell(a, 1, o) : L.cell(a, o, 1);
+  const long st = (DIR == 0) ? 1 : (DIR == 1) ? L.P : L.PY;
+  const long gb = (long)g * L.PG;
+  double *po = lout + gb + base;
+  if (!aloft[g]) {
+    for (int v = 0; v < V; v++)
+      if (c0 + v <= n) po[(long)(c0 + v - 1) * st] = 0.0;
+    return;
+  }
+  const int i = (DIR == 0) ? 1 : a, j = (DIR == 1) ? 1 : (DIR == 0 ? a : o);
+  const LineGeo gsig = line_of<DIR>(sig, a, o);
+  const LineGeo gdtv = line_of<DIR>(dtvt, a, o);
+  const double *pvf = vf.p + (long)(i + 1) * vf.si + (long)(j + 1) * vf.sj + (long)g * vf.sg;
+  const double lam_lo0 = (DIR == 2 && lam_lo && c0 <= 2) ? lam_lo[(long)g * L.nx * L.ny + (long)(j - 1) * L.nx + (i - 1)]
+                                                         : 0.0;
+  const bool fast = c0 - 3 >= 1 && c0 + V + 2 <= n;
+  if (fast)
+    adj_block_body<DIR, LIM, V, false>(L, nocycle, eps, n, c0, st, cq + gb + base, lin + gb + base, po, vel + base,
+                                       pvf, vf.sk, gsig, gdtv, lam_lo0);
+  else
+    adj_block_body<DIR, LIM, V, true>(L, nocycle, eps, n, c0, st, cq + gb + base, lin + gb + base, po, vel + base,
+                                      pvf, vf.sk, gsig, gdtv, lam_lo0);
+}
+
 template <int DIR, int LIM>
 static void launch_adj_dir_lim(a3g_ctx *ctx, const double *cq, const double *lin, double *lout,
                                const double *lam_lo) {
@@ -207,14 +354,25 @@ static void launch_adj_dir_lim(a3g_ctx *ctx, const double *cq, const double *lin
   const bool per = (DIR == 0) && ctx->grid.periodic;
   const double *vel = (DIR == 0) ? ctx->vx : (DIR == 1) ? ctx->vy : ctx->vz;
   const Geo3 &sig = (DIR == 0) ? ctx->snx : (DIR == 1) ? ctx->sny : ctx->snz;
-  if (per)
+  if (per) {
     k_adj_advect<DIR, LIM, true><<<grid, dim3(32, 8), 0, ctx->stream>>>(
         L, ctx->prm.nocycle, ctx->prm.eps_thresh, cq, lin, lout, vel, ctx->vf, sig, ctx->dtv, ctx->aloft,
         lam_lo);
-  else
+  } else if (ctx->adj_gather) {
     k_adj_advect<DIR, LIM, false><<<grid, dim3(32, 8), 0, ctx->stream>>>(
         L, ctx->prm.nocycle, ctx->prm.eps_thresh, cq, lin, lout, vel, ctx->vf, sig, ctx->dtv, ctx->aloft,
         lam_lo);
+  } else {
+    constexpr int V = 4;
+    const int n = (DIR == 0) ? L.nx : (DIR == 1) ? L.ny : L.nz;
+    const int nblk = (n + V - 1) / V;
+    dim3 gb;
+    if (DIR == 0) gb = dim3((nblk + 31) / 32, (L.ny + 3) / 4, L.nz * L.ns);
+    else gb = dim3((L.nx + 31) / 32, (nblk * ((DIR == 1) ? L.nz : L.ny) + 3) / 4, L.ns);
+    k_adj_advect_blk<DIR, LIM, V><<<gb, dim3(32, 4), 0, ctx->stream>>>(
+        L, ctx->prm.nocycle, ctx->prm.eps_thresh, nblk, cq, lin, lout, vel, ctx->vf, sig, ctx->dtv, ctx->aloft,
+        lam_lo);
+  }
 }
 
 template <int DIR>
