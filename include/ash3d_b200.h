@@ -421,8 +421,9 @@ int a3g_vprofiles(a3g_ctx *ctx, int32_t npts, const int32_t *i_pts, const int32_
  * forward state and the outflow accumulators untouched.  dt and the winds
  * must be those of the forward step (a3g_set_dt / a3g_set_winds or
  * a3g_interp_winds). */
-/* Allocates lam, the deposit adjoint and the step's stage buffers (4 levels
- * plus one face); lam starts at zero. */
+/* Allocates lam, the deposit adjoint and the step's stage buffer (3 levels
+ * plus one face); lam starts at zero.  a3g_adj_step recomputes its second
+ * intermediate state into the scratch level ts1. */
 int a3g_adj_enable(a3g_ctx *ctx);
 int a3g_adj_zero(a3g_ctx *ctx);
 /* lam in the layout of concen_pd(:,:,:,:,ts0) (ghost values ignored on

@@ -292,7 +292,7 @@ int a3g_destroy(a3g_ctx *ctx) {
   if (ctx->src_state) cudaFree(ctx->src_state);
   if (ctx->h_umb) cudaFreeHost(ctx->h_umb);
   for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
-  double *aptrs[] = {ctx->lam0, ctx->lam1, ctx->lam_dep, ctx->stage1, ctx->stage2, ctx->adj_face,
+  double *aptrs[] = {ctx->lam0, ctx->lam1, ctx->lam_dep, ctx->stage1, ctx->adj_face,
                      ctx->obs_buf, ctx->ov_buf, ctx->ov_zcc, ctx->topo_buf, ctx->vzh, ctx->umb_buf,
                      ctx->vp_buf, ctx->adj_grad, ctx->cn_state};
   for (double *p : aptrs) if (p) cudaFree(p);
@@ -1357,7 +1357,7 @@ int a3g_adj_enable(a3g_ctx *ctx) {
   const size_t face = sizeof(double) * (size_t)ns *
                       (size_t)std::max(std::max((long)ny * nz, (long)nx * nz), (long)nx * ny);
   const size_t obs = sizeof(double) * std::max((size_t)nx * ny, (size_t)(nz + 1) * ns);
-  double **bufs[] = {&ctx->lam0, &ctx->lam1, &ctx->stage1, &ctx->stage2};
+  double **bufs[] = {&ctx->lam0, &ctx->lam1, &ctx->stage1};
   for (double **b : bufs) {
     if (cudaMalloc((void **)b, lev) != cudaSuccess) return fail(A3G_ERR_NOMEM, "adjoint level allocation failed");
     ctx->bytes += lev;
@@ -1481,8 +1481,9 @@ int a3g_adj_step(a3g_ctx *ctx, int32_t itime) {
   if (ctx->prm.use_diffusion && !ctx->have_diffusivity) return fail(A3G_ERR_STATE, "diffusivity not set");
   // Recompute the states entering the second horizontal sweep and the
   // vertical sweep, keeping the forward state and accumulators intact: the
-  // recomputed sweeps write into the stage buffers and add their outflow
-  // updates to a scratch face.
+  // recomputed sweeps write into the stage buffer and the scratch level ts1
+  // (which every sweep overwrites whole) and add their outflow updates to a
+  // scratch face.
   double *keep_c0 = ctx->c0, *keep_c1 = ctx->c1;
   double *outs[6] = {ctx->out_yz1, ctx->out_yz2, ctx->out_xz1, ctx->out_xz2, ctx->out_xy1, ctx->out_xy2};
   ctx->out_yz1 = ctx->out_yz2 = ctx->out_xz1 = ctx->out_xz2 = ctx->out_xy1 = ctx->out_xy2 = ctx->adj_face;
@@ -1490,8 +1491,8 @@ int a3g_adj_step(a3g_ctx *ctx, int32_t itime) {
   ctx->c1 = ctx->stage1;
   rc = (first == 0) ? launch_advect_x(ctx) : launch_advect_y(ctx);  // c0 := stage1 (state b)
   if (!rc) {
-    ctx->c1 = ctx->stage2;
-    rc = (first == 0) ? launch_advect_y(ctx) : launch_advect_x(ctx);  // c0 := stage2 (state c)
+    ctx->c1 = keep_c1;
+    rc = (first == 0) ? launch_advect_y(ctx) : launch_advect_x(ctx);  // c0 := ts1 (state c)
   }
   ctx->out_yz1 = outs[0]; ctx->out_yz2 = outs[1]; ctx->out_xz1 = outs[2];
   ctx->out_xz2 = outs[3]; ctx->out_xy1 = outs[4]; ctx->out_xy2 = outs[5];
@@ -1504,7 +1505,7 @@ int a3g_adj_step(a3g_ctx *ctx, int32_t itime) {
     if ((rc = adj_diffuse_dir(ctx, 1 - dfirst))) return rc;
     if ((rc = adj_diffuse_dir(ctx, dfirst))) return rc;
   }
-  if ((rc = adj_advect_dir(ctx, 2, ctx->stage2))) return rc;         // AdvectVert^T at state c
+  if ((rc = adj_advect_dir(ctx, 2, ctx->c1))) return rc;             // AdvectVert^T at state c
   if ((rc = adj_advect_dir(ctx, 1 - first, ctx->stage1))) return rc; // second horizontal sweep at b
   return adj_advect_dir(ctx, first, ctx->c0);                        // first horizontal sweep at a
 }

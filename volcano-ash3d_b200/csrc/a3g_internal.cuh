@@ -155,7 +155,7 @@ struct a3g_ctx {
   // discrete adjoint (a3g_adj_*)
   double *lam0, *lam1;      // lam and its scratch level
   double *lam_dep;          // adjoint of DepositGranularity (ns,ny,nx)
-  double *stage1, *stage2;  // recomputed states inside a step
+  double *stage1;           // recomputed state inside a step (ts1 holds the second)
   double *adj_face;         // sink for outflow updates of recomputed sweeps
   double *obs_buf;          // (nx*ny) or ((nz+1)*ns), whichever is larger
   std::vector<double *> snaps;

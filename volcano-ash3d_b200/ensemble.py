@@ -11,8 +11,10 @@ Each member's results are the bits its run gives alone, because members
 share no device data.
 
 autotune() picks, per member, the fastest advection kernel variant for each
-direction and the CN x-solve variant by timing short runs on a scratch
-context; the choice changes speed only, never results.
+direction (x: marching rows, 4- or 8-cell blocks, warp tiles, warp rows; y
+and z: marching lines, 4- or 8-cell blocks, the column march) and the CN
+solve variants by timing short runs on a scratch context; the choice changes
+speed only, never results.
 """
 from __future__ import annotations
 
@@ -61,7 +63,7 @@ def autotune(cfg: syn.Config, device: int = 0, steps: int = 2) -> dict:
     choice = {}
     keys = {0: ("advect_x",), 1: ("advect_y",), 2: ("advect_z",), 3: ("cn_solve_x",),
             4: ("cn_solve_y", "cn_solve_z")}
-    for d, options in ((0, (0, 1, 2, 3, 4)), (1, (0, 1, 2)), (2, (0, 1, 2)), (3, (0, 1)), (4, (0, 1, 2))):
+    for d, options in ((0, (0, 1, 2, 3, 4)), (1, (0, 1, 2, 5)), (2, (0, 1, 2, 5)), (3, (0, 1)), (4, (0, 1, 2))):
         if d >= 3 and not cfg.use_cn:
             continue
         best, best_ms = None, None
