@@ -592,6 +592,107 @@ def run_adjoint(args):
     gpu.close()
 
 
+class CachedMet:
+    """Every met step of a run generated once, by a thread pool (numpy
+    releases the interpreter lock in the generator's fills and array
+    arithmetic), and kept in host memory; an all-zero vz is shared."""
+
+    def __init__(self, cfg, nsteps: int, threads: int = 8):
+        import concurrent.futures as cf
+        src = syn.MetSource(cfg)
+        self.zero = None
+        with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+            steps = list(ex.map(src.step, range(nsteps)))
+        self.steps = []
+        for u, v, w in steps:
+            if not w.any():
+                if self.zero is None:
+                    self.zero = w
+                w = self.zero
+            self.steps.append((u, v, w))
+
+    def step(self, hour: int):
+        return self.steps[hour]
+
+
+def run_adjoint_scale(args):
+    """C5: projected 1500x1000x80 (3 km, dz 0.4 km), 20 grains, superbee, CN,
+    FAST_DT: the forward run of --hours simulated hours (default 48) through
+    the library's checkpointed forward, then the adjoint of the deposit misfit
+    over the last --adj-hours (default 12).  Control: the vent column's mass
+    rate per (level, hour, grain), the Suzuki column for a 25 km plume over 12
+    h with seeded heavy-tailed (Pareto) hourly rates.  Observation: a seeded
+    Gaussian deposit pattern downwind of the vent.  Checkpoints: device memory
+    only, every byte left after the run's buffers but 2 GiB (the library's
+    default budget), binomial placement over the reversal window."""
+    import ctypes as C
+    import torch
+    from volcano_ash3d_b200 import _lib
+    from volcano_ash3d_b200 import adjoint as adj
+    from volcano_ash3d_b200.model import Ash3dGPU
+    cfg = syn.make_config("C5")
+    hours = int(args.hours) if args.hours > 1.0 else int(cfg.sim_hours)
+    win = min(int(args.adj_hours), hours - 1)
+    cfg.sim_hours = float(hours)
+    cfg.fast_dt = not args.no_fast_dt
+    cfg.fast_subgrid = False  # the inversion runs the full box
+    t0 = time.perf_counter()
+    met = CachedMet(cfg, hours + 2)
+    t_met = time.perf_counter() - t0
+    gpu = Ash3dGPU(cfg)
+    prior = adj.SourceInversion(cfg, hours, geo=gpu.geo)
+    p = prior.prior(active_hours=cfg.duration_h)
+    rng = np.random.default_rng(55)
+    rate = 1.0 + rng.pareto(1.5, hours)
+    rate = rate / rate[:int(cfg.duration_h)].mean()
+    p = p * rate[None, :, None]
+    ii, jj = np.meshgrid(np.arange(cfg.nx), np.arange(cfg.ny), indexing="ij")
+    x0, y0 = cfg.ivent + rng.uniform(100, 300), cfg.jvent + rng.uniform(-50, 50)
+    obs_dep = 1.0 * np.exp(-0.5 * (((ii - x0) / 150.0) ** 2 + ((jj - y0) / 40.0) ** 2))
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        gpu.sync()
+        t = time.perf_counter()
+        out = fn()
+        gpu.sync()
+        return out, time.perf_counter() - t
+
+    free0, total = torch.cuda.mem_get_info()
+    (inv, t_setup) = timed(lambda: adj.InversionGPU(gpu, cfg, hours, obs_dep=obs_dep, nbins=hours,
+                                                    dep_from=hours - win, adj_from=hours - win,
+                                                    fast_dt=cfg.fast_dt, met=met, met_cache=False))
+    (J, _, dep), t_fwd = timed(lambda: inv.forward(p))
+    g, t_adj = timed(lambda: inv.adjoint())
+    st = dict(inv.stats)
+    free1, _ = torch.cuda.mem_get_info()
+    steps, wsteps = st["steps"], st["window_steps"]
+    lib = _lib.load()
+    ms_fwd = 1000.0 * t_fwd / steps
+    rec = C.c_int64()
+    lib.a3g_checkpoint_cost(max(wsteps, 1), max(st["slots"] - 1, 0), C.byref(rec), None)
+    level = 8.0 * cfg.nx * cfg.ny * cfg.nz * cfg.ns
+    line = {
+        "metric": "C5 deposit-misfit adjoint wall time", "value": t_adj, "unit": "s", "higher_is_better": False,
+        "n_gpus": 1, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"C5: projected 1500x1000x80, 20 grains, superbee, CN, "
+                               f"{'FAST_DT' if cfg.fast_dt else 'Adjust_DT every step'}, forward {hours} h, "
+                               f"adjoint of the deposit misfit over the last {win} h",
+                   "grid": [cfg.nx, cfg.ny, cfg.nz], "grains": cfg.ns, "controls": int(p.size),
+                   "path": "C-ABI a3g_forward_checkpointed / a3g_adjoint"},
+        "forward_s": t_fwd, "forward_ms_per_step": ms_fwd, "setup_s": t_setup, "met_generation_s": t_met,
+        "steps": steps, "slots": st["slots"], "slot_gb": level / 1e9,
+        "checkpoint_gb": st["slots"] * level / 1e9, "recomputed_steps": st["recomputed"],
+        "recomputed_predicted": int(rec.value), "window_steps": wsteps,
+        "adjoint_over_window_forward": t_adj / (ms_fwd * wsteps / 1000.0),
+        "device_free_gb_before": free0 / 1e9, "device_free_gb_after": free1 / 1e9, "device_total_gb": total / 1e9,
+        "J": J, "grad_abs_max": float(np.abs(g).max()), "grad_finite": bool(np.isfinite(g).all()),
+        "grad_nonzero_bins": int(np.count_nonzero(np.abs(g).sum(axis=(0, 2)))),
+    }
+    print(json.dumps(line), flush=True)
+    gpu.close()
+
+
 def run_ensemble(args):
     """C3: 64 seeded members (nx, ny in [80,400], nz in [30,80], 2-10 grains,
     CN), each run for --hours simulated hours from a clean atmosphere, first
@@ -643,7 +744,11 @@ def main():
                     help="with --adjoint: central-difference checks on this many parameters")
     ap.add_argument("--ensemble", action="store_true",
                     help="time the 64-member C3 ensemble, sequential and concurrent")
-    ap.add_argument("--hours", type=float, default=1.0, help="with --ensemble: simulated hours per member")
+    ap.add_argument("--hours", type=float, default=1.0,
+                    help="with --ensemble: simulated hours per member; with --config C5 --adjoint: the "
+                         "forward run's hours (default 48)")
+    ap.add_argument("--adj-hours", type=float, default=12.0,
+                    help="with --config C5 --adjoint: the reversal window (the last hours of the run)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -654,7 +759,10 @@ def main():
         run_reference(args, rank, world)
         return
     if args.adjoint:
-        run_adjoint(args)
+        if args.config == "C5":
+            run_adjoint_scale(args)
+        else:
+            run_adjoint(args)
         return
     if args.ensemble:
         run_ensemble(args)

@@ -497,6 +497,9 @@ typedef struct a3g_inv_desc {
                               * (a3g_adj_get_lambda) is the misfit's adjoint at that hour */
   double sim_hours;          /* run length, whole hours */
   double snapshot_bytes;     /* device memory for checkpoints; <= 0: the free memory less 2 GiB */
+  int32_t met_cache;         /* 0: every met step of the run on the device when they take at most a
+                              * quarter of the free memory; 1: never (the three met slots of the
+                              * context, each step uploaded from the provider when a run reaches it) */
 } a3g_inv_desc;
 /* Met-step provider: sets three pointers to the FP32 met step of `hour`
  * (vx, vy, vz; nx*ny*nz, m/s, i fastest) in host memory, valid until the next
@@ -525,7 +528,7 @@ int a3g_adjoint(a3g_ctx *ctx, const double *w_load, const double *w_dep, double 
 int a3g_tangent_linear(a3g_ctx *ctx, const double *p, const double *dp, double *dloads, double *ddep);
 /* The last run's observations (loads: nhours*nx*ny, dep: nx*ny; either may
  * be NULL) and stats = {steps, checkpoint slots, forward steps the last
- * reversal recomputed}. */
+ * reversal recomputed, steps in the reversal window} (four entries). */
 int a3g_inv_observations(a3g_ctx *ctx, double *loads, double *dep, int64_t *stats);
 /* Forward steps the binomial reversal of nsteps steps repeats with nslots
  * free checkpoint slots, and its first split (host arithmetic only). */

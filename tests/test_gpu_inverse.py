@@ -15,7 +15,10 @@ a3g_forward_checkpointed, a3g_adjoint, a3g_tangent_linear), on B200:
   direction p returns the observations themselves);
 * central differences of J agree with the gradient to 1e-6 relative (step
   1e-5 of the component);
-* the torch.autograd.Function gives the adjoint's gradient for a torch loss.
+* the torch.autograd.Function gives the adjoint's gradient for a torch loss;
+* with the device met cache off, met steps go through the context's three
+  slots (one upload per hour a run moves on or back) and every result is the
+  same bits as with the cache.
 """
 import ctypes as C
 
@@ -193,4 +196,48 @@ def test_reversal_window():
     assert np.array_equal(g_win[:, 1, :], g_full[:, 1, :])
     assert not np.any(g_win[:, 0, :])
     assert iw.stats["slots"] < ig.stats["slots"]
+    gpu.close()
+
+
+class _CountingMet:
+    """The synthetic met source, recording the hours asked for."""
+
+    def __init__(self, cfg):
+        self.src = syn.MetSource(cfg)
+        self.calls = []
+
+    def step(self, hour):
+        self.calls.append(int(hour))
+        return self.src.step(hour)
+
+
+@pytest.mark.parametrize("fast", [False, True])
+def test_met_slots_without_cache(fast):
+    from volcano_ash3d_b200.model import Ash3dGPU
+    cfg, inv, ref, obs, obs_dep = _problem(fast_dt=fast)
+    p = inv.prior()
+    P = -(-cfg.nx // 8) * 8
+    level = 8.0 * P * cfg.ny * cfg.nz * cfg.ns
+    gpu = Ash3dGPU(cfg)
+    out = []
+    for cache in (True, False):
+        met = _CountingMet(cfg)
+        # two slots: the reversal recomputes across the hour boundary
+        ig = adj.InversionGPU(gpu, cfg, HOURS, obs=obs, obs_dep=obs_dep, dep_from=1, fast_dt=fast,
+                              snapshot_bytes=2.5 * level, met=met, met_cache=cache)
+        n_setup = len(met.calls)
+        J, loads, dep = ig.forward(p)
+        n_fwd = len(met.calls) - n_setup
+        g = ig.adjoint()
+        out.append(dict(J=J, loads=loads, dep=dep, g=g, setup=n_setup, fwd=n_fwd,
+                        adj=len(met.calls) - n_setup - n_fwd, stats=dict(ig.stats)))
+    c, n = out
+    assert c["fwd"] == 0 and c["adj"] == 0 and c["setup"] == HOURS + 2  # every step cached once
+    assert n["fwd"] == HOURS + 1  # hours 0, 1, ..., HOURS, each uploaded once
+    assert n["stats"]["recomputed"] > 0 and n["adj"] >= 1
+    assert n["J"] == c["J"]
+    assert np.array_equal(n["dep"], c["dep"])
+    for h in range(HOURS):
+        assert np.array_equal(n["loads"][h], c["loads"][h]), h
+    assert np.array_equal(n["g"], c["g"])
     gpu.close()

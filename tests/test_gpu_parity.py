@@ -14,7 +14,7 @@ from gpu_common import pair, prime, random_state
 pytestmark = pytest.mark.gpu
 
 CONFIGS = ["tiny_proj", "tiny_cn", "tiny_latlon", "tiny_periodic", "tiny_subgrid", "tiny_wide",
-           "tiny_tall", "tiny_stretch"]
+           "tiny_tall", "tiny_deep", "tiny_stretch"]
 OPS = ["advect_x", "advect_y", "AdvectVert", "DiffuseHorz_even", "DiffuseHorz_odd", "DiffuseVert"]
 
 
@@ -45,7 +45,7 @@ ADVECTION = ("advect_x", "advect_y", "AdvectVert")
 def _variants(op):
     # advection: march / block-4 / block-8 / x warp-tiled / x warp-row / y, z
     # column march; diffusion: the CN x solve warp-tiled / one thread per line
-    # and the y, z solves one / two grains per thread
+    # and the y, z solves one / two / four grains per thread
     return (0, 1, 2, 3, 4, 5) if op in ADVECTION else (0, 1, 2)
 
 

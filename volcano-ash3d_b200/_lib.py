@@ -72,7 +72,7 @@ class GridDesc(C.Structure):
 class InvDesc(C.Structure):
     _fields_ = [("ivent", C.c_int32), ("jvent", C.c_int32), ("nbins", C.c_int32), ("misfit", C.c_int32),
                 ("fast_dt", C.c_int32), ("load_from", C.c_int32), ("dep_from", C.c_int32), ("adj_from", C.c_int32),
-                ("sim_hours", C.c_double), ("snapshot_bytes", C.c_double)]
+                ("sim_hours", C.c_double), ("snapshot_bytes", C.c_double), ("met_cache", C.c_int32)]
 
 
 MISFIT_LOAD, MISFIT_DEPOSIT = 1, 2

@@ -254,17 +254,22 @@ class InversionGPU:
     reverse sweep execute in the library with no per-step host call.
 
     Control p: (nz, nbins, ns) mass rates (kg/h).  Observations: the hourly
-    column loads (hours, nx, ny) and the deposit thickness (nx, ny)."""
+    column loads (hours, nx, ny) and the deposit thickness (nx, ny).  Met
+    steps come from `met` (anything with step(hour) -> (vx, vy, vz); default
+    the configuration's synthetic source); met_cache=False keeps them out of
+    the device cache, so that large grids leave that memory to checkpoints."""
 
     def __init__(self, model, cfg: syn.Config, hours: int, obs: dict | None = None,
                  obs_dep: np.ndarray | None = None, nbins: int | None = None, load_from: int = 0,
-                 dep_from: int = 0, fast_dt: bool = False, snapshot_bytes: float = 0.0, adj_from: int = 0):
+                 dep_from: int = 0, fast_dt: bool = False, snapshot_bytes: float = 0.0, adj_from: int = 0,
+                 met=None, met_cache: bool = True):
         import ctypes as C
         from . import _lib
         self.model, self.cfg, self.hours = model, cfg, hours
         self.nbins = hours if nbins is None else nbins
         self.C, self._lib = C, _lib
-        self.met = syn.MetSource(cfg)
+        # anything with step(hour) -> (vx, vy, vz); FP32 Fortran-order arrays pass without a copy
+        self.met = met if met is not None else syn.MetSource(cfg)
         self._keep = []
 
         def provider(user, hour, pvx, pvy, pvz):
@@ -287,6 +292,7 @@ class InversionGPU:
             d.misfit = _lib.MISFIT_LOAD
         d.fast_dt, d.load_from, d.dep_from, d.adj_from = int(fast_dt), load_from, dep_from, adj_from
         d.sim_hours, d.snapshot_bytes = float(hours), float(snapshot_bytes)
+        d.met_cache = 0 if met_cache else 1
         nxy = (cfg.nx, cfg.ny)
         ol = np.zeros((hours, cfg.ny, cfg.nx))
         for h, y in (obs or {}).items():
@@ -317,9 +323,9 @@ class InversionGPU:
         c, L = self.cfg, self._lib
         loads = np.zeros((self.hours, c.ny, c.nx))
         dep = np.zeros((c.ny, c.nx))
-        st = (self.C.c_int64 * 3)()
+        st = (self.C.c_int64 * 4)()
         L.check(self.model.lib.a3g_inv_observations(self.model.ctx, L.dptr(loads), L.dptr(dep), st))
-        self.stats = {"steps": st[0], "slots": st[1], "recomputed": st[2]}
+        self.stats = {"steps": st[0], "slots": st[1], "recomputed": st[2], "window_steps": st[3]}
         return loads.transpose(0, 2, 1).copy(), dep.T.copy()
 
     def adjoint(self, w_load: np.ndarray | None = None, w_dep: np.ndarray | None = None) -> np.ndarray:

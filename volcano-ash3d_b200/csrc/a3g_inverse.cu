@@ -65,7 +65,7 @@ struct a3g_inv {
   double *tl0, *tl1, *tl_dep;  // tangent-linear state and deposit
   float *met_cache;   // every met step of the run on the device (or null)
   int met_cache_n;
-  int cur_pair;       // met pair loaded in the context's slots (-1: none)
+  int slot_hour[3];   // met step each of the context's three met slots holds (-1: none)
   std::vector<double *> slots;
   size_t max_slots;
   double J;
@@ -246,7 +246,25 @@ int dev_alloc(a3g_ctx *ctx, double **p, size_t n) {
                                                                              : ifail(A3G_ERR_CUDA, "memset");
 }
 
-// the met pair (hour, hour+1) into the context's slots, or its place in the cache
+// the met step `hour` from the provider into met slot `slot`
+int upload_met(a3g_ctx *ctx, a3g_inv *v, int hour, int slot) {
+  const float *a[3];
+  if (v->met(v->user, hour, &a[0], &a[1], &a[2])) return ifail(A3G_ERR_ARG, "the met-step provider failed");
+  const long n = ctx->met_n;
+  for (int q = 0; q < 3; q++) {
+    if (!a[q]) return ifail(A3G_ERR_ARG, "the met-step provider returned a null array");
+    // a copy from pageable memory returns once the source has been staged,
+    // so the provider may reuse its buffers after this call
+    A3G_CUDA(cudaMemcpyAsync(ctx->met + (size_t)3 * n * slot + (size_t)q * n, a[q], sizeof(float) * n,
+                             cudaMemcpyHostToDevice, ctx->stream));
+  }
+  v->slot_hour[slot] = hour;
+  return A3G_OK;
+}
+
+// the met pair (hour, hour+1): its place in the cache, or the context's met
+// slots, which keep the steps they hold: a run that moves on by one hour
+// (forward) or back by one hour (the reversal) uploads one step, not two
 int load_pair(a3g_ctx *ctx, a3g_inv *v, int hour, const float **last, const float **next) {
   const long n = ctx->met_n ? ctx->met_n : (long)ctx->grid.nx * ctx->grid.ny * ctx->grid.nz;
   if (v->met_cache && hour + 1 < v->met_cache_n) {
@@ -254,16 +272,47 @@ int load_pair(a3g_ctx *ctx, a3g_inv *v, int hour, const float **last, const floa
     *next = v->met_cache + (size_t)3 * n * (hour + 1);
     return A3G_OK;
   }
-  if (v->cur_pair != hour) {
+  int rc;
+  if (!ctx->met) {  // the slots do not exist yet: a3g_set_met_steps allocates them
     const float *a[3], *b[3];
     if (v->met(v->user, hour, &a[0], &a[1], &a[2]) || v->met(v->user, hour + 1, &b[0], &b[1], &b[2]))
       return ifail(A3G_ERR_ARG, "the met-step provider failed");
-    int rc = a3g_set_met_steps(ctx, a[0], a[1], a[2], b[0], b[1], b[2]);
-    if (rc) return rc;
-    v->cur_pair = hour;
+    if ((rc = a3g_set_met_steps(ctx, a[0], a[1], a[2], b[0], b[1], b[2]))) return rc;
+    v->slot_hour[ctx->met_last] = hour;
+    v->slot_hour[ctx->met_next] = hour + 1;
+    v->slot_hour[ctx->met_spare] = -1;
+  } else {
+    const int want[2] = {hour, hour + 1};
+    int at[2] = {-1, -1};
+    for (int q = 0; q < 2; q++)
+      for (int s = 0; s < 3; s++)
+        if (v->slot_hour[s] == want[q]) at[q] = s;
+    for (int q = 0; q < 2; q++) {
+      if (at[q] >= 0) continue;
+      int s = 0;  // a slot that holds neither step of the pair
+      while (s < 3 && (s == at[1 - q] || v->slot_hour[s] == want[0] || v->slot_hour[s] == want[1])) s++;
+      if (s == 3) return ifail(A3G_ERR_STATE, "no free met slot");  // cannot happen: one step is missing
+      if ((rc = upload_met(ctx, v, want[q], s))) return rc;
+      at[q] = s;
+    }
+    ctx->met_last = at[0];
+    ctx->met_next = at[1];
+    ctx->met_spare = 3 - at[0] - at[1];
   }
   *last = ctx->met + (size_t)3 * n * ctx->met_last;
   *next = ctx->met + (size_t)3 * n * ctx->met_next;
+  return A3G_OK;
+}
+
+// The inversion's runs use the context's three met slots as their own: a
+// prefetch still pending is waited for and dropped, and what the slots hold
+// is forgotten, since other calls may have written them since the last run.
+int claim_met_slots(a3g_ctx *ctx, a3g_inv *v) {
+  for (int s = 0; s < 3; s++) v->slot_hour[s] = -1;
+  if (ctx->met && ctx->met_prefetched) {
+    A3G_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->met_copy_ev, 0));
+    ctx->met_prefetched = false;
+  }
   return A3G_OK;
 }
 
@@ -407,7 +456,7 @@ int inv_ready(a3g_ctx *ctx) {
   if (ctx->prm.fast_subgrid) return ifail(A3G_ERR_UNSUPPORTED, "the inversion needs fast_subgrid off");
   if (ctx->topo_on) return ifail(A3G_ERR_UNSUPPORTED, "the inversion does not cover the terrain terms");
   if (ctx->umb_on) return ifail(A3G_ERR_UNSUPPORTED, "the inversion covers the vent-column source only");
-  return A3G_OK;
+  return claim_met_slots(ctx, ctx->inv);
 }
 
 }  // namespace
@@ -436,6 +485,7 @@ extern "C" int a3g_inv_setup(a3g_ctx *ctx, const a3g_inv_desc *d, a3g_met_provid
   if (!(d->sim_hours >= 1.0) || d->sim_hours != std::floor(d->sim_hours))
     return ifail(A3G_ERR_ARG, "sim_hours must be a whole number of hours >= 1");
   if ((d->misfit & ~3) || !d->misfit) return ifail(A3G_ERR_ARG, "misfit must be A3G_MISFIT_LOAD and/or A3G_MISFIT_DEPOSIT");
+  if (d->met_cache != 0 && d->met_cache != 1) return ifail(A3G_ERR_ARG, "met_cache must be 0 or 1");
   if ((d->misfit & A3G_MISFIT_LOAD) && !obs_load) return ifail(A3G_ERR_ARG, "column-load misfit without observations");
   if ((d->misfit & A3G_MISFIT_DEPOSIT) && !obs_dep) return ifail(A3G_ERR_ARG, "deposit misfit without an observation");
   if (d->dep_from < 0 || d->dep_from >= (int)d->sim_hours || d->load_from < 0 || d->adj_from < 0 ||
@@ -454,7 +504,7 @@ extern "C" int a3g_inv_setup(a3g_ctx *ctx, const a3g_inv_desc *d, a3g_met_provid
   v->met = met;
   v->user = user;
   v->nhours = (int)d->sim_hours;
-  v->cur_pair = -1;
+  if ((rc = claim_met_slots(ctx, v))) return rc;
   if ((rc = a3g_adj_enable(ctx))) return rc;
   ctx->box = Box{1, nx, 1, ny, 1, nz};
   const size_t ctl = (size_t)nz * d->nbins * ns, plane = (size_t)nx * ny;
@@ -475,7 +525,7 @@ extern "C" int a3g_inv_setup(a3g_ctx *ctx, const a3g_inv_desc *d, a3g_met_provid
     const size_t need = sizeof(float) * 3 * (size_t)n3 * nmet;
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
-    if (need <= fr / 4 && cudaMalloc((void **)&v->met_cache, need) == cudaSuccess) {
+    if (d->met_cache == 0 && need <= fr / 4 && cudaMalloc((void **)&v->met_cache, need) == cudaSuccess) {
       ctx->bytes += need;
       v->met_cache_n = nmet;
       for (int h = 0; h < nmet; h++) {
@@ -796,6 +846,7 @@ extern "C" int a3g_inv_observations(a3g_ctx *ctx, double *loads, double *dep, in
     stats[0] = (int64_t)v->steps.size();
     stats[1] = (int64_t)v->max_slots;
     stats[2] = (int64_t)v->recomputed;
+    stats[3] = (int64_t)v->steps.size() - first_reversed(v);
   }
   return sync_check(ctx);
 }

@@ -161,6 +161,10 @@ def make_config(name: str) -> Config:
                       fall_mps=(0.05, 0.4, 1.5), bin_mass=(0.3, 0.3, 0.4), plume_km=8.0,
                       volume_km3=1.0e-3, duration_h=1.0, use_cn=True, sim_hours=1.0,
                       winds="random", seed=17)
+    if name == "tiny_deep":  # z lines of 80 cells, as in the 1500x1000x80 scale workload
+        return Config("tiny_deep", 26, 14, 80, 2, dx=3.0, dy=3.0, dz=0.4, ivent=13, jvent=7,
+                      fall_mps=(0.1, 1.0), bin_mass=(0.5, 0.5), plume_km=20.0, volume_km3=1.0e-3,
+                      duration_h=1.0, use_cn=True, sim_hours=1.0, winds="random", seed=19)
     if name == "tiny_stretch":  # lon/lat CN, x lines of 3 tiles, dz changing part-way up
         return Config("tiny_stretch", 75, 10, 24, 2, latlon=True, de=0.5, dn=0.5, lonLL=20.0,
                       latLL=40.0, dz=0.3, dz_profile=(0.3,) * 10 + (0.45,) * 8 + (0.7,) * 6,
