@@ -277,6 +277,17 @@ int a3g_cfl_maxima(a3g_ctx *ctx, double *vmax3);
 int a3g_adjust_dt_from_maxima(a3g_ctx *ctx, const double *vmax3, int32_t n_gs_aloft_total,
                               double time, double next_write_time, double simtime,
                               double *dt_out);
+/* The same two halves with the maxima kept on the device, for a sharded loop
+ * that does not wait on the GPU (the same sources): a3g_cfl_maxima_device
+ * queues the reduction on the context's stream into three doubles of the
+ * context's device memory and returns their address (fixed for the
+ * context's life); the caller all-reduces them (MAX) in place, ordered on
+ * the context's stream (a3g_get_stream); a3g_adjust_dt_device_maxima_async
+ * then forms dt from them on the device and queues its copy to the host,
+ * which a3g_wait_dt returns, as a3g_adjust_dt_async does. */
+int a3g_cfl_maxima_device(a3g_ctx *ctx, double **vmax3_dev);
+int a3g_adjust_dt_device_maxima_async(a3g_ctx *ctx, int32_t n_gs_aloft_total, double time,
+                                      double next_write_time, double simtime);
 /* ---- FAST_DT: the time step of the reference's default build
  *      (FASTFPPFLAG = -DFAST_DT, src/makefile:91) ----
  * With FAST_DT the CFL maxima are taken only when a met step is loaded, on the

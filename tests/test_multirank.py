@@ -25,7 +25,45 @@ def _free_port() -> int:
         return s.getsockname()[1]
 
 
-def _rank_main(rank: int, world: int, port: int, cfg_name: str, steps: int, out_dir: str, fast: bool = False):
+def _pipelined_oracle(orc, syn):
+    """The oracle with the entry points of the lag-one loop (driver.Pipeline)
+    that the device provides: the scheduled source, the queued totals, and
+    the CFL maxima in a buffer the ranks all-reduce in place."""
+
+    class PipelinedOracle(orc.OracleModel):
+        def set_source_pulses(self, ivent, jvent, pulses, norm_col):
+            self._pulses, self._norm_col, self._state = pulses, norm_col, [1, 1]
+            self._kappa = syn.geometry(self.cfg)["kappa"]
+
+        def add_source_scheduled(self, time):
+            dt = self._dt_pending
+            flux = syn.scheduled_source_flux(self.cfg, self._pulses, self._norm_col, self._kappa, self._state,
+                                             time, dt)
+            if flux is not None:
+                self.add_source(flux, dt)
+
+        def totals_async(self):  # the totals of this state, kept under a ticket
+            self._tots = getattr(self, "_tots", {})
+            t = self._ticket = getattr(self, "_ticket", -1) + 1
+            self._tots[t] = self.TimeStepTotals()
+            return t
+
+        def totals_get(self, ticket):
+            return self._tots.pop(ticket)
+
+        def cfl_maxima_device(self):
+            self._vmax = self.cfl_maxima()
+            return self._vmax
+
+        def adjust_dt_device_maxima_async(self, n_gs_aloft_total, time, next_write_time, simtime):
+            self._dt_pending = self.adjust_dt_from_maxima(self._vmax, n_gs_aloft_total, time, next_write_time,
+                                                          simtime)
+
+    return PipelinedOracle
+
+
+def _rank_main(rank: int, world: int, port: int, cfg_name: str, steps: int, out_dir: str, fast: bool = False,
+               pipelined: bool = False):
     sys.path.insert(0, str(ROOT / "tests"))
     sys.path.insert(0, str(ROOT / "oracle"))
     import torch.distributed as dist
@@ -41,7 +79,7 @@ def _rank_main(rank: int, world: int, port: int, cfg_name: str, steps: int, out_
         import dataclasses
         gcfg = dataclasses.replace(syn.make_config(cfg_name), fast_dt=fast)
         cfg = pkg.split_grains(gcfg, rank, world)
-        model = orc.OracleModel(cfg, threads=1)
+        model = (_pipelined_oracle(orc, mod.synthetic) if pipelined else orc.OracleModel)(cfg, threads=1)
 
         class CountingComm(pkg.Comm):
             max_calls = 0
@@ -50,8 +88,15 @@ def _rank_main(rank: int, world: int, port: int, cfg_name: str, steps: int, out_
                 CountingComm.max_calls += 1
                 return super().max(a)
 
+            def max_inplace(self, buf):
+                CountingComm.max_calls += 1
+                return super().max_inplace(buf)
+
         comm = CountingComm()
-        st = pkg.run(model, cfg, max_steps=steps, comm=comm, n_gs_aloft_total=gcfg.ns)
+        if pipelined:
+            st = pkg.run_pipelined(model, cfg, max_steps=steps, comm=comm, n_gs_aloft_total=gcfg.ns)
+        else:
+            st = pkg.run(model, cfg, max_steps=steps, comm=comm, n_gs_aloft_total=gcfg.ns)
         hist = np.array([[r.time, r.dt, r.aloft, r.dep, r.outflow, r.tot] for r in st.history])
         np.savez(os.path.join(out_dir, f"rank{rank}.npz"), hist=hist, conc=model.interior(),
                  dep=model.outflows()["deposit"], max_calls=CountingComm.max_calls, hour=st.hour)
@@ -59,11 +104,11 @@ def _rank_main(rank: int, world: int, port: int, cfg_name: str, steps: int, out_
         dist.destroy_process_group()
 
 
-def _sharded(cfg_name: str, world: int, steps: int, tmp_path, fast: bool = False):
+def _sharded(cfg_name: str, world: int, steps: int, tmp_path, fast: bool = False, pipelined: bool = False):
     import torch.multiprocessing as mp
     port = _free_port()
     ctx = mp.get_context("spawn")
-    procs = [ctx.Process(target=_rank_main, args=(r, world, port, cfg_name, steps, str(tmp_path), fast))
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, cfg_name, steps, str(tmp_path), fast, pipelined))
              for r in range(world)]
     for p in procs:
         p.start()
@@ -77,16 +122,21 @@ def _sharded(cfg_name: str, world: int, steps: int, tmp_path, fast: bool = False
     return [np.load(tmp_path / f"rank{r}.npz") for r in range(world)]
 
 
-@pytest.mark.parametrize("cfg_name,steps,fast", [("tiny_proj", 12, False), ("tiny_latlon", 8, False),
-                                                 ("tiny_proj", None, True), ("tiny_latlon", None, True)])
-def test_grain_sharded_matches_single(pkg, oracle_mod, cfg_name, steps, fast, tmp_path):
+@pytest.mark.parametrize("cfg_name,steps,fast,pipelined", [
+    ("tiny_proj", 12, False, False), ("tiny_latlon", 8, False, False),
+    ("tiny_proj", None, True, False), ("tiny_latlon", None, True, False),
+    ("tiny_proj", 12, False, True), ("tiny_latlon", None, True, True)])
+def test_grain_sharded_matches_single(pkg, oracle_mod, cfg_name, steps, fast, pipelined, tmp_path):
     """With FAST_DT the ranks exchange the CFL maxima only at the met-step
-    loads (the first pair: two, then one per later load), not every step."""
+    loads (the first pair: two, then one per later load), not every step.
+    The pipelined sharded loop (driver.Pipeline with a Comm: maxima all-
+    reduced in place, the totals summed when a record is collected) gives the
+    same bits as the plain single-process loop."""
     import dataclasses
     syn, drv = pkg.synthetic, pkg.driver
     gcfg = dataclasses.replace(syn.make_config(cfg_name), fast_dt=fast)
     world = 2
-    ranks = _sharded(cfg_name, world, steps, tmp_path, fast)
+    ranks = _sharded(cfg_name, world, steps, tmp_path, fast, pipelined)
 
     ref = oracle_mod.OracleModel(gcfg, threads=1)
     st = drv.run(ref, gcfg, max_steps=steps)

@@ -36,7 +36,8 @@ EXPORTED = [
     "a3g_diffuse_horz", "a3g_diffuse_vert", "a3g_adjust_dt", "a3g_timestep_totals",
     "a3g_get_minmax_index", "a3g_set_subgrid", "a3g_get_subgrid", "a3g_step",
     "a3g_kernel_launches", "a3g_get_stream", "a3g_kernel_timing", "a3g_kernel_times",
-    "a3g_cfl_maxima", "a3g_adjust_dt_from_maxima", "a3g_selftest_div", "a3g_set_variant",
+    "a3g_cfl_maxima", "a3g_adjust_dt_from_maxima", "a3g_cfl_maxima_device",
+    "a3g_adjust_dt_device_maxima_async", "a3g_selftest_div", "a3g_set_variant",
     "a3g_get_variant", "a3g_mass_aloft_noalloc",
     "a3g_adj_enable", "a3g_adj_zero", "a3g_adj_set_lambda", "a3g_adj_get_lambda",
     "a3g_adj_set_lambda_dep", "a3g_adj_get_lambda_dep", "a3g_adj_advect_x", "a3g_adj_advect_y",
@@ -166,6 +167,8 @@ def load(path: os.PathLike | str | None = None) -> C.CDLL:
                                              C.c_int64, D, C.c_void_p]),
         "a3g_selftest_div": (C.c_int, [C.c_int, C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)]),
         "a3g_adjust_dt_from_maxima": (C.c_int, [P, D, C.c_int32, C.c_double, C.c_double, C.c_double, D]),
+        "a3g_cfl_maxima_device": (C.c_int, [P, C.POINTER(D)]),
+        "a3g_adjust_dt_device_maxima_async": (C.c_int, [P, C.c_int32, C.c_double, C.c_double, C.c_double]),
         "a3g_set_fall_velocity_meso": (C.c_int, [P, F, C.c_int32]),
         "a3g_cfl_maxima_meso": (C.c_int, [P, C.c_int32, D]),
         "a3g_adjust_dt_meso": (C.c_int, [P, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, D]),

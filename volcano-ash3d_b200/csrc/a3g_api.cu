@@ -1131,6 +1131,32 @@ int a3g_adjust_dt_from_maxima(a3g_ctx *ctx, const double *vmax3, int32_t n_gs_al
   return A3G_OK;
 }
 
+int a3g_cfl_maxima_device(a3g_ctx *ctx, double **vmax3_dev) {
+  CTX_CHECK(ctx);
+  if (!vmax3_dev) return fail(A3G_ERR_ARG, "null output");
+  if (!ctx->have_geometry || !ctx->have_vf || !ctx->have_winds)
+    return fail(A3G_ERR_STATE, "geometry, fall velocities and winds must be set");
+  int rc = launch_cfl_maxima(ctx);
+  if (rc) return rc;
+  *vmax3_dev = ctx->sc->vmax;
+  return A3G_OK;
+}
+
+int a3g_adjust_dt_device_maxima_async(a3g_ctx *ctx, int32_t n_gs_aloft_total, double time,
+                                      double next_write_time, double simtime) {
+  CTX_CHECK(ctx);
+  if (ctx->prm.use_diffusion && !ctx->have_diffusivity) return fail(A3G_ERR_STATE, "diffusivity not set");
+  int rc = launch_dt_from_maxima(ctx, n_gs_aloft_total, time, next_write_time, simtime);
+  if (rc) return rc;
+  ctx->dt_stamp++;
+  const int slot = (int)(ctx->dt_seq % 4);
+  A3G_CUDA(cudaMemcpyAsync(ctx->h_sc_ring + slot, ctx->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+  A3G_CUDA(cudaEventRecord(ctx->sc_ev[slot], ctx->stream));
+  ctx->dt_seq++;
+  return A3G_OK;
+}
+
 // ---- FAST_DT (src/makefile:91; src/Adjust_dt.f90:96-135, src/MesoInterpolater.f90:
 // 142-150, 187-195, 250-258) ------------------------------------------------
 int a3g_set_fall_velocity_meso(a3g_ctx *ctx, const float *vf_meso_sp, int32_t per_grain) {

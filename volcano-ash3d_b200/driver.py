@@ -75,6 +75,21 @@ class Comm:
     def max(self, a):
         return self._reduce(a, self.dist.ReduceOp.MAX)
 
+    def max_inplace(self, buf):
+        """MAX all-reduce of ``buf`` in place, with no host read-back: a numpy
+        array (a CPU group), or device memory with __cuda_array_interface__
+        and the `stream` its producer was queued on (model.cfl_maxima_device),
+        in which case the collective is ordered on that stream and the
+        stream's later work waits for it."""
+        torch = self.torch
+        t = torch.as_tensor(buf) if isinstance(buf, np.ndarray) else torch.as_tensor(buf, device=self.device)
+        stream = getattr(buf, "stream", None)
+        if t.is_cuda and stream is not None:
+            with torch.cuda.stream(torch.cuda.ExternalStream(stream, device=t.device)):
+                self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX, group=self.group)
+        else:
+            self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX, group=self.group)
+
     def sum(self, a):
         return self._reduce(a, self.dist.ReduceOp.SUM)
 
@@ -131,16 +146,20 @@ class Comm:
 
 def shard_config(cfg: syn.Config, rank: int, world: int) -> syn.Config:
     """Grain sharding: the global run has ns*world grain bins (fall speeds
-    log-spaced over the global range, equal mass fractions); rank r keeps bins
-    [r*ns, (r+1)*ns).  Every operator acts on grains independently, so only
-    dt (a MAX over all grains' settling speeds) and the totals couple ranks."""
+    log-spaced over the global range, equal mass fractions); rank r keeps
+    bins r, r+world, r+2*world, ...  Dealing the bins round-robin gives every
+    rank the same spread of fall speeds, so the fast-settling bins, which
+    leave the domain early and stop costing anything, are spread over the
+    ranks instead of idling the last ones.  Every operator acts on grains
+    independently, so only dt (a MAX over all grains' settling speeds) and
+    the totals couple ranks."""
     if world == 1:
         return cfg
     ns = cfg.ns
     lo, hi = min(cfg.fall_mps), max(cfg.fall_mps)
     fall = np.logspace(math.log10(lo), math.log10(hi), ns * world)
     c = dataclasses.replace(cfg)
-    c.fall_mps = tuple(float(v) for v in fall[rank * ns:(rank + 1) * ns])
+    c.fall_mps = tuple(float(v) for v in fall[rank::world])
     c.bin_mass = tuple(1.0 / (ns * world) for _ in range(ns))
     return c
 
@@ -327,14 +346,25 @@ class Pipeline:
     only for the early Adjust_DT copy while the GPU runs the step's sweeps,
     and needs it for the next step's time.  The totals of a step are
     collected after the next step is queued.  The host mirrors the source
-    arithmetic for SourceCumulativeVol once it knows dt.  Single rank, vent-
-    column sources, FAST_SUBGRID off (the subgrid box needs the state on the
-    host every step)."""
+    arithmetic for SourceCumulativeVol once it knows dt.  Vent-column
+    sources, FAST_SUBGRID off (the subgrid box needs the state on the host
+    every step).
 
-    def __init__(self, model, cfg: syn.Config, geo: dict | None = None):
+    With ``comm`` (a grain-sharded run) the CFL maxima are all-reduced on the
+    device, in place and ordered on the context's stream
+    (model.cfl_maxima_device, Comm.max_inplace,
+    model.adjust_dt_device_maxima_async), so the loop still queues each step
+    without waiting; with FAST_DT they are exchanged only at met-step loads.
+    The totals and SourceCumulativeVol are summed over the ranks when a step's
+    record is collected."""
+
+    def __init__(self, model, cfg: syn.Config, geo: dict | None = None, comm: Comm | None = None,
+                 n_gs_aloft_total: int | None = None):
         if cfg.fast_subgrid or syn.is_umbrella(cfg):
             raise ValueError("the pipelined loop needs FAST_SUBGRID off and a vent-column source")
         self.model, self.cfg = model, cfg
+        self.comm = comm
+        self.n_total = cfg.ns if n_gs_aloft_total is None else n_gs_aloft_total
         self.st = new_state(cfg, geo)
         self.pulses = syn.eruption_pulses(cfg)
         model.set_source_pulses(cfg.ivent, cfg.jvent, self.pulses, self.st.norm_col)
@@ -350,13 +380,16 @@ class Pipeline:
         h = met_hour(st)
         loaded = update_met(m, st, h)
         if cfg.fast_dt and loaded:
-            meso_dt(m, st, loaded, nwt, simtime, wait=False)
+            meso_dt(m, st, loaded, nwt, simtime, self.comm, self.n_total, wait=False)
         frac = st.time - h
         m.interp_winds(frac)
         if cfg.fast_dt:
             m.fast_dt_async(frac, st.time, nwt, simtime)
-        else:
+        elif self.comm is None:
             m.adjust_dt_async(st.time, nwt, simtime)
+        else:
+            self.comm.max_inplace(m.cfl_maxima_device())
+            m.adjust_dt_device_maxima_async(self.n_total, st.time, nwt, simtime)
         m.add_source_scheduled(st.time)
         m.Set_BC(1)
         m.AdvectHorz(st.itime)
@@ -381,6 +414,9 @@ class Pipeline:
         if self.pending is not None:
             rec, ticket = self.pending
             vols, _ = self.model.totals_get(ticket)
+            if self.comm is not None:  # one SUM of the totals and SourceCumulativeVol
+                s = self.comm.sum(np.append(np.asarray(vols, dtype=np.float64), rec.source_cum))
+                vols, rec.source_cum = s[:4], float(s[4])
             rec.aloft, rec.dep, rec.outflow, rec.tot = (float(v) for v in vols)
             self.pending = None
 
@@ -391,9 +427,10 @@ class Pipeline:
 
 
 def run_pipelined(model, cfg: syn.Config, max_steps: int | None = None, sim_hours: float | None = None,
-                  geo: dict | None = None, totals: bool = True) -> RunState:
+                  geo: dict | None = None, totals: bool = True, comm: Comm | None = None,
+                  n_gs_aloft_total: int | None = None) -> RunState:
     """run() through the lag-one loop (Pipeline)."""
-    p = Pipeline(model, cfg, geo)
+    p = Pipeline(model, cfg, geo, comm, n_gs_aloft_total)
     simtime = cfg.sim_hours if sim_hours is None else sim_hours
     while p.st.time < simtime and (max_steps is None or p.st.itime < max_steps):
         p.step(simtime, totals)

@@ -20,6 +20,20 @@ from . import synthetic as syn
 from ._lib import check, dptr, fptr, iptr
 
 
+class DeviceDoubles:
+    """A few doubles in a context's device memory, exposed through
+    __cuda_array_interface__ so that torch.as_tensor wraps them without a
+    copy; `stream` is the context's stream, on which their producer was
+    queued."""
+
+    def __init__(self, ptr: int, n: int, stream: int):
+        self.ptr, self.n, self.stream = ptr, n, stream
+
+    @property
+    def __cuda_array_interface__(self):
+        return {"shape": (self.n,), "typestr": "<f8", "data": (self.ptr, False), "version": 3}
+
+
 class Ash3dGPU:
     def __init__(self, cfg: syn.Config, device: int = 0, geo: dict | None = None,
                  limiter: str | None = None, use_winds_fp64: bool = False):
@@ -132,6 +146,19 @@ class Ash3dGPU:
         v = np.zeros(3)
         check(self.lib.a3g_cfl_maxima(self.ctx, dptr(v)))
         return v
+
+    def cfl_maxima_device(self) -> "DeviceDoubles":
+        """The three CFL maxima reduced on the context's stream into device
+        memory (a3g_cfl_maxima_device), as an object a torch all-reduce can
+        work on in place (__cuda_array_interface__)."""
+        ptr = C.POINTER(C.c_double)()
+        check(self.lib.a3g_cfl_maxima_device(self.ctx, C.byref(ptr)))
+        return DeviceDoubles(C.cast(ptr, C.c_void_p).value, 3, self.stream_handle())
+
+    def adjust_dt_device_maxima_async(self, n_gs_aloft_total: int, time: float, next_write_time: float,
+                                      simtime: float):
+        check(self.lib.a3g_adjust_dt_device_maxima_async(self.ctx, n_gs_aloft_total, time, next_write_time,
+                                                         simtime))
 
     def adjust_dt_from_maxima(self, vmax3, n_gs_aloft_total: int, time: float,
                               next_write_time: float, simtime: float) -> float:
