@@ -72,8 +72,8 @@ static bool same(double x, double y) {
 
 static void pair_of(int fam, std::mt19937_64 &r, double &a, double &b) {
   switch (fam) {
-    case 0:  // exponents across and beyond the fast range [-200, 200]
-      a = make(r, -230, 230);
+    case 0:  // exponents across and beyond the fast ranges (dividends to 2^+-1000, divisors to 2^+-230)
+      a = make(r, -1000, 1000);
       b = make(r, -230, 230);
       break;
     case 1: {  // quotients within a few ulps of a power of two or of an integer
@@ -89,6 +89,13 @@ static void pair_of(int fam, std::mt19937_64 &r, double &a, double &b) {
       a = c * (1.0 + std::ldexp((double)(r() % 4096) - 2048.0, -20)) - c;
       b = c * (1.0 + std::ldexp((double)(r() % 4096) - 2048.0, -18)) - c;
       if (b == 0.0) b = c;
+      break;
+    }
+    case 3: {  // tails of a diffused cloud: tiny dividends (down to subnormal) over pivots in [1, 4)
+      const int e = -1080 + (int)(r() % 931);  // -1080 .. -150
+      a = make(r, 0, 0);
+      a = std::ldexp(a, e);  // rounds into the subnormal range below 2^-1022
+      b = make(r, 0, 1);
       break;
     }
     default: {  // specials: zeros, infinities, NaN, subnormals, equal operands
@@ -107,10 +114,10 @@ int main(int argc, char **argv) {
   const long n = argc > 1 ? std::atol(argv[1]) : 200000;
   const uint64_t seed = argc > 2 ? std::strtoull(argv[2], nullptr, 10) : 1;
   const double rels[] = {0.0, 1.2e-7, 6.0e-5, 4.0e-3, 0.2};
-  const char *fams[] = {"wide", "near_exact", "limiter", "special"};
+  const char *fams[] = {"wide", "near_exact", "limiter", "tails", "special"};
   int bad_total = 0;
   for (int f = 0; f < 2; f++) {
-    for (int fam = 0; fam < 4; fam++) {
+    for (int fam = 0; fam < 5; fam++) {
       for (double rel : rels) {
         g_rel = rel;
         std::mt19937_64 r(seed * 1000 + fam);

@@ -34,7 +34,7 @@ def results(tmp_path_factory):
         if len(f) == 9 and f[3] == "pairs":
             rows[(f[0], f[1], float(f[2]))] = dict(n=int(f[4]), bad=int(f[6]), fallbacks=int(f[8]))
     assert out.returncode == 0, out.stdout[-2000:]
-    assert len(rows) == 40
+    assert len(rows) == 50
     return rows
 
 
@@ -52,8 +52,18 @@ def test_fast_path_takes_in_range_quotients(results):
 
 def test_poor_estimates_fall_back(results):
     # a 20 % estimate defeats the iteration: the IEEE operator answers, still exactly
-    for fam in ("wide", "near_exact", "limiter", "special"):
+    for fam in ("wide", "near_exact", "limiter", "tails", "special"):
         r = results[("div_rn", fam, 0.2)]
         assert r["fallbacks"] > 0.9 * r["n"], (fam, r)
     # out-of-range operands always take the IEEE operator
     assert results[("div_rn", "wide", 0.0)]["fallbacks"] > 0.1 * 200000
+
+
+def test_tails_take_the_fast_path(results):
+    # dividends down a diffused cloud's tail over pivots in [1, 4): the back
+    # substitution's fast path certifies every dividend of 2^-900 and above
+    # (81 % of the family's exponents, -1080 .. -150); the rest, down to the
+    # subnormals, goes to the IEEE operator
+    r = results[("div_rn_rcp", "tails", 0.0)]
+    assert r["bad"] == 0
+    assert 0.15 * r["n"] < r["fallbacks"] < 0.23 * r["n"], r

@@ -17,15 +17,29 @@
 //        sequential Newton-Raphson steps on y;
 //   r  = a - b*q (exact with an FMA);  q = q + r*y'.
 // The result is then certified exactly: r = a - b*q is computed again with an
-// FMA (exact for a q within an ulp or two of a/b and operands far from the
-// underflow range), and q is accepted only if |r| < |b| * ulp(q)/2, i.e. the
-// true quotient lies strictly inside the rounding interval of q, and q is not
-// a power of two (whose rounding interval is asymmetric).  Everything else --
-// operands outside [2^-200, 2^200], a zero divisor, non-finite values, a
-// residual on or beyond the half-ulp bound -- falls back to the IEEE division
-// operator.  A zero dividend over an in-range divisor returns a*b, the zero
-// whose sign IEEE division gives (the signs' exclusive or).  Every path
-// therefore returns RN(a/b) exactly.
+// FMA, and q is accepted only if |r| < |b| * ulp(q)/2, i.e. the true quotient
+// lies strictly inside the rounding interval of q, and q is not a power of two
+// (whose rounding interval is asymmetric).  Everything else -- operands
+// outside the fast ranges below, a zero divisor, non-finite values, a residual
+// on or beyond the half-ulp bound -- falls back to the IEEE division operator.
+// A zero dividend over an in-range divisor returns a*b, the zero whose sign
+// IEEE division gives (the signs' exclusive or).  Every path therefore
+// returns RN(a/b) exactly.
+//
+// The fast ranges keep every intermediate normal and the residual exact.
+// With q within an ulp or two of a/b, r = a - b*q is a multiple of
+// ulp(b)*ulp(q) = 2^(e_b+e_q-104) smaller than |b|*ulp(q) < 2^(e_b+e_q-51), so
+// it is a double whenever 2^(e_b+e_q-104) >= 2^-1074, i.e. e_a (which is
+// e_b+e_q or one more) >= -969; ulp(q)/2 = 2^(e_q-53) must be normal
+// (e_q >= -969), and nothing may overflow.  Both ranges below give e_a and
+// e_q in [-951, 951]:
+//   div_rn:     |b| in [2^-200, 2^201), |a| in [2^-700, 2^701) or a = 0
+//               (the limiter's theta = dqu/dq divides only when |dq| >= the
+//               cycle threshold, 1e-10 in the reference);
+//   div_rn_rcp: |b| in [2^-50, 2^51), |a| in [2^-900, 2^901) or a = 0
+//               (the back substitution's pivots D' are >= 1 on the
+//               diagonally dominant Crank-Nicolson matrices, and its
+//               dividends run down the diffused tails of a cloud).
 #pragma once
 
 namespace a3g {
@@ -60,10 +74,12 @@ __device__ __forceinline__ double rcp_approx(double b) {
 #endif
 }
 
-// True when |x| is zero or its binary exponent lies in [-200, 200].
-__device__ __forceinline__ bool in_fast_range(double x, bool allow_zero) {
+// True when the binary exponent of x lies in [LO, HI] (or x is zero and
+// ALLOW_ZERO).
+template <int LO, int HI, bool ALLOW_ZERO>
+__device__ __forceinline__ bool exp_in(double x) {
   const unsigned e = ((unsigned)__double2hiint(x) >> 20) & 0x7ffu;
-  return (e - 823u) <= 400u || (allow_zero && x == 0.0);
+  return (e - (unsigned)(1023 + LO)) <= (unsigned)(HI - LO) || (ALLOW_ZERO && x == 0.0);
 }
 
 // Certifies q against a/b (see above); returns true if q == RN(a/b).
@@ -78,7 +94,7 @@ __device__ __forceinline__ bool certified(double a, double b, double q) {
 
 // RN(a/b).
 __device__ __forceinline__ double div_rn(double a, double b) {
-  if (!(in_fast_range(b, false) && in_fast_range(a, true))) return ieee_div(a, b);
+  if (!(exp_in<-200, 200, false>(b) && exp_in<-700, 700, true>(a))) return ieee_div(a, b);
   if (a == 0.0) return a * b;  // +-0 with the quotient's sign (b finite, nonzero)
   double y = rcp_approx(b);
   const double e = fma(-b, y, 1.0);
@@ -96,7 +112,7 @@ __device__ __forceinline__ double div_rn(double a, double b) {
 // RN(a/b) given y = RN(1/b) (precomputed once for a divisor shared by many
 // quotients, e.g. a tridiagonal pivot).
 __device__ __forceinline__ double div_rn_rcp(double a, double b, double y) {
-  if (!(in_fast_range(b, false) && in_fast_range(a, true))) return ieee_div(a, b);
+  if (!(exp_in<-50, 50, false>(b) && exp_in<-900, 900, true>(a))) return ieee_div(a, b);
   if (a == 0.0) return a * b;  // +-0 with the quotient's sign (b finite, nonzero)
   double q = a * y;
   const double r = fma(-b, q, a);

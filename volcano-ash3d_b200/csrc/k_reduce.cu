@@ -1106,9 +1106,12 @@ __device__ double test_operand(uint64_t h) {
   int e;
   if (kind < 8) e = (int)((h >> 5) & 63) - 32;          // moderate magnitudes
   else if (kind < 12) e = (int)((h >> 5) & 1023) - 512;  // wide range (fallbacks)
-  else if (kind < 14) e = (int)((h >> 5) & 15) - 8;
+  else if (kind < 13) e = (int)((h >> 5) & 15) - 8;
+  else if (kind < 14) e = -830 - (int)((h >> 5) & 255);  // tiny, down to subnormal (below)
   else e = (int)((h >> 5) & 7) - 4;
-  double v = __longlong_as_double((long long)(((uint64_t)(1023 + e) << 52) | (kind == 14 ? 0 : m)));
+  double v = __longlong_as_double(
+      (long long)(((uint64_t)(1023 + (kind == 13 ? e + 300 : e)) << 52) | (kind == 14 ? 0 : m)));
+  if (kind == 13) v = v * 0x1p-300;  // exact while normal, rounded below 2^-1022
   if (kind == 15) v = (double)((h >> 20) & 255) - 128.0;  // small integers, zeros, exact ratios
   return sgn * v;
 }
