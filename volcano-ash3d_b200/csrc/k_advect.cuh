@@ -140,6 +140,10 @@ __device__ __forceinline__ LineGeo line_of(const Geo3 &g, int a, int o) {
   return r;
 }
 
+// stride of a broadcast geometry array along sweep direction DIR (0: constant along the line)
+template <int DIR>
+inline long along(const Geo3 &g) { return DIR == 0 ? g.si : DIR == 1 ? g.sj : g.sk; }
+
 struct CkT { static constexpr bool value = true; };     // step with range checks
 struct FastT { static constexpr bool value = false; };  // interior step
 
@@ -447,7 +451,7 @@ __device__ __forceinline__ double fss_select(double dqm, double dq, double dqp, 
   return skip ? 0.0 : cf * ldq;
 }
 
-template <int DIR, int LIM, int V, bool PER, bool CK>
+template <int DIR, int LIM, int V, bool PER, bool CK, bool LC>
 __device__ __forceinline__ void block_body(const Layout &L, const Box &box, int nocycle, double eps,
                                            const double *__restrict__ line, double *__restrict__ oline,
                                            long st, const double *__restrict__ pv,
@@ -492,12 +496,16 @@ __device__ __forceinline__ void block_body(const Layout &L, const Box &box, int 
       }
     }
   }
+  // LC: sigma, dt/kappa and (z) the fall speed do not vary along the line
+  // (zero broadcast stride), so one load of each serves every index
+  const double sig_c = LC ? gsig.p[0] : 0.0, dtv_c = LC ? gdtv.p[0] : 0.0;
   if (DIR == 2) {
+    const double vf_c = LC ? pvf[0] : 0.0;
 #pragma unroll
     for (int m = 0; m < V + 4; m++) {
       const int c = c0 - 2 + m;
       const int cl = CK ? (c < 1 ? 1 : (c > n ? n : c)) : c;
-      vw[m] = vw[m] + pvf[(long)(cl + 1) * vfs];
+      vw[m] = vw[m] + (LC ? vf_c : pvf[(long)(cl + 1) * vfs]);
     }
   }
   auto fs_ok = [&](int I) { return !CK || (I >= rmin - 1 && I <= rmax + 1); };
@@ -507,11 +515,11 @@ __device__ __forceinline__ void block_body(const Layout &L, const Box &box, int 
 #pragma unroll
   for (int u = 0; u < V + 3; u++) {
     const int I = c0 - 1 + u;
-    us[u] = fs_ok(I) ? 0.5 * (vw[u] + vw[u + 1]) * gsig.at(I) : 0.0;
+    us[u] = fs_ok(I) ? 0.5 * (vw[u] + vw[u + 1]) * (LC ? sig_c : gsig.at(I)) : 0.0;
   }
   double dtv[V + 1];
 #pragma unroll
-  for (int m = 0; m <= V; m++) dtv[m] = gdtv.at(c0 + m);
+  for (int m = 0; m <= V; m++) dtv[m] = LC ? dtv_c : gdtv.at(c0 + m);
   // interfaces I = c0+m, m = 0..V
   double fss[V + 1], fsr[V + 1], fsl[V + 1];
 #pragma unroll
@@ -546,10 +554,11 @@ __device__ __forceinline__ void block_body(const Layout &L, const Box &box, int 
   if (CK && al && out_lo && c0 == 1) {
     // cell 0 from interfaces 0 and 1; fss(0) = 0 since rmin = 1
     const double us_m1 = 0.0;  // interface -1 is outside [rmin-1, rmax+1]
-    const Iface f0 = make_iface(us_m1, us[0], us[1], gdtv.at(0), false, true);
+    const double dtv0 = LC ? dtv_c : gdtv.at(0);
+    const Iface f0 = make_iface(us_m1, us[0], us[1], dtv0, false, true);
     const double dq0 = w[1] - w[0];
     const double fsr0 = f0.usp * dq0 + w[1] * f0.divm;
-    const double upd0 = cell_update(gdtv.at(0), fsl[0], fsr0, fss[0], 0.0);
+    const double upd0 = cell_update(dtv0, fsl[0], fsr0, fss[0], 0.0);
     *o1 += upd0;
   }
   if (DIR == 2 && CK && out_hi && ctop < rmin - 1) raise_error(sc, A3G_ERR_UNSUPPORTED, 311);
@@ -567,7 +576,7 @@ __device__ __forceinline__ void block_body(const Layout &L, const Box &box, int 
   }
 }
 
-template <int DIR, int LIM, int V, bool PER>
+template <int DIR, int LIM, int V, bool PER, bool LC>
 // 7 blocks of 128 per SM (at most 72 registers, a few spilled to L1): more
 // warps in flight beat the spills (C2 z sweep 2.15 -> 1.81 ms on B200)
 __global__ void __launch_bounds__(128, 7) k_advect_block(Layout L, Box box, int nocycle, double eps, int nblk,
@@ -623,10 +632,10 @@ __global__ void __launch_bounds__(128, 7) k_advect_block(Layout L, Box box, int 
   const long oo = (long)g * na * nother + (long)(o - 1) * na + (a - 1);
   const bool fast = c0 >= 3 && c0 >= rmin && c0 + V <= rmax && c0 + V <= n - 1;
   if (fast)
-    block_body<DIR, LIM, V, PER, false>(L, box, nocycle, eps, line, oline, st, pv, pvg, pvf, vf.sk, gsig, gdtv,
+    block_body<DIR, LIM, V, PER, false, LC>(L, box, nocycle, eps, line, oline, st, pv, pvg, pvf, vf.sk, gsig, gdtv,
                                         c0, n, lane_active, al, out1 + oo, out2 + oo, sc);
   else
-    block_body<DIR, LIM, V, PER, true>(L, box, nocycle, eps, line, oline, st, pv, pvg, pvf, vf.sk, gsig, gdtv,
+    block_body<DIR, LIM, V, PER, true, LC>(L, box, nocycle, eps, line, oline, st, pv, pvg, pvf, vf.sk, gsig, gdtv,
                                        c0, n, lane_active, al, out1 + oo, out2 + oo, sc);
 }
 
@@ -829,7 +838,7 @@ static void launch_advect_xt(a3g_ctx *ctx) {
 // ---------------------------------------------------------------------------
 constexpr int XW_WARPS = 4;
 
-template <int LIM, int GC, bool PER>
+template <int LIM, int GC, bool PER, bool LC>
 __global__ void __launch_bounds__(32 * XW_WARPS, 6) k_advect_xw(Layout L, Box box, int nocycle, double eps,
                                                           int ngroups, const double *__restrict__ cin,
                                                           double *__restrict__ cout,
@@ -873,6 +882,8 @@ __global__ void __launch_bounds__(32 * XW_WARPS, 6) k_advect_xw(Layout L, Box bo
   }
   const LineGeo gsig = line_of<0>(sig, j, k);
   const LineGeo gdtv = line_of<0>(dtvt, j, k);
+  // LC: sigma and dt/kappa do not vary along the row (zero broadcast stride)
+  const double sig_c = LC ? gsig.p[0] : 0.0, dtv_c = LC ? gdtv.p[0] : 0.0;
   const double *pv = vel + base;
   const bool out_lo = !PER && rmin == 1;
   const bool out_hi = !PER && rmax == n;
@@ -920,11 +931,11 @@ __global__ void __launch_bounds__(32 * XW_WARPS, 6) k_advect_xw(Layout L, Box bo
     else if (i >= rmin - 2 && i <= rmax + 1) vi = pv[(PER ? wrap(i) : (i < 1 ? 1 : (i > n ? n : i))) - 1];
     s_v[wid][sl] = vi;
     __syncwarp();
-    const double usi = (!CK || fs_ok(i)) ? 0.5 * (s_v[wid][sl1] + vi) * gsig.at(i) : 0.0;
+    const double usi = (!CK || fs_ok(i)) ? 0.5 * (s_v[wid][sl1] + vi) * (LC ? sig_c : gsig.at(i)) : 0.0;
     s_u[wid][sl] = usi;
     __syncwarp();
     const int I = i - 1;
-    const double dtvI = (!CK || (I >= -1 && I <= n + 2)) ? gdtv.at(I) : 0.0;
+    const double dtvI = (!CK || (I >= -1 && I <= n + 2)) ? (LC ? dtv_c : gdtv.at(I)) : 0.0;
     const Iface f = make_iface(s_u[wid][sl2], s_u[wid][sl1], usi, dtvI, !CK || fss_ok(I), !CK || fs_ok(I));
     double qm[GC], fsl[GC], fss[GC];
 #pragma unroll
@@ -939,7 +950,7 @@ __global__ void __launch_bounds__(32 * XW_WARPS, 6) k_advect_xw(Layout L, Box bo
     __syncwarp();
     const int c = I - 1;
     if (!CK || (c >= 0 && c <= n + 1)) {
-      const double dtvc = gdtv.at(c);
+      const double dtvc = LC ? dtv_c : gdtv.at(c);
       const bool inbox = !CK || (c >= rmin && c <= rmax);
 #pragma unroll
       for (int q = 0; q < GC; q++) {
@@ -967,15 +978,19 @@ static void launch_advect_xw(a3g_ctx *ctx) {
   const int ngroups = (L.ns + gc - 1) / gc;
   const long nwarps = (long)L.ny * L.nz * ngroups;
   const unsigned blocks = (unsigned)((nwarps + XW_WARPS - 1) / XW_WARPS);
-#define A3G_XW(GC_, PER_)                                                                                   \
-  k_advect_xw<LIM, GC_, PER_><<<blocks, 32 * XW_WARPS, 0, ctx->stream>>>(                                  \
+  const bool lc = along<0>(ctx->snx) == 0 && along<0>(ctx->dtv) == 0;
+#define A3G_XW(GC_, PER_, LC_)                                                                              \
+  k_advect_xw<LIM, GC_, PER_, LC_><<<blocks, 32 * XW_WARPS, 0, ctx->stream>>>(                             \
       L, ctx->box, ctx->prm.nocycle, ctx->prm.eps_thresh, ngroups, ctx->c0, ctx->c1, ctx->vx, ctx->snx,     \
       ctx->dtv, ctx->aloft, ctx->out_yz1, ctx->out_yz2)
+#define A3G_XW_LC(GC_, PER_) \
+  if (lc) A3G_XW(GC_, PER_, true); else A3G_XW(GC_, PER_, false)
   if (gc == 2) {
-    if (ctx->grid.periodic) A3G_XW(2, true); else A3G_XW(2, false);
+    if (ctx->grid.periodic) { A3G_XW_LC(2, true); } else { A3G_XW_LC(2, false); }
   } else {
-    if (ctx->grid.periodic) A3G_XW(1, true); else A3G_XW(1, false);
+    if (ctx->grid.periodic) { A3G_XW_LC(1, true); } else { A3G_XW_LC(1, false); }
   }
+#undef A3G_XW_LC
 #undef A3G_XW
 }
 
@@ -1185,12 +1200,16 @@ static void launch_block_v(a3g_ctx *ctx) {
   dim3 grid;
   if (DIR == 0) grid = dim3((nblk + 31) / 32, (L.ny + 3) / 4, L.nz * L.ns);
   else grid = dim3((L.nx + 31) / 32, (nblk * ((DIR == 1) ? L.nz : L.ny) + 3) / 4, L.ns);
-  k_advect_block<DIR, LIM, V, PER><<<grid, dim3(32, 4), 0, ctx->stream>>>(
-      L, ctx->box, ctx->prm.nocycle, ctx->prm.eps_thresh, nblk, ctx->c0, ctx->c1,
-      dir_vel(ctx, DIR), dir_vghost(ctx, DIR), ctx->vf,
-      (DIR == 0) ? ctx->snx : (DIR == 1) ? ctx->sny : ctx->snz, ctx->dtv, ctx->aloft, ctx->sc,
-      (DIR == 0) ? ctx->out_yz1 : (DIR == 1) ? ctx->out_xz1 : ctx->out_xy1,
-      (DIR == 0) ? ctx->out_yz2 : (DIR == 1) ? ctx->out_xz2 : ctx->out_xy2);
+  const Geo3 &sg = (DIR == 0) ? ctx->snx : (DIR == 1) ? ctx->sny : ctx->snz;
+  const bool lc = along<DIR>(sg) == 0 && along<DIR>(ctx->dtv) == 0 && (DIR != 2 || ctx->vf.sk == 0);
+#define A3G_BLK(LC_)                                                                                  \
+  k_advect_block<DIR, LIM, V, PER, LC_><<<grid, dim3(32, 4), 0, ctx->stream>>>(                       \
+      L, ctx->box, ctx->prm.nocycle, ctx->prm.eps_thresh, nblk, ctx->c0, ctx->c1,                     \
+      dir_vel(ctx, DIR), dir_vghost(ctx, DIR), ctx->vf, sg, ctx->dtv, ctx->aloft, ctx->sc,            \
+      (DIR == 0) ? ctx->out_yz1 : (DIR == 1) ? ctx->out_xz1 : ctx->out_xy1,                           \
+      (DIR == 0) ? ctx->out_yz2 : (DIR == 1) ? ctx->out_xz2 : ctx->out_xy2)
+  if (lc) A3G_BLK(true); else A3G_BLK(false);
+#undef A3G_BLK
 }
 
 template <int DIR, int LIM>
