@@ -384,13 +384,38 @@ __global__ void __launch_bounds__(256) k_totals(Layout L, const double *__restri
     case 2: case 3: n = (long)L.ny * L.nz; break;
     default: n = (long)L.nx * L.nz; break;
   }
-  if (job == 0) {  // airborne mass: block-strided rows (j,k), threads along i
+  if (job == 0) {
+    // airborne mass: block b sums a contiguous run of the (j,k) rows, threads
+    // along i.  A thread adds its few cells of a row in double (their loads
+    // all in flight at once), times kappa once per row when kappa does not
+    // vary along i, and carries the row terms in double-double: a relative
+    // error of a few ulps per row term, far inside the 1e-13 the totals keep
     const double *cg = c + (long)g * L.PG;
     const int nrow = L.ny * L.nz;
-    for (int r = blockIdx.x; r < nrow; r += gridDim.x) {
-      const int j = r % L.ny + 1, k = r / L.ny + 1;
+    const int per = (nrow + (int)gridDim.x - 1) / (int)gridDim.x;
+    const int r0 = (int)blockIdx.x * per, r1 = min(nrow, r0 + per);
+    int j = r0 % L.ny + 1, k = r0 / L.ny + 1;
+    const bool row_const = kap.si == 0;
+    const int bd = (int)blockDim.x;
+    for (int r = r0; r < r1; r++) {
       const double *row = cg + (long)r * L.P;
-      for (int i = threadIdx.x; i < L.nx; i += blockDim.x) acc = dd_add(acc, row[i] * kap.at(i + 1, j, k));
+      double part = 0.0;
+      for (int i0 = 0; i0 < L.nx; i0 += 4 * bd) {
+        double v[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const int i = i0 + (int)threadIdx.x + q * bd;
+          v[q] = i < L.nx ? (row_const ? row[i] : row[i] * kap.at(i + 1, j, k)) : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) part = part + v[q];
+      }
+      if (row_const) part = part * kap.at(1, j, k);
+      acc = dd_add(acc, part);
+      if (++j > L.ny) {
+        j = 1;
+        k++;
+      }
     }
     n = 0;
   }
@@ -424,16 +449,19 @@ __global__ void __launch_bounds__(256) k_totals(Layout L, const double *__restri
   }
 }
 
+// one warp per (g, job): lanes take every 32nd block partial, then a fixed
+// shuffle tree (the same order on every run)
 __global__ void k_totals_final(int ns, int nblk, const double *__restrict__ part,
                                double *__restrict__ out) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;  // (g, job)
-  if (t >= ns * NJOBS) return;
+  const int t = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;  // (g, job)
+  if (t >= ns * NJOBS) return;  // whole warps
   DD s = {0.0, 0.0};
-  for (int b = 0; b < nblk; b++) {
+  for (int b = lane; b < nblk; b += 32) {
     const long o = ((long)t * nblk + b) * 2;
     s = dd_add(s, DD{part[o], part[o + 1]});
   }
-  out[t] = s.hi + s.lo;  // out[g*NJOBS + job]
+  for (int o = 16; o > 0; o >>= 1) s = dd_add(s, dd_shfl(s, o));
+  if (lane == 0) out[t] = s.hi + s.lo;  // out[g*NJOBS + job]
 }
 
 // the partial sums of the totals, copied (asynchronously) to h_dst
@@ -450,7 +478,7 @@ int launch_totals_partials(a3g_ctx *ctx, double *h_dst) {
   A3G_LAUNCH_CHECK(ctx);
   double *fin = ctx->red_buf + (size_t)2 * TOT_BLOCKS * NJOBS * ns;
   tbegin(ctx, A3G_K_TOTALS);
-  k_totals_final<<<(ns * NJOBS + 127) / 128, 128, 0, ctx->stream>>>(ns, TOT_BLOCKS, ctx->red_buf, fin);
+  k_totals_final<<<(ns * NJOBS * 32 + 127) / 128, 128, 0, ctx->stream>>>(ns, TOT_BLOCKS, ctx->red_buf, fin);
   tend(ctx);
   A3G_LAUNCH_CHECK(ctx);
   A3G_CUDA(cudaMemcpyAsync(h_dst, fin, sizeof(double) * ns * NJOBS, cudaMemcpyDeviceToHost, ctx->stream));
@@ -490,7 +518,7 @@ int launch_totals(a3g_ctx *ctx, double *out4, double *mass_aloft) {
   A3G_LAUNCH_CHECK(ctx);
   double *fin = ctx->red_buf + (size_t)2 * TOT_BLOCKS * NJOBS * ns;
   tbegin(ctx, A3G_K_TOTALS);
-  k_totals_final<<<(ns * NJOBS + 127) / 128, 128, 0, ctx->stream>>>(ns, TOT_BLOCKS, ctx->red_buf, fin);
+  k_totals_final<<<(ns * NJOBS * 32 + 127) / 128, 128, 0, ctx->stream>>>(ns, TOT_BLOCKS, ctx->red_buf, fin);
   tend(ctx);
   A3G_LAUNCH_CHECK(ctx);
   A3G_CUDA(cudaMemcpyAsync(ctx->h_tot, fin, sizeof(double) * ns * NJOBS, cudaMemcpyDeviceToHost,
