@@ -333,6 +333,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     cfg = driver.shard_config(cfg_g, rank, world)
     geo = syn.geometry(cfg)
     gpu = Ash3dGPU(cfg, device=local_rank, geo=geo)
+    for dv in args.variant:  # kernel variant overrides, "dir=variant"
+        d, v = (int(x) for x in dv.split("="))
+        gpu.set_variant(d, v)
     gpu.set_interior(filled_state(cfg, seed=17 + rank))
     stream = torch.cuda.ExternalStream(gpu.stream_handle(), device=torch.device("cuda", local_rank))
     n_total = cfg.ns * world
@@ -755,6 +758,8 @@ def main():
                          "forward run's hours (default 48)")
     ap.add_argument("--adj-hours", type=float, default=12.0,
                     help="with --config C5 --adjoint: the reversal window (the last hours of the run)")
+    ap.add_argument("--variant", action="append", default=[], metavar="DIR=V",
+                    help="kernel variant override (a3g_set_variant), repeatable")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

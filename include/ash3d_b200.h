@@ -45,6 +45,7 @@ extern "C" {
 #define A3G_ERR_STATE       7   /* call out of order (e.g. no geometry bound yet) */
 #define A3G_ERR_UNSUPPORTED 8   /* option outside the implemented variants */
 #define A3G_ERR_NONFINITE   9   /* NaN/Inf detected in a device reduction */
+#define A3G_ERR_TIMEOUT    10   /* a bounded device-side wait (TMA tile copy) ran out */
 
 /* limiters: the LIM_* preprocessor choices of src/makefile:126 */
 #define A3G_LIM_NONE     0
@@ -386,7 +387,9 @@ int a3g_kernel_times(a3g_ctx *ctx, double *ms, uint64_t *count);
  * (defaults: x 4, y 1, z 1).
  * dir 3: the Crank-Nicolson x solve, variant 0 warp-tiled (default), 1 one
  * thread per line.  dir 4: the Crank-Nicolson y and z solves, variant 0 one
- * grain per thread, 1 two grains of a line per thread (default), 2 four.
+ * grain per thread, 1 two grains of a line per thread, 2 four, 3 tiles of
+ * 32 lines staged in shared memory by TMA tensor copies (default; where the
+ * coefficients vary along i, or nz > 256, variant 3 runs variant 1).
  * dir 1, 2 variant 5: the column march (one thread per line and grain, lanes
  * along i, each interface formed once).  dir 5: the adjoint advection sweeps,
  * variant 0 four-cell blocks (default), 1 one cell per thread.  All variants

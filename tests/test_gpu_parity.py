@@ -45,8 +45,8 @@ ADVECTION = ("advect_x", "advect_y", "AdvectVert")
 def _variants(op):
     # advection: march / block-4 / block-8 / x warp-tiled / x warp-row / y, z
     # column march; diffusion: the CN x solve warp-tiled / one thread per line
-    # and the y, z solves one / two / four grains per thread
-    return (0, 1, 2, 3, 4, 5) if op in ADVECTION else (0, 1, 2)
+    # and the y, z solves one / two / four grains per thread / TMA tiles
+    return (0, 1, 2, 3, 4, 5) if op in ADVECTION else (0, 1, 2, 3)
 
 
 def _adv_variant(d, variant):
@@ -130,7 +130,7 @@ def test_run_bitwise(name, variant):
     for d in range(3):
         gpu.set_variant(d, _adv_variant(d, variant))
     gpu.set_variant(3, variant % 2)
-    gpu.set_variant(4, min(variant, 2))
+    gpu.set_variant(4, variant if variant <= 3 else 3 - variant % 2)
     sg = driver.run(gpu, cfg, max_steps=16)
     sr = driver.run(ref, cfg, max_steps=16)
     assert [h.dt for h in sg.history] == [h.dt for h in sr.history]

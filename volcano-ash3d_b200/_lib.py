@@ -20,7 +20,7 @@ A3G_OK = 0
 ERR_NAMES = {
     1: "A3G_ERR_ARG", 2: "A3G_ERR_CUDA", 3: "A3G_ERR_NOMEM", 4: "A3G_ERR_BC_CODE",
     5: "A3G_ERR_SUBGRID", 6: "A3G_ERR_PIVOT", 7: "A3G_ERR_STATE",
-    8: "A3G_ERR_UNSUPPORTED", 9: "A3G_ERR_NONFINITE",
+    8: "A3G_ERR_UNSUPPORTED", 9: "A3G_ERR_NONFINITE", 10: "A3G_ERR_TIMEOUT",
 }
 LIMITERS = {"none": 0, "laxwen": 1, "bw": 2, "fromm": 3, "minmod": 4, "superbee": 5, "mc": 6}
 

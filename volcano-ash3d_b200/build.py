@@ -34,7 +34,7 @@ def needs_build() -> bool:
         return True
     t = OUT.stat().st_mtime
     deps = [HERE / "csrc" / s for s in SRCS] + [HERE / "csrc" / "a3g_internal.cuh", HERE / "csrc" / "k_advect.cuh",
-                                               HERE / "csrc" / "exact_div.cuh",
+                                               HERE / "csrc" / "exact_div.cuh", HERE / "csrc" / "tma.cuh",
                                                HERE.parent / "include" / "ash3d_b200.h"]
     return any(d.stat().st_mtime > t for d in deps)
 

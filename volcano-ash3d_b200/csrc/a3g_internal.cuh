@@ -19,6 +19,7 @@
 //     one per (j,k).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stddef.h>
@@ -65,6 +66,15 @@ struct Layout {
 
 struct Box {
   int imin, imax, jmin, jmax, kmin, kmax;
+};
+
+// A TMA tensor map over one concentration level (cached per device pointer
+// and tile shape; see tensor_map()).
+enum TmapKind { TM_COLUMN = 0, TM_YCHUNK_IN = 1, TM_YCHUNK_OUT = 2 };
+struct TmapEntry {
+  const void *p;
+  int kind;
+  CUtensorMap map;
 };
 
 // Per-step device scalars (read by kernels so that a step can be replayed).
@@ -202,6 +212,10 @@ struct a3g_ctx {
   cudaEvent_t umb_event;
   // source inversion (a3g_inv_setup)
   a3g_inv *inv;
+  // TMA tensor maps over the levels the tiled solves read and write, and the
+  // persistent grid size of each tiled kernel (0 until first computed)
+  std::vector<a3g::TmapEntry> tmaps;
+  int tma_grid[4];
   // optional per-kernel timing (a3g_kernel_timing)
   bool timing;
   std::vector<cudaEvent_t> ev_pool;
@@ -273,6 +287,10 @@ int launch_vent_column(a3g_ctx *ctx, int ivent, int jvent, const double *lam, do
 int launch_output_vars(a3g_ctx *ctx, double time, double *load, double *maxh, double *minh, double *maxc,
                        int32_t *mcl, double *dthick, int32_t *mdep, double *carr, double *darr);
 int refresh_dtv(a3g_ctx *ctx);
+// The tensor map of kind `kind` over the level at p (encoded on first use,
+// then cached), copied to *out; false when the driver cannot encode it (the
+// caller falls back).
+bool tensor_map(a3g_ctx *ctx, const double *p, int kind, CUtensorMap *out);
 // per-kernel timing brackets (no-ops unless a3g_kernel_timing(ctx,1))
 void tbegin(a3g_ctx *ctx, int kind);
 void tend(a3g_ctx *ctx);

@@ -20,6 +20,7 @@
 // A3G_ERR_PIVOT instead of silently diverging from dgtsv.
 #include "a3g_internal.cuh"
 #include "exact_div.cuh"
+#include "tma.cuh"
 
 namespace a3g {
 
@@ -690,6 +691,452 @@ __global__ void __launch_bounds__(128, 5) k_cn_solve_xt(Layout L, Box box, LineM
 }
 
 // ---------------------------------------------------------------------------
+// z lines through TMA column tiles.  A warp owns the 32 z lines of 32
+// consecutive i at one (j, grain): one tensor load brings the whole tile
+// (32 i x nz levels, tile[k][lane]) into shared memory, each lane runs its
+// line's elimination and back substitution in place (the same operations as
+// cn_line, so the same bits), and one tensor store writes the tile back.  The
+// level is read once and written once, with no B' round trip through global
+// memory, and the copies run asynchronously to the other warps' arithmetic.
+// The factor-table rows of the tile's line (the same for its 32 lines: the
+// coefficients do not vary along i) are staged in shared memory by the warp,
+// so the recurrences read only shared memory.  Warps are persistent and take
+// contiguous runs of tiles (neighbouring i, then j), which share table rows.
+// ---------------------------------------------------------------------------
+constexpr int ZT_BAR_BYTES = 128;  // barriers ahead of the tiles (keeps tiles 128-byte aligned)
+
+// doubles of shared memory per warp: the tile and the staged table rows,
+// rounded up to 128 bytes so that every warp's tile stays aligned
+__host__ __device__ __forceinline__ long zt_warp_doubles(int nz) {
+  return (32L * nz + CN_NF * (long)nz + 15) / 16 * 16;
+}
+
+__global__ void __launch_bounds__(64, 8) k_cn_solve_zt(const __grid_constant__ CUtensorMap tin,
+                                                    const __grid_constant__ CUtensorMap tout, Layout L,
+                                                    Box box, LineMap map, const double *__restrict__ tab,
+                                                    const int32_t *__restrict__ aloft, DevScalars *sc,
+                                                    int wpb) {
+  extern __shared__ __align__(128) unsigned char zt_smem[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int nz = L.nz;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(zt_smem) + wid;
+  double *tile = reinterpret_cast<double *>(zt_smem + ZT_BAR_BYTES) + (long)wid * zt_warp_doubles(nz);
+  double *stab = tile + 32L * nz;  // staged table: field f, row l at stab[f*nz + l]
+  if (lane == 0) {
+    mbar_init(bar, 1);
+    mbar_init_fence();
+    prefetch_tensormap(&tin);
+    prefetch_tensormap(&tout);
+  }
+  __syncwarp();
+  const int nti = (L.nx + 31) >> 5;
+  const long ntiles = (long)nti * L.ny * L.ns;
+  const long nwarps = (long)gridDim.x * wpb;
+  const long per = (ntiles + nwarps - 1) / nwarps;
+  const long t0 = ((long)blockIdx.x * wpb + wid) * per;
+  const long t1 = t0 + per < ntiles ? t0 + per : ntiles;
+  const int rmin = box.kmin, rmax = box.kmax;
+  const int ncells = rmax - rmin + 1;
+  const long U = map.U;
+  const long F = (long)ncells * U;
+  const uint32_t tile_bytes = 32u * (uint32_t)nz * 8u;
+  uint32_t phase = 0;
+  int staged = -1;            // the line index u whose rows stab holds
+  double *col = tile + lane;  // this lane's line: level k (1-based) at col[(k-1)*32]
+  for (long t = t0; t < t1; t++) {
+    const int it = (int)(t % nti);
+    const long r = t / nti;
+    const int j = (int)(r % L.ny) + 1;
+    const int g = (int)(r / L.ny);
+    const int i = (it << 5) + lane + 1;
+    const bool act = i <= L.nx && i >= box.imin && i <= box.imax && j >= box.jmin && j <= box.jmax &&
+                     aloft[g] != 0;
+    const bool any = __any_sync(0xffffffffu, act);
+    // the previous tile's store must have read the buffer before it is refilled
+    if (lane == 0) bulk_wait_read0();
+    __syncwarp();
+    if (any) {
+      if (lane == 0) {
+        mbar_arrive_expect_tx(bar, tile_bytes);
+        tma_load_4d(tile, &tin, bar, it << 5, j - 1, 0, g);
+      }
+      const int u = map.u(1, j);  // the coefficients do not vary along i (map.da == 0)
+      if (u != staged) {          // stage the rows while the tile is in flight
+        const double *tl = tab + u;
+        for (int l = lane; l < ncells; l += 32)
+#pragma unroll
+          for (int f = 0; f < CN_NF; f++) stab[f * nz + l] = tl[f * F + (long)l * U];
+        staged = u;
+      }
+      if (!mbar_wait(bar, phase)) {
+        if (lane == 0) {
+          raise_error(sc, A3G_ERR_TIMEOUT, 2);
+          bulk_wait0();
+        }
+        return;
+      }
+      phase ^= 1u;
+      __syncwarp();
+    }
+    if (act) {
+      auto co = [&](int f, int l) { return stab[f * nz + l]; };
+      double *xx = col + (long)(rmin - 1) * 32;  // row l at xx[l*32]
+      // forward elimination with the right-hand side built on the fly, :813-851
+      double qm = xx[0];  // BC_left_t0 = q(rmin)
+      double qc = qm;
+      double bp = 0.0;
+#pragma unroll 4
+      for (int l = 0; l < ncells; l++) {
+        const double qp = (l + 1 < ncells) ? xx[(l + 1) * 32] : qc;  // BC_right_t0 = q(rmax)
+        const double B = co(CN_CL, l) * qm + co(CN_CC, l) * qc + co(CN_CR, l) * qp;
+        bp = (l == 0) ? B : B - co(CN_FACT, l) * bp;
+        xx[l * 32] = bp;
+        qm = qc;
+        qc = qp;
+      }
+      // back substitution
+      double xn = 0.0;
+#pragma unroll 4
+      for (int l = ncells - 1; l >= 0; l--) {
+        const double b2 = xx[l * 32];
+        const double num = (l == ncells - 1) ? b2 : b2 - co(CN_DU, l) * xn;
+        const double v = div_rn_rcp(num, co(CN_DP, l), co(CN_RDP, l));
+        xx[l * 32] = v;
+        xn = v;
+      }
+      for (int k = 1; k < rmin; k++) col[(k - 1) * 32] = 0.0;  // outside the box
+      for (int k = rmax + 1; k <= nz; k++) col[(k - 1) * 32] = 0.0;
+    } else {
+      for (int k = 1; k <= nz; k++) col[(k - 1) * 32] = 0.0;  // the reference leaves zeros
+    }
+    fence_proxy_async_smem();
+    __syncwarp();
+    if (lane == 0) {
+      tma_store_4d(&tout, tile, it << 5, j - 1, 0, g);
+      bulk_commit();
+    }
+  }
+  if (lane == 0) bulk_wait0();
+}
+
+// ---------------------------------------------------------------------------
+// y lines through TMA chunk tiles.  A warp owns the 32 y lines of 32
+// consecutive i at one (k, grain) and walks them in chunks of YT_CH cells;
+// each chunk arrives by one tensor load as a tile of YT_CH + 2 rows (the
+// cell before the chunk and the cell after it included; row r holds line
+// position l0 - 1 + r), tile[r][lane].  Two buffers per warp: the next
+// chunk's load is in flight while the lanes work on the current one.
+//   pass 1 (forward): the elimination of B' over the whole line, keeping only
+//     B' at the last cell of every chunk (a checkpoint, in shared memory);
+//   pass 2 (backward, last chunk first, which pass 1 left in its buffer):
+//     recompute the chunk's B' from the previous chunk's checkpoint (same
+//     operations, same bits), back-substitute in place, and store the chunk
+//     with one tensor store.
+// The arithmetic is cn_line's, operation for operation.  Each chunk's
+// factor-table rows (the same for the warp's 32 lines) are staged in shared
+// memory while its tile is in flight.  Warps take contiguous runs of line
+// groups (neighbouring i, then k), which share table rows.
+// ---------------------------------------------------------------------------
+constexpr int YT_CH = 32;
+constexpr int YT_ROWS = YT_CH + 2;
+
+__global__ void __launch_bounds__(64) k_cn_solve_yt(const __grid_constant__ CUtensorMap tin,
+                                                    const __grid_constant__ CUtensorMap tout, Layout L,
+                                                    Box box, LineMap map, double *__restrict__ cout,
+                                                    const double *__restrict__ tab,
+                                                    const int32_t *__restrict__ aloft, DevScalars *sc,
+                                                    int wpb, int nch_max) {
+  extern __shared__ __align__(128) unsigned char yt_smem[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  constexpr int BUF = 32 * YT_ROWS;  // doubles per buffer (a multiple of 16: 128-byte aligned buffers)
+  uint64_t *bar = reinterpret_cast<uint64_t *>(yt_smem) + 2 * wid;
+  double *wbase =
+      reinterpret_cast<double *>(yt_smem + ZT_BAR_BYTES) + (long)wid * (2 * BUF + nch_max * 32 + CN_NF * 32);
+  auto buf = [&](int bi) { return wbase + (bi ? BUF : 0); };
+  double *ck = wbase + 2 * BUF;  // checkpoint of chunk ch at ck[ch*32 + lane]
+  double *stab = ck + nch_max * 32;  // staged table of the chunk: field f, row c at stab[f*32 + c]
+  if (lane == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_init_fence();
+    prefetch_tensormap(&tin);
+    prefetch_tensormap(&tout);
+  }
+  __syncwarp();
+  const int nti = (L.nx + 31) >> 5;
+  const long ngroups = (long)nti * L.nz * L.ns;
+  const long nwarps = (long)gridDim.x * wpb;
+  const long per = (ngroups + nwarps - 1) / nwarps;
+  const long t0 = ((long)blockIdx.x * wpb + wid) * per;
+  const long t1 = t0 + per < ngroups ? t0 + per : ngroups;
+  const int rmin = box.jmin, rmax = box.jmax;
+  const int ncells = rmax - rmin + 1;
+  const int nch = (ncells + YT_CH - 1) / YT_CH;
+  const long U = map.U;
+  const long F = (long)ncells * U;
+  const uint32_t tile_bytes = 32u * YT_ROWS * 8u;
+  uint32_t ph = 0u;  // bit b: the parity of buffer b's barrier
+  for (long t = t0; t < t1; t++) {
+    const int it = (int)(t % nti);
+    const long r = t / nti;
+    const int k = (int)(r % L.nz) + 1;
+    const int g = (int)(r / L.nz);
+    const int i = (it << 5) + lane + 1;
+    const bool act = i <= L.nx && i >= box.imin && i <= box.imax && k >= box.kmin && k <= box.kmax &&
+                     aloft[g] != 0;
+    const bool any = __any_sync(0xffffffffu, act);
+    double *xg = cout + (long)g * L.PG + (long)(k - 1) * L.PY + (i - 1);  // cell (i, 1, k) of this lane
+    if (!any) {  // the reference leaves zeros
+      if (i <= L.nx)
+        for (int j = 1; j <= L.ny; j++) xg[(long)(j - 1) * L.P] = 0.0;
+      continue;
+    }
+    if (i <= L.nx) {  // cells that no chunk store covers: outside [rmin, rmin + nch*YT_CH)
+      for (int j = 1; j < rmin; j++) xg[(long)(j - 1) * L.P] = 0.0;
+      for (int j = rmin + nch * YT_CH; j <= L.ny; j++) xg[(long)(j - 1) * L.P] = 0.0;
+    }
+    auto issue = [&](int bi, int ch) {  // tensor load of chunk ch into buffer bi
+      if (lane == 0) {
+        bulk_wait_read0();  // a store from this buffer must have read it first
+        mbar_arrive_expect_tx(&bar[bi], tile_bytes);
+        tma_load_4d(buf(bi), &tin, &bar[bi], it << 5, rmin - 2 + ch * YT_CH, k - 1, g);
+      }
+    };
+    bool ok = true;
+    auto wait = [&](int bi) {
+      ok = mbar_wait(&bar[bi], (ph >> bi) & 1u);
+      ph ^= 1u << bi;
+    };
+    const double *tl = tab + map.u(1, k);  // the coefficients do not vary along i (map.da == 0)
+    auto stage = [&](int l0, int nf) {      // fields 0..nf-1 of rows l0..l0+31 into stab
+      const int l = l0 + lane;
+      if (l < ncells)
+        for (int f = 0; f < nf; f++) stab[f * 32 + lane] = tl[f * F + (long)l * U];
+    };
+    auto co = [&](int f, int c) { return stab[f * 32 + c]; };
+    // pass 1: forward elimination, checkpoints only (:813-851 and dgtsv)
+    double qm = 0.0, qc = 0.0, bp = 0.0;
+    issue(0, 0);
+    for (int ch = 0; ch < nch && ok; ch++) {
+      const int bi = ch & 1;
+      if (ch + 1 < nch) issue(bi ^ 1, ch + 1);
+      const int l0 = ch * YT_CH;
+      stage(l0, CN_CR + 1);  // FACT, DP, DU, CL, CC, CR
+      wait(bi);
+      if (!ok) break;
+      __syncwarp();
+      const double *T = buf(bi) + lane;
+      const int cnt = (ncells - l0) < YT_CH ? (ncells - l0) : YT_CH;
+      if (act) {
+        if (ch == 0) {
+          qm = T[32];  // BC_left_t0 = q(rmin)
+          qc = qm;
+        }
+#pragma unroll 4
+        for (int c = 0; c < cnt; c++) {
+          const int l = l0 + c;
+          const double qp = (l + 1 < ncells) ? T[(c + 2) * 32] : qc;  // BC_right_t0 = q(rmax)
+          const double B = co(CN_CL, c) * qm + co(CN_CC, c) * qc + co(CN_CR, c) * qp;
+          bp = (l == 0) ? B : B - co(CN_FACT, c) * bp;
+          qm = qc;
+          qc = qp;
+        }
+        ck[ch * 32 + lane] = bp;
+      }
+      __syncwarp();
+    }
+    // pass 2: per chunk, last first: recompute B', back-substitute, store
+    double xn = 0.0;
+    for (int ch = nch - 1; ch >= 0 && ok; ch--) {
+      const int bi = ch & 1;
+      if (ch - 1 >= 0) issue(bi ^ 1, ch - 1);
+      const int l0 = ch * YT_CH;
+      stage(l0, CN_NF);
+      if (ch != nch - 1) {
+        wait(bi);
+        if (!ok) break;
+      }
+      __syncwarp();
+      double *T = buf(bi) + lane;
+      const int cnt = (ncells - l0) < YT_CH ? (ncells - l0) : YT_CH;
+      if (act) {
+        double bq = ch > 0 ? ck[(ch - 1) * 32 + lane] : 0.0;
+        double qm2 = (ch == 0) ? T[32] : T[0];
+        double qc2 = T[32];
+#pragma unroll 4
+        for (int c = 0; c < cnt; c++) {
+          const int l = l0 + c;
+          const double qp = (l + 1 < ncells) ? T[(c + 2) * 32] : qc2;
+          const double B = co(CN_CL, c) * qm2 + co(CN_CC, c) * qc2 + co(CN_CR, c) * qp;
+          bq = (l == 0) ? B : B - co(CN_FACT, c) * bq;
+          T[(c + 1) * 32] = bq;
+          qm2 = qc2;
+          qc2 = qp;
+        }
+#pragma unroll 4
+        for (int c = cnt - 1; c >= 0; c--) {
+          const int l = l0 + c;
+          const double b2 = T[(c + 1) * 32];
+          const double num = (l == ncells - 1) ? b2 : b2 - co(CN_DU, c) * xn;
+          const double v = div_rn_rcp(num, co(CN_DP, c), co(CN_RDP, c));
+          T[(c + 1) * 32] = v;
+          xn = v;
+        }
+        for (int c = cnt; c < YT_CH; c++) T[(c + 1) * 32] = 0.0;  // beyond rmax
+      } else {
+        for (int c = 0; c < YT_CH; c++) T[(c + 1) * 32] = 0.0;  // the reference leaves zeros
+      }
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) {
+        tma_store_4d(&tout, buf(bi) + 32, it << 5, rmin - 1 + l0, k - 1, g);
+        bulk_commit();
+      }
+    }
+    if (!ok) {
+      if (lane == 0) {
+        raise_error(sc, A3G_ERR_TIMEOUT, 1);
+        bulk_wait0();
+      }
+      return;
+    }
+  }
+  if (lane == 0) bulk_wait0();
+}
+
+// ---------------------------------------------------------------------------
+// TMA tensor maps over the concentration levels
+// ---------------------------------------------------------------------------
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
+                                  CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                  CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+    else
+      cudaGetLastError();
+  }
+  return fn;
+}
+
+// A level as a 4-D tensor (i, j, k, grain) of doubles with the device
+// layout's pitches; the box is one tile of the given kind:
+//   TM_COLUMN: 32 i x 1 j x nz k (the z solve's column tile);
+//   TM_YCHUNK_IN / TM_YCHUNK_OUT: 32 i x (YT_CH + 2) / YT_CH j (the y solve's
+//   chunk tile with the cells before and after it, and the chunk it stores).
+bool tensor_map(a3g_ctx *ctx, const double *p, int kind, CUtensorMap *out) {
+  for (const TmapEntry &e : ctx->tmaps)
+    if (e.p == p && e.kind == kind) {
+      *out = e.map;
+      return true;
+    }
+  EncodeTiledFn enc = encode_tiled_fn();
+  if (!enc) return false;
+  const Layout &L = ctx->L;
+  const cuuint64_t dims[4] = {(cuuint64_t)L.nx, (cuuint64_t)L.ny, (cuuint64_t)L.nz, (cuuint64_t)L.ns};
+  const cuuint64_t strides[3] = {(cuuint64_t)L.P * 8, (cuuint64_t)L.PY * 8, (cuuint64_t)L.PG * 8};
+  cuuint32_t box[4] = {32, 1, 1, 1};
+  if (kind == TM_COLUMN) {
+    if (L.nz > 256) return false;
+    box[2] = (cuuint32_t)L.nz;
+  } else if (kind == TM_YCHUNK_IN) {
+    box[1] = YT_ROWS;
+  } else if (kind == TM_YCHUNK_OUT) {
+    box[1] = YT_CH;
+  } else {
+    return false;
+  }
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  TmapEntry e;
+  e.p = p;
+  e.kind = kind;
+  if (enc(&e.map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double *>(p), dims, strides, box, estr,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  if (ctx->tmaps.size() >= 16) ctx->tmaps.erase(ctx->tmaps.begin());
+  ctx->tmaps.push_back(e);
+  *out = e.map;
+  return true;
+}
+
+// Launches the z solve through column tiles; false when the shape is outside
+// what the tiles cover (the caller takes the per-thread kernel).
+static bool launch_cn_solve_zt(a3g_ctx *ctx, const LineMap &map, const double *tab) {
+  const Layout &L = ctx->L;
+  if (L.nz > 256 || map.da) return false;
+  CUtensorMap tin, tout;
+  if (!tensor_map(ctx, ctx->c0, TM_COLUMN, &tin) || !tensor_map(ctx, ctx->c1, TM_COLUMN, &tout)) return false;
+  const int wpb = L.nz <= 128 ? 2 : 1;
+  const size_t smem = ZT_BAR_BYTES + (size_t)wpb * zt_warp_doubles(L.nz) * sizeof(double);
+  if (ctx->tma_grid[0] == 0) {
+    // the opt-in maximum, so that contexts of any nz can share the attribute
+    int optin = 0;
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device) != cudaSuccess ||
+        (size_t)optin < smem ||
+        cudaFuncSetAttribute(k_cn_solve_zt, cudaFuncAttributeMaxDynamicSharedMemorySize, optin) != cudaSuccess ||
+        cudaFuncSetAttribute(k_cn_solve_zt, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared) != cudaSuccess)
+      return false;
+    int per_sm = 0, nsm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cn_solve_zt, 32 * wpb, smem) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device) != cudaSuccess || per_sm < 1)
+      return false;
+    ctx->tma_grid[0] = per_sm * nsm;
+  }
+  const long ntiles = (long)((L.nx + 31) / 32) * L.ny * L.ns;
+  const long need = (ntiles + wpb - 1) / wpb;
+  const int grid = (int)(need < ctx->tma_grid[0] ? need : ctx->tma_grid[0]);
+  k_cn_solve_zt<<<grid, 32 * wpb, smem, ctx->stream>>>(tin, tout, L, ctx->box, map, tab, ctx->aloft, ctx->sc,
+                                                       wpb);
+  return true;
+}
+
+// Launches the y solve through chunk tiles; false when the maps cannot be
+// made (the caller takes the per-thread kernel).
+static bool launch_cn_solve_yt(a3g_ctx *ctx, const LineMap &map, const double *tab) {
+  const Layout &L = ctx->L;
+  if (map.da) return false;
+  CUtensorMap tin, tout;
+  if (!tensor_map(ctx, ctx->c0, TM_YCHUNK_IN, &tin) || !tensor_map(ctx, ctx->c1, TM_YCHUNK_OUT, &tout))
+    return false;
+  const int wpb = 2;
+  const int nch_max = (L.ny + YT_CH - 1) / YT_CH;
+  const size_t smem =
+      ZT_BAR_BYTES + (size_t)wpb * (2 * 32 * YT_ROWS + nch_max * 32 + CN_NF * 32) * sizeof(double);
+  if (ctx->tma_grid[1] == 0) {
+    int optin = 0;
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device) != cudaSuccess ||
+        (size_t)optin < smem ||
+        cudaFuncSetAttribute(k_cn_solve_yt, cudaFuncAttributeMaxDynamicSharedMemorySize, optin) != cudaSuccess ||
+        cudaFuncSetAttribute(k_cn_solve_yt, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared) != cudaSuccess)
+      return false;
+    int per_sm = 0, nsm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cn_solve_yt, 32 * wpb, smem) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device) != cudaSuccess || per_sm < 1)
+      return false;
+    ctx->tma_grid[1] = per_sm * nsm;
+  }
+  const long ngroups = (long)((L.nx + 31) / 32) * L.nz * L.ns;
+  const long need = (ngroups + wpb - 1) / wpb;
+  const int grid = (int)(need < ctx->tma_grid[1] ? need : ctx->tma_grid[1]);
+  k_cn_solve_yt<<<grid, 32 * wpb, smem, ctx->stream>>>(tin, tout, L, ctx->box, map, ctx->c1, tab, ctx->aloft,
+                                                       ctx->sc, wpb, nch_max);
+  return true;
+}
+
+// ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
 template <int DIR>
@@ -791,7 +1238,11 @@ static int launch_cn_dir(a3g_ctx *ctx) {
     const long nwarps = (nlines + 31) / 32;
     k_cn_solve_xt<<<(unsigned)((nwarps + XT_WARPS - 1) / XT_WARPS), 32 * XT_WARPS, 0, ctx->stream>>>(
         L, box, map, ctx->c0, ctx->c1, tab, ctx->aloft);
-  } else if (DIR != 0 && ctx->tune_cn_yz == 1 && L.ns >= 2) {
+  } else if (DIR == 2 && ctx->tune_cn_yz == 3 && launch_cn_solve_zt(ctx, map, tab)) {
+    // column tiles through TMA
+  } else if (DIR == 1 && ctx->tune_cn_yz == 3 && launch_cn_solve_yt(ctx, map, tab)) {
+    // chunk tiles through TMA
+  } else if (DIR != 0 && (ctx->tune_cn_yz == 1 || ctx->tune_cn_yz == 3) && L.ns >= 2) {
     launch_cn_solve_gc<DIR == 0 ? 1 : DIR, 2>(ctx, map, tab);
   } else if (DIR != 0 && ctx->tune_cn_yz == 2 && L.ns >= 2) {
     launch_cn_solve_gc<DIR == 0 ? 1 : DIR, 4>(ctx, map, tab);
