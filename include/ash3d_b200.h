@@ -384,14 +384,17 @@ int a3g_kernel_times(a3g_ctx *ctx, double *ms, uint64_t *count);
  * variant 0 marching threads, 1 blocks of 4 cells, 2 blocks of 8 cells, and
  * for x only 3, warps marching 32 rows through shared-memory tiles, and 4,
  * one warp per row walking it in 32-cell chunks with the lanes along i
- * (defaults: x 4, y 1, z 1).
+ * (defaults: x 4, y 6, z 6).
  * dir 3: the Crank-Nicolson x solve, variant 0 warp-tiled (default), 1 one
  * thread per line.  dir 4: the Crank-Nicolson y and z solves, variant 0 one
  * grain per thread, 1 two grains of a line per thread, 2 four, 3 tiles of
  * 32 lines staged in shared memory by TMA tensor copies (default; where the
  * coefficients vary along i, or nz > 256, variant 3 runs variant 1).
  * dir 1, 2 variant 5: the column march (one thread per line and grain, lanes
- * along i, each interface formed once).  dir 5: the adjoint advection sweeps,
+ * along i, each interface formed once); variant 6, the same march reading
+ * the concentration and wind from chunks that TMA tensor copies stage in
+ * shared memory (default for y and z; where the geometry varies along i or
+ * the fall speed within a grain, variant 6 runs variant 1).  dir 5: the adjoint advection sweeps,
  * variant 0 four-cell blocks (default), 1 one cell per thread.  All variants
  * produce identical results; only their speed differs. */
 int a3g_set_variant(a3g_ctx *ctx, int32_t dir, int32_t variant);

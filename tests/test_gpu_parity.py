@@ -46,15 +46,16 @@ def _variants(op):
     # advection: march / block-4 / block-8 / x warp-tiled / x warp-row / y, z
     # column march; diffusion: the CN x solve warp-tiled / one thread per line
     # and the y, z solves one / two / four grains per thread / TMA tiles
-    return (0, 1, 2, 3, 4, 5) if op in ADVECTION else (0, 1, 2, 3)
+    return (0, 1, 2, 3, 4, 5, 6) if op in ADVECTION else (0, 1, 2, 3)
 
 
 def _adv_variant(d, variant):
     """The variant a direction takes for a parametrised advection variant:
-    3 and 4 exist for x only, 5 (the column march) for y and z only."""
+    3 and 4 exist for x only, 5 and 6 (the column marches, from global memory
+    and from TMA chunks) for y and z only."""
     if d == 0:
-        return 4 if variant == 5 else variant
-    return 5 if variant == 5 else min(variant, 2)
+        return 4 if variant in (5, 6) else variant
+    return variant if variant in (5, 6) else min(variant, 2)
 
 
 def _set_variant(gpu, op, variant):
@@ -123,14 +124,14 @@ def test_timestep_totals(name):
 
 
 @pytest.mark.parametrize("name", CONFIGS)
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6])
 def test_run_bitwise(name, variant):
     from volcano_ash3d_b200 import driver
     cfg, gpu, ref = pair(name)
     for d in range(3):
         gpu.set_variant(d, _adv_variant(d, variant))
     gpu.set_variant(3, variant % 2)
-    gpu.set_variant(4, variant if variant <= 3 else 3 - variant % 2)
+    gpu.set_variant(4, variant if variant <= 3 else 3 - variant % 2 if variant < 6 else 1)
     sg = driver.run(gpu, cfg, max_steps=16)
     sr = driver.run(ref, cfg, max_steps=16)
     assert [h.dt for h in sg.history] == [h.dt for h in sr.history]

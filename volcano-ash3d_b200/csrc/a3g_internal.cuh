@@ -68,9 +68,25 @@ struct Box {
   int imin, imax, jmin, jmax, kmin, kmax;
 };
 
-// A TMA tensor map over one concentration level (cached per device pointer
-// and tile shape; see tensor_map()).
-enum TmapKind { TM_COLUMN = 0, TM_YCHUNK_IN = 1, TM_YCHUNK_OUT = 2 };
+// A TMA tensor map over one concentration level or one wind array (cached
+// per device pointer and tile shape; see tensor_map()).  Tile kinds:
+//   TM_COLUMN      level, 32 i x 1 j x nz k (the CN z solve's column tile)
+//   TM_YCHUNK_IN   level, 32 i x (YT_CH + 2) j (a CN y chunk and its neighbours)
+//   TM_YCHUNK_OUT  level, 32 i x YT_CH j (the CN y chunk it stores)
+//   TM_ADV_QY/QZ   level, 32 i x ACH j / ACH k (an advection chunk)
+//   TM_ADV_VY/VZ   wind array, the same chunks
+enum TmapKind {
+  TM_COLUMN = 0,
+  TM_YCHUNK_IN = 1,
+  TM_YCHUNK_OUT = 2,
+  TM_ADV_QY = 3,
+  TM_ADV_QZ = 4,
+  TM_ADV_VY = 5,
+  TM_ADV_VZ = 6
+};
+constexpr int YT_CH = 32;            // cells per CN y chunk
+constexpr int YT_ROWS = YT_CH + 2;   // with the cell before and the cell after
+constexpr int ACH = 8;               // cells per advection chunk
 struct TmapEntry {
   const void *p;
   int kind;

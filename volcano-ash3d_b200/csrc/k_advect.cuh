@@ -30,6 +30,7 @@
 // zero-then-copy-back of the reference (AdvectionHorz_DCU.f90:122,302-303).
 #include "a3g_internal.cuh"
 #include "exact_div.cuh"
+#include "tma.cuh"
 
 namespace a3g {
 
@@ -1169,6 +1170,230 @@ static void launch_col(a3g_ctx *ctx) {
 }
 
 // ---------------------------------------------------------------------------
+// Column march fed by TMA chunks (y and z sweeps).  The march of k_advect_col
+// -- one warp per 32 lines of 32 consecutive i at one (other index, grain),
+// each interface formed once, the same step() arithmetic and so the same bits
+// -- but the interior steps read the concentration and the wind of cell c+2
+// from shared memory: chunks of ACH cells of both arrive by two tensor loads
+// into one of two buffers per warp, the next chunk in flight while the lanes
+// march through the current one, and the geometry of the chunk's cells
+// (sigma, dt/kappa: the same for the warp's lines) is staged beside them.
+// The prologue and the few checked steps at the line ends keep the global
+// loads of k_advect_col.  Warps are ordered grain-fastest, so the grains of a
+// tile run side by side and share its wind rows through L2.  Taken when the
+// geometry is constant along i and the fall speed is one value per grain.
+// ---------------------------------------------------------------------------
+constexpr int ACT_WARPS = 2;
+// doubles per warp: two buffers of (q, v) chunks and two of staged geometry
+constexpr int ACT_WARP_D = 2 * 2 * ACH * 32 + 2 * 2 * ACH;
+static_assert((ACT_WARP_D * 8) % 128 == 0, "warp regions stay 128-byte aligned");
+
+template <int DIR, int LIM>
+__global__ void __launch_bounds__(32 * ACT_WARPS) k_advect_colt(
+    const __grid_constant__ CUtensorMap tq, const __grid_constant__ CUtensorMap tv, Layout L, Box box,
+    int nocycle, double eps, const double *__restrict__ cin, double *__restrict__ cout,
+    const double *__restrict__ vel, const double *__restrict__ vghost, Geo4 vf, Geo3 sig, Geo3 dtvt,
+    const int32_t *__restrict__ aloft, DevScalars *sc, double *__restrict__ out1, double *__restrict__ out2) {
+  static_assert(DIR == 1 || DIR == 2, "lanes along i: y and z sweeps only");
+  extern __shared__ __align__(128) unsigned char act_smem[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(act_smem) + 2 * wid;
+  double *wsm = reinterpret_cast<double *>(act_smem + 128) + (long)wid * ACT_WARP_D;
+  // buffer b: q chunk at wsm + b*2*ACH*32, v chunk after it; geometry of
+  // buffer b at wsm + 4*ACH*32 + b*2*ACH (sigma(c+2), then dt/kappa(c+1))
+  const int nother = (DIR == 1) ? L.nz : L.ny;
+  const int nti = (L.nx + 31) >> 5;
+  const long t = (long)blockIdx.x * ACT_WARPS + wid;
+  if (t >= (long)nti * nother * L.ns) return;  // whole warps only; no block barrier below
+  const int g = (int)(t % L.ns);
+  const long rr = t / L.ns;
+  const int it = (int)(rr % nti);
+  const int o = (int)(rr / nti) + 1;  // k (y sweep) or j (z sweep)
+  const int a = (it << 5) + lane + 1;  // i
+  const bool valid = a <= L.nx;
+  const int n = (DIR == 1) ? L.ny : L.nz;
+  const int rmin = (DIR == 1) ? box.jmin : box.kmin;
+  const int rmax = (DIR == 1) ? box.jmax : box.kmax;
+  const int ncells = rmax - rmin + 1;
+  const int st = (DIR == 1) ? (int)L.P : (int)L.PY;
+  const int ac = valid ? a : 1;
+  const long base = (DIR == 1) ? L.cell(ac, 1, o) : L.cell(ac, o, 1);
+  const bool lane_active = (DIR == 1) ? (a >= box.imin && a <= box.imax && o >= box.kmin && o <= box.kmax)
+                                      : (a >= box.imin && a <= box.imax && o >= box.jmin && o <= box.jmax);
+  const bool al = valid && lane_active && aloft[g] != 0;
+  double *po = cout + (long)g * L.PG + base;
+  if (!__any_sync(0xffffffffu, al)) {  // the reference leaves zeros
+    if (valid)
+      for (int c = 1; c <= n; c++) po[(c - 1) * st] = 0.0;
+    return;
+  }
+  if (valid && !al)
+    for (int c = 1; c <= n; c++) po[(c - 1) * st] = 0.0;
+  if (lane == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_init_fence();
+  }
+  __syncwarp();
+  const double *pq = cin + (long)g * L.PG + base;
+  const double *pv = vel + base;
+  const double *pvg = vghost + base;
+  const LineGeo gsig = line_of<DIR>(sig, ac, o);   // constant along i: the same line for every lane
+  const LineGeo gdtv = line_of<DIR>(dtvt, ac, o);
+  const double vf0 = (DIR == 2) ? vf.p[(long)g * vf.sg] : 0.0;  // one fall speed per grain
+  const bool out_lo = rmin == 1;
+  const bool out_hi = rmax == n;
+  const int ctop = (DIR == 2) ? ncells + 1 : rmax + 1;  // update_cc(ncells+1) for z (:309-311)
+  if (DIR == 2 && out_hi && ctop < rmin - 1 && lane == 0) raise_error(sc, A3G_ERR_UNSUPPORTED, 311);
+  const long na = L.nx;
+  const long oo = (long)g * na * nother + (long)(o - 1) * na + (ac - 1);
+  auto fs_ok = [&](int I) { return I >= rmin - 1 && I <= rmax + 1; };
+  auto fss_ok = [&](int I) { return I >= rmin && I <= rmax + 1; };
+  auto qload = [&](int c) -> double {
+    return (c >= rmin - 2 && c <= rmax + 2 && c >= 1 && c <= n) ? pq[(c - 1) * st] : 0.0;
+  };
+  auto vload = [&](int c) -> double {
+    const int cl = c < 1 ? 1 : (c > n ? n : c);
+    double v = ((DIR == 2 && (c < 1 || c > n)) ? pvg : pv)[(cl - 1) * st];
+    if (DIR == 2) v = v + vf0;
+    return v;
+  };
+  const int cs = out_lo ? 0 : 1;
+  const int ce = out_hi ? n + 1 : n;
+  // ---- interface cs and the window at cs (k_advect_col's prologue) ----------
+  double q0 = qload(cs), q1 = qload(cs + 1);
+  double d0 = q0 - qload(cs - 1), d1 = q1 - q0;
+  double usA, usB, vB, dtv0 = gdtv.at(cs), fss0, fsr0;
+  {
+    const double vm2 = vload(cs - 2), vm1 = vload(cs - 1), v0 = vload(cs);
+    vB = vload(cs + 1);
+    const double usm1 = fs_ok(cs - 1) ? 0.5 * (vm2 + vm1) * gsig.at(cs - 1) : 0.0;
+    usA = fs_ok(cs) ? 0.5 * (vm1 + v0) * gsig.at(cs) : 0.0;
+    usB = fs_ok(cs + 1) ? 0.5 * (v0 + vB) * gsig.at(cs + 1) : 0.0;
+    const double qm1 = qload(cs - 1);
+    const double dm = qm1 - qload(cs - 2);
+    const Iface f = make_iface(usm1, usA, usB, dtv0, fss_ok(cs), fs_ok(cs));
+    fss0 = fss_select<LIM>(dm, d0, d1, f.up, f.cf, f.fss_ok, eps, nocycle);
+    fsr0 = f.fs_ok ? (f.usp * d0) + q0 * f.divm : 0.0;
+  }
+  // ---- one step: interface c+1 and the update of cell c (k_advect_col's) ----
+  auto step = [&](int c, auto checked, double q2, double vn, double s2, double dtv1) {
+    constexpr bool CK = decltype(checked)::value;
+    const int I = c + 1;
+    const bool fsok2 = !CK || fs_ok(c + 2);
+    const double usC = fsok2 ? 0.5 * (vB + vn) * s2 : 0.0;
+    vB = vn;
+    const Iface f = make_iface(usA, usB, usC, dtv1, !CK || fss_ok(I), !CK || fs_ok(I));
+    usA = usB;
+    usB = usC;
+    const double d2 = q2 - q1;
+    const double fss1 = fss_select<LIM>(d0, d1, d2, f.up, f.cf, f.fss_ok, eps, nocycle);
+    double fsr1 = 0.0, fsl1 = 0.0;
+    if (f.fs_ok) {
+      fsr1 = f.usp * d1;
+      fsl1 = f.usm * d1;
+      fsr1 = fsr1 + q1 * f.divm;
+      fsl1 = fsl1 + q0 * f.divp;
+    }
+    const double upd = cell_update(dtv0, fsl1, fsr0, fss1, fss0);
+    if (al) {
+      if (!CK || (c >= 1 && c <= n)) {
+        const bool inbox = !CK || (c >= rmin && c <= rmax);
+        po[(c - 1) * st] = inbox ? q0 + upd : 0.0;
+      }
+      if (CK && out_lo && c == 0) out1[oo] += upd;
+      if (out_hi && c == ctop) out2[oo] += upd;
+    }
+    fss0 = fss1;
+    fsr0 = fsr1;
+    q0 = q1;
+    q1 = q2;
+    d0 = d1;
+    d1 = d2;
+    dtv0 = dtv1;
+  };
+  auto checked_step = [&](int c) {
+    step(c, CkT{}, qload(c + 2), vload(c + 2), fs_ok(c + 2) ? gsig.at(c + 2) : 0.0, gdtv.at(c + 1));
+  };
+  // steps without range checks: c >= rmin, c+2 <= min(n, rmax+1)
+  int fa = max(cs, rmin), fb = min(n - 2, rmax - 1);
+  if (fb < fa) { fa = ce + 1; fb = ce; }
+  int c = cs;
+  for (; c < fa; c++) checked_step(c);
+  if (fa <= fb) {
+    // chunk m holds cells C0(m) .. C0(m)+ACH-1, C0(m) = fa+2+m*ACH: the cell
+    // c+2 of the steps c = fa+m*ACH .. (clipped to fb)
+    const int nchunk = (fb - fa) / ACH + 1;
+    constexpr uint32_t bytes = 2u * ACH * 32u * 8u;
+    auto issue = [&](int m) {
+      const int bi = m & 1;
+      double *qb = wsm + bi * 2 * ACH * 32;
+      const int C0 = fa + 2 + m * ACH;
+      if (lane == 0) {
+        mbar_arrive_expect_tx(&bar[bi], bytes);
+        if (DIR == 1) {
+          tma_load_4d(qb, &tq, &bar[bi], it << 5, C0 - 1, o - 1, g);
+          tma_load_4d(qb + ACH * 32, &tv, &bar[bi], it << 5, C0 - 1, o - 1, 0);
+        } else {
+          tma_load_4d(qb, &tq, &bar[bi], it << 5, o - 1, C0 - 1, g);
+          tma_load_4d(qb + ACH * 32, &tv, &bar[bi], it << 5, o - 1, C0 - 1, 0);
+        }
+      }
+      double *gb = wsm + 4 * ACH * 32 + bi * 2 * ACH;
+      if (lane < ACH && C0 + lane <= fb + 2) {
+        gb[lane] = gsig.at(C0 + lane);            // sigma(c+2)
+        gb[ACH + lane] = gdtv.at(C0 + lane - 1);  // dt/kappa(c+1)
+      }
+    };
+    uint32_t ph = 0u;
+    issue(0);
+    for (int m = 0; m < nchunk; m++) {
+      const int bi = m & 1;
+      if (m + 1 < nchunk) issue(m + 1);
+      if (!mbar_wait(&bar[bi], (ph >> bi) & 1u)) {
+        if (lane == 0) raise_error(sc, A3G_ERR_TIMEOUT, 3);
+        return;
+      }
+      ph ^= 1u << bi;
+      __syncwarp();
+      const double *qb = wsm + bi * 2 * ACH * 32 + lane;
+      const double *vb = qb + ACH * 32;
+      const double *gb = wsm + 4 * ACH * 32 + bi * 2 * ACH;
+      const int cend = min(fb, fa + m * ACH + ACH - 1);
+#pragma unroll 4
+      for (int e = 0; c <= cend; c++, e++)
+        step(c, FastT{}, qb[e * 32], (DIR == 2) ? vb[e * 32] + vf0 : vb[e * 32], gb[e], gb[ACH + e]);
+      __syncwarp();
+    }
+  }
+  for (; c <= ce; c++) checked_step(c);
+}
+
+// Launches the TMA-fed column march; false when its conditions do not hold
+// (the caller takes another variant).
+template <int DIR, int LIM>
+static bool launch_colt(a3g_ctx *ctx) {
+  const Layout &L = ctx->L;
+  const Geo3 &sg = (DIR == 1) ? ctx->sny : ctx->snz;
+  if (sg.si != 0 || ctx->dtv.si != 0) return false;  // geometry must not vary along i
+  if (DIR == 2 && (ctx->vf.si != 0 || ctx->vf.sj != 0 || ctx->vf.sk != 0)) return false;
+  CUtensorMap tq, tv;
+  const double *vel = dir_vel(ctx, DIR);
+  if (!tensor_map(ctx, ctx->c0, DIR == 1 ? TM_ADV_QY : TM_ADV_QZ, &tq) ||
+      !tensor_map(ctx, vel, DIR == 1 ? TM_ADV_VY : TM_ADV_VZ, &tv))
+    return false;
+  const size_t smem = 128 + (size_t)ACT_WARPS * ACT_WARP_D * sizeof(double);
+  static_assert(128 + ACT_WARPS * ACT_WARP_D * 8 <= 48 * 1024, "fits the default dynamic limit");
+  const int nother = (DIR == 1) ? L.nz : L.ny;
+  const long nw = (long)((L.nx + 31) / 32) * nother * L.ns;
+  k_advect_colt<DIR, LIM><<<(unsigned)((nw + ACT_WARPS - 1) / ACT_WARPS), 32 * ACT_WARPS, smem, ctx->stream>>>(
+      tq, tv, L, ctx->box, ctx->prm.nocycle, ctx->prm.eps_thresh, ctx->c0, ctx->c1, vel, dir_vghost(ctx, DIR),
+      ctx->vf, sg, ctx->dtv, ctx->aloft, ctx->sc, (DIR == 1) ? ctx->out_xz1 : ctx->out_xy1,
+      (DIR == 1) ? ctx->out_xz2 : ctx->out_xy2);
+  return true;
+}
+
+// ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
 template <int DIR, int LIM, int GC, bool PER, bool TOPO = false>
@@ -1245,6 +1470,10 @@ static void launch_dir_lim(a3g_ctx *ctx) {
   if constexpr (DIR != 0) {
     if (variant == 5) {
       launch_col<DIR, LIM>(ctx);
+      return;
+    }
+    if (variant == 6) {
+      if (!launch_colt<DIR, LIM>(ctx)) launch_block_v<DIR, LIM, 4, false>(ctx);
       return;
     }
   }

@@ -837,8 +837,6 @@ __global__ void __launch_bounds__(64, 8) k_cn_solve_zt(const __grid_constant__ C
 // memory while its tile is in flight.  Warps take contiguous runs of line
 // groups (neighbouring i, then k), which share table rows.
 // ---------------------------------------------------------------------------
-constexpr int YT_CH = 32;
-constexpr int YT_ROWS = YT_CH + 2;
 
 __global__ void __launch_bounds__(64) k_cn_solve_yt(const __grid_constant__ CUtensorMap tin,
                                                     const __grid_constant__ CUtensorMap tout, Layout L,
@@ -1030,10 +1028,8 @@ static EncodeTiledFn encode_tiled_fn() {
 }
 
 // A level as a 4-D tensor (i, j, k, grain) of doubles with the device
-// layout's pitches; the box is one tile of the given kind:
-//   TM_COLUMN: 32 i x 1 j x nz k (the z solve's column tile);
-//   TM_YCHUNK_IN / TM_YCHUNK_OUT: 32 i x (YT_CH + 2) / YT_CH j (the y solve's
-//   chunk tile with the cells before and after it, and the chunk it stores).
+// layout's pitches (a wind array: the same with one grain); the box is one
+// tile of the given kind (TmapKind).
 bool tensor_map(a3g_ctx *ctx, const double *p, int kind, CUtensorMap *out) {
   for (const TmapEntry &e : ctx->tmaps)
     if (e.p == p && e.kind == kind) {
@@ -1043,7 +1039,9 @@ bool tensor_map(a3g_ctx *ctx, const double *p, int kind, CUtensorMap *out) {
   EncodeTiledFn enc = encode_tiled_fn();
   if (!enc) return false;
   const Layout &L = ctx->L;
-  const cuuint64_t dims[4] = {(cuuint64_t)L.nx, (cuuint64_t)L.ny, (cuuint64_t)L.nz, (cuuint64_t)L.ns};
+  const bool wind = kind == TM_ADV_VY || kind == TM_ADV_VZ;
+  const cuuint64_t dims[4] = {(cuuint64_t)L.nx, (cuuint64_t)L.ny, (cuuint64_t)L.nz,
+                              (cuuint64_t)(wind ? 1 : L.ns)};
   const cuuint64_t strides[3] = {(cuuint64_t)L.P * 8, (cuuint64_t)L.PY * 8, (cuuint64_t)L.PG * 8};
   cuuint32_t box[4] = {32, 1, 1, 1};
   if (kind == TM_COLUMN) {
@@ -1053,6 +1051,10 @@ bool tensor_map(a3g_ctx *ctx, const double *p, int kind, CUtensorMap *out) {
     box[1] = YT_ROWS;
   } else if (kind == TM_YCHUNK_OUT) {
     box[1] = YT_CH;
+  } else if (kind == TM_ADV_QY || kind == TM_ADV_VY) {
+    box[1] = ACH;
+  } else if (kind == TM_ADV_QZ || kind == TM_ADV_VZ) {
+    box[2] = ACH;
   } else {
     return false;
   }
