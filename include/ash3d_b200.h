@@ -382,9 +382,10 @@ int a3g_kernel_times(a3g_ctx *ctx, double *ms, uint64_t *count);
 /* ---- tuning (no counterpart in the reference) ---- */
 /* Selects a kernel variant.  dir 0, 1, 2: the advection sweep along x, y, z,
  * variant 0 marching threads, 1 blocks of 4 cells, 2 blocks of 8 cells, and
- * for x only 3, warps marching 32 rows through shared-memory tiles, and 4,
- * one warp per row walking it in 32-cell chunks with the lanes along i
- * (defaults: x 4, y 6, z 6).
+ * for x only 3, warps marching 32 rows through shared-memory tiles, 4,
+ * one warp per row walking it in 32-cell chunks with the lanes along i, and
+ * 5, the same with the interior chunks staged one ahead by TMA tensor copies
+ * (defaults: x 5, y 6, z 6).
  * dir 3: the Crank-Nicolson x solve, variant 0 warp-tiled (default), 1 one
  * thread per line.  dir 4: the Crank-Nicolson y and z solves, variant 0 one
  * grain per thread, 1 two grains of a line per thread, 2 four, 3 tiles of

@@ -52,9 +52,10 @@ def _variants(op):
 def _adv_variant(d, variant):
     """The variant a direction takes for a parametrised advection variant:
     3 and 4 exist for x only, 5 and 6 (the column marches, from global memory
-    and from TMA chunks) for y and z only."""
+    and from TMA chunks) for y and z only; 6 takes x's warp rows fed by TMA
+    (x variant 5)."""
     if d == 0:
-        return 4 if variant in (5, 6) else variant
+        return {5: 4, 6: 5}.get(variant, variant)
     return variant if variant in (5, 6) else min(variant, 2)
 
 

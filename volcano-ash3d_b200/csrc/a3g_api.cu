@@ -192,12 +192,12 @@ int a3g_create(const a3g_grid_desc *grid, const a3g_params *params, int device, 
   ctx->h_aloft.assign(grid->ns, 1);
   ctx->n_gs_aloft = grid->ns;
   ctx->last_bc = 0;
-  // fastest measured advection variants on B200 (x: warp-row chunks, C2
-  // 1.62 ms against 2.16 for marching rows; y, z: the column march fed by
-  // TMA chunks, C2 y 1.43 -> 1.24 ms and z 1.64 -> 1.28 ms against 4-cell
-  // blocks, which remain where the march's conditions do not hold);
-  // a3g_set_variant overrides them
-  ctx->tune_advect[0] = 4;
+  // fastest measured advection variants on B200 (x: warp-row chunks with
+  // the interior chunks fed by TMA, C2 1.27 ms against 1.38 without and 2.16
+  // for marching rows; y, z: the column march fed by TMA chunks, C2 y 1.43 ->
+  // 1.24 ms and z 1.64 -> 1.28 ms against 4-cell blocks, which remain where
+  // the march's conditions do not hold); a3g_set_variant overrides them
+  ctx->tune_advect[0] = 5;
   ctx->tune_advect[1] = 6;
   ctx->tune_advect[2] = 6;
   ctx->tune_cn_x = 0;
@@ -1334,7 +1334,7 @@ int a3g_set_variant(a3g_ctx *ctx, int32_t dir, int32_t variant) {
   if (!ctx) return fail(A3G_ERR_ARG, "null context");
   const bool col = (dir == 1 || dir == 2) && (variant == 5 || variant == 6);  // the column marches (y, z)
   if (dir < 0 || dir > 5 || variant < 0 ||
-      (!col && variant > (dir == 0 ? 4 : dir == 3 ? 1 : dir == 4 ? 3 : dir == 5 ? 1 : 2)))
+      (!col && variant > (dir == 0 ? 5 : dir == 3 ? 1 : dir == 4 ? 3 : dir == 5 ? 1 : 2)))
     return fail(A3G_ERR_ARG, "bad direction or variant");
   if (dir == 3) ctx->tune_cn_x = variant;
   else if (dir == 4) ctx->tune_cn_yz = variant;

@@ -75,6 +75,8 @@ struct Box {
 //   TM_YCHUNK_OUT  level, 32 i x YT_CH j (the CN y chunk it stores)
 //   TM_ADV_QY/QZ   level, 32 i x ACH j / ACH k (an advection chunk)
 //   TM_ADV_VY/VZ   wind array, the same chunks
+//   TM_ADV_QX1/QX2 level, 32 i x 1 j x 1 k x 1 / 2 grains (an x chunk)
+//   TM_ADV_VX      wind array, 32 i (an x chunk)
 enum TmapKind {
   TM_COLUMN = 0,
   TM_YCHUNK_IN = 1,
@@ -82,9 +84,12 @@ enum TmapKind {
   TM_ADV_QY = 3,
   TM_ADV_QZ = 4,
   TM_ADV_VY = 5,
-  TM_ADV_VZ = 6
+  TM_ADV_VZ = 6,
+  TM_ADV_QX1 = 7,
+  TM_ADV_QX2 = 8,
+  TM_ADV_VX = 9
 };
-constexpr int YT_CH = 32;            // cells per CN y chunk
+constexpr int YT_CH = 16;            // cells per CN y chunk
 constexpr int YT_ROWS = YT_CH + 2;   // with the cell before and the cell after
 constexpr int ACH = 8;               // cells per advection chunk
 struct TmapEntry {

@@ -32,6 +32,8 @@
 #include "exact_div.cuh"
 #include "tma.cuh"
 
+#include <cstring>
+
 namespace a3g {
 
 // Fortran MAX/MIN of two reals as one FP64 min/max instruction.  For the
@@ -836,16 +838,24 @@ static void launch_advect_xt(a3g_ctx *ctx) {
 // the march's expressions (make_iface, iface_grain, cell_update), so the
 // results are the same bits.  Nothing is carried in registers between
 // chunks, which keeps the register count and the L1 traffic low.
+// With TMA, the loads of the interior chunks (the ones without range checks)
+// arrive by tensor copies instead: the warp's GC grains and the wind of the
+// chunk, one chunk ahead, into one of two staging buffers, so that the
+// lanes no longer wait on global loads there.  Same arithmetic, same bits.
 // ---------------------------------------------------------------------------
 constexpr int XW_WARPS = 4;
 
-template <int LIM, int GC, bool PER, bool LC>
-__global__ void __launch_bounds__(32 * XW_WARPS, 6) k_advect_xw(Layout L, Box box, int nocycle, double eps,
+template <int LIM, int GC, bool PER, bool LC, bool TMA>
+__global__ void __launch_bounds__(32 * XW_WARPS, 6) k_advect_xw(const __grid_constant__ CUtensorMap tq,
+                                                          const __grid_constant__ CUtensorMap tv, Layout L,
+                                                          Box box, int nocycle, double eps,
                                                           int ngroups, const double *__restrict__ cin,
                                                           double *__restrict__ cout,
                                                           const double *__restrict__ vel, Geo3 sig, Geo3 dtvt,
-                                                          const int32_t *__restrict__ aloft,
+                                                          const int32_t *__restrict__ aloft, DevScalars *sc,
                                                           double *__restrict__ out1, double *__restrict__ out2) {
+  __shared__ __align__(128) double s_st[TMA ? XW_WARPS : 1][2][(GC + 1) * 32];  // staged q (GC grains), v
+  __shared__ __align__(8) uint64_t s_bar[XW_WARPS][2];
   __shared__ double s_q[XW_WARPS][GC][64];
   __shared__ double s_fss[XW_WARPS][GC][64];
   __shared__ double s_fsr[XW_WARPS][GC][64];
@@ -908,7 +918,7 @@ __global__ void __launch_bounds__(32 * XW_WARPS, 6) k_advect_xw(Layout L, Box bo
   // areas inside [rmin, rmax+1], no ghost or outflow cell); the others take
   // the checked body.
   const int ilo = max(rmin + 2, 1), ihi = min(n, rmax + 1);
-  auto chunk = [&](int t, auto checked) {
+  auto chunk = [&](int t, auto checked, const double *stg) {
     constexpr bool CK = decltype(checked)::value;
     __syncwarp();
     const int i = 32 * t - 1 + lane;
@@ -919,7 +929,7 @@ __global__ void __launch_bounds__(32 * XW_WARPS, 6) k_advect_xw(Layout L, Box bo
     for (int q = 0; q < GC; q++) {
       double v = 0.0;
       if (!CK) {
-        v = pq[q][i - 1];
+        v = TMA ? stg[q * 32 + lane] : pq[q][i - 1];
       } else if (i >= rmin - 2 && i <= rmax + 2) {  // ghost cells of Set_BC(1): zero, or wrapped
         if (i >= 1 && i <= n) v = pq[q][i - 1];
         else if (PER) v = pq[q][wrap(i) - 1];
@@ -928,7 +938,7 @@ __global__ void __launch_bounds__(32 * XW_WARPS, 6) k_advect_xw(Layout L, Box bo
       s_q[wid][q][sl] = v;
     }
     double vi = 0.0;  // vel(i) is read by us(i) and us(i+1) only
-    if (!CK) vi = pv[i - 1];
+    if (!CK) vi = TMA ? stg[GC * 32 + lane] : pv[i - 1];
     else if (i >= rmin - 2 && i <= rmax + 1) vi = pv[(PER ? wrap(i) : (i < 1 ? 1 : (i > n ? n : i))) - 1];
     s_v[wid][sl] = vi;
     __syncwarp();
@@ -966,26 +976,71 @@ __global__ void __launch_bounds__(32 * XW_WARPS, 6) k_advect_xw(Layout L, Box bo
       }
     }
   };
+  // the interior chunks form the run tf0..tf1
+  const int tf0 = (ilo + 32) / 32, tf1 = ihi >= 30 ? (ihi - 30) / 32 : -1;
+  uint32_t ph = 0u;  // bit b: the parity of staging buffer b's barrier
+  auto issue = [&](int t) {  // chunk t's loads i = 32t-1 .. 32t+30 (x from 32t-2 >= 0, even)
+    const int bi = (t - tf0) & 1;
+    if (lane == 0) {
+      mbar_arrive_expect_tx(&s_bar[wid][bi], (GC + 1) * 32 * 8);
+      tma_load_4d(s_st[wid][bi], &tq, &s_bar[wid][bi], 32 * t - 2, j - 1, k - 1, g0);
+      tma_load_4d(s_st[wid][bi] + GC * 32, &tv, &s_bar[wid][bi], 32 * t - 2, j - 1, k - 1, 0);
+    }
+  };
+  if (TMA) {
+    if (lane == 0) {
+      mbar_init(&s_bar[wid][0], 1);
+      mbar_init(&s_bar[wid][1], 1);
+      mbar_init_fence();
+    }
+    __syncwarp();
+    if (tf0 <= tf1) issue(tf0);
+  }
   for (int t = 0; 32 * t - 3 <= n + 1; t++) {
-    if (32 * t - 1 >= ilo && 32 * t + 30 <= ihi) chunk(t, FastT{});
-    else chunk(t, CkT{});
+    if (t >= tf0 && t <= tf1) {
+      if (TMA) {
+        const int bi = (t - tf0) & 1;
+        if (t + 1 <= tf1) issue(t + 1);
+        if (!mbar_wait(&s_bar[wid][bi], (ph >> bi) & 1u)) {
+          if (lane == 0) raise_error(sc, A3G_ERR_TIMEOUT, 4);
+          return;
+        }
+        ph ^= 1u << bi;
+        chunk(t, FastT{}, s_st[wid][bi]);
+      } else {
+        chunk(t, FastT{}, nullptr);
+      }
+    } else {
+      chunk(t, CkT{}, nullptr);
+    }
   }
 }
 
 template <int LIM>
-static void launch_advect_xw(a3g_ctx *ctx) {
+static void launch_advect_xw(a3g_ctx *ctx, bool tma) {
   const Layout &L = ctx->L;
   const int gc = (L.ns >= 2) ? 2 : 1;
   const int ngroups = (L.ns + gc - 1) / gc;
   const long nwarps = (long)L.ny * L.nz * ngroups;
   const unsigned blocks = (unsigned)((nwarps + XW_WARPS - 1) / XW_WARPS);
   const bool lc = along<0>(ctx->snx) == 0 && along<0>(ctx->dtv) == 0;
+  CUtensorMap tq, tv;
+  std::memset(&tq, 0, sizeof(tq));
+  std::memset(&tv, 0, sizeof(tv));
+  if (tma && !(tensor_map(ctx, ctx->c0, gc == 2 ? TM_ADV_QX2 : TM_ADV_QX1, &tq) &&
+               tensor_map(ctx, ctx->vx, TM_ADV_VX, &tv)))
+    tma = false;
 #define A3G_XW(GC_, PER_, LC_)                                                                              \
-  k_advect_xw<LIM, GC_, PER_, LC_><<<blocks, 32 * XW_WARPS, 0, ctx->stream>>>(                             \
-      L, ctx->box, ctx->prm.nocycle, ctx->prm.eps_thresh, ngroups, ctx->c0, ctx->c1, ctx->vx, ctx->snx,     \
-      ctx->dtv, ctx->aloft, ctx->out_yz1, ctx->out_yz2)
+  if (tma)                                                                                                   \
+    k_advect_xw<LIM, GC_, PER_, LC_, true><<<blocks, 32 * XW_WARPS, 0, ctx->stream>>>(                      \
+        tq, tv, L, ctx->box, ctx->prm.nocycle, ctx->prm.eps_thresh, ngroups, ctx->c0, ctx->c1, ctx->vx,      \
+        ctx->snx, ctx->dtv, ctx->aloft, ctx->sc, ctx->out_yz1, ctx->out_yz2);                                \
+  else                                                                                                       \
+    k_advect_xw<LIM, GC_, PER_, LC_, false><<<blocks, 32 * XW_WARPS, 0, ctx->stream>>>(                     \
+        tq, tv, L, ctx->box, ctx->prm.nocycle, ctx->prm.eps_thresh, ngroups, ctx->c0, ctx->c1, ctx->vx,      \
+        ctx->snx, ctx->dtv, ctx->aloft, ctx->sc, ctx->out_yz1, ctx->out_yz2)
 #define A3G_XW_LC(GC_, PER_) \
-  if (lc) A3G_XW(GC_, PER_, true); else A3G_XW(GC_, PER_, false)
+  if (lc) { A3G_XW(GC_, PER_, true); } else { A3G_XW(GC_, PER_, false); }
   if (gc == 2) {
     if (ctx->grid.periodic) { A3G_XW_LC(2, true); } else { A3G_XW_LC(2, false); }
   } else {
@@ -1462,8 +1517,8 @@ static void launch_dir_lim(a3g_ctx *ctx) {
       launch_advect_xt<LIM>(ctx);
       return;
     }
-    if (variant == 4) {
-      launch_advect_xw<LIM>(ctx);
+    if (variant == 4 || variant == 5) {
+      launch_advect_xw<LIM>(ctx, variant == 5);
       return;
     }
   }

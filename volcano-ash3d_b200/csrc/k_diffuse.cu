@@ -827,7 +827,8 @@ __global__ void __launch_bounds__(64, 8) k_cn_solve_zt(const __grid_constant__ C
 // position l0 - 1 + r), tile[r][lane].  Two buffers per warp: the next
 // chunk's load is in flight while the lanes work on the current one.
 //   pass 1 (forward): the elimination of B' over the whole line, keeping only
-//     B' at the last cell of every chunk (a checkpoint, in shared memory);
+//     B' at the last cell of every chunk (a checkpoint, parked in the output
+//     line at that cell, which the chunk's own store overwrites later);
 //   pass 2 (backward, last chunk first, which pass 1 left in its buffer):
 //     recompute the chunk's B' from the previous chunk's checkpoint (same
 //     operations, same bits), back-substitute in place, and store the chunk
@@ -843,16 +844,14 @@ __global__ void __launch_bounds__(64) k_cn_solve_yt(const __grid_constant__ CUte
                                                     Box box, LineMap map, double *__restrict__ cout,
                                                     const double *__restrict__ tab,
                                                     const int32_t *__restrict__ aloft, DevScalars *sc,
-                                                    int wpb, int nch_max) {
+                                                    int wpb) {
   extern __shared__ __align__(128) unsigned char yt_smem[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   constexpr int BUF = 32 * YT_ROWS;  // doubles per buffer (a multiple of 16: 128-byte aligned buffers)
   uint64_t *bar = reinterpret_cast<uint64_t *>(yt_smem) + 2 * wid;
-  double *wbase =
-      reinterpret_cast<double *>(yt_smem + ZT_BAR_BYTES) + (long)wid * (2 * BUF + nch_max * 32 + CN_NF * 32);
+  double *wbase = reinterpret_cast<double *>(yt_smem + ZT_BAR_BYTES) + (long)wid * (2 * BUF + CN_NF * 32);
   auto buf = [&](int bi) { return wbase + (bi ? BUF : 0); };
-  double *ck = wbase + 2 * BUF;  // checkpoint of chunk ch at ck[ch*32 + lane]
-  double *stab = ck + nch_max * 32;  // staged table of the chunk: field f, row c at stab[f*32 + c]
+  double *stab = wbase + 2 * BUF;  // staged table of the chunk: field f, row c at stab[f*32 + c]
   if (lane == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
@@ -906,9 +905,9 @@ __global__ void __launch_bounds__(64) k_cn_solve_yt(const __grid_constant__ CUte
       ph ^= 1u << bi;
     };
     const double *tl = tab + map.u(1, k);  // the coefficients do not vary along i (map.da == 0)
-    auto stage = [&](int l0, int nf) {      // fields 0..nf-1 of rows l0..l0+31 into stab
+    auto stage = [&](int l0, int nf) {      // fields 0..nf-1 of the chunk's rows into stab
       const int l = l0 + lane;
-      if (l < ncells)
+      if (lane < YT_CH && l < ncells)
         for (int f = 0; f < nf; f++) stab[f * 32 + lane] = tl[f * F + (long)l * U];
     };
     auto co = [&](int f, int c) { return stab[f * 32 + c]; };
@@ -939,10 +938,11 @@ __global__ void __launch_bounds__(64) k_cn_solve_yt(const __grid_constant__ CUte
           qm = qc;
           qc = qp;
         }
-        ck[ch * 32 + lane] = bp;
+        if (ch + 1 < nch) xg[(long)(rmin + l0 + YT_CH - 2) * L.P] = bp;  // checkpoint B'(l0+YT_CH-1)
       }
       __syncwarp();
     }
+    fence_proxy_async_all();  // the checkpoints land before any store of this line's chunks
     // pass 2: per chunk, last first: recompute B', back-substitute, store
     double xn = 0.0;
     for (int ch = nch - 1; ch >= 0 && ok; ch--) {
@@ -958,7 +958,7 @@ __global__ void __launch_bounds__(64) k_cn_solve_yt(const __grid_constant__ CUte
       double *T = buf(bi) + lane;
       const int cnt = (ncells - l0) < YT_CH ? (ncells - l0) : YT_CH;
       if (act) {
-        double bq = ch > 0 ? ck[(ch - 1) * 32 + lane] : 0.0;
+        double bq = ch > 0 ? xg[(long)(rmin + l0 - 2) * L.P] : 0.0;
         double qm2 = (ch == 0) ? T[32] : T[0];
         double qc2 = T[32];
 #pragma unroll 4
@@ -1039,7 +1039,7 @@ bool tensor_map(a3g_ctx *ctx, const double *p, int kind, CUtensorMap *out) {
   EncodeTiledFn enc = encode_tiled_fn();
   if (!enc) return false;
   const Layout &L = ctx->L;
-  const bool wind = kind == TM_ADV_VY || kind == TM_ADV_VZ;
+  const bool wind = kind == TM_ADV_VY || kind == TM_ADV_VZ || kind == TM_ADV_VX;
   const cuuint64_t dims[4] = {(cuuint64_t)L.nx, (cuuint64_t)L.ny, (cuuint64_t)L.nz,
                               (cuuint64_t)(wind ? 1 : L.ns)};
   const cuuint64_t strides[3] = {(cuuint64_t)L.P * 8, (cuuint64_t)L.PY * 8, (cuuint64_t)L.PG * 8};
@@ -1055,6 +1055,10 @@ bool tensor_map(a3g_ctx *ctx, const double *p, int kind, CUtensorMap *out) {
     box[1] = ACH;
   } else if (kind == TM_ADV_QZ || kind == TM_ADV_VZ) {
     box[2] = ACH;
+  } else if (kind == TM_ADV_QX1 || kind == TM_ADV_VX) {
+  } else if (kind == TM_ADV_QX2) {
+    if (L.ns < 2) return false;
+    box[3] = 2;
   } else {
     return false;
   }
@@ -1113,9 +1117,7 @@ static bool launch_cn_solve_yt(a3g_ctx *ctx, const LineMap &map, const double *t
   if (!tensor_map(ctx, ctx->c0, TM_YCHUNK_IN, &tin) || !tensor_map(ctx, ctx->c1, TM_YCHUNK_OUT, &tout))
     return false;
   const int wpb = 2;
-  const int nch_max = (L.ny + YT_CH - 1) / YT_CH;
-  const size_t smem =
-      ZT_BAR_BYTES + (size_t)wpb * (2 * 32 * YT_ROWS + nch_max * 32 + CN_NF * 32) * sizeof(double);
+  const size_t smem = ZT_BAR_BYTES + (size_t)wpb * (2 * 32 * YT_ROWS + CN_NF * 32) * sizeof(double);
   if (ctx->tma_grid[1] == 0) {
     int optin = 0;
     if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device) != cudaSuccess ||
@@ -1134,7 +1136,7 @@ static bool launch_cn_solve_yt(a3g_ctx *ctx, const LineMap &map, const double *t
   const long need = (ngroups + wpb - 1) / wpb;
   const int grid = (int)(need < ctx->tma_grid[1] ? need : ctx->tma_grid[1]);
   k_cn_solve_yt<<<grid, 32 * wpb, smem, ctx->stream>>>(tin, tout, L, ctx->box, map, ctx->c1, tab, ctx->aloft,
-                                                       ctx->sc, wpb, nch_max);
+                                                       ctx->sc, wpb);
   return true;
 }
 
