@@ -386,8 +386,9 @@ int a3g_kernel_times(a3g_ctx *ctx, double *ms, uint64_t *count);
  * one warp per row walking it in 32-cell chunks with the lanes along i, and
  * 5, the same with the interior chunks staged one ahead by TMA tensor copies
  * (defaults: x 5, y 6, z 6).
- * dir 3: the Crank-Nicolson x solve, variant 0 warp-tiled (default), 1 one
- * thread per line.  dir 4: the Crank-Nicolson y and z solves, variant 0 one
+ * dir 3: the Crank-Nicolson x solve, variant 0 warp-tiled, 1 one thread per
+ * line, 2 warp-tiled with each tile loaded one chunk ahead by a TMA tensor
+ * copy (default).  dir 4: the Crank-Nicolson y and z solves, variant 0 one
  * grain per thread, 1 two grains of a line per thread, 2 four, 3 tiles of
  * 32 lines staged in shared memory by TMA tensor copies (default; where the
  * coefficients vary along i, or nz > 256, variant 3 runs variant 1).

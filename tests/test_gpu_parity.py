@@ -64,7 +64,7 @@ def _set_variant(gpu, op, variant):
         for d in range(3):
             gpu.set_variant(d, _adv_variant(d, variant))
     else:
-        gpu.set_variant(3, variant % 2)
+        gpu.set_variant(3, variant % 3)
         gpu.set_variant(4, variant)
 
 
@@ -131,7 +131,7 @@ def test_run_bitwise(name, variant):
     cfg, gpu, ref = pair(name)
     for d in range(3):
         gpu.set_variant(d, _adv_variant(d, variant))
-    gpu.set_variant(3, variant % 2)
+    gpu.set_variant(3, variant % 3)
     gpu.set_variant(4, variant if variant <= 3 else 3 - variant % 2 if variant < 6 else 1)
     sg = driver.run(gpu, cfg, max_steps=16)
     sr = driver.run(ref, cfg, max_steps=16)

@@ -77,6 +77,8 @@ struct Box {
 //   TM_ADV_VY/VZ   wind array, the same chunks
 //   TM_ADV_QX1/QX2 level, 32 i x 1 j x 1 k x 1 / 2 grains (an x chunk)
 //   TM_ADV_VX      wind array, 32 i (an x chunk)
+//   TM_XROWS       level as a 2-D array of rows (i, row = (grain, k, j)),
+//                  36 i x 32 rows (a CN x tile with its neighbour cells)
 enum TmapKind {
   TM_COLUMN = 0,
   TM_YCHUNK_IN = 1,
@@ -87,11 +89,13 @@ enum TmapKind {
   TM_ADV_VZ = 6,
   TM_ADV_QX1 = 7,
   TM_ADV_QX2 = 8,
-  TM_ADV_VX = 9
+  TM_ADV_VX = 9,
+  TM_XROWS = 10
 };
 constexpr int YT_CH = 16;            // cells per CN y chunk
 constexpr int YT_ROWS = YT_CH + 2;   // with the cell before and the cell after
 constexpr int ACH = 8;               // cells per advection chunk
+constexpr int XT2_COLS = 36;         // cells per CN x tile row as loaded (even start, 16-byte rule)
 struct TmapEntry {
   const void *p;
   int kind;

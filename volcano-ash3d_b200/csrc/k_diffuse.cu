@@ -691,6 +691,207 @@ __global__ void __launch_bounds__(128, 5) k_cn_solve_xt(Layout L, Box box, LineM
 }
 
 // ---------------------------------------------------------------------------
+// x lines, warp-tiled, with TMA tiles.  The walk of k_cn_solve_xt (a warp
+// owns 32 consecutive x rows, chunks of 32 cells, checkpoints of B' in pass
+// 1, recompute and back substitution in pass 2; the same operations and the
+// same bits), but each chunk's tile arrives by one tensor load of 36 cells x
+// 32 rows (the rows of a level are a 2-D array of pitch P) into a dense
+// staging buffer, one chunk ahead: the lanes copy it into the odd-stride
+// tile (conflict-free per-lane rows), and the next chunk's load then runs
+// while they work through the current one.  The load starts on the even
+// cell at or before the chunk's left neighbour (the 16-byte rule for the
+// innermost coordinate); cells outside the level read as zero.
+// Chunks are loaded in the order the two passes use them (0 .. nch-1, then
+// nch-2 .. 0): the last chunk of pass 1 is still in the tile for pass 2.
+// ---------------------------------------------------------------------------
+constexpr int ZT_BAR_BYTES = 128;  // barriers ahead of the tiles (keeps tiles 128-byte aligned)
+constexpr int XT2_WARPS = 2;
+constexpr int XT2_DENSE = 32 * XT2_COLS;             // doubles of the staging buffer
+constexpr int XT2_WARP_D = XT2_DENSE + 32 * XT_S;    // staging buffer + tile
+static_assert((XT2_DENSE * 8) % 128 == 0 && (XT2_WARP_D * 8) % 128 == 0, "128-byte aligned buffers");
+
+__global__ void __launch_bounds__(32 * XT2_WARPS) k_cn_solve_xt2(const __grid_constant__ CUtensorMap trow,
+                                                                Layout L, Box box, LineMap map,
+                                                                const double *__restrict__ cin,
+                                                                double *__restrict__ cout,
+                                                                const double *__restrict__ tab,
+                                                                const int32_t *__restrict__ aloft,
+                                                                DevScalars *sc) {
+  extern __shared__ __align__(128) unsigned char x2_smem[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(x2_smem) + w;
+  double *dense = reinterpret_cast<double *>(x2_smem + ZT_BAR_BYTES) + (long)w * XT2_WARP_D;
+  double *tile = dense + XT2_DENSE;
+  const long nrows = (long)L.ny * L.nz * L.ns;
+  const long r0 = ((long)blockIdx.x * XT2_WARPS + w) * 32;
+  if (r0 >= nrows) return;  // uniform over the warp
+  if (lane == 0) {
+    mbar_init(bar, 1);
+    mbar_init_fence();
+  }
+  __syncwarp();
+  const long r = r0 + lane;
+  const bool valid = r < nrows;
+  const long rc = valid ? r : nrows - 1;
+  const int j = (int)(rc % L.ny) + 1;
+  const long t1 = rc / L.ny;
+  const int k = (int)(t1 % L.nz) + 1;
+  const int g = (int)(t1 / L.nz);
+  const bool active =
+      valid && j >= box.jmin && j <= box.jmax && k >= box.kmin && k <= box.kmax && aloft[g] != 0;
+  const unsigned amask = __ballot_sync(0xffffffffu, active);
+  const int nvalid = (int)((nrows - r0) < 32 ? (nrows - r0) : 32);
+  const int rmin = box.imin, rmax = box.imax;
+  const int ncells = rmax - rmin + 1;
+  const long P = L.P;
+  if (valid) {  // cells outside [rmin, rmax] (FAST_SUBGRID box)
+    double *xr = cout + r * P;
+    for (int c = 1; c < rmin; c++) xr[c - 1] = 0.0;
+    for (int c = rmax + 1; c <= L.nx; c++) xr[c - 1] = 0.0;
+  }
+  double *x0 = cout + r0 * P + (rmin - 1);
+  double *xown = x0 + (long)lane * P;
+  const long U = map.U;
+  const long F = (long)ncells * U;
+  const long u = map.u(j, k);
+  const double *t = tab + u;
+  CnRun R;
+  cn_load_run(t, F, U, tab + CN_NF * F, u, R);
+  double *tr = tile + lane * XT_S;  // this lane's row of the tile
+  const int nch = (ncells + 31) >> 5;
+  const int nload = 2 * nch - 1;  // chunks 0 .. nch-1, then nch-2 .. 0
+  auto chunk_of = [&](int p) { return p < nch ? p : 2 * nch - 2 - p; };
+  // tile columns: 0 = cell l0-1, 1..32 = cells l0..l0+31, 33 = cell l0+32;
+  // cell l0-1 is line position l0-1, 0-based x = rmin + l0 - 2
+  auto issue = [&](int p) {
+    if (lane == 0) {
+      const int xa = rmin + (chunk_of(p) << 5) - 2;
+      mbar_arrive_expect_tx(bar, XT2_DENSE * 8);
+      tma_load_2d(dense, &trow, bar, xa & ~1, (int)r0);
+    }
+  };
+  uint32_t phase = 0u;
+  bool ok = true;
+  // waits for load p, copies it into the tile, then starts load p+1
+  auto next_tile = [&](int p) {
+    if (!mbar_wait(bar, phase)) {
+      ok = false;
+      return;
+    }
+    phase ^= 1u;
+    const int off = (rmin + (chunk_of(p) << 5) - 2) & 1;
+#pragma unroll 8
+    for (int row = 0; row < 32; row++) tile[row * XT_S + lane] = dense[row * XT2_COLS + off + lane];
+    tr[32] = dense[lane * XT2_COLS + off + 32];
+    tr[33] = dense[lane * XT2_COLS + off + 33];
+    __syncwarp();
+    if (p + 1 < nload) issue(p + 1);
+  };
+
+  int lo_w = R.lo;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) lo_w = max(lo_w, __shfl_xor_sync(0xffffffffu, lo_w, o));
+  auto fast_chunk = [&](int l0, int cnt) { return cnt == 32 && l0 > lo_w && l0 + 31 <= ncells - 2; };
+  const double fCL = R.v[CN_CL], fCC = R.v[CN_CC], fCR = R.v[CN_CR], fFA = R.v[CN_FACT];
+  const double fDU = R.v[CN_DU], fDP = R.v[CN_DP], fRD = R.v[CN_RDP];
+
+  // pass 1: forward elimination, checkpoints only (:813-851 and dgtsv)
+  double qm = 0.0, qc = 0.0, bp = 0.0;
+  issue(0);
+  for (int ch = 0; ch < nch; ch++) {
+    const int l0 = ch << 5;
+    const int cnt = (ncells - l0) < 32 ? (ncells - l0) : 32;
+    next_tile(ch);
+    if (!ok) break;
+    if (ch == 0) {
+      qm = tr[1];  // BC_left_t0 = q(rmin)
+      qc = qm;
+    }
+    if (fast_chunk(l0, cnt)) {  // rows l0..l0+31 < ncells-1: qp always from the tile
+#pragma unroll 8
+      for (int c = 0; c < 32; c++) {
+        const double qp = tr[c + 2];
+        const double B = fCL * qm + fCC * qc + fCR * qp;
+        bp = B - fFA * bp;
+        qm = qc;
+        qc = qp;
+      }
+    } else {
+      for (int c = 0; c < cnt; c++) {
+        const int l = l0 + c;
+        const double qp = (l + 1 < ncells) ? tr[c + 2] : qc;  // BC_right_t0 = q(rmax)
+        const double B = cn_coef(t, F, U, R, CN_CL, l) * qm + cn_coef(t, F, U, R, CN_CC, l) * qc +
+                         cn_coef(t, F, U, R, CN_CR, l) * qp;
+        bp = (l == 0) ? B : B - cn_coef(t, F, U, R, CN_FACT, l) * bp;
+        qm = qc;
+        qc = qp;
+      }
+    }
+    if (valid && ch + 1 < nch) xown[l0 + 31] = bp;  // checkpoint B'(l0+31)
+    if (ch + 1 < nch) __syncwarp();  // the last chunk stays in the tile for pass 2
+  }
+
+  // pass 2: per chunk, last first: recompute B', back-substitute, store
+  double xn = 0.0;
+  for (int ch = nch - 1; ch >= 0 && ok; ch--) {
+    const int l0 = ch << 5;
+    const int cnt = (ncells - l0) < 32 ? (ncells - l0) : 32;
+    if (ch != nch - 1) {
+      next_tile(2 * nch - 2 - ch);
+      if (!ok) break;
+    }
+    double bq = (valid && ch > 0) ? xown[l0 - 1] : 0.0;
+    double qm2 = (ch == 0) ? tr[1] : tr[0];
+    double qc2 = tr[1];
+    if (fast_chunk(l0, cnt)) {
+#pragma unroll 8
+      for (int c = 0; c < 32; c++) {
+        const double qp = tr[c + 2];
+        const double B = fCL * qm2 + fCC * qc2 + fCR * qp;
+        bq = B - fFA * bq;
+        tr[c + 1] = bq;
+        qm2 = qc2;
+        qc2 = qp;
+      }
+#pragma unroll 8
+      for (int c = 31; c >= 0; c--) {
+        const double num = tr[c + 1] - fDU * xn;
+        const double v = div_rn_rcp(num, fDP, fRD);
+        tr[c + 1] = v;
+        xn = v;
+      }
+    } else {
+      for (int c = 0; c < cnt; c++) {
+        const int l = l0 + c;
+        const double qp = (l + 1 < ncells) ? tr[c + 2] : qc2;
+        const double B = cn_coef(t, F, U, R, CN_CL, l) * qm2 + cn_coef(t, F, U, R, CN_CC, l) * qc2 +
+                         cn_coef(t, F, U, R, CN_CR, l) * qp;
+        bq = (l == 0) ? B : B - cn_coef(t, F, U, R, CN_FACT, l) * bq;
+        tr[c + 1] = bq;
+        qm2 = qc2;
+        qc2 = qp;
+      }
+      for (int c = cnt - 1; c >= 0; c--) {
+        const int l = l0 + c;
+        const double b2 = tr[c + 1];
+        const double num = (l == ncells - 1) ? b2 : b2 - cn_coef(t, F, U, R, CN_DU, l) * xn;
+        const double v = div_rn_rcp(num, cn_coef(t, F, U, R, CN_DP, l), cn_coef(t, F, U, R, CN_RDP, l));
+        tr[c + 1] = v;
+        xn = v;
+      }
+    }
+    __syncwarp();
+#pragma unroll 8
+    for (int row = 0; row < 32; row++) {
+      if (row < nvalid && lane < cnt)
+        x0[(long)row * P + l0 + lane] = ((amask >> row) & 1u) ? tile[row * XT_S + 1 + lane] : 0.0;
+    }
+    __syncwarp();
+  }
+  if (!ok && lane == 0) raise_error(sc, A3G_ERR_TIMEOUT, 5);
+}
+
+// ---------------------------------------------------------------------------
 // z lines through TMA column tiles.  A warp owns the 32 z lines of 32
 // consecutive i at one (j, grain): one tensor load brings the whole tile
 // (32 i x nz levels, tile[k][lane]) into shared memory, each lane runs its
@@ -703,7 +904,6 @@ __global__ void __launch_bounds__(128, 5) k_cn_solve_xt(Layout L, Box box, LineM
 // so the recurrences read only shared memory.  Warps are persistent and take
 // contiguous runs of tiles (neighbouring i, then j), which share table rows.
 // ---------------------------------------------------------------------------
-constexpr int ZT_BAR_BYTES = 128;  // barriers ahead of the tiles (keeps tiles 128-byte aligned)
 
 // doubles of shared memory per warp: the tile and the staged table rows,
 // rounded up to 128 bytes so that every warp's tile stays aligned
@@ -1044,7 +1244,14 @@ bool tensor_map(a3g_ctx *ctx, const double *p, int kind, CUtensorMap *out) {
                               (cuuint64_t)(wind ? 1 : L.ns)};
   const cuuint64_t strides[3] = {(cuuint64_t)L.P * 8, (cuuint64_t)L.PY * 8, (cuuint64_t)L.PG * 8};
   cuuint32_t box[4] = {32, 1, 1, 1};
-  if (kind == TM_COLUMN) {
+  cuuint32_t rank = 4;
+  // the rows of a level form a 2-D array: row r = (g*nz + k-1)*ny + j-1 at r*P
+  const cuuint64_t rdims[2] = {(cuuint64_t)L.nx, (cuuint64_t)L.ny * L.nz * L.ns};
+  if (kind == TM_XROWS) {
+    rank = 2;
+    box[0] = XT2_COLS;
+    box[1] = 32;
+  } else if (kind == TM_COLUMN) {
     if (L.nz > 256) return false;
     box[2] = (cuuint32_t)L.nz;
   } else if (kind == TM_YCHUNK_IN) {
@@ -1053,6 +1260,7 @@ bool tensor_map(a3g_ctx *ctx, const double *p, int kind, CUtensorMap *out) {
     box[1] = YT_CH;
   } else if (kind == TM_ADV_QY || kind == TM_ADV_VY) {
     box[1] = ACH;
+
   } else if (kind == TM_ADV_QZ || kind == TM_ADV_VZ) {
     box[2] = ACH;
   } else if (kind == TM_ADV_QX1 || kind == TM_ADV_VX) {
@@ -1066,7 +1274,8 @@ bool tensor_map(a3g_ctx *ctx, const double *p, int kind, CUtensorMap *out) {
   TmapEntry e;
   e.p = p;
   e.kind = kind;
-  if (enc(&e.map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double *>(p), dims, strides, box, estr,
+  if (enc(&e.map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, rank, const_cast<double *>(p), rank == 2 ? rdims : dims,
+          strides, box, estr,
           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return false;
@@ -1137,6 +1346,26 @@ static bool launch_cn_solve_yt(a3g_ctx *ctx, const LineMap &map, const double *t
   const int grid = (int)(need < ctx->tma_grid[1] ? need : ctx->tma_grid[1]);
   k_cn_solve_yt<<<grid, 32 * wpb, smem, ctx->stream>>>(tin, tout, L, ctx->box, map, ctx->c1, tab, ctx->aloft,
                                                        ctx->sc, wpb);
+  return true;
+}
+
+// Launches the x solve through TMA tiles; false when the map cannot be made.
+static bool launch_cn_solve_xt2(a3g_ctx *ctx, const LineMap &map, const double *tab) {
+  const Layout &L = ctx->L;
+  CUtensorMap trow;
+  if (!tensor_map(ctx, ctx->c0, TM_XROWS, &trow)) return false;
+  const size_t smem = ZT_BAR_BYTES + (size_t)XT2_WARPS * XT2_WARP_D * sizeof(double);
+  if (ctx->tma_grid[2] == 0) {
+    int optin = 0;
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device) != cudaSuccess ||
+        (size_t)optin < smem ||
+        cudaFuncSetAttribute(k_cn_solve_xt2, cudaFuncAttributeMaxDynamicSharedMemorySize, optin) != cudaSuccess)
+      return false;
+    ctx->tma_grid[2] = 1;
+  }
+  const long nwarps = ((long)L.ny * L.nz * L.ns + 31) / 32;
+  k_cn_solve_xt2<<<(unsigned)((nwarps + XT2_WARPS - 1) / XT2_WARPS), 32 * XT2_WARPS, smem, ctx->stream>>>(
+      trow, L, ctx->box, map, ctx->c0, ctx->c1, tab, ctx->aloft, ctx->sc);
   return true;
 }
 
@@ -1238,7 +1467,9 @@ static int launch_cn_dir(a3g_ctx *ctx) {
   const double *tab = ctx->cn_tab[DIR];
   const long nlines = (long)map.na * map.nb * L.ns;
   tbegin(ctx, A3G_K_CN_SOLVE_X + DIR);
-  if (DIR == 0 && ctx->tune_cn_x == 0) {
+  if (DIR == 0 && ctx->tune_cn_x == 2 && launch_cn_solve_xt2(ctx, map, tab)) {
+    // tiles through TMA
+  } else if (DIR == 0 && ctx->tune_cn_x == 0) {
     const long nwarps = (nlines + 31) / 32;
     k_cn_solve_xt<<<(unsigned)((nwarps + XT_WARPS - 1) / XT_WARPS), 32 * XT_WARPS, 0, ctx->stream>>>(
         L, box, map, ctx->c0, ctx->c1, tab, ctx->aloft);

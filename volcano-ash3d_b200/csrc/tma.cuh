@@ -76,6 +76,15 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, u
       : "memory");
 }
 
+// Tiled 2-D tensor load of one box into shared memory (as tma_load_4d).
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+
 // Tiled 4-D tensor store of one box from shared memory; elements outside the
 // tensor are not written.  Tracked by the issuing thread's bulk groups.
 __device__ __forceinline__ void tma_store_4d(const CUtensorMap *map, const void *src, int x, int y, int z,

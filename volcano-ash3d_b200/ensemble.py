@@ -63,7 +63,7 @@ def autotune(cfg: syn.Config, device: int = 0, steps: int = 2) -> dict:
     choice = {}
     keys = {0: ("advect_x",), 1: ("advect_y",), 2: ("advect_z",), 3: ("cn_solve_x",),
             4: ("cn_solve_y", "cn_solve_z")}
-    for d, options in ((0, (0, 1, 2, 3, 4, 5)), (1, (0, 1, 2, 5, 6)), (2, (0, 1, 2, 5, 6)), (3, (0, 1)), (4, (0, 1, 2, 3))):
+    for d, options in ((0, (0, 1, 2, 3, 4, 5)), (1, (0, 1, 2, 5, 6)), (2, (0, 1, 2, 5, 6)), (3, (0, 1, 2)), (4, (0, 1, 2, 3))):
         if d >= 3 and not cfg.use_cn:
             continue
         best, best_ms = None, None
