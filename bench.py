@@ -726,7 +726,7 @@ def run_ensemble(args):
                    "steps_total": int(sum(r.steps for r in con))},
         "speedup_vs_sequential": t_seq / t_con, "sequential_s": t_seq, "concurrent_s": t_con,
         "sequential_value": work / t_seq, "autotune_s": t_tune,
-        "variant_counts": {str(k): {str(v): sum(1 for m in e.variants if m.get(k) == v) for v in range(6)
+        "variant_counts": {str(k): {str(v): sum(1 for m in e.variants if m.get(k) == v) for v in range(8)
                                     if any(m.get(k) == v for m in e.variants)} for k in range(5)},
     }
     print(json.dumps(line), flush=True)
