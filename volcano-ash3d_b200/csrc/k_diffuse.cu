@@ -1279,7 +1279,9 @@ bool tensor_map(a3g_ctx *ctx, const double *p, int kind, CUtensorMap *out) {
           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return false;
-  if (ctx->tmaps.size() >= 16) ctx->tmaps.erase(ctx->tmaps.begin());
+  // a step uses about 17 (two levels alternating under each tile shape, and
+  // the wind arrays); the adjoint's stage levels add more
+  if (ctx->tmaps.size() >= 64) ctx->tmaps.erase(ctx->tmaps.begin());
   ctx->tmaps.push_back(e);
   *out = e.map;
   return true;
