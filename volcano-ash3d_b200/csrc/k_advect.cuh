@@ -1415,9 +1415,14 @@ __global__ void __launch_bounds__(32 * ACT_WARPS) k_advect_colt(
       const double *vb = qb + ACH * 32;
       const double *gb = wsm + 4 * ACH * 32 + bi * 2 * ACH;
       const int cend = min(fb, fa + m * ACH + ACH - 1);
-#pragma unroll 4
-      for (int e = 0; c <= cend; c++, e++)
-        step(c, FastT{}, qb[e * 32], (DIR == 2) ? vb[e * 32] + vf0 : vb[e * 32], gb[e], gb[ACH + e]);
+      if (cend - c + 1 == ACH) {  // a whole chunk: straight-line steps
+#pragma unroll
+        for (int e = 0; e < ACH; e++, c++)
+          step(c, FastT{}, qb[e * 32], (DIR == 2) ? vb[e * 32] + vf0 : vb[e * 32], gb[e], gb[ACH + e]);
+      } else {
+        for (int e = 0; c <= cend; c++, e++)
+          step(c, FastT{}, qb[e * 32], (DIR == 2) ? vb[e * 32] + vf0 : vb[e * 32], gb[e], gb[ACH + e]);
+      }
       __syncwarp();
     }
   }
