@@ -1039,7 +1039,7 @@ __global__ void __launch_bounds__(64, 8) k_cn_solve_zt(const __grid_constant__ C
 // groups (neighbouring i, then k), which share table rows.
 // ---------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(64) k_cn_solve_yt(const __grid_constant__ CUtensorMap tin,
+__global__ void __launch_bounds__(64, 10) k_cn_solve_yt(const __grid_constant__ CUtensorMap tin,
                                                     const __grid_constant__ CUtensorMap tout, Layout L,
                                                     Box box, LineMap map, double *__restrict__ cout,
                                                     const double *__restrict__ tab,
@@ -1129,14 +1129,25 @@ __global__ void __launch_bounds__(64) k_cn_solve_yt(const __grid_constant__ CUte
           qm = T[32];  // BC_left_t0 = q(rmin)
           qc = qm;
         }
+        if (ch > 0 && l0 + YT_CH <= ncells - 1) {  // interior chunk: rows 1 .. ncells-2 only
+#pragma unroll
+          for (int c = 0; c < YT_CH; c++) {
+            const double qp = T[(c + 2) * 32];
+            const double B = co(CN_CL, c) * qm + co(CN_CC, c) * qc + co(CN_CR, c) * qp;
+            bp = B - co(CN_FACT, c) * bp;
+            qm = qc;
+            qc = qp;
+          }
+        } else {
 #pragma unroll 4
-        for (int c = 0; c < cnt; c++) {
-          const int l = l0 + c;
-          const double qp = (l + 1 < ncells) ? T[(c + 2) * 32] : qc;  // BC_right_t0 = q(rmax)
-          const double B = co(CN_CL, c) * qm + co(CN_CC, c) * qc + co(CN_CR, c) * qp;
-          bp = (l == 0) ? B : B - co(CN_FACT, c) * bp;
-          qm = qc;
-          qc = qp;
+          for (int c = 0; c < cnt; c++) {
+            const int l = l0 + c;
+            const double qp = (l + 1 < ncells) ? T[(c + 2) * 32] : qc;  // BC_right_t0 = q(rmax)
+            const double B = co(CN_CL, c) * qm + co(CN_CC, c) * qc + co(CN_CR, c) * qp;
+            bp = (l == 0) ? B : B - co(CN_FACT, c) * bp;
+            qm = qc;
+            qc = qp;
+          }
         }
         if (ch + 1 < nch) xg[(long)(rmin + l0 + YT_CH - 2) * L.P] = bp;  // checkpoint B'(l0+YT_CH-1)
       }
@@ -1161,24 +1172,43 @@ __global__ void __launch_bounds__(64) k_cn_solve_yt(const __grid_constant__ CUte
         double bq = ch > 0 ? xg[(long)(rmin + l0 - 2) * L.P] : 0.0;
         double qm2 = (ch == 0) ? T[32] : T[0];
         double qc2 = T[32];
+        if (ch > 0 && l0 + YT_CH <= ncells - 1) {  // interior chunk: rows 1 .. ncells-2 only
+#pragma unroll
+          for (int c = 0; c < YT_CH; c++) {
+            const double qp = T[(c + 2) * 32];
+            const double B = co(CN_CL, c) * qm2 + co(CN_CC, c) * qc2 + co(CN_CR, c) * qp;
+            bq = B - co(CN_FACT, c) * bq;
+            T[(c + 1) * 32] = bq;
+            qm2 = qc2;
+            qc2 = qp;
+          }
+#pragma unroll
+          for (int c = YT_CH - 1; c >= 0; c--) {
+            const double num = T[(c + 1) * 32] - co(CN_DU, c) * xn;
+            const double v = div_rn_rcp(num, co(CN_DP, c), co(CN_RDP, c));
+            T[(c + 1) * 32] = v;
+            xn = v;
+          }
+        } else {
 #pragma unroll 4
-        for (int c = 0; c < cnt; c++) {
-          const int l = l0 + c;
-          const double qp = (l + 1 < ncells) ? T[(c + 2) * 32] : qc2;
-          const double B = co(CN_CL, c) * qm2 + co(CN_CC, c) * qc2 + co(CN_CR, c) * qp;
-          bq = (l == 0) ? B : B - co(CN_FACT, c) * bq;
-          T[(c + 1) * 32] = bq;
-          qm2 = qc2;
-          qc2 = qp;
-        }
+          for (int c = 0; c < cnt; c++) {
+            const int l = l0 + c;
+            const double qp = (l + 1 < ncells) ? T[(c + 2) * 32] : qc2;
+            const double B = co(CN_CL, c) * qm2 + co(CN_CC, c) * qc2 + co(CN_CR, c) * qp;
+            bq = (l == 0) ? B : B - co(CN_FACT, c) * bq;
+            T[(c + 1) * 32] = bq;
+            qm2 = qc2;
+            qc2 = qp;
+          }
 #pragma unroll 4
-        for (int c = cnt - 1; c >= 0; c--) {
-          const int l = l0 + c;
-          const double b2 = T[(c + 1) * 32];
-          const double num = (l == ncells - 1) ? b2 : b2 - co(CN_DU, c) * xn;
-          const double v = div_rn_rcp(num, co(CN_DP, c), co(CN_RDP, c));
-          T[(c + 1) * 32] = v;
-          xn = v;
+          for (int c = cnt - 1; c >= 0; c--) {
+            const int l = l0 + c;
+            const double b2 = T[(c + 1) * 32];
+            const double num = (l == ncells - 1) ? b2 : b2 - co(CN_DU, c) * xn;
+            const double v = div_rn_rcp(num, co(CN_DP, c), co(CN_RDP, c));
+            T[(c + 1) * 32] = v;
+            xn = v;
+          }
         }
         for (int c = cnt; c < YT_CH; c++) T[(c + 1) * 32] = 0.0;  // beyond rmax
       } else {
