@@ -982,24 +982,41 @@ __global__ void __launch_bounds__(64, 8) k_cn_solve_zt(const __grid_constant__ C
       auto co = [&](int f, int l) { return stab[f * nz + l]; };
       double *xx = col + (long)(rmin - 1) * 32;  // row l at xx[l*32]
       // forward elimination with the right-hand side built on the fly, :813-851
+      // (ncells >= 2: a single-row line is skipped before the launch; the
+      // first and last rows are taken out of the loops, which then need no
+      // per-row boundary tests)
       double qm = xx[0];  // BC_left_t0 = q(rmin)
       double qc = qm;
-      double bp = 0.0;
+      double bp;
+      {
+        const double qp = xx[32];
+        bp = co(CN_CL, 0) * qm + co(CN_CC, 0) * qc + co(CN_CR, 0) * qp;
+        xx[0] = bp;
+        qm = qc;
+        qc = qp;
+      }
 #pragma unroll 4
-      for (int l = 0; l < ncells; l++) {
-        const double qp = (l + 1 < ncells) ? xx[(l + 1) * 32] : qc;  // BC_right_t0 = q(rmax)
+      for (int l = 1; l < ncells - 1; l++) {
+        const double qp = xx[(l + 1) * 32];
         const double B = co(CN_CL, l) * qm + co(CN_CC, l) * qc + co(CN_CR, l) * qp;
-        bp = (l == 0) ? B : B - co(CN_FACT, l) * bp;
+        bp = B - co(CN_FACT, l) * bp;
         xx[l * 32] = bp;
         qm = qc;
         qc = qp;
       }
+      {
+        const int l = ncells - 1;
+        const double qp = qc;  // BC_right_t0 = q(rmax)
+        const double B = co(CN_CL, l) * qm + co(CN_CC, l) * qc + co(CN_CR, l) * qp;
+        bp = B - co(CN_FACT, l) * bp;
+        xx[l * 32] = bp;
+      }
       // back substitution
-      double xn = 0.0;
+      double xn = div_rn_rcp(xx[(ncells - 1) * 32], co(CN_DP, ncells - 1), co(CN_RDP, ncells - 1));
+      xx[(ncells - 1) * 32] = xn;
 #pragma unroll 4
-      for (int l = ncells - 1; l >= 0; l--) {
-        const double b2 = xx[l * 32];
-        const double num = (l == ncells - 1) ? b2 : b2 - co(CN_DU, l) * xn;
+      for (int l = ncells - 2; l >= 0; l--) {
+        const double num = xx[l * 32] - co(CN_DU, l) * xn;
         const double v = div_rn_rcp(num, co(CN_DP, l), co(CN_RDP, l));
         xx[l * 32] = v;
         xn = v;
