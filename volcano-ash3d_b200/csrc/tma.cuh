@@ -11,8 +11,8 @@
 //   * the proxy fences between the threads' own shared-memory accesses and
 //     the asynchronous (TMA) proxy.
 //
-// No load here uses cluster multicast: every tensor map covers this GPU's
-// own memory, and each CTA fetches its own tiles.
+// Every load here copies from this GPU's own memory into the shared memory
+// of the CTA that issues it alone; each CTA fetches its own tiles.
 //
 // Host side: tensor maps are encoded with the driver's cuTensorMapEncodeTiled,
 // reached through cudaGetDriverEntryPoint so the library links no libcuda.
