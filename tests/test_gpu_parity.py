@@ -10,6 +10,7 @@ import numpy as np
 import pytest
 
 from gpu_common import pair, prime, random_state
+from volcano_ash3d_b200 import synthetic as syn
 
 pytestmark = pytest.mark.gpu
 
@@ -232,4 +233,30 @@ def test_totals_follow_the_state():
         m.DiffuseVert()
         m.add_source(np.full((cfg.nz + 1, cfg.ns), 3.0e4, order="F"), 0.1)
     same_totals()
+    gpu.close()
+
+
+# Sub-boxes with odd and even first cells along every direction, on lines of
+# several TMA tiles or chunks in each direction (x: 100 cells = 4 CN x tiles,
+# whose loads start on the even cell at or before the tile; y: 70 cells = 5
+# CN y chunks; z: 40-cell columns), so that the default kernels' staged tiles
+# meet every start parity and a ragged last tile.
+TILE_BOXES = [(5, 93, 4, 66, 3, 37), (6, 96, 3, 61, 2, 38), (1, 100, 2, 70, 1, 39)]
+
+
+@pytest.mark.parametrize("box", TILE_BOXES)
+@pytest.mark.parametrize("op", OPS)
+def test_default_kernels_on_sub_boxes_bitwise(op, box):
+    cfg = syn.Config("tile_boxes", 100, 70, 40, 2, dx=4.0, dy=5.0, dz=0.5, ivent=50, jvent=35,
+                     fall_mps=(0.2, 1.5), bin_mass=(0.5, 0.5), plume_km=8.0, volume_km3=1.0e-3,
+                     duration_h=1.0, use_cn=True, sim_hours=1.0, winds="random", seed=23,
+                     fast_subgrid=True)
+    cfg, gpu, ref = pair(cfg)
+    prime(cfg, gpu, ref, seed=29, box=box)
+    _apply(gpu, op)
+    _apply(ref, op)
+    qg, qr = gpu.interior(), ref.interior()
+    bad = np.argwhere(qg != qr)
+    assert bad.size == 0, f"{len(bad)} cells differ, first {bad[:3].tolist()}"
+    _assert_outflows_equal(gpu, ref)
     gpu.close()
