@@ -237,8 +237,10 @@ struct a3g_ctx {
   cudaEvent_t umb_event;
   // source inversion (a3g_inv_setup)
   a3g_inv *inv;
-  // TMA tensor maps over the levels the tiled solves read and write, and the
-  // persistent grid size of each tiled kernel (0 until first computed)
+  // TMA tensor maps over the levels and winds the tiled kernels read and
+  // write, and per tiled CN kernel its set-up state: 0 until its first
+  // launch, then the persistent grid size (z: [0], y: [1]) or 1 once its
+  // shared-memory attributes are set (x: [2])
   std::vector<a3g::TmapEntry> tmaps;
   int tma_grid[4];
   // optional per-kernel timing (a3g_kernel_timing)
